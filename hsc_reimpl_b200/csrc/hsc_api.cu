@@ -1,0 +1,1146 @@
+// C ABI and host orchestration of the B200 HSC solver.
+//
+// Flow of hsc_solve (the LinearHSC::do_solve of linear_hsc.cu:344-436):
+//   analysis (host, once per sparsity pattern): classify BCOO triplets into
+//     FEM-FEM / ABD-ABD / ABD-FEM, build the full row-owner BSR plan
+//     (sorted columns, source triplet + transpose flag per entry), the
+//     sorted active FEM dofs and the per-CTA row partition;
+//   numeric (device, no host sync): BSR fill, Dd^-1, A/E extraction, ACA,
+//     ABD inverse, W = P U, C = U^T W, C = L D L^T, Vt = V L, rhs;
+//   one persistent cooperative PCG launch (hsc_pcg.cu);
+//   back-substitution dq = P bq - W V^T x, full residual |b - H x| / |b|;
+//   one D2H copy of the per-system scalars, then the status checks of
+//   linear_hsc.cu:394-435.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_set>
+#include <vector>
+
+#include "../../include/hsc_c_api.h"
+#include "hsc_setup.cuh"
+
+using namespace hsc;
+
+namespace {
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    ~DevBuf() { if (p) cudaFree(p); }
+    cudaError_t grow(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(bytes, 256));
+        if (e == cudaSuccess) cap = std::max<size_t>(bytes, 256);
+        return e;
+    }
+    template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+// device scalars of one system, copied to the host once per solve
+struct DevScal {
+    double pcg[8];            // it, rel, status, normb, nrep (written by the PCG kernel)
+    double aca_err;
+    double abd_err2;          // |I - A P|_F^2
+    double resid[3];          // |b - Hx|^2, |b|^2, b.x
+    double nd[2];             // line-search numerator / denominator
+    unsigned long long hash;
+    int rank;
+    int bad_fem;              // FEM diagonal blocks with det <= 0
+    int bad_abd;              // non-SPD ABD blocks
+    int bad_ldlt;             // zero / non-finite reduced-core pivot
+    int pad[4];
+};
+
+struct System {
+    // analysis key
+    const int* rows = nullptr;
+    const int* cols = nullptr;
+    long long nnzb = -1;
+    int nblock = -1;
+    hsc_dof_layout lay{};
+    int kmax_for = -1;
+    bool analyzed = false;
+    unsigned long long hash = 0;
+    // sizes
+    int n = 0, nnz = 0, a = 0, nqq = 0, nqf = 0, kmax = 0, qm = 0, qo = 0, fo = 0, fn = 0;
+    std::vector<int> h_rowptr, h_act;
+    // plan
+    DevBuf rowptr, colidx, src, diag_pos, qq, qf, act, ident, rowflag;
+    // numeric
+    DevBuf v64, vmt, dinv, A, E, R0, R1, U, V, hist, P, Ptmp, T, term, Binv, L, W, C, Lc, dpiv, vt64, vtmt,
+        cvec, tt, ttx, bq, bf, x, r, z, p0, p1, y, t0, t1, node_nz, xq, ypad, yq, work, cg, scal, dact, pact, yact,
+        zpart;
+    DevBuf dvec[4];           // contiguous-N scratch for refinement
+    DevScal h_scal{};
+    std::vector<int> h_node_nz;
+};
+
+}  // namespace
+
+struct hsc_ctx {
+    hsc_options opt{};
+    std::string err;
+    int device = 0;
+    int num_sms = 148;
+    std::vector<System> sys;
+    // PCG launch state
+    DevBuf d_desc, d_cta_sys, d_cta_row, d_cta_act, d_part, d_bar, d_remaining;
+    int grid = 0;
+    int part_key_gen = -1;
+    // ACA
+    DevBuf aca_psum, aca_pmax, aca_pidx, aca_bar;
+    int aca_grid = 0;
+    DevBuf res_part;
+    cudaEvent_t ev[9] = {};
+    bool stage_events = false;  // record the per-stage events (single system, no graph)
+    // graph cache (batch)
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<const void*> gkey;
+    DevScal* h_pinned = nullptr;
+    size_t h_pinned_n = 0;
+};
+
+namespace {
+
+constexpr int kResParts = 148;
+
+int fail(hsc_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                               \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(ctx, HSC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define GROW(buf, bytes)                                                                        \
+    do {                                                                                        \
+        cudaError_t e_ = (buf).grow(bytes);                                                     \
+        if (e_ != cudaSuccess)                                                                  \
+            return fail(ctx, HSC_ERR_ALLOC, std::string("allocation failed: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+size_t vt_bytes(int precision) { return precision == 0 ? sizeof(double) : sizeof(float); }
+size_t mt_bytes(int precision) { return precision == 0 ? 8 : (precision == 1 ? 4 : 2); }
+
+int validate_options(const hsc_options* o, std::string& why) {
+    if (o->max_rank < 1 || o->max_rank > 256) { why = "max_rank must be in [1, 256]"; return 0; }
+    if (o->neumann_order < 1 || o->neumann_order > HSC_MAX_POLY) { why = "neumann_order must be in [1, 16]"; return 0; }
+    if (!(o->omega > 0 && o->omega <= 1)) { why = "omega must be in (0, 1]"; return 0; }
+    if (o->max_iter < 1) { why = "max_iter must be positive"; return 0; }
+    if (!(o->tol >= 0)) { why = "tol must be >= 0"; return 0; }
+    if (o->precision < 0 || o->precision > 2) { why = "unknown precision"; return 0; }
+    if (o->abd_inverse < 0 || o->abd_inverse > 2) { why = "unknown abd_inverse"; return 0; }
+    if (o->preconditioner == HSC_PRECOND_POLY && (o->poly_degree < 1 || o->poly_degree > HSC_MAX_POLY)) {
+        why = "poly_degree must be in [1, 16]";
+        return 0;
+    }
+    if (o->threads_per_row != 2 && o->threads_per_row != 4 && o->threads_per_row != 8) {
+        why = "threads_per_row must be 2, 4 or 8";
+        return 0;
+    }
+    if (o->spin_limit < 1000) { why = "spin_limit too small"; return 0; }
+    return 1;
+}
+
+// ---------------------------------------------------------------------------
+// analysis: sparsity pattern -> plans (host; runs when the pattern changes)
+// ---------------------------------------------------------------------------
+int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L, cudaStream_t st) {
+    const hsc_options& o = ctx->opt;
+    if (M.nnzb < 0 || M.nblock <= 0 || M.nnzb >= (1ll << 30)) return fail(ctx, HSC_ERR_INVALID, "bad BCOO sizes");
+    if (L.qm < 0 || L.fn <= 0 || L.qm % 12 || L.fn % 3 || L.qo % 3 || L.fo % 3 || L.qm + L.fn != 3 * M.nblock ||
+        L.qo < 0 || L.fo < 0 || L.qo + L.qm > 3 * M.nblock || L.fo + L.fn > 3 * M.nblock ||
+        (L.qm > 0 && !(L.qo + L.qm <= L.fo || L.fo + L.fn <= L.qo)))
+        return fail(ctx, HSC_ERR_INVALID, "HSC requires only ABD (12/body) and FEM (3/node) dofs");  // linear_hsc.cu:199-200
+    S.qm = L.qm; S.qo = L.qo; S.fo = L.fo; S.fn = L.fn;
+    S.n = L.fn / 3;
+    const long long T = M.nnzb;
+    std::vector<int> rows(T), cols(T);
+    if (T) {
+        CK(cudaMemcpyAsync(rows.data(), M.d_rows, sizeof(int) * T, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(cols.data(), M.d_cols, sizeof(int) * T, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    const int qb0 = L.qo / 3, qb1 = (L.qo + L.qm) / 3, fb0 = L.fo / 3, fb1 = (L.fo + L.fn) / 3;
+    auto isQ = [&](int b) { return b >= qb0 && b < qb1; };
+    auto isF = [&](int b) { return b >= fb0 && b < fb1; };
+    std::vector<int> cnt(S.n + 1, 0);
+    std::vector<int> qq, qfraw;  // qf raw: t, q, fnode, orient
+    std::vector<char> fnode_active(S.n, 0);
+    for (long long t = 0; t < T; ++t) {
+        const int r = rows[t], c = cols[t];
+        if (r < 0 || c < 0 || r >= M.nblock || c >= M.nblock) return fail(ctx, HSC_ERR_INVALID, "block index out of range");
+        if (isF(r) && isF(c)) {
+            cnt[r - fb0]++;
+            if (r != c) cnt[c - fb0]++;
+        } else if (isQ(r) && isQ(c)) {
+            qq.push_back((int)t); qq.push_back(r - qb0); qq.push_back(c - qb0);
+        } else if (isQ(r) && isF(c)) {
+            qfraw.push_back((int)t); qfraw.push_back(r - qb0); qfraw.push_back(c - fb0); qfraw.push_back(0);
+            fnode_active[c - fb0] = 1;
+        } else if (isF(r) && isQ(c)) {
+            qfraw.push_back((int)t); qfraw.push_back(c - qb0); qfraw.push_back(r - fb0); qfraw.push_back(1);
+            fnode_active[r - fb0] = 1;
+        } else {
+            return fail(ctx, HSC_ERR_INVALID, "triplet outside the ABD and FEM dof ranges");
+        }
+    }
+    // full BSR plan: rows of D, columns sorted
+    S.h_rowptr.assign(S.n + 1, 0);
+    for (int i = 0; i < S.n; ++i) S.h_rowptr[i + 1] = S.h_rowptr[i] + cnt[i];
+    S.nnz = S.h_rowptr[S.n];
+    std::vector<int> fillpos(S.h_rowptr.begin(), S.h_rowptr.end() - 1);
+    std::vector<long long> ent(S.nnz);  // (col << 32) | packed src
+    for (long long t = 0; t < T; ++t) {
+        const int r = rows[t], c = cols[t];
+        if (isF(r) && isF(c)) {
+            const int i = r - fb0, j = c - fb0;
+            ent[fillpos[i]++] = ((long long)j << 32) | (unsigned)(2 * t);
+            if (i != j) ent[fillpos[j]++] = ((long long)i << 32) | (unsigned)(2 * t + 1);
+        }
+    }
+    std::vector<int> colidx(S.nnz), src(S.nnz), diag(S.n, -1);
+    for (int i = 0; i < S.n; ++i) {
+        auto b = ent.begin() + S.h_rowptr[i], e = ent.begin() + S.h_rowptr[i + 1];
+        std::sort(b, e);
+        for (int k = S.h_rowptr[i]; k < S.h_rowptr[i + 1]; ++k) {
+            colidx[k] = (int)(ent[k] >> 32);
+            src[k] = (int)(ent[k] & 0xffffffffll);
+            if (k > S.h_rowptr[i] && colidx[k] == colidx[k - 1])
+                return fail(ctx, HSC_ERR_INVALID, "duplicate FEM block (both triangles stored?)");
+            if (colidx[k] == i) diag[i] = k;
+        }
+        if (diag[i] < 0) return fail(ctx, HSC_ERR_NONSPD, "HSC: FEM node without a diagonal block");
+    }
+    // ABD duplicates (both triangles of one pair)
+    {
+        const int nb = L.qm / 3;
+        std::vector<char> seen((size_t)nb * nb, 0);
+        for (size_t e = 0; e < qq.size(); e += 3) {
+            const int i = std::min(qq[e + 1], qq[e + 2]), j = std::max(qq[e + 1], qq[e + 2]);
+            if (seen[(size_t)i * nb + j]) return fail(ctx, HSC_ERR_INVALID, "duplicate ABD block (both triangles stored?)");
+            seen[(size_t)i * nb + j] = 1;
+        }
+    }
+    // active FEM nodes (structural) and the coupling list
+    std::vector<int> act_index(S.n, -1);
+    int nact = 0;
+    for (int i = 0; i < S.n; ++i)
+        if (fnode_active[i]) act_index[i] = nact++;
+    S.a = 3 * nact;
+    S.h_act.resize(S.a);
+    for (int i = 0; i < S.n; ++i)
+        if (act_index[i] >= 0)
+            for (int c = 0; c < 3; ++c) S.h_act[3 * act_index[i] + c] = 3 * i + c;
+    std::vector<int> rowflag(S.n, -1);
+    for (int i = 0; i < S.n; ++i) rowflag[i] = act_index[i];
+    std::vector<int> qf;
+    qf.reserve(qfraw.size());
+    {
+        std::unordered_set<long long> seen;
+        for (size_t e = 0; e < qfraw.size(); e += 4) {
+            const long long key = (long long)qfraw[e + 1] * S.n + qfraw[e + 2];
+            if (!seen.insert(key).second) return fail(ctx, HSC_ERR_INVALID, "duplicate coupling block (both triangles stored?)");
+            qf.push_back(qfraw[e]); qf.push_back(qfraw[e + 1]); qf.push_back(act_index[qfraw[e + 2]]); qf.push_back(qfraw[e + 3]);
+        }
+    }
+    S.nqq = (int)qq.size() / 3;
+    S.nqf = (int)qf.size() / 4;
+    S.kmax = std::min(std::min(o.max_rank, L.qm), S.a);
+    // ---- device plans and buffers ----
+    const int P = o.precision;
+    GROW(S.rowptr, sizeof(int) * (S.n + 1));
+    GROW(S.colidx, sizeof(int) * std::max(1, S.nnz));
+    GROW(S.src, sizeof(int) * std::max(1, S.nnz));
+    GROW(S.diag_pos, sizeof(int) * S.n);
+    GROW(S.qq, sizeof(int) * std::max<size_t>(3, qq.size()));
+    GROW(S.qf, sizeof(int) * std::max<size_t>(4, qf.size()));
+    GROW(S.act, sizeof(int) * std::max(1, S.a));
+    GROW(S.rowflag, sizeof(int) * std::max(1, S.n));
+    CK(cudaMemcpyAsync(S.rowptr.p, S.h_rowptr.data(), sizeof(int) * (S.n + 1), cudaMemcpyHostToDevice, st));
+    if (S.nnz) {
+        CK(cudaMemcpyAsync(S.colidx.p, colidx.data(), sizeof(int) * S.nnz, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(S.src.p, src.data(), sizeof(int) * S.nnz, cudaMemcpyHostToDevice, st));
+    }
+    CK(cudaMemcpyAsync(S.diag_pos.p, diag.data(), sizeof(int) * S.n, cudaMemcpyHostToDevice, st));
+    if (!qq.empty()) CK(cudaMemcpyAsync(S.qq.p, qq.data(), sizeof(int) * qq.size(), cudaMemcpyHostToDevice, st));
+    if (!qf.empty()) CK(cudaMemcpyAsync(S.qf.p, qf.data(), sizeof(int) * qf.size(), cudaMemcpyHostToDevice, st));
+    if (S.a) CK(cudaMemcpyAsync(S.act.p, S.h_act.data(), sizeof(int) * S.a, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(S.rowflag.p, rowflag.data(), sizeof(int) * S.n, cudaMemcpyHostToDevice, st));
+    const size_t nz = std::max(1, S.nnz), n4 = 4 * (size_t)std::max(1, S.n), qm = std::max(1, S.qm);
+    const size_t km = std::max(1, S.kmax), aa = std::max(1, S.a);
+    GROW(S.v64, 9 * sizeof(double) * nz);
+    if (P != 0) GROW(S.vmt, 9 * mt_bytes(P) * nz);
+    GROW(S.dinv, 9 * (P == 0 ? 8 : 4) * (size_t)std::max(1, S.n));
+    GROW(S.A, sizeof(double) * qm * qm);
+    GROW(S.E, sizeof(double) * qm * aa);
+    GROW(S.R0, sizeof(double) * qm * aa);
+    GROW(S.R1, sizeof(double) * qm * aa);
+    GROW(S.U, sizeof(double) * qm * km);
+    GROW(S.V, sizeof(double) * aa * km);
+    GROW(S.hist, sizeof(double) * (km + 1));
+    GROW(S.P, sizeof(double) * qm * qm);
+    GROW(S.Ptmp, sizeof(double) * qm * qm);
+    GROW(S.T, sizeof(double) * qm * qm);
+    GROW(S.term, sizeof(double) * qm * qm);
+    GROW(S.Binv, sizeof(double) * qm * qm);
+    GROW(S.L, sizeof(double) * qm * qm);
+    GROW(S.ident, sizeof(double) * qm * qm);
+    GROW(S.W, sizeof(double) * qm * km);
+    GROW(S.C, sizeof(double) * km * km);
+    GROW(S.Lc, sizeof(double) * km * km);
+    GROW(S.dpiv, sizeof(double) * km);
+    GROW(S.vt64, sizeof(double) * aa * km);
+    GROW(S.cvec, sizeof(double) * km);
+    GROW(S.tt, sizeof(double) * 256);
+    GROW(S.ttx, sizeof(double) * 256);
+    GROW(S.dact, sizeof(double) * 9 * std::max(1, S.a / 3));
+    GROW(S.pact, sizeof(double) * aa);
+    GROW(S.yact, sizeof(double) * aa);
+    GROW(S.bq, sizeof(double) * qm);
+    GROW(S.bf, sizeof(double) * n4);
+    GROW(S.x, sizeof(double) * n4);
+    GROW(S.r, sizeof(double) * n4);
+    GROW(S.z, vt_bytes(P) * n4);
+    GROW(S.p0, vt_bytes(P) * n4);
+    GROW(S.p1, vt_bytes(P) * n4);
+    GROW(S.y, vt_bytes(P) * n4);
+    GROW(S.t0, vt_bytes(P) * n4);
+    GROW(S.t1, vt_bytes(P) * n4);
+    GROW(S.node_nz, sizeof(int) * std::max(1, S.a / 3));
+    GROW(S.xq, sizeof(double) * qm);
+    GROW(S.ypad, sizeof(double) * n4);
+    GROW(S.yq, sizeof(double) * qm);
+    GROW(S.work, sizeof(double) * qm * qm);
+    GROW(S.cg, sizeof(double) * 2 * 64);
+    GROW(S.scal, sizeof(DevScal));
+    const size_t N = 3 * (size_t)M.nblock;
+    for (auto& d : S.dvec) GROW(d, sizeof(double) * N);
+    if (S.qm) {
+        std::vector<double> I((size_t)S.qm * S.qm, 0.0);
+        for (int i = 0; i < S.qm; ++i) I[(size_t)i * S.qm + i] = 1.0;
+        CK(cudaMemcpyAsync(S.ident.p, I.data(), sizeof(double) * I.size(), cudaMemcpyHostToDevice, st));
+    }
+    // pattern hash at analysis time
+    launch_pattern_hash(M.d_rows, M.d_cols, T, &S.scal.as<DevScal>()->hash, st);
+    CK(cudaMemcpyAsync(&S.hash, &S.scal.as<DevScal>()->hash, sizeof(S.hash), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    S.rows = M.d_rows; S.cols = M.d_cols; S.nnzb = M.nnzb; S.nblock = M.nblock; S.lay = L;
+    S.kmax_for = o.max_rank * 16 + o.precision;
+    S.analyzed = true;
+    ctx->part_key_gen = -1;  // CTA partition must be rebuilt
+    if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+    return HSC_OK;
+}
+
+bool same_key(const System& S, const hsc_bcoo3& M, const hsc_dof_layout& L, const hsc_options& o) {
+    return S.analyzed && S.rows == M.d_rows && S.cols == M.d_cols && S.nnzb == M.nnzb && S.nblock == M.nblock &&
+           S.lay.qo == L.qo && S.lay.qm == L.qm && S.lay.fo == L.fo && S.lay.fn == L.fn &&
+           S.kmax_for == o.max_rank * 16 + o.precision;
+}
+
+// ---------------------------------------------------------------------------
+// numeric setup (device only, no host sync except the adaptive ABD inverse)
+// ---------------------------------------------------------------------------
+void gemm(const double* A, int lda, int tA, const double* B, int ldb, int tB, double* C, int ldc, int M, int N, int K,
+          double alpha, double beta, cudaStream_t st, const int* dM = nullptr, const int* dN = nullptr,
+          const int* dK = nullptr) {
+    GemmArgs g{A, B, C, M, N, K, dM, dN, dK, lda, ldb, ldc, tA, tB, alpha, beta};
+    launch_gemm(g, M, N, st);
+}
+
+int abd_inverse(hsc_ctx* ctx, System& S, cudaStream_t st, bool allow_sync) {
+    const hsc_options& o = ctx->opt;
+    const int m = S.qm;
+    DevScal* ds = S.scal.as<DevScal>();
+    double* P = S.P.as<double>();
+    if (m == 0) return HSC_OK;
+    if (o.abd_inverse == HSC_ABD_EXACT) {
+        launch_cholesky(S.A.as<double>(), m, S.L.as<double>(), &ds->bad_abd, st);
+        launch_chol_solve(S.L.as<double>(), m, S.ident.as<double>(), m, P, m, m, nullptr, S.work.as<double>(), st);
+        launch_symmetrize(P, m, st);
+        // |I - A P|_F^2 for the stats
+        CK(cudaMemcpyAsync(S.T.p, S.ident.p, sizeof(double) * m * m, cudaMemcpyDeviceToDevice, st));
+        gemm(S.A.as<double>(), m, 0, P, m, 0, S.T.as<double>(), m, m, m, m, -1.0, 1.0, st);
+        launch_frob(S.T.as<double>(), m * m, &ds->abd_err2, st);
+        return HSC_OK;
+    }
+    // block-Jacobi Neumann (linear_hsc.cu:263-275)
+    const double w = o.omega;
+    launch_block12_inverse(S.A.as<double>(), m, S.Binv.as<double>(), &ds->bad_abd, st);
+    // T = I - w Binv A
+    CK(cudaMemcpyAsync(S.T.p, S.ident.p, sizeof(double) * m * m, cudaMemcpyDeviceToDevice, st));
+    gemm(S.Binv.as<double>(), m, 0, S.A.as<double>(), m, 0, S.T.as<double>(), m, m, m, m, -w, 1.0, st);
+    // term = w Binv, P = term
+    CK(cudaMemsetAsync(S.term.p, 0, sizeof(double) * m * m, st));
+    launch_axpby_mat(S.term.as<double>(), S.Binv.as<double>(), w, 0.0, m * m, 0, 0.0, st);
+    CK(cudaMemcpyAsync(P, S.term.p, sizeof(double) * m * m, cudaMemcpyDeviceToDevice, st));
+    for (int k = 1; k < o.neumann_order; ++k) {
+        gemm(S.T.as<double>(), m, 0, S.term.as<double>(), m, 0, S.Ptmp.as<double>(), m, m, m, m, 1.0, 0.0, st);
+        std::swap(S.term.p, S.Ptmp.p);
+        std::swap(S.term.cap, S.Ptmp.cap);
+        launch_axpby_mat(P, S.term.as<double>(), 1.0, 1.0, m * m, 0, 0.0, st);
+    }
+    launch_symmetrize(P, m, st);
+    // Rr = I - A P ; err
+    auto residual = [&]() {
+        cudaMemcpyAsync(S.T.p, S.ident.p, sizeof(double) * m * m, cudaMemcpyDeviceToDevice, st);
+        gemm(S.A.as<double>(), m, 0, P, m, 0, S.T.as<double>(), m, m, m, m, -1.0, 1.0, st);
+        launch_frob(S.T.as<double>(), m * m, &ds->abd_err2, st);
+    };
+    residual();
+    if (o.abd_inverse != HSC_ABD_ADAPTIVE) return HSC_OK;
+    if (!allow_sync) return fail(ctx, HSC_ERR_INVALID, "the adaptive ABD inverse needs host syncs (not graph-capturable)");
+    // adaptive doubling P <- P + P (I - A P) (linear_hsc.cu:276-297)
+    int d = 0;
+    double err2 = 0;
+    CK(cudaMemcpyAsync(&err2, &ds->abd_err2, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double err = std::sqrt(err2 / m);
+    while (err > o.abd_inverse_tol && d < 48) {
+        gemm(P, m, 0, S.T.as<double>(), m, 0, S.Ptmp.as<double>(), m, m, m, m, 1.0, 0.0, st);
+        launch_axpby_mat(P, S.Ptmp.as<double>(), 1.0, 1.0, m * m, 0, 0.0, st);
+        launch_symmetrize(P, m, st);
+        residual();
+        CK(cudaMemcpyAsync(&err2, &ds->abd_err2, sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        err = std::sqrt(err2 / m);
+        ++d;
+        if (!std::isfinite(err)) return fail(ctx, HSC_ERR_NONSPD, "HSC ABD Neumann extension diverged");
+    }
+    S.h_scal.pcg[7] = d;  // doublings (host side)
+    if (err > o.abd_inverse_tol)
+        return fail(ctx, HSC_ERR_NONSPD, "HSC ABD inverse residual exceeds abd_inverse_tol after 48 doublings");
+    return HSC_OK;
+}
+
+void stage_mark(hsc_ctx* ctx, int i, cudaStream_t st) {
+    if (ctx->stage_events) cudaEventRecord(ctx->ev[i], st);
+}
+
+int numeric_setup(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, cudaStream_t st, bool allow_sync) {
+    const hsc_options& o = ctx->opt;
+    const int P = o.precision;
+    DevScal* ds = S.scal.as<DevScal>();
+    S.h_scal.pcg[7] = 0;
+    CK(cudaMemsetAsync(ds, 0, sizeof(DevScal), st));
+    launch_pattern_hash(M.d_rows, M.d_cols, M.nnzb, &ds->hash, st);
+    launch_fill_bsr(P, S.src.as<int>(), M.d_values, S.nnz, S.v64.as<double>(), P ? S.vmt.p : nullptr, st);
+    launch_dinv(P, S.diag_pos.as<int>(), S.v64.as<double>(), S.nnz, S.n, S.dinv.p, &ds->bad_fem, st);
+    launch_split_active_diag(P, S.act.as<int>(), S.a / 3, S.diag_pos.as<int>(), S.v64.as<double>(), S.nnz,
+                             P ? S.vmt.p : nullptr, S.dact.as<double>(), st);
+    launch_extract(S.qq.as<int>(), S.nqq, S.qf.as<int>(), S.nqf, M.d_values, S.qm, S.a, S.A.as<double>(),
+                   S.E.as<double>(), S.node_nz.as<int>(), st);
+    // ACA of E (qm x a)
+    if (S.kmax > 0) {
+        CK(cudaMemcpyAsync(S.R0.p, S.E.p, sizeof(double) * S.qm * S.a, cudaMemcpyDeviceToDevice, st));
+        AcaParams ap{};
+        ap.R0 = S.R0.as<double>(); ap.R1 = S.R1.as<double>();
+        ap.m = S.qm; ap.nc = S.a; ap.cap = S.kmax; ap.rtol = o.aca_rtol > 0 ? o.aca_rtol : 0.0;
+        ap.U = S.U.as<double>(); ap.V = S.V.as<double>(); ap.hist = S.hist.as<double>();
+        ap.rank = &ds->rank; ap.err = &ds->aca_err;
+        ap.psum = ctx->aca_psum.as<double>(); ap.pmax = ctx->aca_pmax.as<double>(); ap.pidx = ctx->aca_pidx.as<long long>();
+        ap.bar = ctx->aca_bar.as<GridBar>(); ap.spin_limit = o.spin_limit;
+        CK(cudaMemsetAsync(ctx->aca_bar.p, 0, sizeof(GridBar), st));
+        const long long total = (long long)S.qm * S.a;
+        const int grid = (int)std::max<long long>(1, std::min<long long>(ctx->aca_grid, (total + 2047) / 2048));
+        CK(launch_aca(ap, grid, st));
+    }
+    stage_mark(ctx, 2, st);
+    int rc = abd_inverse(ctx, S, st, allow_sync);
+    if (rc) return rc;
+    stage_mark(ctx, 3, st);
+    if (S.kmax > 0) {
+        const int* dk = &ds->rank;
+        // W = P U  (qm x k, ld kmax); U column-major (qm x cap) == row-major U^T
+        gemm(S.P.as<double>(), S.qm, 0, S.U.as<double>(), S.qm, 1, S.W.as<double>(), S.kmax, S.qm, S.kmax, S.qm,
+             1.0, 0.0, st, nullptr, dk, nullptr);
+        // C = U^T W (k x k, ld kmax)
+        gemm(S.U.as<double>(), S.qm, 0, S.W.as<double>(), S.kmax, 0, S.C.as<double>(), S.kmax, S.kmax, S.kmax, S.qm,
+             1.0, 0.0, st, dk, dk, nullptr);
+        launch_ldlt(S.C.as<double>(), S.kmax, dk, S.Lc.as<double>(), S.dpiv.as<double>(), &ds->bad_ldlt, st);
+        // Vt^T (k x a row-major == Vt column-major a x k) = Lc^T V^T
+        CK(cudaMemsetAsync(S.vt64.p, 0, sizeof(double) * S.a * S.kmax, st));
+        gemm(S.Lc.as<double>(), S.kmax, 1, S.V.as<double>(), S.a, 0, S.vt64.as<double>(), S.a, S.kmax, S.a, S.kmax,
+             1.0, 0.0, st, dk, nullptr, dk);
+    } else {
+        CK(cudaMemsetAsync(&ds->rank, 0, sizeof(int), st));
+    }
+    stage_mark(ctx, 4, st);
+    return HSC_OK;
+}
+
+// rhs of the Schur system for right-hand side b (contiguous N)
+void schur_rhs(System& S, const double* b, cudaStream_t st) {
+    DevScal* ds = S.scal.as<DevScal>();
+    launch_split_rhs(b, S.qo, S.qm, S.fo, S.n, S.bq.as<double>(), S.bf.as<double>(), st);
+    if (S.kmax > 0) {
+        launch_wt_vec(S.W.as<double>(), S.qm, S.kmax, &ds->rank, S.bq.as<double>(), S.cvec.as<double>(), st);
+        launch_rhs_lowrank(S.V.as<double>(), S.a, &ds->rank, S.cvec.as<double>(), S.act.as<int>(), S.bf.as<double>(), st);
+    }
+}
+
+// x_out = [dq; dx] after the PCG; also the full residual of (b_orig) if asked
+void back_substitute(System& S, const double* b, double* x_out, bool residual, cudaStream_t st) {
+    DevScal* ds = S.scal.as<DevScal>();
+    // recover the untouched FEM rhs: bf was overwritten by rhs; re-split b
+    if (S.kmax > 0)
+        launch_vt_x(S.V.as<double>(), S.a, S.kmax, &ds->rank, S.act.as<int>(), S.x.as<double>(), S.cvec.as<double>(), st);
+    else
+        cudaMemsetAsync(S.cvec.p, 0, sizeof(double) * std::max(1, S.kmax), st);
+    launch_split_rhs(b, S.qo, S.qm, S.fo, S.n, S.bq.as<double>(), S.bf.as<double>(), st);
+    if (S.qm)
+        launch_backsub(S.P.as<double>(), S.W.as<double>(), S.qm, std::max(1, S.kmax), &ds->rank, S.bq.as<double>(),
+                       S.cvec.as<double>(), x_out + S.qo, S.xq.as<double>(), st);
+    launch_scatter_x(S.x.as<double>(), S.n, S.fo, x_out, st);
+    if (residual) {
+        FullSpmv f{S.rowptr.as<int>(), S.colidx.as<int>(), S.v64.as<double>(), S.nnz, S.n, S.A.as<double>(),
+                   S.E.as<double>(), S.qm, S.a, S.act.as<int>(), S.xq.as<double>(), S.x.as<double>(),
+                   S.ypad.as<double>(), S.yq.as<double>()};
+        launch_full_spmv(f, st);
+    }
+}
+
+// full-system residual dots (after back_substitute with residual=true)
+void residual_dots(hsc_ctx* ctx, System& S, cudaStream_t st) {
+    DevScal* ds = S.scal.as<DevScal>();
+    launch_residual(S.bf.as<double>(), S.ypad.as<double>(), S.x.as<double>(), S.n, S.bq.as<double>(),
+                    S.yq.as<double>(), S.xq.as<double>(), S.qm, ctx->res_part.as<double>(), kResParts, ds->resid, st);
+}
+
+// y = H x for contiguous N vectors
+void full_spmv_contig(System& S, const double* x, double* y, cudaStream_t st) {
+    double* xpad = S.dvec[3].as<double>();
+    launch_gather_x(x, S.n, S.fo, xpad, st);
+    if (S.qm) cudaMemcpyAsync(S.xq.p, x + S.qo, sizeof(double) * S.qm, cudaMemcpyDeviceToDevice, st);
+    FullSpmv f{S.rowptr.as<int>(), S.colidx.as<int>(), S.v64.as<double>(), S.nnz, S.n, S.A.as<double>(),
+               S.E.as<double>(), S.qm, S.a, S.act.as<int>(), S.xq.as<double>(), xpad, S.ypad.as<double>(),
+               S.yq.as<double>()};
+    launch_full_spmv(f, st);
+    launch_scatter_y(S.ypad.as<double>(), S.n, S.fo, S.yq.as<double>(), S.qm, S.qo, y, st);
+}
+
+// CTA partition of the persistent launch over the systems in `idx`
+int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) {
+    const hsc_options& o = ctx->opt;
+    const int bps = std::max(1, pcg_blocks_per_sm(o.precision, o.threads_per_row));
+    int G = bps * ctx->num_sms;
+    const int ns = (int)idx.size();
+    if (ns > G) return fail(ctx, HSC_ERR_INVALID, "more systems than co-resident CTAs");
+    long long tot = 0;
+    std::vector<long long> w(ns);
+    for (int s = 0; s < ns; ++s) {
+        const System& S = ctx->sys[idx[s]];
+        w[s] = std::max<long long>(1, (long long)S.nnz + S.n);
+        tot += w[s];
+    }
+    // CTAs per system proportional to work, at least one, at most one per 16 rows
+    std::vector<int> nc(ns);
+    int used = 0;
+    for (int s = 0; s < ns; ++s) {
+        const System& S = ctx->sys[idx[s]];
+        int want = (int)std::floor((double)G * w[s] / tot);
+        want = std::max(1, std::min(want, std::max(1, S.n / 16)));
+        nc[s] = want;
+        used += want;
+    }
+    while (used > G) {
+        int big = (int)(std::max_element(nc.begin(), nc.end()) - nc.begin());
+        nc[big]--; used--;
+    }
+    G = used;
+    std::vector<int> cta_sys(G), cta_row(2 * G), cta_act(2 * G);
+    std::vector<SysDesc> desc(ns);
+    int c = 0;
+    for (int s = 0; s < ns; ++s) {
+        System& S = ctx->sys[idx[s]];
+        const int b = c;
+        const long long rows_w = (long long)S.nnz + S.n;
+        int row = 0;
+        for (int k = 0; k < nc[s]; ++k, ++c) {
+            const long long target = rows_w * (k + 1) / nc[s];
+            const int rb = row;
+            if (k == nc[s] - 1) row = S.n;
+            else
+                while (row < S.n && (long long)S.h_rowptr[row] + row < target) ++row;
+            cta_sys[c] = s;
+            cta_row[2 * c] = rb;
+            cta_row[2 * c + 1] = row;
+            cta_act[2 * c] = (int)(std::lower_bound(S.h_act.begin(), S.h_act.end(), 3 * rb) - S.h_act.begin());
+            cta_act[2 * c + 1] = (int)(std::lower_bound(S.h_act.begin(), S.h_act.end(), 3 * row) - S.h_act.begin());
+        }
+        SysDesc& d = desc[s];
+        d.n = S.n; d.nnz = S.nnz; d.a = S.a; d.kmax = S.kmax; d.cta_begin = b; d.cta_end = c;
+        d.rowptr = S.rowptr.as<int>(); d.colidx = S.colidx.as<int>();
+        d.vals = o.precision ? S.vmt.p : S.v64.p; d.vals64 = S.v64.as<double>(); d.dinv = S.dinv.p;
+        d.act = S.act.as<int>(); d.rowflag = S.rowflag.as<int>(); d.dact = S.dact.as<double>();
+        d.vt64 = S.vt64.as<double>(); d.dpiv = S.dpiv.as<double>(); d.rank = &S.scal.as<DevScal>()->rank;
+        d.pact = S.pact.as<double>(); d.yact = S.yact.as<double>(); d.ttx = S.ttx.as<double>();
+        GROW(S.zpart, sizeof(double) * std::max(1, S.kmax) * (size_t)(c - b));
+        d.zpart = S.zpart.as<double>();
+        d.x = S.x.as<double>(); d.r = S.r.as<double>(); d.rhs = S.bf.as<double>(); d.z = S.z.p;
+        d.p[0] = S.p0.p; d.p[1] = S.p1.p; d.y = S.y.p; d.t[0] = S.t0.p; d.t[1] = S.t1.p; d.tt = S.tt.as<double>();
+        d.out = S.scal.as<DevScal>()->pcg; d.cg_coef = S.cg.as<double>(); d.max_coef = 64;
+    }
+    GROW(ctx->d_desc, sizeof(SysDesc) * ns);
+    GROW(ctx->d_cta_sys, sizeof(int) * G);
+    GROW(ctx->d_cta_row, sizeof(int) * 2 * G);
+    GROW(ctx->d_cta_act, sizeof(int) * 2 * G);
+    GROW(ctx->d_part, sizeof(double) * 3 * G);
+    GROW(ctx->d_bar, sizeof(GridBar));
+    GROW(ctx->d_remaining, sizeof(int));
+    CK(cudaMemcpyAsync(ctx->d_desc.p, desc.data(), sizeof(SysDesc) * ns, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->d_cta_sys.p, cta_sys.data(), sizeof(int) * G, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->d_cta_row.p, cta_row.data(), sizeof(int) * 2 * G, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->d_cta_act.p, cta_act.data(), sizeof(int) * 2 * G, cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));  // host vectors die here
+    ctx->grid = G;
+    return HSC_OK;
+}
+
+int launch_pcg_all(hsc_ctx* ctx, int nsys, cudaStream_t st) {
+    const hsc_options& o = ctx->opt;
+    PcgParams prm{};
+    prm.sys = ctx->d_desc.as<SysDesc>();
+    prm.nsys = nsys;
+    prm.cta_sys = ctx->d_cta_sys.as<int>();
+    prm.cta_row = ctx->d_cta_row.as<int>();
+    prm.cta_act = ctx->d_cta_act.as<int>();
+    prm.part = ctx->d_part.as<double>();
+    prm.bar = ctx->d_bar.as<GridBar>();
+    prm.remaining = ctx->d_remaining.as<int>();
+    prm.omega = o.omega;
+    if (o.preconditioner == HSC_PRECOND_POLY) {
+        prm.nterms = o.poly_degree;
+        for (int k = 0; k < o.poly_degree; ++k) prm.w[k] = o.poly_weights[k];
+    } else {
+        prm.nterms = o.neumann_order;
+        for (int k = 0; k < o.neumann_order; ++k) prm.w[k] = 1.0;
+    }
+    prm.tol = o.tol;
+    prm.max_iter = o.max_iter;
+    prm.rr_every = o.residual_replacement;
+    prm.spin_limit = o.spin_limit;
+    CK(cudaMemsetAsync(ctx->d_bar.p, 0, sizeof(GridBar), st));
+    set_int(ctx->d_remaining.as<int>(), nsys, st);
+    CK(launch_pcg(o.precision, o.threads_per_row, prm, ctx->grid, st));
+    return HSC_OK;
+}
+
+// extreme Ritz values of the CG Lanczos tridiagonal (bisection on Sturm counts)
+void lanczos_extremes(const double* coef, int m, double& lo, double& hi) {
+    lo = hi = 0.0;
+    std::vector<double> d, e;
+    for (int i = 0; i < m; ++i) {
+        const double a = coef[2 * i];
+        if (!(a > 0) || !std::isfinite(a)) break;
+        double di = 1.0 / a;
+        if (i > 0) {
+            const double bprev = coef[2 * (i - 1) + 1], aprev = coef[2 * (i - 1)];
+            if (!(bprev > 0)) break;
+            di += bprev / aprev;
+            e.push_back(std::sqrt(bprev) / aprev);
+        }
+        d.push_back(di);
+    }
+    const int n = (int)d.size();
+    if (n == 0) return;
+    if ((int)e.size() > n - 1) e.resize(n - 1);
+    double gl = 1e300, gu = -1e300;
+    for (int i = 0; i < n; ++i) {
+        double rad = (i > 0 ? std::fabs(e[i - 1]) : 0) + (i < n - 1 ? std::fabs(e[i]) : 0);
+        gl = std::min(gl, d[i] - rad);
+        gu = std::max(gu, d[i] + rad);
+    }
+    auto count_below = [&](double x) {
+        int c = 0;
+        double q = d[0] - x;
+        if (q < 0) ++c;
+        for (int i = 1; i < n; ++i) {
+            if (q == 0) q = 1e-300;
+            q = d[i] - x - e[i - 1] * e[i - 1] / q;
+            if (q < 0) ++c;
+        }
+        return c;
+    };
+    auto kth = [&](int k) {
+        double a = gl, b = gu;
+        for (int it = 0; it < 200; ++it) {
+            const double mid = 0.5 * (a + b);
+            if (count_below(mid) > k) b = mid; else a = mid;
+        }
+        return 0.5 * (a + b);
+    };
+    lo = kth(0);
+    hi = kth(n - 1);
+}
+
+void fill_stats(hsc_ctx* ctx, System& S, const DevScal& h, hsc_stats* out, bool residual, int refinement_steps,
+                int total_iters) {
+    const hsc_options& o = ctx->opt;
+    hsc_stats s{};
+    s.fem_dofs = S.fn;
+    s.abd_dofs = S.qm;
+    int nzn = 0;
+    for (int v : S.h_node_nz) nzn += v != 0;
+    s.active_fem_dofs = 3 * nzn;
+    s.rank = h.rank;
+    s.pcg_iterations = total_iters >= 0 ? total_iters : (int)h.pcg[0];
+    s.neumann_doublings = (int)S.h_scal.pcg[7];
+    s.refinement_steps = refinement_steps;
+    s.precision = o.precision;
+    s.preconditioner = o.preconditioner;
+    s.residual_replacements = (int)h.pcg[4];
+    s.aca_relative_error = h.aca_err;
+    s.schur_relative_residual = h.pcg[1];
+    s.abd_inverse_residual = S.qm ? std::sqrt(h.abd_err2 / S.qm) : 0.0;
+    s.full_residual_limit = o.full_residual_limit;
+    s.nnzb = S.nnzb;
+    if (residual) {
+        s.full_relative_residual = h.resid[1] > 0 ? std::sqrt(h.resid[0] / h.resid[1]) : 0.0;
+        s.descent = h.resid[2];
+    } else {
+        s.full_relative_residual = NAN;
+        s.descent = NAN;
+    }
+    *out = s;
+}
+
+// status of one system from its scalars (the asserts of linear_hsc.cu)
+int system_status(hsc_ctx* ctx, const System& S, const DevScal& h, bool residual, int grid_abort, std::string& msg) {
+    const hsc_options& o = ctx->opt;
+    char buf[256];
+    if (h.bad_fem) { snprintf(buf, sizeof buf, "HSC: %d non-positive FEM diagonal blocks", h.bad_fem); msg = buf; return HSC_ERR_NONSPD; }
+    if (h.bad_abd) { msg = "HSC: non-SPD ABD block"; return HSC_ERR_NONSPD; }
+    if (h.bad_ldlt) { msg = "HSC: singular reduced core U^T P U"; return HSC_ERR_NONSPD; }
+    const int st = (int)h.pcg[2];
+    if (grid_abort || st < 0) { msg = "HSC: a device-side wait gave up (grid barrier timeout)"; return HSC_ERR_TIMEOUT; }
+    if (st == 3) { snprintf(buf, sizeof buf, "HSC Schur PCG breakdown at iteration %d. No fallback.", (int)h.pcg[0]); msg = buf; return HSC_ERR_BREAKDOWN; }
+    if (st == 4) { snprintf(buf, sizeof buf, "HSC Schur PCG did not converge: iterations=%d, residual=%g", (int)h.pcg[0], h.pcg[1]); msg = buf; return HSC_ERR_NOCONV; }
+    if (residual) {
+        const double bn2 = h.resid[1];
+        const double full = bn2 > 0 ? std::sqrt(h.resid[0] / bn2) : 0.0;
+        if (!(std::isfinite(h.resid[2]) && (h.resid[2] > 0 || bn2 == 0))) { msg = "HSC returned a non-descent direction"; return HSC_ERR_NONDESCENT; }
+        if (!(std::isfinite(full) && full <= o.full_residual_limit)) {
+            snprintf(buf, sizeof buf, "HSC full-system residual %g exceeds %g. No fallback.", full, o.full_residual_limit);
+            msg = buf;
+            return HSC_ERR_RESIDUAL;
+        }
+    }
+    return HSC_OK;
+}
+
+int ensure_common(hsc_ctx* ctx, cudaStream_t st) {
+    GROW(ctx->aca_psum, sizeof(double) * 4096);
+    GROW(ctx->aca_pmax, sizeof(double) * 4096);
+    GROW(ctx->aca_pidx, sizeof(long long) * 4096);
+    GROW(ctx->aca_bar, sizeof(GridBar));
+    GROW(ctx->res_part, sizeof(double) * 3 * kResParts);
+    if (!ctx->aca_grid) ctx->aca_grid = std::min(4096, std::max(1, aca_blocks_per_sm()) * ctx->num_sms);
+    if (!ctx->ev[0])
+        for (auto& e : ctx->ev) CK(cudaEventCreate(&e));
+    (void)st;
+    return HSC_OK;
+}
+
+int read_scalars(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st, int& grid_abort) {
+    if (ctx->h_pinned_n < idx.size()) {
+        if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+        ctx->h_pinned = nullptr;
+        CK(cudaMallocHost((void**)&ctx->h_pinned, sizeof(DevScal) * idx.size()));
+        ctx->h_pinned_n = idx.size();
+    }
+    for (size_t s = 0; s < idx.size(); ++s)
+        CK(cudaMemcpyAsync(ctx->h_pinned + s, ctx->sys[idx[s]].scal.p, sizeof(DevScal), cudaMemcpyDeviceToHost, st));
+    GridBar gb{}, ga{};
+    if (ctx->d_bar.p) CK(cudaMemcpyAsync(&gb, ctx->d_bar.p, sizeof(GridBar), cudaMemcpyDeviceToHost, st));
+    if (ctx->aca_bar.p) CK(cudaMemcpyAsync(&ga, ctx->aca_bar.p, sizeof(GridBar), cudaMemcpyDeviceToHost, st));
+    for (size_t s = 0; s < idx.size(); ++s) {
+        System& S = ctx->sys[idx[s]];
+        S.h_node_nz.resize(S.a / 3);
+        if (S.a) CK(cudaMemcpyAsync(S.h_node_nz.data(), S.node_nz.p, sizeof(int) * (S.a / 3), cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    grid_abort = gb.abort | ga.abort;
+    for (size_t s = 0; s < idx.size(); ++s) {
+        const double d7 = ctx->sys[idx[s]].h_scal.pcg[7];
+        ctx->sys[idx[s]].h_scal = ctx->h_pinned[s];
+        ctx->sys[idx[s]].h_scal.pcg[7] = d7;
+    }
+    return HSC_OK;
+}
+
+int prepare_system(hsc_ctx* ctx, int s, const hsc_bcoo3& M, const hsc_dof_layout& L, cudaStream_t st, bool& reanalyzed) {
+    if ((int)ctx->sys.size() <= s) ctx->sys.resize(s + 1);
+    System& S = ctx->sys[s];
+    reanalyzed = false;
+    if (!same_key(S, M, L, ctx->opt)) {
+        int rc = analyze(ctx, S, M, L, st);
+        if (rc) return rc;
+        reanalyzed = true;
+    }
+    return HSC_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int hsc_version(void) { return HSC_API_VERSION; }
+
+long long hsc_kernel_launches(void) { return launch_count(); }
+
+int hsc_options_default(hsc_options* o) {
+    if (!o) return HSC_ERR_INVALID;
+    std::memset(o, 0, sizeof(*o));
+    o->max_rank = 128;
+    o->aca_rtol = 0.0;
+    o->neumann_order = 2;
+    o->omega = 0.7;
+    o->max_iter = 20000;
+    o->tol = 1e-6;
+    o->abd_inverse = HSC_ABD_EXACT;
+    o->abd_inverse_tol = 1e-5;
+    o->full_residual_limit = 0.1;
+    o->precision = HSC_FP64;
+    o->preconditioner = HSC_PRECOND_NEUMANN;
+    o->poly_degree = 0;
+    o->residual_replacement = 0;
+    o->refine_target = 0.0;
+    o->max_refinements = 20;
+    o->fallback_on_stall = 1;
+    o->threads_per_row = 4;
+    o->spin_limit = 20000000;
+    o->check_residual = 1;
+    return HSC_OK;
+}
+
+int hsc_options_reference(hsc_options* o) {
+    int rc = hsc_options_default(o);
+    if (rc) return rc;
+    o->max_rank = 128;          // linear_hsc.cu:162-164
+    o->neumann_order = 5;
+    o->max_iter = 2000;
+    o->abd_inverse = HSC_ABD_ADAPTIVE;
+    o->omega = 0.7;
+    o->tol = 1e-4;
+    o->abd_inverse_tol = 1e-5;
+    o->full_residual_limit = 0.1;
+    return HSC_OK;
+}
+
+int hsc_create(const hsc_options* opt, hsc_ctx** out) {
+    if (!out) return HSC_ERR_INVALID;
+    *out = nullptr;
+    hsc_options o;
+    if (opt) o = *opt; else hsc_options_default(&o);
+    std::string why;
+    if (!validate_options(&o, why)) return HSC_ERR_INVALID;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return HSC_ERR_CUDA;
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    if (!coop) return HSC_ERR_CUDA;
+    hsc_ctx* c = new hsc_ctx();
+    c->opt = o;
+    c->device = dev;
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev);
+    *out = c;
+    return HSC_OK;
+}
+
+void hsc_destroy(hsc_ctx* ctx) {
+    if (!ctx) return;
+    if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    delete ctx;
+}
+
+int hsc_set_options(hsc_ctx* ctx, const hsc_options* opt) {
+    if (!ctx || !opt) return HSC_ERR_INVALID;
+    std::string why;
+    if (!validate_options(opt, why)) return fail(ctx, HSC_ERR_INVALID, why);
+    const bool relayout = opt->precision != ctx->opt.precision || opt->max_rank != ctx->opt.max_rank ||
+                          opt->threads_per_row != ctx->opt.threads_per_row;
+    ctx->opt = *opt;
+    if (relayout) {
+        for (auto& S : ctx->sys) S.analyzed = false;
+        ctx->part_key_gen = -1;
+    }
+    if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+    return HSC_OK;
+}
+
+const char* hsc_last_error(const hsc_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof_layout* lay,
+                      const double* const* d_b, double* const* d_x, int use_graph, cudaStream_t st,
+                      hsc_stats* out, int depth) {
+    const hsc_options& o = ctx->opt;
+    ctx->err.clear();
+    int rc = ensure_common(ctx, st);
+    if (rc) return rc;
+    bool any_new = false;
+    std::vector<int> idx(count);
+    for (int s = 0; s < count; ++s) {
+        bool re = false;
+        rc = prepare_system(ctx, s, A[s], lay[s], st, re);
+        if (rc) { if (out) out[s].status = rc; return rc; }
+        any_new |= re;
+        idx[s] = s;
+    }
+    if (any_new || ctx->part_key_gen != count) {
+        rc = build_partition(ctx, idx, st);
+        if (rc) return rc;
+        ctx->part_key_gen = count;
+        if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+    }
+    const bool refine = o.refine_target > 0 && count == 1;
+    const bool residual = o.check_residual || refine;
+    // graph key: every pointer the numeric phase touches
+    std::vector<const void*> key;
+    for (int s = 0; s < count; ++s) {
+        key.push_back(A[s].d_rows); key.push_back(A[s].d_cols); key.push_back(A[s].d_values);
+        key.push_back(d_b[s]); key.push_back(d_x[s]);
+    }
+    key.push_back((const void*)st);
+    const bool graph_ok = use_graph && !refine && o.abd_inverse != HSC_ABD_ADAPTIVE;
+    if (use_graph && !st) return fail(ctx, HSC_ERR_INVALID, "graph replay needs a non-default stream");
+    ctx->stage_events = !graph_ok && count == 1;
+    CK(cudaEventRecord(ctx->ev[0], st));
+    auto enqueue = [&](bool allow_sync) -> int {
+        for (int s = 0; s < count; ++s) {
+            int r2 = numeric_setup(ctx, ctx->sys[s], A[s], st, allow_sync);
+            if (r2) return r2;
+            schur_rhs(ctx->sys[s], d_b[s], st);
+        }
+        CK(cudaEventRecord(ctx->ev[5], st));
+        int r3 = launch_pcg_all(ctx, count, st);
+        if (r3) return r3;
+        CK(cudaEventRecord(ctx->ev[6], st));
+        for (int s = 0; s < count; ++s) {
+            back_substitute(ctx->sys[s], d_b[s], d_x[s], residual, st);
+            if (residual) residual_dots(ctx, ctx->sys[s], st);
+        }
+        CK(cudaEventRecord(ctx->ev[7], st));
+        return HSC_OK;
+    };
+    if (graph_ok) {
+        if (!ctx->gexec || ctx->gkey != key) {
+            if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            int r2 = enqueue(false);
+            cudaError_t ce = cudaStreamEndCapture(st, &g);
+            if (r2) { if (g) cudaGraphDestroy(g); return r2; }
+            if (ce != cudaSuccess) return fail(ctx, HSC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+            ce = cudaGraphInstantiate(&ctx->gexec, g, 0);
+            cudaGraphDestroy(g);
+            if (ce != cudaSuccess) return fail(ctx, HSC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+            ctx->gkey = key;
+        }
+        CK(cudaGraphLaunch(ctx->gexec, st));
+    } else {
+        rc = enqueue(true);
+        if (rc) return rc;
+    }
+    CK(cudaEventRecord(ctx->ev[8], st));
+    int grid_abort = 0;
+    rc = read_scalars(ctx, idx, st, grid_abort);
+    if (rc) return rc;
+    // a pattern changed behind the same pointers: analyse again and redo once
+    bool stale = false;
+    for (int s = 0; s < count; ++s) stale |= ctx->sys[s].h_scal.hash != ctx->sys[s].hash;
+    if (stale) {
+        if (depth > 0) return fail(ctx, HSC_ERR_INVALID, "sparsity pattern changed during the solve");
+        for (int s = 0; s < count; ++s) ctx->sys[s].analyzed = false;
+        return solve_impl(ctx, count, A, lay, d_b, d_x, use_graph, st, out, depth + 1);
+    }
+    float ms_setup = 0, ms_pcg = 0, ms_total = 0;
+    float ms_stage[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (!graph_ok) {
+        cudaEventElapsedTime(&ms_setup, ctx->ev[0], ctx->ev[5]);
+        cudaEventElapsedTime(&ms_pcg, ctx->ev[5], ctx->ev[6]);
+        cudaEventElapsedTime(&ms_stage[6], ctx->ev[6], ctx->ev[7]);
+        if (ctx->stage_events)
+            for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms_stage[i], ctx->ev[i], ctx->ev[i + 1]);
+        ms_stage[5] = ms_pcg;
+    }
+    cudaEventElapsedTime(&ms_total, ctx->ev[0], ctx->ev[8]);
+    int total_iters = -1, steps = 1;
+    int worst = HSC_OK;
+    if (refine) {
+        // quadratic refinement with exact line search (core.py:171-198):
+        // x <- x + alpha d,  d = HSC(b - H x),  alpha = min(1, r.d / d.H d)
+        System& S = ctx->sys[0];
+        const int N = 3 * S.nblock;
+        std::string msg;
+        int st0 = system_status(ctx, S, S.h_scal, false, grid_abort, msg);
+        if (st0) { if (out) { fill_stats(ctx, S, S.h_scal, out, false, 0, -1); out->status = st0; } return fail(ctx, st0, msg); }
+        double* xacc = S.dvec[0].as<double>();
+        double* res = S.dvec[1].as<double>();
+        double* Hd = S.dvec[2].as<double>();
+        total_iters = (int)S.h_scal.pcg[0];
+        // first direction d = d_x[0] (already computed); line step from x = 0
+        CK(cudaMemsetAsync(xacc, 0, sizeof(double) * N, st));
+        CK(cudaMemcpyAsync(res, d_b[0], sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+        double bn = 0;
+        {
+            launch_dot2(d_b[0], d_b[0], d_b[0], N, S.scal.as<DevScal>()->nd, st);
+            double nd[2];
+            CK(cudaMemcpyAsync(nd, S.scal.as<DevScal>()->nd, sizeof nd, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            bn = std::sqrt(nd[0]);
+        }
+        double full = 1.0;
+        steps = 0;
+        for (;;) {
+            ++steps;
+            full_spmv_contig(S, d_x[0], Hd, st);
+            launch_dot2(res, d_x[0], Hd, N, S.scal.as<DevScal>()->nd, st);
+            launch_line_step(xacc, d_x[0], N, S.scal.as<DevScal>()->nd, st);
+            full_spmv_contig(S, xacc, Hd, st);
+            launch_sub(d_b[0], Hd, res, N, st);
+            launch_dot2(res, res, res, N, S.scal.as<DevScal>()->resid, st);
+            double h2[2];
+            CK(cudaMemcpyAsync(h2, S.scal.as<DevScal>()->resid, sizeof h2, cudaMemcpyDeviceToHost, st));
+            double nd[2];
+            CK(cudaMemcpyAsync(nd, S.scal.as<DevScal>()->nd, sizeof nd, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (!(nd[0] > 0 && nd[1] > 0)) {
+                worst = HSC_ERR_NONDESCENT;
+                ctx->err = "approximate HSC direction is not descent";
+                break;
+            }
+            full = bn > 0 ? std::sqrt(h2[0]) / bn : 0.0;
+            if (full <= o.refine_target || steps >= o.max_refinements) break;
+            // next direction
+            schur_rhs(S, res, st);
+            int r4 = launch_pcg_all(ctx, 1, st);
+            if (r4) return r4;
+            back_substitute(S, res, d_x[0], false, st);
+            int ga = 0;
+            r4 = read_scalars(ctx, idx, st, ga);
+            if (r4) return r4;
+            total_iters += (int)S.h_scal.pcg[0];
+            st0 = system_status(ctx, S, S.h_scal, false, ga, msg);
+            if (st0) { worst = st0; ctx->err = msg; break; }
+        }
+        CK(cudaMemcpyAsync(d_x[0], xacc, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+        // final full residual and descent with the accumulated x
+        launch_dot2(d_b[0], d_x[0], d_x[0], N, S.scal.as<DevScal>()->nd, st);
+        double nd[2];
+        CK(cudaMemcpyAsync(nd, S.scal.as<DevScal>()->nd, sizeof nd, cudaMemcpyDeviceToHost, st));
+        CK(cudaEventRecord(ctx->ev[8], st));
+        CK(cudaStreamSynchronize(st));
+        cudaEventElapsedTime(&ms_total, ctx->ev[0], ctx->ev[8]);
+        S.h_scal.resid[0] = full * full * bn * bn;
+        S.h_scal.resid[1] = bn * bn;
+        S.h_scal.resid[2] = nd[0];
+        if (!worst && full > o.refine_target) {
+            worst = HSC_ERR_NOCONV;
+            ctx->err = "refinement did not reach refine_target";
+        }
+    }
+    for (int s = 0; s < count; ++s) {
+        System& S = ctx->sys[s];
+        std::string msg;
+        int st_s = system_status(ctx, S, S.h_scal, residual, grid_abort, msg);
+        if (refine && worst) st_s = worst;
+        if (out) {
+            fill_stats(ctx, S, S.h_scal, out + s, residual, refine ? steps : 1, refine ? total_iters : -1);
+            out[s].status = st_s;
+            out[s].setup_ms = ms_setup;
+            out[s].pcg_ms = ms_pcg;
+            out[s].total_ms = ms_total;
+            for (int i = 0; i < 8; ++i) out[s].stage_ms[i] = ms_stage[i];
+            out[s].accepted = st_s == HSC_OK;
+            out[s].fallback = 0;
+            double lo = 0, hi = 0;
+            std::vector<double> coef(128);
+            if (cudaMemcpy(coef.data(), S.cg.p, sizeof(double) * 128, cudaMemcpyDeviceToHost) == cudaSuccess) {
+                const int m = std::min(64, std::max(0, (int)S.h_scal.pcg[0]));
+                lanczos_extremes(coef.data(), m, lo, hi);
+            }
+            out[s].lanczos_min = lo;
+            out[s].lanczos_max = hi;
+        }
+        if (st_s && !worst) { worst = st_s; ctx->err = msg; }
+    }
+    return worst;
+}
+
+int hsc_solve(hsc_ctx* ctx, const hsc_bcoo3* A, const hsc_dof_layout* layout, const double* d_b, double* d_x,
+              void* stream, hsc_stats* out) {
+    if (!ctx || !A || !layout || !d_b || !d_x) return HSC_ERR_INVALID;
+    int rc = solve_impl(ctx, 1, A, layout, &d_b, &d_x, 0, (cudaStream_t)stream, out, 0);
+    if (rc && out && out->status == 0) out->status = rc;
+    return rc;
+}
+
+int hsc_solve_batch(hsc_ctx* ctx, int32_t count, const hsc_bcoo3* A, const hsc_dof_layout* layouts,
+                    const double* const* d_b, double* const* d_x, int32_t use_graph, void* stream, hsc_stats* out) {
+    if (!ctx || count < 1 || !A || !layouts || !d_b || !d_x) return HSC_ERR_INVALID;
+    return solve_impl(ctx, count, A, layouts, d_b, d_x, use_graph, (cudaStream_t)stream, out, 0);
+}
+
+int hsc_spmv(hsc_ctx* ctx, const hsc_bcoo3* A, const hsc_dof_layout* layout, const double* d_x, double* d_y,
+             void* stream) {
+    if (!ctx || !A || !layout || !d_x || !d_y) return HSC_ERR_INVALID;
+    cudaStream_t st = (cudaStream_t)stream;
+    ctx->err.clear();
+    int rc = ensure_common(ctx, st);
+    if (rc) return rc;
+    bool re = false;
+    rc = prepare_system(ctx, 0, *A, *layout, st, re);
+    if (rc) return rc;
+    System& S = ctx->sys[0];
+    DevScal* ds = S.scal.as<DevScal>();
+    launch_fill_bsr(0, S.src.as<int>(), A->d_values, S.nnz, S.v64.as<double>(), nullptr, st);
+    launch_extract(S.qq.as<int>(), S.nqq, S.qf.as<int>(), S.nqf, A->d_values, S.qm, S.a, S.A.as<double>(),
+                   S.E.as<double>(), S.node_nz.as<int>(), st);
+    (void)ds;
+    full_spmv_contig(S, d_x, d_y, st);
+    CK(cudaStreamSynchronize(st));
+    if (re) ctx->part_key_gen = -1;
+    return HSC_OK;
+}
+
+int hsc_get_factors(hsc_ctx* ctx, int32_t sys, int32_t* rank, int32_t* n_active, double* U, int32_t ldu, double* V,
+                    int32_t ldv, int32_t* active) {
+    if (!ctx || sys < 0 || sys >= (int)ctx->sys.size() || !ctx->sys[sys].analyzed) return HSC_ERR_NOTREADY;
+    System& S = ctx->sys[sys];
+    const int k = S.h_scal.rank;
+    if (rank) *rank = k;
+    if (n_active) *n_active = S.a;
+    if (active && S.a) std::memcpy(active, S.h_act.data(), sizeof(int) * S.a);
+    if (U && k) CK(cudaMemcpy2D(U, sizeof(double) * ldu, S.U.p, sizeof(double) * S.qm, sizeof(double) * S.qm, k,
+                                 cudaMemcpyDeviceToHost));
+    if (V && k) CK(cudaMemcpy2D(V, sizeof(double) * ldv, S.V.p, sizeof(double) * S.a, sizeof(double) * S.a, k,
+                                 cudaMemcpyDeviceToHost));
+    return HSC_OK;
+}
+
+int hsc_get_abd_inverse(hsc_ctx* ctx, int32_t sys, double* P) {
+    if (!ctx || sys < 0 || sys >= (int)ctx->sys.size() || !ctx->sys[sys].analyzed || !P) return HSC_ERR_NOTREADY;
+    System& S = ctx->sys[sys];
+    if (S.qm) CK(cudaMemcpy(P, S.P.p, sizeof(double) * S.qm * S.qm, cudaMemcpyDeviceToHost));
+    return HSC_OK;
+}
+
+}  // extern "C"

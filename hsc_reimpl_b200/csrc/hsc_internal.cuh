@@ -1,0 +1,190 @@
+// Internal declarations of the B200 HSC solver (device data layout, kernels,
+// the bounded grid barrier).  Host orchestration lives in hsc_api.cu.
+//
+// Device layout of one system (all FP64 unless the precision mode says
+// otherwise):
+//   * FEM block D as a full (both-triangle) row-owner BSR over nodes:
+//     rowptr[n+1], colidx[nnz], and the 3x3 values as 9 planes
+//     vals[e*nnz + k] (e = 3*r + c, row-major inside the block) so that the
+//     lanes of one row read consecutive k of a plane: coalesced.
+//   * 3x3 diagonal-block inverses Dinv as 9 planes over nodes.
+//   * FEM vectors padded to 4 entries per node (x, y, z, 0): one 32-byte
+//     (FP64) or 16-byte (FP32) aligned load per node in the gathers.
+//   * low-rank coupling: sorted active FEM dofs act[a], Vt = V L (a x kmax,
+//     column-major) and the LDL^T pivots dpiv[kmax] of C = U^T P U, so that
+//     V C V^T = Vt diag(dpiv) Vt^T.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+namespace hsc {
+
+constexpr int kThreads = 256;            // persistent-kernel CTA size
+constexpr int kWarps = kThreads / 32;
+
+struct GridBar {
+    unsigned int count;
+    unsigned int gen;
+    int abort;
+    int where;                           // phase id of the wait that gave up
+};
+
+// ----------------------------------------------------------------------------
+// memory-order helpers
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned int* p, unsigned int v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ int ld_volatile_i32(const int* p) {
+    return *reinterpret_cast<const volatile int*>(p);
+}
+
+// Grid-wide barrier for a cooperative launch.  Every wait is bounded by
+// `limit` polls; a wait that gives up raises gb->abort, after which every
+// CTA leaves at its next barrier.  Returns false when the grid must exit.
+__device__ __forceinline__ bool grid_sync(GridBar* gb, unsigned int nblocks, long long limit, int where) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        unsigned int g = ld_acquire_u32(&gb->gen);
+        __threadfence();
+        unsigned int prev = atomicAdd(&gb->count, 1u);
+        if (prev == nblocks - 1) {
+            atomicExch(&gb->count, 0u);
+            __threadfence();
+            st_release_u32(&gb->gen, g + 1);
+        } else {
+            long long n = 0;
+            while (ld_acquire_u32(&gb->gen) == g) {
+                ++n;
+                if (n > 32) __nanosleep(40);
+                if ((n & 127) == 0 && ld_volatile_i32(&gb->abort)) { ok = 0; break; }
+                if (n > limit) {
+                    atomicExch(&gb->abort, 1);
+                    atomicExch(&gb->where, where);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        if (ld_volatile_i32(&gb->abort)) ok = 0;
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// ----------------------------------------------------------------------------
+// value types
+// ----------------------------------------------------------------------------
+template <class T> struct Num;
+template <> struct Num<double> {
+    __device__ __forceinline__ static double get(double v) { return v; }
+    __device__ __forceinline__ static double put(double v) { return v; }
+};
+template <> struct Num<float> {
+    __device__ __forceinline__ static float get(float v) { return v; }
+    __device__ __forceinline__ static float put(double v) { return (float)v; }
+};
+template <> struct Num<__nv_bfloat16> {
+    __device__ __forceinline__ static float get(__nv_bfloat16 v) { return __bfloat162float(v); }
+    __device__ __forceinline__ static __nv_bfloat16 put(double v) { return __float2bfloat16_rn((float)v); }
+};
+
+// node-padded vector element access: 4 entries per node
+template <class VT> struct Vec4;
+template <> struct Vec4<double> {
+    __device__ __forceinline__ static void load(const double* v, int node, double& a, double& b, double& c) {
+        const double2* q = reinterpret_cast<const double2*>(v + 4 * (size_t)node);
+        double2 u = q[0];
+        double2 w = q[1];
+        a = u.x; b = u.y; c = w.x;
+    }
+    __device__ __forceinline__ static void store(double* v, int node, double a, double b, double c) {
+        double2* q = reinterpret_cast<double2*>(v + 4 * (size_t)node);
+        q[0] = make_double2(a, b);
+        q[1] = make_double2(c, 0.0);
+    }
+};
+template <> struct Vec4<float> {
+    __device__ __forceinline__ static void load(const float* v, int node, float& a, float& b, float& c) {
+        float4 u = reinterpret_cast<const float4*>(v)[node];
+        a = u.x; b = u.y; c = u.z;
+    }
+    __device__ __forceinline__ static void store(float* v, int node, float a, float b, float c) {
+        reinterpret_cast<float4*>(v)[node] = make_float4(a, b, c, 0.f);
+    }
+};
+
+// ----------------------------------------------------------------------------
+// per-system device descriptor used by the persistent PCG kernel
+// ----------------------------------------------------------------------------
+struct SysDesc {
+    int n;                 // FEM nodes (block rows of D)
+    int nnz;               // full BSR entries
+    int a;                 // active FEM dofs (3 per active node)
+    int kmax;              // allocated rank columns
+    int cta_begin, cta_end;
+    const int* rowflag;    // per node: active-node index, or -1
+    const int* rowptr;
+    const int* colidx;
+    const void* vals;      // MT planes (mixed modes: active diagonal blocks zeroed)
+    const double* vals64;  // FP64 planes (true-residual replacement)
+    const double* dact;    // FP64 active diagonal blocks (mixed modes), row-major 9 per active node
+    const void* dinv;      // Dd^-1 planes over nodes (omega NOT folded in)
+    const int* act;        // active FEM dofs (a), sorted
+    const double* vt64;    // Vt = V L (a x kmax, column-major), FP64
+    const double* dpiv;    // LDL^T pivots (kmax)
+    const int* rank;       // device scalar
+    double* x;             // FP64 node-padded
+    double* r;             // FP64 node-padded
+    const double* rhs;     // FP64 node-padded
+    void* z;               // VT node-padded
+    void* p[2];            // VT node-padded ping-pong
+    void* y;               // VT node-padded
+    void* t[2];            // VT node-padded ping-pong polynomial terms
+    double* pact;          // FP64 direction at the active dofs (a)
+    double* yact;          // FP64 S p at the active dofs (a)
+    double* zpart;         // kmax x ncta: per-CTA partials of Vt^T z (own active dofs)
+    double* tt;            // kmax: Vt^T p (recurrence Vt^T z + beta Vt^T p_prev)
+    double* ttx;           // kmax: Vt^T x (true-residual slot)
+    double* out;           // per-system results [0]=iters [1]=rel [2]=status [3]=normb [4]=replacements
+    double* cg_coef;       // 2*max_coef: alpha_k, beta_k for the Lanczos estimate
+    int max_coef;
+};
+
+struct PcgParams {
+    const SysDesc* sys;
+    int nsys;
+    const int* cta_sys;        // per CTA: its system
+    const int* cta_row;        // per CTA: [row_begin, row_end) pairs
+    const int* cta_act;        // per CTA: [act_begin, act_end) pairs in the system's act list
+    double* part;              // 3 * gridDim partials
+    GridBar* bar;
+    int* remaining;            // systems still iterating
+    double omega;
+    int nterms;                // polynomial terms (Neumann order or poly degree)
+    double w[16];              // polynomial weights
+    double tol;
+    int max_iter;
+    int rr_every;              // residual replacement interval (0 = only at convergence)
+    long long spin_limit;
+};
+
+// launch counter of this library (hsc_setup.cu)
+void count_launch();
+long long launch_count();
+
+// kernel launchers (hsc_pcg.cu)
+cudaError_t launch_pcg(int precision, int tpr, const PcgParams& prm, int grid, cudaStream_t st);
+int pcg_blocks_per_sm(int precision, int tpr);
+
+}  // namespace hsc

@@ -1,0 +1,542 @@
+// Persistent Schur-complement PCG for one or many HSC systems.
+//
+// One cooperative launch runs the whole PCG loop of linear_hsc.cu:359-393
+// (reference loop; core.py:95-138 is the oracle's form) for every system of a
+// batch.  Each CTA owns a contiguous range of FEM block rows of one system;
+// grid-wide barriers (bounded waits) separate the phases of an iteration:
+//
+//   A  p = z + beta p_old (formed on the fly in the gathers),  y = D p,
+//      tt_j = (Vt^T p)_j by designated warps, partial p.Dp - sum d_j tt_j^2
+//   -- barrier --
+//   B  alpha = rz / pSp;  y[act] -= Vt (d .* tt);  x += alpha p;
+//      r -= alpha y;  t = w Dd^-1 r;  z = w_0 t;  partial r.r
+//   -- barrier --
+//   C_k (k = 1 .. terms-1): t' = t - w Dd^-1 (D t);  z += w_k t';  partial r.z
+//   -- barrier each --
+//
+// so one iteration costs terms+1 barriers and `terms` passes over D, and all
+// scalars are reduced redundantly (same order, same bits) by every CTA of a
+// system: no atomics in any sum, results are bit-reproducible.  The true
+// residual check at convergence (linear_hsc.cu:375-387) and the FP64 residual
+// replacement of the mixed-precision modes run as a replacement slot
+// (A' r = rhs - D x in FP64, B' r += Vt d Vt^T x) with the same barrier count.
+#include <type_traits>
+
+#include "hsc_internal.cuh"
+
+namespace hsc {
+
+namespace {
+
+template <class MT> struct Cmp { using T = float; };
+template <> struct Cmp<double> { using T = double; };
+template <class MT> struct DinvT { using T = float; };
+template <> struct DinvT<double> { using T = double; };
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// deterministic CTA sum; result valid in every thread
+__device__ __forceinline__ double block_sum(double v, double* s_red, double* s_out) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) s_red[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        double t = lane < kWarps ? s_red[lane] : 0.0;
+        t = warp_sum(t);
+        if (lane == 0) *s_out = t;
+    }
+    __syncthreads();
+    return *s_out;
+}
+
+// deterministic sum of part[b..e) (same order in every CTA); valid in every thread
+__device__ __forceinline__ double sum_parts(const double* part, int b, int e, double* s_out) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (warp == 0) {
+        double t = 0.0;
+        for (int i = b + lane; i < e; i += 32) t += part[i];
+        t = warp_sum(t);
+        if (lane == 0) *s_out = t;
+    }
+    __syncthreads();
+    return *s_out;
+}
+
+template <class VT>
+__device__ __forceinline__ VT& elem(void* v, int dof) {
+    return reinterpret_cast<VT*>(v)[4 * (dof / 3) + dof % 3];
+}
+
+// y_row = sum_k B_k x[col_k] over own rows; TPR lanes per row, then the
+// group leader runs the epilogue.
+template <class MT, class CT, int TPR, class Gather, class Epi>
+__device__ __forceinline__ void spmv_own(const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                                         const MT* __restrict__ vals, int nnz, int rb, int re,
+                                         const Gather& gather, Epi& epi) {
+    constexpr int kGroups = kThreads / TPR;
+    const int grp = threadIdx.x / TPR, sub = threadIdx.x % TPR;
+    for (int row0 = rb; row0 < re; row0 += kGroups) {
+        const int row = row0 + grp;
+        CT a0 = 0, a1 = 0, a2 = 0;
+        if (row < re) {
+            const int k0 = __ldg(rowptr + row), k1 = __ldg(rowptr + row + 1);
+            for (int k = k0 + sub; k < k1; k += TPR) {
+                const int c = __ldg(colidx + k);
+                CT x0, x1, x2;
+                gather(c, x0, x1, x2);
+                const MT* v = vals + k;
+                const CT b0 = Num<MT>::get(__ldg(v)), b1 = Num<MT>::get(__ldg(v + nnz)),
+                         b2 = Num<MT>::get(__ldg(v + 2 * (size_t)nnz));
+                const CT b3 = Num<MT>::get(__ldg(v + 3 * (size_t)nnz)), b4 = Num<MT>::get(__ldg(v + 4 * (size_t)nnz)),
+                         b5 = Num<MT>::get(__ldg(v + 5 * (size_t)nnz));
+                const CT b6 = Num<MT>::get(__ldg(v + 6 * (size_t)nnz)), b7 = Num<MT>::get(__ldg(v + 7 * (size_t)nnz)),
+                         b8 = Num<MT>::get(__ldg(v + 8 * (size_t)nnz));
+                a0 += b0 * x0 + b1 * x1 + b2 * x2;
+                a1 += b3 * x0 + b4 * x1 + b5 * x2;
+                a2 += b6 * x0 + b7 * x1 + b8 * x2;
+            }
+        }
+#pragma unroll
+        for (int o = TPR / 2; o > 0; o >>= 1) {
+            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        }
+        if (row < re && sub == 0) epi(row, a0, a1, a2);
+    }
+}
+
+template <class DT>
+__device__ __forceinline__ void dinv_apply(const DT* __restrict__ dinv, int n, int row, double s,
+                                           double r0, double r1, double r2, double& o0, double& o1, double& o2) {
+    const DT* d = dinv + row;
+    const double d0 = __ldg(d), d1 = __ldg(d + n), d2 = __ldg(d + 2 * (size_t)n);
+    const double d3 = __ldg(d + 3 * (size_t)n), d4 = __ldg(d + 4 * (size_t)n), d5 = __ldg(d + 5 * (size_t)n);
+    const double d6 = __ldg(d + 6 * (size_t)n), d7 = __ldg(d + 7 * (size_t)n), d8 = __ldg(d + 8 * (size_t)n);
+    o0 = s * (d0 * r0 + d1 * r1 + d2 * r2);
+    o1 = s * (d3 * r0 + d4 * r1 + d5 * r2);
+    o2 = s * (d6 * r0 + d7 * r1 + d8 * r2);
+}
+
+enum SlotKind { kIdle = 0, kNormal = 1, kReplace = 2 };
+
+template <class MT, class VT, int TPR>
+__global__ void __launch_bounds__(kThreads, 2) pcg_kernel(const PcgParams prm) {
+    using CT = typename Cmp<MT>::T;
+    using DT = typename DinvT<MT>::T;
+    // mixed modes keep the diagonal blocks of the coupled (active) nodes out of
+    // the bulk planes and apply them in FP64: those blocks carry the contact /
+    // stitch stiffness that cancels against the low-rank term in S = D - V C V^T
+    constexpr bool kSplit = !std::is_same<MT, double>::value;
+    __shared__ double s_red[kWarps];
+    __shared__ double s_out;
+    extern __shared__ double s_dtt[];  // kmax doubles
+
+    const int cta = blockIdx.x;
+    const unsigned int G = gridDim.x;
+    const int sidx = prm.cta_sys[cta];
+    const SysDesc& S = prm.sys[sidx];
+    const int rb = prm.cta_row[2 * cta], re = prm.cta_row[2 * cta + 1];
+    const int ab = prm.cta_act[2 * cta], ae = prm.cta_act[2 * cta + 1];
+    const int cb = S.cta_begin, ce = S.cta_end;
+    const int ncta = ce - cb, lcta = cta - cb;
+    const bool leader_cta = (cta == cb);
+    const int n = S.n, nnz = S.nnz, a = S.a;
+    const int rank = *S.rank;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int gwarp = lcta * kWarps + warp, nwarp = ncta * kWarps;
+    double* partA = prm.part;
+    double* partB = prm.part + G;
+    double* partC = prm.part + 2 * G;
+    const double omega = prm.omega;
+    const int nterms = prm.nterms;
+    const MT* vals = reinterpret_cast<const MT*>(S.vals);
+    const DT* dinv = reinterpret_cast<const DT*>(S.dinv);
+    const double* vt = S.vt64;
+    double* x = S.x;
+    double* r = S.r;
+    const double* rhs = S.rhs;
+    VT* z = reinterpret_cast<VT*>(S.z);
+    VT* y = reinterpret_cast<VT*>(S.y);
+    VT* pbuf[2] = {reinterpret_cast<VT*>(S.p[0]), reinterpret_cast<VT*>(S.p[1])};
+    VT* tbuf[2] = {reinterpret_cast<VT*>(S.t[0]), reinterpret_cast<VT*>(S.t[1])};
+
+    int it = 0, status = 0, nrep = 0;
+    double rz = 0.0, normb = 0.0, rel = 1.0, beta = 0.0;
+    bool done = false, counted = false, first = true;
+    int slot = kNormal, prev_slot = kNormal;
+    bool conv_check = false;
+    int pc = 0;  // p buffer holding the previous direction
+    int tc = 0;  // t buffer holding the current term
+    int bar_id = 0;
+
+    auto dact_mul = [&](int an, double p0, double p1, double p2, double& o0, double& o1, double& o2) {
+        const double* d = S.dact + 9 * (size_t)an;
+        o0 = d[0] * p0 + d[1] * p1 + d[2] * p2;
+        o1 = d[3] * p0 + d[4] * p1 + d[5] * p2;
+        o2 = d[6] * p0 + d[7] * p1 + d[8] * p2;
+    };
+    // per-CTA partials of Vt^T z over the CTA's own active dofs (z final)
+    auto compute_zpart = [&]() {
+        if (ab >= ae) return;  // uniform within the CTA
+        __syncthreads();
+        for (int j = warp; j < rank; j += kWarps) {
+            const double* col = vt + (size_t)j * a;
+            double sacc = 0.0;
+            for (int i = ab + lane; i < ae; i += 32) sacc += __ldg(col + i) * (double)elem<VT>(z, __ldg(S.act + i));
+            sacc = warp_sum(sacc);
+            if (lane == 0) S.zpart[(size_t)j * ncta + lcta] = sacc;
+        }
+    };
+
+    // ---------------- prologue: r = rhs, x = 0, z = M r ----------------
+    {
+        double acc_rr = 0.0, acc_rz = 0.0;
+        for (int row = rb + threadIdx.x; row < re; row += kThreads) {
+            double r0, r1, r2;
+            Vec4<double>::load(rhs, row, r0, r1, r2);
+            Vec4<double>::store(r, row, r0, r1, r2);
+            Vec4<double>::store(x, row, 0.0, 0.0, 0.0);
+            Vec4<VT>::store(pbuf[0], row, (VT)0, (VT)0, (VT)0);  // beta * p_prev must be 0, not NaN
+            double t0, t1, t2;
+            dinv_apply(dinv, n, row, omega, r0, r1, r2, t0, t1, t2);
+            Vec4<VT>::store(tbuf[0], row, (VT)t0, (VT)t1, (VT)t2);
+            const double w0 = prm.w[0];
+            const VT z0 = (VT)(w0 * t0), z1 = (VT)(w0 * t1), z2 = (VT)(w0 * t2);
+            Vec4<VT>::store(z, row, z0, z1, z2);
+            acc_rr += r0 * r0 + r1 * r1 + r2 * r2;
+            acc_rz += r0 * (double)z0 + r1 * (double)z1 + r2 * (double)z2;
+        }
+        for (int i = ab + threadIdx.x; i < ae; i += kThreads) S.pact[i] = 0.0;
+        if (ab >= ae)
+            for (int j = threadIdx.x; j < rank; j += kThreads) S.zpart[(size_t)j * ncta + lcta] = 0.0;
+        if (leader_cta)
+            for (int j = threadIdx.x; j < rank; j += kThreads) S.tt[j] = 0.0;
+        const double srr = block_sum(acc_rr, s_red, &s_out);
+        const double srz = block_sum(acc_rz, s_red, &s_out);
+        if (threadIdx.x == 0) { partA[cta] = srr; partB[cta] = srz; }
+        if (nterms == 1) compute_zpart();
+    }
+    if (!grid_sync(prm.bar, G, prm.spin_limit, bar_id++)) return;
+
+    // C_k phases k = 1..nterms-1 of the preconditioner polynomial
+    auto precond_tail = [&](bool active_sys) -> bool {
+        for (int k = 1; k < nterms; ++k) {
+            double acc = 0.0;
+            const bool last = (k == nterms - 1);
+            if (active_sys) {
+                const VT* tcur = tbuf[tc];
+                VT* tnew = tbuf[tc ^ 1];
+                const double wk = prm.w[k];
+                auto gather = [&](int c, CT& g0, CT& g1, CT& g2) {
+                    VT u0, u1, u2;
+                    Vec4<VT>::load(tcur, c, u0, u1, u2);
+                    g0 = (CT)u0; g1 = (CT)u1; g2 = (CT)u2;
+                };
+                auto epi = [&](int row, CT w0, CT w1, CT w2) {
+                    VT c0, c1, c2;
+                    Vec4<VT>::load(tcur, row, c0, c1, c2);
+                    double v0 = w0, v1 = w1, v2 = w2;
+                    if (kSplit) {
+                        const int an = __ldg(S.rowflag + row);
+                        if (an >= 0) {
+                            double d0, d1, d2;
+                            dact_mul(an, (double)c0, (double)c1, (double)c2, d0, d1, d2);
+                            v0 += d0; v1 += d1; v2 += d2;
+                        }
+                    }
+                    double e0, e1, e2;
+                    dinv_apply(dinv, n, row, omega, v0, v1, v2, e0, e1, e2);
+                    const double n0 = (double)c0 - e0, n1 = (double)c1 - e1, n2 = (double)c2 - e2;
+                    Vec4<VT>::store(tnew, row, (VT)n0, (VT)n1, (VT)n2);
+                    VT q0, q1, q2;
+                    Vec4<VT>::load(z, row, q0, q1, q2);
+                    const VT s0 = (VT)((double)q0 + wk * n0), s1 = (VT)((double)q1 + wk * n1),
+                             s2 = (VT)((double)q2 + wk * n2);
+                    Vec4<VT>::store(z, row, s0, s1, s2);
+                    if (last) {
+                        double r0, r1, r2;
+                        Vec4<double>::load(r, row, r0, r1, r2);
+                        acc += r0 * (double)s0 + r1 * (double)s1 + r2 * (double)s2;
+                    }
+                };
+                spmv_own<MT, CT, TPR>(S.rowptr, S.colidx, vals, nnz, rb, re, gather, epi);
+                if (last) compute_zpart();
+            }
+            if (last) {
+                const double sum = block_sum(acc, s_red, &s_out);
+                if (threadIdx.x == 0) partB[cta] = sum;
+            }
+            tc ^= 1;
+            if (!grid_sync(prm.bar, G, prm.spin_limit, bar_id++)) return false;
+        }
+        return true;
+    };
+    if (!precond_tail(true)) return;
+
+    // ---------------- main loop: one slot per iteration ----------------
+    for (;;) {
+        const double rr = sum_parts(partA, cb, ce, &s_out);
+        const double rzn = sum_parts(partB, cb, ce, &s_out);
+        if (!done) {
+            if (first) {
+                normb = sqrt(rr);
+                rel = normb > 0 ? 1.0 : 0.0;
+                if (!(normb > 0)) { done = true; status = 0; }
+                if (!isfinite(normb)) { done = true; status = 3; }
+            } else {
+                rel = sqrt(rr) / normb;
+            }
+            if (!done) {
+                if (prev_slot == kReplace) {
+                    ++nrep;
+                    if (rel <= prm.tol) { done = true; status = 0; }
+                    else if (it >= prm.max_iter) { done = true; status = 4; }
+                    else {
+                        beta = conv_check ? 0.0 : rzn / rz;                    // restart after a failed check
+                        slot = kNormal;
+                    }
+                    conv_check = false;
+                } else if (!first && rel <= prm.tol) {
+                    slot = kReplace; conv_check = true;                        // linear_hsc.cu:375-387
+                } else if (it >= prm.max_iter) {
+                    done = true; status = 4;
+                } else if (!first && prm.rr_every > 0 && it % prm.rr_every == 0) {
+                    slot = kReplace; conv_check = false;                       // FP64 reliable update
+                } else {
+                    beta = first ? 0.0 : rzn / rz;
+                    slot = kNormal;
+                }
+                if (!done && slot == kNormal) {
+                    if (!(isfinite(rzn) && rzn > 0)) { done = true; status = 3; }   // linear_hsc.cu:370-371
+                    else rz = rzn;
+                    if (!done && leader_cta && threadIdx.x == 0 && it < S.max_coef && it > 0)
+                        S.cg_coef[2 * (it - 1) + 1] = beta;
+                }
+            }
+            first = false;
+        }
+        if (done) slot = kIdle;
+        if (done && !counted) {
+            counted = true;
+            if (leader_cta && threadIdx.x == 0) {
+                S.out[0] = it; S.out[1] = rel; S.out[2] = status; S.out[3] = normb; S.out[4] = nrep;
+                __threadfence();
+                atomicSub(prm.remaining, 1);
+            }
+        }
+
+        // ---- phase A: y = D p (p = z + beta p_prev on the fly), tt = Vt^T p ----
+        {
+            double acc = 0.0;
+            if (slot == kNormal) {
+                VT* pnew = pbuf[pc ^ 1];
+                const VT* pprev = pbuf[pc];
+                const CT bc = (CT)beta;
+                const double bd = beta;
+                auto gather = [&](int c, CT& g0, CT& g1, CT& g2) {
+                    VT z0, z1, z2, q0, q1, q2;
+                    Vec4<VT>::load(z, c, z0, z1, z2);
+                    Vec4<VT>::load(pprev, c, q0, q1, q2);
+                    g0 = (CT)(VT)((CT)z0 + bc * (CT)q0);
+                    g1 = (CT)(VT)((CT)z1 + bc * (CT)q1);
+                    g2 = (CT)(VT)((CT)z2 + bc * (CT)q2);
+                };
+                auto epi = [&](int row, CT y0, CT y1, CT y2) {
+                    CT g0, g1, g2;
+                    gather(row, g0, g1, g2);
+                    Vec4<VT>::store(pnew, row, (VT)g0, (VT)g1, (VT)g2);
+                    const int an = __ldg(S.rowflag + row);
+                    if (an >= 0) {
+                        // FP64 direction and product at a coupled node
+                        VT z0, z1, z2;
+                        Vec4<VT>::load(z, row, z0, z1, z2);
+                        double* pa = S.pact + 3 * (size_t)an;
+                        const double a0 = (double)z0 + bd * pa[0], a1 = (double)z1 + bd * pa[1],
+                                     a2 = (double)z2 + bd * pa[2];
+                        pa[0] = a0; pa[1] = a1; pa[2] = a2;
+                        double v0 = y0, v1 = y1, v2 = y2;
+                        if (kSplit) {
+                            double d0, d1, d2;
+                            dact_mul(an, a0, a1, a2, d0, d1, d2);
+                            v0 += d0; v1 += d1; v2 += d2;
+                        }
+                        double* ya = S.yact + 3 * (size_t)an;
+                        ya[0] = v0; ya[1] = v1; ya[2] = v2;
+                        acc += a0 * v0 + a1 * v1 + a2 * v2;
+                    } else {
+                        Vec4<VT>::store(y, row, (VT)y0, (VT)y1, (VT)y2);
+                        acc += (double)g0 * (double)(VT)y0 + (double)g1 * (double)(VT)y1 + (double)g2 * (double)(VT)y2;
+                    }
+                };
+                spmv_own<MT, CT, TPR>(S.rowptr, S.colidx, vals, nnz, rb, re, gather, epi);
+                // tt_j = (Vt^T z)_j + beta tt_j (per-CTA partials of Vt^T z from the last phase)
+                for (int j = gwarp; j < rank; j += nwarp) {
+                    double sz = 0.0;
+                    for (int c = lane; c < ncta; c += 32) sz += S.zpart[(size_t)j * ncta + c];
+                    sz = warp_sum(sz);
+                    if (lane == 0) {
+                        const double t = sz + bd * S.tt[j];
+                        S.tt[j] = t;
+                        acc -= __ldg(S.dpiv + j) * t * t;
+                    }
+                }
+            } else if (slot == kReplace) {
+                // r = rhs - D x in FP64 (the assembled matrix, not the bulk precision)
+                auto gather = [&](int c, double& g0, double& g1, double& g2) { Vec4<double>::load(x, c, g0, g1, g2); };
+                auto epi = [&](int row, double y0, double y1, double y2) {
+                    double h0, h1, h2;
+                    Vec4<double>::load(rhs, row, h0, h1, h2);
+                    Vec4<double>::store(r, row, h0 - y0, h1 - y1, h2 - y2);
+                };
+                spmv_own<double, double, TPR>(S.rowptr, S.colidx, S.vals64, nnz, rb, re, gather, epi);
+                for (int j = gwarp; j < rank; j += nwarp) {
+                    const double* col = vt + (size_t)j * a;
+                    double d = 0.0;
+                    for (int i = lane; i < a; i += 32) {
+                        const int dof = __ldg(S.act + i);
+                        d += __ldg(col + i) * x[4 * (dof / 3) + dof % 3];
+                    }
+                    d = warp_sum(d);
+                    if (lane == 0) S.ttx[j] = d;
+                }
+            }
+            const double sum = block_sum(acc, s_red, &s_out);
+            if (threadIdx.x == 0) partC[cta] = sum;
+        }
+        if (!grid_sync(prm.bar, G, prm.spin_limit, bar_id++)) return;
+        if (ld_volatile_i32(prm.remaining) == 0) break;
+
+        // ---- phase B: alpha, low-rank correction, x/r update, t = w Dd^-1 r ----
+        {
+            double acc_rr = 0.0, acc_rz = 0.0;
+            bool work = slot != kIdle;
+            double alpha = 0.0;
+            if (slot == kNormal) {
+                const double pAp = sum_parts(partC, cb, ce, &s_out);
+                if (!(isfinite(pAp) && pAp > 0)) {
+                    done = true; status = 3; work = false;                      // linear_hsc.cu:370-371
+                } else {
+                    alpha = rz / pAp;
+                    if (leader_cta && threadIdx.x == 0 && it < S.max_coef) S.cg_coef[2 * it] = alpha;
+                }
+            }
+            if (work) {
+                const double* tsrc = slot == kNormal ? S.tt : S.ttx;
+                if (ab < ae) {
+                    for (int j = threadIdx.x; j < rank; j += kThreads) s_dtt[j] = __ldg(S.dpiv + j) * tsrc[j];
+                    __syncthreads();
+                    for (int i = ab + threadIdx.x; i < ae; i += kThreads) {
+                        double c = 0.0;
+                        for (int j = 0; j < rank; ++j) c += __ldg(vt + (size_t)j * a + i) * s_dtt[j];
+                        if (slot == kNormal) S.yact[i] -= c;                       // y = D p - Vt d Vt^T p
+                        else elem<double>(r, __ldg(S.act + i)) += c;              // r = rhs - D x + Vt d Vt^T x
+                    }
+                }
+                __syncthreads();
+                const VT* pnew = pbuf[pc ^ 1];
+                const double w0 = prm.w[0];
+                for (int row = rb + threadIdx.x; row < re; row += kThreads) {
+                    double r0, r1, r2;
+                    if (slot == kNormal) {
+                        double p0, p1, p2, y0, y1, y2;
+                        const int an = __ldg(S.rowflag + row);
+                        if (an >= 0) {
+                            const double* pa = S.pact + 3 * (size_t)an;
+                            const double* ya = S.yact + 3 * (size_t)an;
+                            p0 = pa[0]; p1 = pa[1]; p2 = pa[2];
+                            y0 = ya[0]; y1 = ya[1]; y2 = ya[2];
+                        } else {
+                            VT q0, q1, q2, u0, u1, u2;
+                            Vec4<VT>::load(pnew, row, q0, q1, q2);
+                            Vec4<VT>::load(y, row, u0, u1, u2);
+                            p0 = q0; p1 = q1; p2 = q2; y0 = u0; y1 = u1; y2 = u2;
+                        }
+                        double x0, x1, x2;
+                        Vec4<double>::load(x, row, x0, x1, x2);
+                        Vec4<double>::load(r, row, r0, r1, r2);
+                        x0 += alpha * p0; x1 += alpha * p1; x2 += alpha * p2;
+                        r0 -= alpha * y0; r1 -= alpha * y1; r2 -= alpha * y2;
+                        Vec4<double>::store(x, row, x0, x1, x2);
+                        Vec4<double>::store(r, row, r0, r1, r2);
+                    } else {
+                        Vec4<double>::load(r, row, r0, r1, r2);
+                    }
+                    double t0, t1, t2;
+                    dinv_apply(dinv, n, row, omega, r0, r1, r2, t0, t1, t2);
+                    Vec4<VT>::store(tbuf[tc], row, (VT)t0, (VT)t1, (VT)t2);
+                    const VT z0 = (VT)(w0 * t0), z1 = (VT)(w0 * t1), z2 = (VT)(w0 * t2);
+                    Vec4<VT>::store(z, row, z0, z1, z2);
+                    acc_rr += r0 * r0 + r1 * r1 + r2 * r2;
+                    acc_rz += r0 * (double)z0 + r1 * (double)z1 + r2 * (double)z2;
+                }
+                if (slot == kNormal) {
+                    ++it;
+                    pc ^= 1;
+                }
+                if (nterms == 1) compute_zpart();
+            }
+            const double srr = block_sum(acc_rr, s_red, &s_out);
+            const double srz = block_sum(acc_rz, s_red, &s_out);
+            if (threadIdx.x == 0) { partA[cta] = srr; if (nterms == 1) partB[cta] = srz; }
+            if (!work) slot = kIdle;
+        }
+        if (!grid_sync(prm.bar, G, prm.spin_limit, bar_id++)) return;
+        prev_slot = slot;
+        // ---- phases C ----
+        if (!precond_tail(slot != kIdle)) return;
+    }
+}
+
+template <class MT, class VT, int TPR>
+cudaError_t launch_t(const PcgParams& prm, int grid, cudaStream_t st, size_t smem) {
+    void* args[] = {(void*)&prm};
+    return cudaLaunchCooperativeKernel((void*)pcg_kernel<MT, VT, TPR>, dim3(grid), dim3(kThreads), args, smem, st);
+}
+
+template <class MT, class VT, int TPR>
+int bps_t(size_t smem) {
+    int b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, pcg_kernel<MT, VT, TPR>, kThreads, smem);
+    return b;
+}
+
+}  // namespace
+
+constexpr size_t kDttSmem = 256 * sizeof(double);
+
+cudaError_t launch_pcg(int precision, int tpr, const PcgParams& prm, int grid, cudaStream_t st) {
+    count_launch();
+#define HSC_PCG_CASE(MT, VT)                                                   \
+    switch (tpr) {                                                             \
+        case 2: return launch_t<MT, VT, 2>(prm, grid, st, kDttSmem);           \
+        case 8: return launch_t<MT, VT, 8>(prm, grid, st, kDttSmem);           \
+        default: return launch_t<MT, VT, 4>(prm, grid, st, kDttSmem);          \
+    }
+    if (precision == 0) { HSC_PCG_CASE(double, double) }
+    if (precision == 1) { HSC_PCG_CASE(float, float) }
+    HSC_PCG_CASE(__nv_bfloat16, float)
+#undef HSC_PCG_CASE
+}
+
+int pcg_blocks_per_sm(int precision, int tpr) {
+#define HSC_BPS_CASE(MT, VT)                                                   \
+    switch (tpr) {                                                             \
+        case 2: return bps_t<MT, VT, 2>(kDttSmem);                             \
+        case 8: return bps_t<MT, VT, 8>(kDttSmem);                             \
+        default: return bps_t<MT, VT, 4>(kDttSmem);                            \
+    }
+    if (precision == 0) { HSC_BPS_CASE(double, double) }
+    if (precision == 1) { HSC_BPS_CASE(float, float) }
+    HSC_BPS_CASE(__nv_bfloat16, float)
+#undef HSC_BPS_CASE
+}
+
+}  // namespace hsc

@@ -1,0 +1,881 @@
+// Numeric setup kernels of one HSC solve (everything the reference does in
+// LinearHSC::setup, linear_hsc.cu:195-304, moved onto the GPU):
+//   * pattern hash of the BCOO indices (detects a changed pattern behind the
+//     same pointers);
+//   * BCOO (one triangle, column-major 3x3) -> full row-owner BSR planes;
+//   * FEM 3x3 diagonal inverses with the det > 0 check (linear_hsc.cu:70-80);
+//   * dense A (qm x qm) and coupling E (qm x a) over the sorted active FEM
+//     dofs (linear_hsc.cu:216-247);
+//   * full-pivot ACA of E as one cooperative kernel (core.py:22-50);
+//   * small dense FP64 algebra for the ABD inverse and the reduced core
+//     (Cholesky, triangular solves, tiled GEMM, LDL^T);
+//   * right-hand side, back-substitution and the full-system residual.
+#include "hsc_setup.cuh"
+
+#include <atomic>
+#include <cfloat>
+
+namespace hsc {
+
+// kernels launched by this library (for the launch count a benchmark reports)
+static std::atomic<long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+#define HSC_COUNTED(...)      \
+    do {                      \
+        ::hsc::count_launch(); \
+        __VA_ARGS__;          \
+    } while (0)
+
+namespace {
+
+__device__ __forceinline__ double wsum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double bsum(double v) {
+    __shared__ double s[32];
+    v = wsum(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    __syncthreads();
+    if (lane == 0) s[warp] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (warp == 0) {
+        t = lane < nw ? s[lane] : 0.0;
+        t = wsum(t);
+    }
+    return t;  // valid in thread 0
+}
+
+// ---------------------------------------------------------------------------
+__global__ void pattern_hash_kernel(const int* rows, const int* cols, long long nnzb,
+                                    unsigned long long* out) {
+    unsigned long long h = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nnzb;
+         t += (long long)gridDim.x * blockDim.x) {
+        unsigned long long v = ((unsigned long long)(unsigned)rows[t] << 32) | (unsigned)cols[t];
+        v ^= (unsigned long long)(t + 1) * 0x9E3779B97F4A7C15ull;
+        v ^= v >> 31; v *= 0xBF58476D1CE4E5B9ull; v ^= v >> 29;
+        h += v;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, h);
+}
+
+template <class MT>
+__global__ void fill_bsr_kernel(const int* src, const double* values, int nnz, double* v64, MT* vmt) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nnz) return;
+    const int packed = src[k];
+    const long long t = packed >> 1;
+    const int tr = packed & 1;
+    const double* B = values + 9 * t;  // B(r, c) = B[r + 3 c]
+#pragma unroll
+    for (int rr = 0; rr < 3; ++rr)
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+            const double v = tr ? B[cc + 3 * rr] : B[rr + 3 * cc];
+            v64[(size_t)(3 * rr + cc) * nnz + k] = v;
+            if (vmt) vmt[(size_t)(3 * rr + cc) * nnz + k] = Num<MT>::put(v);
+        }
+}
+
+template <class DT>
+__global__ void dinv_kernel(const int* diag_pos, const double* v64, int nnz, int n, DT* dinv, int* bad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int k = diag_pos[i];
+    double b[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) b[e] = v64[(size_t)e * nnz + k];
+    // adjugate / det
+    const double c00 = b[4] * b[8] - b[5] * b[7];
+    const double c01 = b[5] * b[6] - b[3] * b[8];
+    const double c02 = b[3] * b[7] - b[4] * b[6];
+    const double det = b[0] * c00 + b[1] * c01 + b[2] * c02;
+    double inv[9];
+    if (!(det > 0.0) || !isfinite(det)) {
+        atomicAdd(bad, 1);
+#pragma unroll
+        for (int e = 0; e < 9; ++e) inv[e] = 0.0;
+    } else {
+        const double id = 1.0 / det;
+        inv[0] = c00 * id;
+        inv[1] = (b[2] * b[7] - b[1] * b[8]) * id;
+        inv[2] = (b[1] * b[5] - b[2] * b[4]) * id;
+        inv[3] = c01 * id;
+        inv[4] = (b[0] * b[8] - b[2] * b[6]) * id;
+        inv[5] = (b[2] * b[3] - b[0] * b[5]) * id;
+        inv[6] = c02 * id;
+        inv[7] = (b[1] * b[6] - b[0] * b[7]) * id;
+        inv[8] = (b[0] * b[4] - b[1] * b[3]) * id;
+    }
+#pragma unroll
+    for (int e = 0; e < 9; ++e) dinv[(size_t)e * n + i] = (DT)inv[e];
+}
+
+__global__ void extract_A_kernel(const int* list, int count, const double* values, int qm, double* A) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= count) return;
+    const long long t = list[3 * e];
+    const int ar = list[3 * e + 1], ac = list[3 * e + 2];
+    const double* B = values + 9 * t;
+    for (int rr = 0; rr < 3; ++rr)
+        for (int cc = 0; cc < 3; ++cc) {
+            const double v = B[rr + 3 * cc];
+            A[(size_t)(3 * ar + rr) * qm + 3 * ac + cc] = v;
+            if (ar != ac) A[(size_t)(3 * ac + cc) * qm + 3 * ar + rr] = v;
+        }
+}
+
+__global__ void extract_E_kernel(const int* list, int count, const double* values, int a, double* E,
+                                 int* node_nz) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= count) return;
+    const long long t = list[4 * e];
+    const int q = list[4 * e + 1], an = list[4 * e + 2], orient = list[4 * e + 3];
+    const double* B = values + 9 * t;
+    double sq = 0.0;
+    for (int rr = 0; rr < 3; ++rr)
+        for (int cc = 0; cc < 3; ++cc) {
+            const double v = orient ? B[cc + 3 * rr] : B[rr + 3 * cc];
+            E[(size_t)(3 * q + rr) * a + 3 * an + cc] = v;
+            sq += v * v;
+        }
+    if (sq != 0.0) node_nz[an] = 1;
+}
+
+// ---------------------------------------------------------------------------
+// full-pivot ACA (cooperative; R double-buffered; one barrier per step)
+// ---------------------------------------------------------------------------
+struct MaxIdx {
+    double v;
+    long long i;
+};
+__device__ __forceinline__ MaxIdx better(MaxIdx p, MaxIdx q) {
+    if (q.v > p.v || (q.v == p.v && q.i < p.i)) return q;
+    return p;
+}
+__device__ __forceinline__ MaxIdx warp_best(MaxIdx m) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        MaxIdx q;
+        q.v = __shfl_xor_sync(0xffffffffu, m.v, o);
+        q.i = __shfl_xor_sync(0xffffffffu, m.i, o);
+        m = better(m, q);
+    }
+    return m;
+}
+
+__global__ void __launch_bounds__(256) aca_kernel(AcaParams p) {
+    __shared__ double s_sum[8];
+    __shared__ MaxIdx s_max[8];
+    __shared__ double s_bc[4];
+    __shared__ long long s_bi;
+    const int m = p.m, nc = p.nc;
+    const long long total = (long long)m * nc;
+    const unsigned G = gridDim.x;
+    const long long chunk = (total + G - 1) / G;
+    const long long f0 = min(total, (long long)blockIdx.x * chunk), f1 = min(total, f0 + chunk);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double* R[2] = {p.R0, p.R1};
+    int cur = 0;
+
+    auto reduce_local = [&](double lsum, MaxIdx lm) {
+        lsum = wsum(lsum);
+        lm = warp_best(lm);
+        if (lane == 0) { s_sum[warp] = lsum; s_max[warp] = lm; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s = 0.0;
+            MaxIdx b{-1.0, (long long)total};
+            for (int w = 0; w < 8; ++w) { s += s_sum[w]; b = better(b, s_max[w]); }
+            p.psum[blockIdx.x] = s;
+            p.pmax[blockIdx.x] = b.v;
+            p.pidx[blockIdx.x] = b.i;
+        }
+        __syncthreads();
+    };
+    // pass 0 over E
+    {
+        double ls = 0.0;
+        MaxIdx lm{-1.0, (long long)total};
+        for (long long f = f0 + threadIdx.x; f < f1; f += blockDim.x) {
+            const double v = R[0][f];
+            ls += v * v;
+            lm = better(lm, MaxIdx{fabs(v), f});
+        }
+        reduce_local(ls, lm);
+    }
+    if (!grid_sync(p.bar, G, p.spin_limit, 100)) return;
+    double scale = 0.0, residual = 0.0;
+    int k = 0;
+    for (;; ++k) {
+        // global reduction, same order in every CTA (warp 0, lanes stride the partials)
+        if (warp == 0) {
+            double s = 0.0;
+            MaxIdx b{-1.0, (long long)total};
+            for (unsigned c = lane; c < G; c += 32) {
+                s += p.psum[c];
+                b = better(b, MaxIdx{p.pmax[c], p.pidx[c]});
+            }
+            s = wsum(s);
+            b = warp_best(b);
+            if (lane == 0) { s_bc[0] = s; s_bc[1] = b.v; s_bi = b.i; }
+        }
+        __syncthreads();
+        const double gsum = s_bc[0];
+        const long long gi = s_bi;
+        if (k == 0) {
+            scale = sqrt(gsum);
+            residual = scale > 0 ? 1.0 : 0.0;
+        } else {
+            residual = sqrt(gsum) / scale;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) p.hist[k] = residual;
+        if (!(residual > p.rtol) || k >= p.cap) break;
+        const int i = (int)(gi / nc), j = (int)(gi - (long long)i * nc);
+        const double* Rc = R[cur];
+        double* Rn = R[cur ^ 1];
+        const double pivot = Rc[gi];
+        if (!(fabs(pivot) > DBL_EPSILON * fmax(scale, DBL_MIN))) break;
+        if (blockIdx.x == 0) {
+            for (int r = threadIdx.x; r < m; r += blockDim.x) p.U[(size_t)k * m + r] = Rc[(size_t)r * nc + j];
+            for (int c = threadIdx.x; c < nc; c += blockDim.x) p.V[(size_t)k * nc + c] = Rc[(size_t)i * nc + c] / pivot;
+        }
+        double ls = 0.0;
+        MaxIdx lm{-1.0, (long long)total};
+        for (long long f = f0 + threadIdx.x; f < f1; f += blockDim.x) {
+            const int rr = (int)(f / nc), cc = (int)(f - (long long)rr * nc);
+            const double u = Rc[(size_t)rr * nc + j];
+            const double v = Rc[(size_t)i * nc + cc] / pivot;
+            const double val = __dsub_rn(Rc[f], __dmul_rn(u, v));  // numpy: R - outer(u, v), no FMA
+            Rn[f] = val;
+            ls += val * val;
+            lm = better(lm, MaxIdx{fabs(val), f});
+        }
+        reduce_local(ls, lm);
+        cur ^= 1;
+        if (!grid_sync(p.bar, G, p.spin_limit, 101)) return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *p.rank = k;
+        *p.err = residual;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// small dense FP64 algebra
+// ---------------------------------------------------------------------------
+// C = alpha * op(A) * op(B) + beta * C, row-major; op = transpose when t* != 0.
+// M, N, K may be device scalars (dims given as pointers override when non-null).
+__global__ void __launch_bounds__(256) gemm_kernel(GemmArgs g) {
+    __shared__ double As[32][33];
+    __shared__ double Bs[32][33];
+    const int M = g.dM ? *g.dM : g.M, N = g.dN ? *g.dN : g.N, K = g.dK ? *g.dK : g.K;
+    const int bm = blockIdx.y * 32, bn = blockIdx.x * 32;
+    if (bm >= M || bn >= N) return;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 8 rows of 32
+    double acc[4] = {0, 0, 0, 0};
+    for (int k0 = 0; k0 < K; k0 += 32) {
+        for (int rr = ty; rr < 32; rr += 8) {
+            const int row = bm + rr, kk = k0 + tx;
+            double va = 0.0;
+            if (row < M && kk < K) va = g.tA ? g.A[(size_t)kk * g.lda + row] : g.A[(size_t)row * g.lda + kk];
+            As[rr][tx] = va;
+            const int kr = k0 + rr, col = bn + tx;
+            double vb = 0.0;
+            if (kr < K && col < N) vb = g.tB ? g.B[(size_t)col * g.ldb + kr] : g.B[(size_t)kr * g.ldb + col];
+            Bs[rr][tx] = vb;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int kk = 0; kk < 32; ++kk) {
+            const double b = Bs[kk][tx];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[q] += As[ty + 8 * q][kk] * b;
+        }
+        __syncthreads();
+    }
+    for (int q = 0; q < 4; ++q) {
+        const int row = bm + ty + 8 * q, col = bn + tx;
+        if (row < M && col < N) {
+            double* c = g.C + (size_t)row * g.ldc + col;
+            const double prev = g.beta == 0.0 ? 0.0 : g.beta * *c;
+            *c = g.alpha * acc[q] + prev;
+        }
+    }
+}
+
+// Cholesky A = L L^T (lower, row-major) in one CTA; L overwrites Lout.
+// Shared memory holds the matrix when it fits, else it works in Lout.
+__global__ void __launch_bounds__(1024) cholesky_kernel(const double* A, int m, double* Lout, int use_smem,
+                                                        int* bad) {
+    extern __shared__ double sm[];
+    double* L = use_smem ? sm : Lout;
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) L[e] = A[e];
+    __syncthreads();
+    __shared__ int s_bad;
+    if (threadIdx.x == 0) s_bad = 0;
+    __syncthreads();
+    for (int j = 0; j < m; ++j) {
+        if (threadIdx.x == 0) {
+            const double d = L[(size_t)j * m + j];
+            if (!(d > 0.0) || !isfinite(d)) { s_bad = 1; L[(size_t)j * m + j] = 1.0; }
+            else L[(size_t)j * m + j] = sqrt(d);
+        }
+        __syncthreads();
+        const double dj = L[(size_t)j * m + j];
+        for (int i = j + 1 + threadIdx.x; i < m; i += blockDim.x) L[(size_t)i * m + j] /= dj;
+        __syncthreads();
+        const int rem = m - j - 1;
+        for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
+            const int i = j + 1 + e / rem, l = j + 1 + e % rem;
+            if (l <= i) L[(size_t)i * m + l] -= L[(size_t)i * m + j] * L[(size_t)l * m + j];
+        }
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+        const int i = e / m, l = e % m;
+        Lout[e] = l <= i ? L[e] : 0.0;
+    }
+    if (threadIdx.x == 0 && s_bad) atomicAdd(bad, 1);
+}
+
+// X = A^-1 B with A = L L^T; B, X row-major m x ncol (may alias).  One warp
+// per right-hand-side column: forward then backward substitution.
+__global__ void chol_solve_kernel(const double* L, int m, const double* B, int ldb, double* X, int ldx,
+                                  int ncol, const int* dncol, double* work) {
+    const int nc = dncol ? *dncol : ncol;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (gw >= nc) return;
+    double* y = work + (size_t)gw * m;
+    for (int i = 0; i < m; ++i) {
+        double s = 0.0;
+        for (int k = lane; k < i; k += 32) s += L[(size_t)i * m + k] * y[k];
+        s = wsum(s);
+        if (lane == 0) y[i] = (B[(size_t)i * ldb + gw] - s) / L[(size_t)i * m + i];
+        __syncwarp();
+    }
+    for (int i = m - 1; i >= 0; --i) {
+        double s = 0.0;
+        for (int k = i + 1 + lane; k < m; k += 32) s += L[(size_t)k * m + i] * y[k];
+        s = wsum(s);
+        if (lane == 0) y[i] = (y[i] - s) / L[(size_t)i * m + i];
+        __syncwarp();
+    }
+    for (int i = lane; i < m; i += 32) X[(size_t)i * ldx + gw] = y[i];
+}
+
+// C (k x k, row-major, k from device) = L diag(d) L^T in one CTA: L unit lower
+// (row-major, ld kmax) and d written out; C symmetrised first.
+__global__ void __launch_bounds__(1024) ldlt_kernel(double* C, int kmax, const int* dk, double* L, double* d,
+                                                    int use_smem, int* bad) {
+    extern __shared__ double sm[];
+    const int k = *dk;
+    double* W = use_smem ? sm : C;
+    for (int e = threadIdx.x; e < k * k; e += blockDim.x) {
+        const int i = e / k, l = e % k;
+        W[e] = 0.5 * (C[(size_t)i * kmax + l] + C[(size_t)l * kmax + i]);
+    }
+    __syncthreads();
+    __shared__ int s_bad;
+    if (threadIdx.x == 0) s_bad = 0;
+    __syncthreads();
+    for (int j = 0; j < k; ++j) {
+        const double dj = W[(size_t)j * k + j];
+        if (threadIdx.x == 0 && !(isfinite(dj) && dj != 0.0)) s_bad = 1;
+        __syncthreads();
+        const double djs = (isfinite(dj) && dj != 0.0) ? dj : 1.0;
+        // column j of L: W[i][j] / d_j (keep W[i][j] unscaled until the update is done)
+        const int rem = k - j - 1;
+        for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
+            const int i = j + 1 + e / rem, l = j + 1 + e % rem;
+            if (l <= i) W[(size_t)i * k + l] -= W[(size_t)i * k + j] * W[(size_t)l * k + j] / djs;
+        }
+        __syncthreads();
+        for (int i = j + 1 + threadIdx.x; i < k; i += blockDim.x) W[(size_t)i * k + j] /= djs;
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < kmax * kmax; e += blockDim.x) {
+        const int i = e / kmax, l = e % kmax;
+        double v = 0.0;
+        if (i < k && l < k) v = (l < i) ? W[(size_t)i * k + l] : (l == i ? 1.0 : 0.0);
+        L[e] = v;
+    }
+    for (int j = threadIdx.x; j < kmax; j += blockDim.x) d[j] = j < k ? W[(size_t)j * k + j] : 0.0;
+    if (threadIdx.x == 0 && s_bad) atomicAdd(bad, 1);
+}
+
+// 12x12 diagonal-block Cholesky inverses (one thread per body) into a dense
+// qm x qm block-diagonal Binv (row-major)
+__global__ void block12_inverse_kernel(const double* A, int qm, double* Binv, int* bad) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= qm / 12) return;
+    double L[12][12];
+    const int o = 12 * b;
+    for (int i = 0; i < 12; ++i)
+        for (int j = 0; j < 12; ++j) L[i][j] = A[(size_t)(o + i) * qm + o + j];
+    bool ok = true;
+    for (int j = 0; j < 12; ++j) {
+        double d = L[j][j];
+        for (int k = 0; k < j; ++k) d -= L[j][k] * L[j][k];
+        if (!(d > 0.0) || !isfinite(d)) { ok = false; d = 1.0; }
+        d = sqrt(d);
+        L[j][j] = d;
+        for (int i = j + 1; i < 12; ++i) {
+            double s = L[i][j];
+            for (int k = 0; k < j; ++k) s -= L[i][k] * L[j][k];
+            L[i][j] = s / d;
+        }
+    }
+    if (!ok) atomicAdd(bad, 1);
+    for (int c = 0; c < 12; ++c) {
+        double y[12];
+        for (int i = 0; i < 12; ++i) {
+            double s = (i == c) ? 1.0 : 0.0;
+            for (int k = 0; k < i; ++k) s -= L[i][k] * y[k];
+            y[i] = s / L[i][i];
+        }
+        for (int i = 11; i >= 0; --i) {
+            double s = y[i];
+            for (int k = i + 1; k < 12; ++k) s -= L[k][i] * y[k];
+            y[i] = s / L[i][i];
+        }
+        for (int i = 0; i < 12; ++i) Binv[(size_t)(o + i) * qm + o + c] = y[i];
+    }
+}
+
+__global__ void axpby_mat_kernel(double* Y, const double* X, double a, double b, int n, int diag_m, double diag_add) {
+    // Y = a X + b Y (+ diag_add on the diagonal of an m x m matrix when diag_m > 0)
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    double v = a * (X ? X[e] : 0.0) + b * Y[e];
+    if (diag_m > 0 && (e / diag_m) == (e % diag_m)) v += diag_add;
+    Y[e] = v;
+}
+
+__global__ void symmetrize_kernel(double* P, int m) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m * m) return;
+    const int i = e / m, j = e % m;
+    if (j <= i) return;
+    const double v = 0.5 * (P[(size_t)i * m + j] + P[(size_t)j * m + i]);
+    P[(size_t)i * m + j] = v;
+    P[(size_t)j * m + i] = v;
+}
+
+__global__ void frob_kernel(const double* X, int n, double* out) {
+    double s = 0.0;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) s += X[e] * X[e];
+    s = bsum(s);
+    if (threadIdx.x == 0) *out = s;
+}
+
+// ---------------------------------------------------------------------------
+// vectors
+// ---------------------------------------------------------------------------
+// split b (contiguous N) into bq (qm) and node-padded FEM part bf
+__global__ void split_rhs_kernel(const double* b, int qo, int qm, int fo, int n, double* bq, double* bf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < qm) bq[i] = b[qo + i];
+    if (i < n) {
+        const double* s = b + fo + 3 * (size_t)i;
+        bf[4 * (size_t)i] = s[0];
+        bf[4 * (size_t)i + 1] = s[1];
+        bf[4 * (size_t)i + 2] = s[2];
+        bf[4 * (size_t)i + 3] = 0.0;
+    }
+}
+
+// c = W^T bq (k from device); one warp per output
+__global__ void wt_vec_kernel(const double* W, int qm, int kmax, const int* dk, const double* bq, double* c) {
+    const int k = *dk;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (gw >= k) return;
+    double s = 0.0;
+    for (int i = lane; i < qm; i += 32) s += W[(size_t)i * kmax + gw] * bq[i];
+    s = wsum(s);
+    if (lane == 0) c[gw] = s;
+}
+
+// rhs[act_i] -= (V c)_i ; V column-major a x kmax
+__global__ void rhs_lowrank_kernel(const double* V, int a, const int* dk, const double* c, const int* act,
+                                   double* rhs) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a) return;
+    const int k = *dk;
+    double s = 0.0;
+    for (int j = 0; j < k; ++j) s += V[(size_t)j * a + i] * c[j];
+    const int dof = act[i];
+    rhs[4 * (size_t)(dof / 3) + dof % 3] -= s;
+}
+
+// t = V^T x[act] ; one warp per column
+__global__ void vt_x_kernel(const double* V, int a, const int* dk, const int* act, const double* x, double* t) {
+    const int k = *dk;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (gw >= k) return;
+    double s = 0.0;
+    for (int i = lane; i < a; i += 32) {
+        const int dof = act[i];
+        s += V[(size_t)gw * a + i] * x[4 * (size_t)(dof / 3) + dof % 3];
+    }
+    s = wsum(s);
+    if (lane == 0) t[gw] = s;
+}
+
+// dq = P bq - W t  (one warp per ABD row), written to x_out[qo + i]
+__global__ void backsub_kernel(const double* P, const double* W, int qm, int kmax, const int* dk,
+                               const double* bq, const double* t, double* xq_out, double* xq_copy) {
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (gw >= qm) return;
+    const int k = *dk;
+    double s = 0.0;
+    for (int j = lane; j < qm; j += 32) s += P[(size_t)gw * qm + j] * bq[j];
+    for (int j = lane; j < k; j += 32) s -= W[(size_t)gw * kmax + j] * t[j];
+    s = wsum(s);
+    if (lane == 0) {
+        xq_out[gw] = s;
+        if (xq_copy) xq_copy[gw] = s;
+    }
+}
+
+__global__ void scatter_x_kernel(const double* xpad, int n, int fo, double* xout) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double* d = xout + fo + 3 * (size_t)i;
+    d[0] = xpad[4 * (size_t)i];
+    d[1] = xpad[4 * (size_t)i + 1];
+    d[2] = xpad[4 * (size_t)i + 2];
+}
+
+__global__ void gather_x_kernel(const double* x, int n, int fo, double* xpad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double* s = x + fo + 3 * (size_t)i;
+    xpad[4 * (size_t)i] = s[0];
+    xpad[4 * (size_t)i + 1] = s[1];
+    xpad[4 * (size_t)i + 2] = s[2];
+    xpad[4 * (size_t)i + 3] = 0.0;
+}
+
+// y_f = D x_f (FP64, row-owner) for the node-padded x; written contiguously
+// into y_out[fo + 3 i] (y_out may be null) and node-padded into ypad
+__global__ void bsr_spmv64_kernel(const int* rowptr, const int* colidx, const double* v64, int nnz, int n,
+                                  const double* xpad, double* ypad) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = tid >> 2, sub = tid & 3;
+    double a0 = 0, a1 = 0, a2 = 0;
+    if (row < n) {
+        for (int k = rowptr[row] + sub; k < rowptr[row + 1]; k += 4) {
+            const int c = colidx[k];
+            const double x0 = xpad[4 * (size_t)c], x1 = xpad[4 * (size_t)c + 1], x2 = xpad[4 * (size_t)c + 2];
+            const double* v = v64 + k;
+            a0 += v[0] * x0 + v[(size_t)nnz] * x1 + v[2 * (size_t)nnz] * x2;
+            a1 += v[3 * (size_t)nnz] * x0 + v[4 * (size_t)nnz] * x1 + v[5 * (size_t)nnz] * x2;
+            a2 += v[6 * (size_t)nnz] * x0 + v[7 * (size_t)nnz] * x1 + v[8 * (size_t)nnz] * x2;
+        }
+    }
+#pragma unroll
+    for (int o = 2; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    }
+    if (row < n && sub == 0) {
+        ypad[4 * (size_t)row] = a0;
+        ypad[4 * (size_t)row + 1] = a1;
+        ypad[4 * (size_t)row + 2] = a2;
+        ypad[4 * (size_t)row + 3] = 0.0;
+    }
+}
+
+// y_f[act_c] += sum_r E[r, c] xq[r]   (one thread per active column)
+__global__ void et_xq_kernel(const double* E, int qm, int a, const int* act, const double* xq, double* ypad) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a) return;
+    double s = 0.0;
+    for (int r = 0; r < qm; ++r) s += E[(size_t)r * a + c] * xq[r];
+    const int dof = act[c];
+    ypad[4 * (size_t)(dof / 3) + dof % 3] += s;
+}
+
+// yq = A xq + E x_f[act]   (one warp per ABD row)
+__global__ void abd_rows_kernel(const double* A, const double* E, int qm, int a, const int* act,
+                                const double* xq, const double* xpad, double* yq) {
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (gw >= qm) return;
+    double s = 0.0;
+    for (int j = lane; j < qm; j += 32) s += A[(size_t)gw * qm + j] * xq[j];
+    for (int c = lane; c < a; c += 32) {
+        const int dof = act[c];
+        s += E[(size_t)gw * a + c] * xpad[4 * (size_t)(dof / 3) + dof % 3];
+    }
+    s = wsum(s);
+    if (lane == 0) yq[gw] = s;
+}
+
+// deterministic dots for the full residual: out = {|b - y|^2, |b|^2, b.x}
+__global__ void residual_partial_kernel(const double* bf, const double* yf, const double* xf, int n4,
+                                        const double* bq, const double* yq, const double* xq, int qm,
+                                        double* part) {
+    double s0 = 0, s1 = 0, s2 = 0;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n4; e += gridDim.x * blockDim.x) {
+        const double d = bf[e] - yf[e];
+        s0 += d * d; s1 += bf[e] * bf[e]; s2 += bf[e] * xf[e];
+    }
+    if (blockIdx.x == 0)
+        for (int e = threadIdx.x; e < qm; e += blockDim.x) {
+            const double d = bq[e] - yq[e];
+            s0 += d * d; s1 += bq[e] * bq[e]; s2 += bq[e] * xq[e];
+        }
+    s0 = bsum(s0);
+    s1 = bsum(s1);
+    s2 = bsum(s2);
+    if (threadIdx.x == 0) {
+        part[3 * blockIdx.x] = s0;
+        part[3 * blockIdx.x + 1] = s1;
+        part[3 * blockIdx.x + 2] = s2;
+    }
+}
+
+__global__ void residual_final_kernel(const double* part, int np, double* out) {
+    if (threadIdx.x != 0) return;
+    double s0 = 0, s1 = 0, s2 = 0;
+    for (int i = 0; i < np; ++i) { s0 += part[3 * i]; s1 += part[3 * i + 1]; s2 += part[3 * i + 2]; }
+    out[0] = s0; out[1] = s1; out[2] = s2;
+}
+
+// y (contiguous N) from node-padded y_f and yq
+__global__ void scatter_y_kernel(const double* ypad, int n, int fo, const double* yq, int qm, int qo, double* y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        double* d = y + fo + 3 * (size_t)i;
+        d[0] = ypad[4 * (size_t)i];
+        d[1] = ypad[4 * (size_t)i + 1];
+        d[2] = ypad[4 * (size_t)i + 2];
+    }
+    if (i < qm) y[qo + i] = yq[i];
+}
+
+// x_acc += alpha * d (device alpha = min(1, num/den)); both contiguous N
+__global__ void line_step_kernel(double* x, const double* d, int N, const double* nd) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double num = nd[0], den = nd[1];
+    const double alpha = (num > 0 && den > 0) ? fmin(1.0, num / den) : 0.0;
+    x[i] += alpha * d[i];
+}
+
+__global__ void dot2_kernel(const double* a, const double* b, const double* c, int N, double* out) {
+    // out[0] = a.b, out[1] = b.c  (one CTA, deterministic)
+    double s0 = 0, s1 = 0;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) { s0 += a[i] * b[i]; s1 += b[i] * c[i]; }
+    s0 = bsum(s0);
+    s1 = bsum(s1);
+    if (threadIdx.x == 0) { out[0] = s0; out[1] = s1; }
+}
+
+__global__ void sub_kernel(const double* b, const double* y, double* r, int N) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) r[i] = b[i] - y[i];
+}
+
+// FP64 copies of the coupled nodes' diagonal blocks; in the mixed modes the
+// bulk planes drop them (they are applied in FP64 by the PCG kernel)
+template <class MT>
+__global__ void split_active_diag_kernel(const int* act, int nact_nodes, const int* diag_pos, const double* v64,
+                                         int nnz, MT* vmt, double* dact) {
+    const int an = blockIdx.x * blockDim.x + threadIdx.x;
+    if (an >= nact_nodes) return;
+    const int node = act[3 * an] / 3;
+    const int k = diag_pos[node];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+        dact[9 * (size_t)an + e] = v64[(size_t)e * nnz + k];
+        if (vmt) vmt[(size_t)e * nnz + k] = Num<MT>::put(0.0);
+    }
+}
+
+__global__ void f64_to_f32_kernel(const double* src, float* dst, long long n) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = (float)src[i];
+}
+
+__global__ void set_int_kernel(int* p, int v) { *p = v; }
+
+inline int blocks(long long n, int t = 256) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+
+// ===========================================================================
+// launchers
+// ===========================================================================
+void launch_pattern_hash(const int* rows, const int* cols, long long nnzb, unsigned long long* out, cudaStream_t st) {
+    cudaMemsetAsync(out, 0, sizeof(unsigned long long), st);
+    const int g = (int)std::min<long long>(1184, std::max<long long>(1, (nnzb + 255) / 256));
+    HSC_COUNTED(pattern_hash_kernel<<<g, 256, 0, st>>>(rows, cols, nnzb, out));
+}
+
+void launch_fill_bsr(int precision, const int* src, const double* values, int nnz, double* v64, void* vmt,
+                     cudaStream_t st) {
+    if (nnz == 0) return;
+    if (precision == 0) HSC_COUNTED(fill_bsr_kernel<double><<<blocks(nnz), 256, 0, st>>>(src, values, nnz, v64, nullptr));
+    else if (precision == 1) HSC_COUNTED(fill_bsr_kernel<float><<<blocks(nnz), 256, 0, st>>>(src, values, nnz, v64, (float*)vmt));
+    else HSC_COUNTED(fill_bsr_kernel<__nv_bfloat16><<<blocks(nnz), 256, 0, st>>>(src, values, nnz, v64, (__nv_bfloat16*)vmt));
+}
+
+void launch_dinv(int precision, const int* diag_pos, const double* v64, int nnz, int n, void* dinv, int* bad,
+                 cudaStream_t st) {
+    if (n == 0) return;
+    if (precision == 0) HSC_COUNTED(dinv_kernel<double><<<blocks(n), 256, 0, st>>>(diag_pos, v64, nnz, n, (double*)dinv, bad));
+    else HSC_COUNTED(dinv_kernel<float><<<blocks(n), 256, 0, st>>>(diag_pos, v64, nnz, n, (float*)dinv, bad));
+}
+
+void launch_extract(const int* qq, int nqq, const int* qf, int nqf, const double* values, int qm, int a, double* A,
+                    double* E, int* node_nz, cudaStream_t st) {
+    if (qm) cudaMemsetAsync(A, 0, sizeof(double) * qm * qm, st);
+    if (qm && a) cudaMemsetAsync(E, 0, sizeof(double) * qm * a, st);
+    if (a) cudaMemsetAsync(node_nz, 0, sizeof(int) * (a / 3), st);
+    if (nqq) HSC_COUNTED(extract_A_kernel<<<blocks(nqq), 256, 0, st>>>(qq, nqq, values, qm, A));
+    if (nqf) HSC_COUNTED(extract_E_kernel<<<blocks(nqf), 256, 0, st>>>(qf, nqf, values, a, E, node_nz));
+}
+
+cudaError_t launch_aca(const AcaParams& p, int grid, cudaStream_t st) {
+    count_launch();
+    void* args[] = {(void*)&p};
+    return cudaLaunchCooperativeKernel((void*)aca_kernel, dim3(grid), dim3(256), args, 0, st);
+}
+
+int aca_blocks_per_sm() {
+    int b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, aca_kernel, 256, 0);
+    return b;
+}
+
+void launch_gemm(const GemmArgs& g, int M, int N, cudaStream_t st) {
+    if (M <= 0 || N <= 0) return;
+    dim3 grid((N + 31) / 32, (M + 31) / 32);
+    HSC_COUNTED(gemm_kernel<<<grid, 256, 0, st>>>(g));
+}
+
+void launch_cholesky(const double* A, int m, double* L, int* bad, cudaStream_t st) {
+    const size_t bytes = sizeof(double) * (size_t)m * m;
+    const int use = bytes <= 200 * 1024;
+    if (use) cudaFuncSetAttribute(cholesky_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    HSC_COUNTED(cholesky_kernel<<<1, 1024, use ? bytes : 0, st>>>(A, m, L, use, bad));
+}
+
+void launch_chol_solve(const double* L, int m, const double* B, int ldb, double* X, int ldx, int ncol,
+                       const int* dncol, double* work, cudaStream_t st) {
+    if (ncol <= 0) return;
+    HSC_COUNTED(chol_solve_kernel<<<blocks((long long)ncol * 32), 256, 0, st>>>(L, m, B, ldb, X, ldx, ncol, dncol, work));
+}
+
+void launch_ldlt(double* C, int kmax, const int* dk, double* L, double* d, int* bad, cudaStream_t st) {
+    const size_t bytes = sizeof(double) * (size_t)kmax * kmax;
+    const int use = bytes <= 200 * 1024;
+    if (use) cudaFuncSetAttribute(ldlt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    HSC_COUNTED(ldlt_kernel<<<1, 1024, use ? bytes : 0, st>>>(C, kmax, dk, L, d, use, bad));
+}
+
+void launch_block12_inverse(const double* A, int qm, double* Binv, int* bad, cudaStream_t st) {
+    cudaMemsetAsync(Binv, 0, sizeof(double) * qm * qm, st);
+    HSC_COUNTED(block12_inverse_kernel<<<blocks(qm / 12, 64), 64, 0, st>>>(A, qm, Binv, bad));
+}
+
+void launch_axpby_mat(double* Y, const double* X, double a, double b, int n, int diag_m, double diag_add,
+                      cudaStream_t st) {
+    HSC_COUNTED(axpby_mat_kernel<<<blocks(n), 256, 0, st>>>(Y, X, a, b, n, diag_m, diag_add));
+}
+
+void launch_symmetrize(double* P, int m, cudaStream_t st) { HSC_COUNTED(symmetrize_kernel<<<blocks((long long)m * m), 256, 0, st>>>(P, m)); }
+
+void launch_frob(const double* X, int n, double* out, cudaStream_t st) { HSC_COUNTED(frob_kernel<<<1, 1024, 0, st>>>(X, n, out)); }
+
+void launch_split_rhs(const double* b, int qo, int qm, int fo, int n, double* bq, double* bf, cudaStream_t st) {
+    HSC_COUNTED(split_rhs_kernel<<<blocks(std::max(qm, n)), 256, 0, st>>>(b, qo, qm, fo, n, bq, bf));
+}
+
+void launch_wt_vec(const double* W, int qm, int kmax, const int* dk, const double* bq, double* c, cudaStream_t st) {
+    if (kmax) HSC_COUNTED(wt_vec_kernel<<<blocks((long long)kmax * 32), 256, 0, st>>>(W, qm, kmax, dk, bq, c));
+}
+
+void launch_rhs_lowrank(const double* V, int a, const int* dk, const double* c, const int* act, double* rhs,
+                        cudaStream_t st) {
+    if (a) HSC_COUNTED(rhs_lowrank_kernel<<<blocks(a), 256, 0, st>>>(V, a, dk, c, act, rhs));
+}
+
+void launch_vt_x(const double* V, int a, int kmax, const int* dk, const int* act, const double* x, double* t,
+                 cudaStream_t st) {
+    if (kmax) HSC_COUNTED(vt_x_kernel<<<blocks((long long)kmax * 32), 256, 0, st>>>(V, a, dk, act, x, t));
+}
+
+void launch_backsub(const double* P, const double* W, int qm, int kmax, const int* dk, const double* bq,
+                    const double* t, double* xq_out, double* xq_copy, cudaStream_t st) {
+    if (qm) HSC_COUNTED(backsub_kernel<<<blocks((long long)qm * 32), 256, 0, st>>>(P, W, qm, kmax, dk, bq, t, xq_out, xq_copy));
+}
+
+void launch_scatter_x(const double* xpad, int n, int fo, double* xout, cudaStream_t st) {
+    HSC_COUNTED(scatter_x_kernel<<<blocks(n), 256, 0, st>>>(xpad, n, fo, xout));
+}
+
+void launch_gather_x(const double* x, int n, int fo, double* xpad, cudaStream_t st) {
+    HSC_COUNTED(gather_x_kernel<<<blocks(n), 256, 0, st>>>(x, n, fo, xpad));
+}
+
+void launch_full_spmv(const FullSpmv& f, cudaStream_t st) {
+    HSC_COUNTED(bsr_spmv64_kernel<<<blocks((long long)f.n * 4), 256, 0, st>>>(f.rowptr, f.colidx, f.v64, f.nnz, f.n, f.xpad,
+                                                                  f.ypad));
+    if (f.qm && f.a) HSC_COUNTED(et_xq_kernel<<<blocks(f.a), 256, 0, st>>>(f.E, f.qm, f.a, f.act, f.xq, f.ypad));
+    if (f.qm)
+        HSC_COUNTED(abd_rows_kernel<<<blocks((long long)f.qm * 32), 256, 0, st>>>(f.A, f.E, f.qm, f.a, f.act, f.xq, f.xpad,
+                                                                      f.yq));
+}
+
+void launch_residual(const double* bf, const double* yf, const double* xf, int n, const double* bq, const double* yq,
+                     const double* xq, int qm, double* part, int np, double* out, cudaStream_t st) {
+    HSC_COUNTED(residual_partial_kernel<<<np, 256, 0, st>>>(bf, yf, xf, 4 * n, bq, yq, xq, qm, part));
+    HSC_COUNTED(residual_final_kernel<<<1, 32, 0, st>>>(part, np, out));
+}
+
+void launch_scatter_y(const double* ypad, int n, int fo, const double* yq, int qm, int qo, double* y, cudaStream_t st) {
+    HSC_COUNTED(scatter_y_kernel<<<blocks(std::max(n, qm)), 256, 0, st>>>(ypad, n, fo, yq, qm, qo, y));
+}
+
+void launch_line_step(double* x, const double* d, int N, const double* nd, cudaStream_t st) {
+    HSC_COUNTED(line_step_kernel<<<blocks(N), 256, 0, st>>>(x, d, N, nd));
+}
+
+void launch_dot2(const double* a, const double* b, const double* c, int N, double* out, cudaStream_t st) {
+    HSC_COUNTED(dot2_kernel<<<1, 1024, 0, st>>>(a, b, c, N, out));
+}
+
+void launch_sub(const double* b, const double* y, double* r, int N, cudaStream_t st) {
+    HSC_COUNTED(sub_kernel<<<blocks(N), 256, 0, st>>>(b, y, r, N));
+}
+
+void launch_split_active_diag(int precision, const int* act, int nact_nodes, const int* diag_pos, const double* v64,
+                              int nnz, void* vmt, double* dact, cudaStream_t st) {
+    if (nact_nodes <= 0) return;
+    if (precision == 0)
+        HSC_COUNTED(split_active_diag_kernel<double><<<blocks(nact_nodes), 256, 0, st>>>(act, nact_nodes, diag_pos, v64, nnz, nullptr, dact));
+    else if (precision == 1)
+        HSC_COUNTED(split_active_diag_kernel<float><<<blocks(nact_nodes), 256, 0, st>>>(act, nact_nodes, diag_pos, v64, nnz, (float*)vmt, dact));
+    else
+        HSC_COUNTED(split_active_diag_kernel<__nv_bfloat16><<<blocks(nact_nodes), 256, 0, st>>>(act, nact_nodes, diag_pos, v64, nnz,
+                                                                                  (__nv_bfloat16*)vmt, dact));
+}
+
+void convert_f64_f32(const double* src, float* dst, long long n, cudaStream_t st) {
+    if (n > 0) HSC_COUNTED(f64_to_f32_kernel<<<blocks(n), 256, 0, st>>>(src, dst, n));
+}
+
+void set_int(int* p, int v, cudaStream_t st) { HSC_COUNTED(set_int_kernel<<<1, 1, 0, st>>>(p, v)); }
+
+}  // namespace hsc

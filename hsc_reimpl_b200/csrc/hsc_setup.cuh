@@ -1,0 +1,95 @@
+// Launchers of the numeric setup, dense-algebra and vector kernels (hsc_setup.cu).
+#pragma once
+#include <algorithm>
+
+#include "hsc_internal.cuh"
+
+namespace hsc {
+
+struct AcaParams {
+    double* R0;            // holds E on entry (row-major m x nc); overwritten
+    double* R1;            // second buffer
+    int m, nc, cap;
+    double rtol;           // stop when |R|_F/|E|_F <= rtol (0: only the zero-pivot guard)
+    double* U;             // m x cap, column-major
+    double* V;             // nc x cap, column-major
+    double* hist;          // cap + 1 residuals
+    int* rank;
+    double* err;
+    double* psum;          // per-CTA partials
+    double* pmax;
+    long long* pidx;
+    GridBar* bar;
+    long long spin_limit;
+};
+
+struct GemmArgs {
+    const double* A;
+    const double* B;
+    double* C;
+    int M, N, K;
+    const int* dM;         // device overrides (rank-dependent sizes), may be null
+    const int* dN;
+    const int* dK;
+    int lda, ldb, ldc;
+    int tA, tB;
+    double alpha, beta;
+};
+
+struct FullSpmv {
+    const int* rowptr;
+    const int* colidx;
+    const double* v64;
+    int nnz, n;
+    const double* A;       // qm x qm row-major
+    const double* E;       // qm x a row-major
+    int qm, a;
+    const int* act;
+    const double* xq;      // qm
+    const double* xpad;    // node-padded FEM x
+    double* ypad;          // node-padded FEM y
+    double* yq;            // qm
+};
+
+void launch_pattern_hash(const int* rows, const int* cols, long long nnzb, unsigned long long* out, cudaStream_t st);
+void launch_fill_bsr(int precision, const int* src, const double* values, int nnz, double* v64, void* vmt,
+                     cudaStream_t st);
+void launch_dinv(int precision, const int* diag_pos, const double* v64, int nnz, int n, void* dinv, int* bad,
+                 cudaStream_t st);
+void launch_extract(const int* qq, int nqq, const int* qf, int nqf, const double* values, int qm, int a, double* A,
+                    double* E, int* node_nz, cudaStream_t st);
+cudaError_t launch_aca(const AcaParams& p, int grid, cudaStream_t st);
+int aca_blocks_per_sm();
+void launch_gemm(const GemmArgs& g, int M, int N, cudaStream_t st);
+void launch_cholesky(const double* A, int m, double* L, int* bad, cudaStream_t st);
+void launch_chol_solve(const double* L, int m, const double* B, int ldb, double* X, int ldx, int ncol,
+                       const int* dncol, double* work, cudaStream_t st);
+void launch_ldlt(double* C, int kmax, const int* dk, double* L, double* d, int* bad, cudaStream_t st);
+void launch_block12_inverse(const double* A, int qm, double* Binv, int* bad, cudaStream_t st);
+void launch_axpby_mat(double* Y, const double* X, double a, double b, int n, int diag_m, double diag_add,
+                      cudaStream_t st);
+void launch_symmetrize(double* P, int m, cudaStream_t st);
+void launch_frob(const double* X, int n, double* out, cudaStream_t st);
+void launch_split_rhs(const double* b, int qo, int qm, int fo, int n, double* bq, double* bf, cudaStream_t st);
+void launch_wt_vec(const double* W, int qm, int kmax, const int* dk, const double* bq, double* c, cudaStream_t st);
+void launch_rhs_lowrank(const double* V, int a, const int* dk, const double* c, const int* act, double* rhs,
+                        cudaStream_t st);
+void launch_vt_x(const double* V, int a, int kmax, const int* dk, const int* act, const double* x, double* t,
+                 cudaStream_t st);
+void launch_backsub(const double* P, const double* W, int qm, int kmax, const int* dk, const double* bq,
+                    const double* t, double* xq_out, double* xq_copy, cudaStream_t st);
+void launch_scatter_x(const double* xpad, int n, int fo, double* xout, cudaStream_t st);
+void launch_gather_x(const double* x, int n, int fo, double* xpad, cudaStream_t st);
+void launch_full_spmv(const FullSpmv& f, cudaStream_t st);
+void launch_residual(const double* bf, const double* yf, const double* xf, int n, const double* bq, const double* yq,
+                     const double* xq, int qm, double* part, int np, double* out, cudaStream_t st);
+void launch_scatter_y(const double* ypad, int n, int fo, const double* yq, int qm, int qo, double* y, cudaStream_t st);
+void launch_line_step(double* x, const double* d, int N, const double* nd, cudaStream_t st);
+void launch_dot2(const double* a, const double* b, const double* c, int N, double* out, cudaStream_t st);
+void launch_sub(const double* b, const double* y, double* r, int N, cudaStream_t st);
+void launch_split_active_diag(int precision, const int* act, int nact_nodes, const int* diag_pos, const double* v64,
+                              int nnz, void* vmt, double* dact, cudaStream_t st);
+void convert_f64_f32(const double* src, float* dst, long long n, cudaStream_t st);
+void set_int(int* p, int v, cudaStream_t st);
+
+}  // namespace hsc

@@ -1,0 +1,174 @@
+/*
+ * hsc_c_api.h -- C ABI of the B200 HSC linear solver.
+ *
+ * One call solves one Newton-step linear system
+ *
+ *     [ A   E ] [dq]   [bq]      A: affine bodies (12 dof each)
+ *     [ E^T D ] [dx] = [bx]      D: FEM Tet4 nodes (3 dof each)
+ *
+ * by heterogeneous subspace correction: full-pivot ACA of the coupling
+ * E ~ U V^T, an approximate ABD inverse P, Schur-complement PCG on
+ * S = D - V (U^T P U) V^T with a Neumann-series preconditioner, then
+ * back-substitution dq = P (bq - U V^T dx) and a full-system residual check.
+ *
+ * It replaces the libuipc linear-system plugin body of the reference
+ * (reproduction/hsc_backend/linear_hsc.cu):
+ *   class LinearHSC : IterativeSolver  (linear_hsc.cu:153-437)
+ *     do_build(BuildInfo&)             (linear_hsc.cu:172-193)  -> hsc_create / hsc_options
+ *     do_solve(SolvingInfo&)           (linear_hsc.cu:344-436)  -> hsc_solve
+ *   IterativeSolver::spmv(x, y)        (iterative_solver.h:28-32) -> hsc_spmv
+ * The inputs are the ones SolvingInfo exposes (global_linear_system.h:347-365):
+ * x() a device FP64 vector (written), b() a device FP64 vector (read) and
+ * A() a device CBCOOMatrixView<double,3>.
+ *
+ * All pointers named d_* are device pointers.  No function throws; every
+ * function returns an HSC_* status.  A context serves one host thread.
+ */
+#ifndef HSC_C_API_H
+#define HSC_C_API_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define HSC_EXPORT __attribute__((visibility("default")))
+#else
+#define HSC_EXPORT
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HSC_API_VERSION 1
+
+/* status codes (linear_hsc.cu raises UIPC_ASSERT / runtime_error for these) */
+#define HSC_OK 0
+#define HSC_ERR_INVALID 1     /* bad arguments or input layout (linear_hsc.cu:199-200) */
+#define HSC_ERR_NONSPD 2      /* FEM 3x3 diagonal det<=0 (:208), ABD block not SPD (:269) */
+#define HSC_ERR_BREAKDOWN 3   /* PCG pSp<=0 or rz<=0 or non-finite (:370-371) */
+#define HSC_ERR_NOCONV 4      /* PCG hit max_iter above tol (:394) */
+#define HSC_ERR_NONDESCENT 5  /* b^T x <= 0 (:400-402) */
+#define HSC_ERR_RESIDUAL 6    /* full residual above full_residual_limit (:433-435) */
+#define HSC_ERR_CUDA 7        /* CUDA runtime error (hsc::check, :34-37) */
+#define HSC_ERR_TIMEOUT 8     /* a bounded device-side wait gave up */
+#define HSC_ERR_ALLOC 9       /* device allocation failed */
+#define HSC_ERR_NOTREADY 10   /* query before any solve */
+
+/* arithmetic of the Schur PCG bulk (SpMV, Neumann terms, low-rank apply) */
+#define HSC_FP64 0            /* everything FP64 (the reference form) */
+#define HSC_FP32 1            /* FP32 values and search vectors, FP64 x/r, FP64 residual replacement */
+#define HSC_BF16 2            /* BF16 matrix values, FP32 vectors and accumulation, FP64 replacement */
+
+/* approximate ABD inverse P (linear_hsc.cu:263-297, core.py:148-150) */
+#define HSC_ABD_NEUMANN 0     /* fixed-order block-Jacobi Neumann */
+#define HSC_ABD_ADAPTIVE 1    /* Neumann extended by doubling until |I-AP|_F/sqrt(qm) <= tol */
+#define HSC_ABD_EXACT 2       /* dense FP64 Cholesky inverse */
+
+/* FEM preconditioner polynomial z = sum_k w_k (I - w Dd^-1 D)^k w Dd^-1 r */
+#define HSC_PRECOND_NEUMANN 0 /* w_k = 1, k < neumann_order (linear_hsc.cu:330-343) */
+#define HSC_PRECOND_POLY 1    /* caller-supplied w_k (e.g. from the learned model) */
+
+#define HSC_MAX_POLY 16
+
+typedef struct hsc_options {
+    int32_t max_rank;            /* linear_system/hsc/max_rank (reference default 128) */
+    double aca_rtol;             /* 0: fixed rank with a roundoff zero-pivot guard (reference) */
+    int32_t neumann_order;       /* linear_system/hsc/neumann_order (reference default 5) */
+    double omega;                /* linear_system/hsc/omega (0.7) */
+    int32_t max_iter;            /* linear_system/hsc/max_iter (2000) */
+    double tol;                  /* linear_system/tol_rate: relative Schur residual */
+    int32_t abd_inverse;         /* HSC_ABD_*; adaptive_abd_inverse=1 maps to HSC_ABD_ADAPTIVE */
+    double abd_inverse_tol;      /* linear_system/hsc/abd_inverse_tol (1e-5) */
+    double full_residual_limit;  /* linear_system/hsc/full_residual_limit (0.1) */
+    int32_t precision;           /* HSC_FP64 / HSC_FP32 / HSC_BF16 */
+    int32_t preconditioner;      /* HSC_PRECOND_* */
+    int32_t poly_degree;         /* number of weights used with HSC_PRECOND_POLY */
+    double poly_weights[HSC_MAX_POLY];
+    int32_t residual_replacement;/* iterations between FP64 true-residual replacements; 0 = only at convergence */
+    double refine_target;        /* > 0: repeat HSC directions with exact line search until
+                                    |b - H x|/|b| <= target (core.py:171-198) */
+    int32_t max_refinements;
+    int32_t fallback_on_stall;   /* with HSC_PRECOND_POLY: redo with plain Neumann when PCG breaks down or stalls */
+    int32_t threads_per_row;     /* SpMV lanes per block row: 2, 4 or 8 (autotuned) */
+    int64_t spin_limit;          /* bound on every device-side barrier wait */
+    int32_t check_residual;      /* 1: compute the full residual and enforce full_residual_limit */
+} hsc_options;
+
+typedef struct hsc_stats {        /* superset of the hsc_stats.jsonl record (linear_hsc.cu:420-431) */
+    int32_t status;
+    int32_t fem_dofs, abd_dofs, active_fem_dofs, rank;
+    int32_t pcg_iterations, neumann_doublings, refinement_steps;
+    int32_t precision, preconditioner, fallback, accepted;
+    int32_t residual_replacements;
+    double aca_relative_error;
+    double schur_relative_residual;   /* recursive residual at exit (true residual after a check) */
+    double full_relative_residual;    /* |b - H x| / |b| in FP64 on the assembled H */
+    double abd_inverse_residual;      /* |I - A P|_F / sqrt(qm) */
+    double full_residual_limit;
+    double descent;                   /* b^T x */
+    double setup_ms, pcg_ms, total_ms;/* device time between stream events */
+    double lanczos_min, lanczos_max;  /* extreme Ritz values of the preconditioned Schur operator */
+    double stage_ms[8];               /* fill+extract, ACA, ABD inverse, reduced core, rhs, PCG, back-sub+residual, unused */
+    int64_t nnzb;
+} hsc_stats;
+
+typedef struct hsc_bcoo3 {        /* CBCOOMatrixView<double,3> */
+    const int32_t* d_rows;        /* block row index per triplet */
+    const int32_t* d_cols;        /* block column index per triplet */
+    const double* d_values;       /* 9 doubles per triplet, column-major 3x3 (Eigen Matrix3x3) */
+    int64_t nnzb;                 /* triplet count; ONE triangle stored, (row, col) unique */
+    int32_t nblock;               /* block rows = dofs / 3 */
+} hsc_bcoo3;
+
+typedef struct hsc_dof_layout {   /* ABDLinearSubsystem / FEMLinearSubsystem dof_offset, dof_count */
+    int32_t qo, qm, fo, fn;
+} hsc_dof_layout;
+
+typedef struct hsc_ctx hsc_ctx;
+
+/* Fill *opt with the framework defaults (FP64, exact ABD inverse, order 2). */
+HSC_EXPORT int hsc_options_default(hsc_options* opt);
+/* The reference plugin's defaults (linear_hsc.cu:162-164): order 5, adaptive ABD, tol 1e-4. */
+HSC_EXPORT int hsc_options_reference(hsc_options* opt);
+
+/* do_build: create a context on the current CUDA device. */
+HSC_EXPORT int hsc_create(const hsc_options* opt, hsc_ctx** out);
+HSC_EXPORT void hsc_destroy(hsc_ctx* ctx);
+HSC_EXPORT int hsc_set_options(hsc_ctx* ctx, const hsc_options* opt);
+/* Message of the last failing call on this context ("" when none). */
+HSC_EXPORT const char* hsc_last_error(const hsc_ctx* ctx);
+
+/* do_solve: x = HSC(A, b).  The sparsity analysis is cached while the A
+ * pointers, nnzb, nblock and layout stay the same; a changed pattern behind
+ * the same pointers is detected on the device and triggers a fresh analysis.
+ * `stream` is a cudaStream_t (NULL = legacy default stream). */
+HSC_EXPORT int hsc_solve(hsc_ctx* ctx, const hsc_bcoo3* A, const hsc_dof_layout* layout,
+              const double* d_b, double* d_x, void* stream, hsc_stats* out);
+
+/* Many independent systems in one persistent PCG launch.  With
+ * use_graph != 0 the numeric phase is captured once into a CUDA graph and
+ * replayed while the pointers and patterns are unchanged. */
+HSC_EXPORT int hsc_solve_batch(hsc_ctx* ctx, int32_t count, const hsc_bcoo3* A, const hsc_dof_layout* layouts,
+                    const double* const* d_b, double* const* d_x, int32_t use_graph,
+                    void* stream, hsc_stats* out);
+
+/* IterativeSolver::spmv: y = H x with the full symmetric H (both triangles). */
+HSC_EXPORT int hsc_spmv(hsc_ctx* ctx, const hsc_bcoo3* A, const hsc_dof_layout* layout,
+             const double* d_x, double* d_y, void* stream);
+
+/* Host copies of the last solve's coupling factors (tests / diagnostics).
+ * U: qm x rank, V: active x rank, both column-major; active: FEM dof indices. */
+HSC_EXPORT int hsc_get_factors(hsc_ctx* ctx, int32_t sys, int32_t* rank, int32_t* n_active,
+                    double* U, int32_t ldu, double* V, int32_t ldv, int32_t* active);
+
+/* Host copy of the last solve's ABD inverse P (qm x qm, row-major). */
+HSC_EXPORT int hsc_get_abd_inverse(hsc_ctx* ctx, int32_t sys, double* P);
+
+HSC_EXPORT int hsc_version(void);
+/* Kernels this library has launched in the process so far (all contexts). */
+HSC_EXPORT long long hsc_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HSC_C_API_H */
