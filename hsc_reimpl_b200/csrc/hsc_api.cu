@@ -26,9 +26,23 @@ using namespace hsc;
 
 namespace {
 
+// Owning device buffer (grow-only).  Move-only: a copy would free the same
+// allocation twice when a container of systems reallocates.
 struct DevBuf {
     void* p = nullptr;
     size_t cap = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), cap(o.cap) { o.p = nullptr; o.cap = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) {
+            if (p) cudaFree(p);
+            p = o.p; cap = o.cap;
+            o.p = nullptr; o.cap = 0;
+        }
+        return *this;
+    }
     ~DevBuf() { if (p) cudaFree(p); }
     cudaError_t grow(size_t bytes) {
         if (bytes <= cap) return cudaSuccess;
@@ -73,12 +87,13 @@ struct System {
     // plan
     DevBuf rowptr, colidx, src, diag_pos, qq, qf, act, ident, rowflag;
     // numeric
-    DevBuf v64, vmt, dinv, A, E, R0, R1, U, V, hist, P, Ptmp, T, term, Binv, L, W, C, Lc, dpiv, vt64, vtmt,
+    DevBuf v64, vf32, vbf16, dinv, A, E, R0, R1, U, V, hist, P, Ptmp, T, term, Binv, L, W, C, Lc, dpiv, vt64, vtmt,
         cvec, tt, ttx, bq, bf, x, r, z, p0, p1, y, t0, t1, node_nz, xq, ypad, yq, work, cg, scal, dact, pact, yact,
         zpart;
     DevBuf dvec[4];           // contiguous-N scratch for refinement
     DevScal h_scal{};
     std::vector<int> h_node_nz;
+    bool aca_on_cluster = false;
 };
 
 }  // namespace
@@ -92,10 +107,16 @@ struct hsc_ctx {
     // PCG launch state
     DevBuf d_desc, d_cta_sys, d_cta_row, d_cta_act, d_part, d_bar, d_remaining;
     int grid = 0;
+    int vt_smem = 0;           // doubles of PCG shared memory after the d.*tt slot
+    size_t pcg_smem = 0;       // dynamic shared memory bytes of the PCG launch
     int part_key_gen = -1;
     // ACA
     DevBuf aca_psum, aca_pmax, aca_pidx, aca_bar;
     int aca_grid = 0;
+    DevBuf d_aca_sys;          // AcaSys descriptors of the systems on the cluster ACA
+    int aca_cluster_n = 0;
+    size_t aca_cluster_smem = 0;
+    int aca_cluster_ok = -1;   // the device can schedule a 16-CTA cluster of the ACA kernel
     DevBuf res_part;
     cudaEvent_t ev[9] = {};
     bool stage_events = false;  // record the per-stage events (single system, no graph)
@@ -280,7 +301,8 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
     const size_t nz = std::max(1, S.nnz), n4 = 4 * (size_t)std::max(1, S.n), qm = std::max(1, S.qm);
     const size_t km = std::max(1, S.kmax), aa = std::max(1, S.a);
     GROW(S.v64, 9 * sizeof(double) * nz);
-    if (P != 0) GROW(S.vmt, 9 * mt_bytes(P) * nz);
+    if (P != 0) GROW(S.vf32, 9 * sizeof(float) * nz);
+    if (P == 2) GROW(S.vbf16, 9 * sizeof(__nv_bfloat16) * nz);
     GROW(S.dinv, 9 * (P == 0 ? 8 : 4) * (size_t)std::max(1, S.n));
     GROW(S.A, sizeof(double) * qm * qm);
     GROW(S.E, sizeof(double) * qm * aa);
@@ -366,8 +388,10 @@ int abd_inverse(hsc_ctx* ctx, System& S, cudaStream_t st, bool allow_sync) {
     double* P = S.P.as<double>();
     if (m == 0) return HSC_OK;
     if (o.abd_inverse == HSC_ABD_EXACT) {
-        launch_cholesky(S.A.as<double>(), m, S.L.as<double>(), &ds->bad_abd, st);
-        launch_chol_solve(S.L.as<double>(), m, S.ident.as<double>(), m, P, m, m, nullptr, S.work.as<double>(), st);
+        if (!launch_chol_inverse(S.A.as<double>(), m, P, &ds->bad_abd, st)) {
+            launch_cholesky(S.A.as<double>(), m, S.L.as<double>(), &ds->bad_abd, st);
+            launch_chol_solve(S.L.as<double>(), m, S.ident.as<double>(), m, P, m, m, nullptr, S.work.as<double>(), st);
+        }
         launch_symmetrize(P, m, st);
         // |I - A P|_F^2 for the stats
         CK(cudaMemcpyAsync(S.T.p, S.ident.p, sizeof(double) * m * m, cudaMemcpyDeviceToDevice, st));
@@ -428,21 +452,35 @@ void stage_mark(hsc_ctx* ctx, int i, cudaStream_t st) {
     if (ctx->stage_events) cudaEventRecord(ctx->ev[i], st);
 }
 
-int numeric_setup(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, cudaStream_t st, bool allow_sync) {
-    const hsc_options& o = ctx->opt;
-    const int P = o.precision;
+// numeric setup, part 1: BSR fill, Dd^-1, coupled diagonal blocks, A and E
+int numeric_pre(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, cudaStream_t st) {
+    const int P = ctx->opt.precision;
     DevScal* ds = S.scal.as<DevScal>();
     S.h_scal.pcg[7] = 0;
     CK(cudaMemsetAsync(ds, 0, sizeof(DevScal), st));
     launch_pattern_hash(M.d_rows, M.d_cols, M.nnzb, &ds->hash, st);
-    launch_fill_bsr(P, S.src.as<int>(), M.d_values, S.nnz, S.v64.as<double>(), P ? S.vmt.p : nullptr, st);
+    float* vf = P ? S.vf32.as<float>() : nullptr;
+    __nv_bfloat16* vb = P == 2 ? S.vbf16.as<__nv_bfloat16>() : nullptr;
+    launch_fill_bsr(S.src.as<int>(), M.d_values, S.nnz, S.v64.as<double>(), vf, vb, st);
     launch_dinv(P, S.diag_pos.as<int>(), S.v64.as<double>(), S.nnz, S.n, S.dinv.p, &ds->bad_fem, st);
-    launch_split_active_diag(P, S.act.as<int>(), S.a / 3, S.diag_pos.as<int>(), S.v64.as<double>(), S.nnz,
-                             P ? S.vmt.p : nullptr, S.dact.as<double>(), st);
+    launch_split_active_diag(S.act.as<int>(), S.a / 3, S.diag_pos.as<int>(), S.v64.as<double>(), S.nnz, vf, vb,
+                             S.dact.as<double>(), st);
     launch_extract(S.qq.as<int>(), S.nqq, S.qf.as<int>(), S.nqf, M.d_values, S.qm, S.a, S.A.as<double>(),
                    S.E.as<double>(), S.node_nz.as<int>(), st);
-    // ACA of E (qm x a)
-    if (S.kmax > 0) {
+    if (S.kmax <= 0) CK(cudaMemsetAsync(&ds->rank, 0, sizeof(int), st));
+    return HSC_OK;
+}
+
+// ACA of every system's coupling: one cluster launch for the systems whose E
+// fits a 16-CTA cluster, the cooperative grid kernel for the others
+int aca_all(hsc_ctx* ctx, int count, cudaStream_t st) {
+    const hsc_options& o = ctx->opt;
+    if (ctx->aca_cluster_n > 0) CK(launch_aca_cluster(ctx->d_aca_sys.as<AcaSys>(), ctx->aca_cluster_n,
+                                                      ctx->aca_cluster_smem, st));
+    for (int s = 0; s < count; ++s) {
+        System& S = ctx->sys[s];
+        if (S.kmax <= 0 || S.aca_on_cluster) continue;
+        DevScal* ds = S.scal.as<DevScal>();
         CK(cudaMemcpyAsync(S.R0.p, S.E.p, sizeof(double) * S.qm * S.a, cudaMemcpyDeviceToDevice, st));
         AcaParams ap{};
         ap.R0 = S.R0.as<double>(); ap.R1 = S.R1.as<double>();
@@ -456,7 +494,12 @@ int numeric_setup(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, cudaStream_t st, 
         const int grid = (int)std::max<long long>(1, std::min<long long>(ctx->aca_grid, (total + 2047) / 2048));
         CK(launch_aca(ap, grid, st));
     }
-    stage_mark(ctx, 2, st);
+    return HSC_OK;
+}
+
+// numeric setup, part 2: ABD inverse P, W = P U, C = U^T W = L D L^T, Vt = V L
+int numeric_post(hsc_ctx* ctx, System& S, cudaStream_t st, bool allow_sync) {
+    DevScal* ds = S.scal.as<DevScal>();
     int rc = abd_inverse(ctx, S, st, allow_sync);
     if (rc) return rc;
     stage_mark(ctx, 3, st);
@@ -473,8 +516,6 @@ int numeric_setup(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, cudaStream_t st, 
         CK(cudaMemsetAsync(S.vt64.p, 0, sizeof(double) * S.a * S.kmax, st));
         gemm(S.Lc.as<double>(), S.kmax, 1, S.V.as<double>(), S.a, 0, S.vt64.as<double>(), S.a, S.kmax, S.a, S.kmax,
              1.0, 0.0, st, dk, nullptr, dk);
-    } else {
-        CK(cudaMemsetAsync(&ds->rank, 0, sizeof(int), st));
     }
     stage_mark(ctx, 4, st);
     return HSC_OK;
@@ -533,7 +574,8 @@ void full_spmv_contig(System& S, const double* x, double* y, cudaStream_t st) {
 // CTA partition of the persistent launch over the systems in `idx`
 int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) {
     const hsc_options& o = ctx->opt;
-    const int bps = std::max(1, pcg_blocks_per_sm(o.precision, o.threads_per_row));
+    const size_t smem_cap = 200 * 1024;  // dynamic shared memory budget of one PCG CTA
+    const int bps = std::max(1, pcg_blocks_per_sm(o.precision, o.threads_per_row, smem_cap));
     int G = bps * ctx->num_sms;
     const int ns = (int)idx.size();
     if (ns > G) return fail(ctx, HSC_ERR_INVALID, "more systems than co-resident CTAs");
@@ -582,7 +624,9 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
         SysDesc& d = desc[s];
         d.n = S.n; d.nnz = S.nnz; d.a = S.a; d.kmax = S.kmax; d.cta_begin = b; d.cta_end = c;
         d.rowptr = S.rowptr.as<int>(); d.colidx = S.colidx.as<int>();
-        d.vals = o.precision ? S.vmt.p : S.v64.p; d.vals64 = S.v64.as<double>(); d.dinv = S.dinv.p;
+        d.vals = o.precision ? S.vf32.p : S.v64.p;
+        d.vals_pc = o.precision == 2 ? S.vbf16.p : d.vals;
+        d.vals64 = S.v64.as<double>(); d.dinv = S.dinv.p;
         d.act = S.act.as<int>(); d.rowflag = S.rowflag.as<int>(); d.dact = S.dact.as<double>();
         d.vt64 = S.vt64.as<double>(); d.dpiv = S.dpiv.as<double>(); d.rank = &S.scal.as<DevScal>()->rank;
         d.pact = S.pact.as<double>(); d.yact = S.yact.as<double>(); d.ttx = S.ttx.as<double>();
@@ -592,6 +636,20 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
         d.p[0] = S.p0.p; d.p[1] = S.p1.p; d.y = S.y.p; d.t[0] = S.t0.p; d.t[1] = S.t1.p; d.tt = S.tt.as<double>();
         d.out = S.scal.as<DevScal>()->pcg; d.cg_coef = S.cg.as<double>(); d.max_coef = 64;
     }
+    // shared memory: every CTA stages its coupled-dof z values; the Vt block too
+    // when all blocks fit the budget
+    int need_z = 0, need_vt = 0;
+    for (int k = 0; k < G; ++k) {
+        const System& S = ctx->sys[idx[cta_sys[k]]];
+        const int na = cta_act[2 * k + 1] - cta_act[2 * k];
+        const int pz = (na + 1) & ~1;
+        need_z = std::max(need_z, pz);
+        need_vt = std::max(need_vt, pz + na * std::max(0, S.kmax));
+    }
+    const int budget = (int)(smem_cap / sizeof(double)) - kMaxRank;
+    ctx->vt_smem = need_vt <= budget ? need_vt : need_z;
+    ctx->pcg_smem = pcg_smem_bytes(ctx->vt_smem, 0);
+    if (need_z > budget) return fail(ctx, HSC_ERR_INVALID, "too many coupled dofs in one CTA row range");
     GROW(ctx->d_desc, sizeof(SysDesc) * ns);
     GROW(ctx->d_cta_sys, sizeof(int) * G);
     GROW(ctx->d_cta_row, sizeof(int) * 2 * G);
@@ -603,6 +661,28 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
     CK(cudaMemcpyAsync(ctx->d_cta_sys.p, cta_sys.data(), sizeof(int) * G, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->d_cta_row.p, cta_row.data(), sizeof(int) * 2 * G, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->d_cta_act.p, cta_act.data(), sizeof(int) * 2 * G, cudaMemcpyHostToDevice, st));
+    // cluster-ACA descriptors (pointers only: valid for every numeric pass of this analysis)
+    std::vector<AcaSys> aca;
+    size_t aca_smem = 0;
+    for (int s2 = 0; s2 < ns; ++s2) {
+        System& S = ctx->sys[idx[s2]];
+        S.aca_on_cluster = false;
+        if (S.kmax <= 0 || !aca_cluster_fits(S.qm, S.a)) continue;
+        const size_t need = aca_cluster_smem_doubles(S.qm, S.a);
+        if (ctx->aca_cluster_ok < 0) ctx->aca_cluster_ok = aca_cluster_supported(25600) > 0 ? 1 : 0;
+        if (!ctx->aca_cluster_ok) continue;
+        DevScal* ds = S.scal.as<DevScal>();
+        aca.push_back(AcaSys{S.E.as<double>(), S.qm, S.a, S.kmax, o.aca_rtol > 0 ? o.aca_rtol : 0.0,
+                             S.U.as<double>(), S.V.as<double>(), S.hist.as<double>(), &ds->rank, &ds->aca_err});
+        aca_smem = std::max(aca_smem, need);
+        S.aca_on_cluster = true;
+    }
+    ctx->aca_cluster_n = (int)aca.size();
+    ctx->aca_cluster_smem = aca_smem;
+    if (!aca.empty()) {
+        GROW(ctx->d_aca_sys, sizeof(AcaSys) * aca.size());
+        CK(cudaMemcpyAsync(ctx->d_aca_sys.p, aca.data(), sizeof(AcaSys) * aca.size(), cudaMemcpyHostToDevice, st));
+    }
     CK(cudaStreamSynchronize(st));  // host vectors die here
     ctx->grid = G;
     return HSC_OK;
@@ -616,7 +696,10 @@ int launch_pcg_all(hsc_ctx* ctx, int nsys, cudaStream_t st) {
     prm.cta_sys = ctx->d_cta_sys.as<int>();
     prm.cta_row = ctx->d_cta_row.as<int>();
     prm.cta_act = ctx->d_cta_act.as<int>();
-    prm.part = ctx->d_part.as<double>();
+    prm.part_rr = ctx->d_part.as<double>();
+    prm.part_rz = ctx->d_part.as<double>() + ctx->grid;
+    prm.part_pap = ctx->d_part.as<double>() + 2 * ctx->grid;
+    prm.vt_smem = ctx->vt_smem;
     prm.bar = ctx->d_bar.as<GridBar>();
     prm.remaining = ctx->d_remaining.as<int>();
     prm.omega = o.omega;
@@ -633,7 +716,7 @@ int launch_pcg_all(hsc_ctx* ctx, int nsys, cudaStream_t st) {
     prm.spin_limit = o.spin_limit;
     CK(cudaMemsetAsync(ctx->d_bar.p, 0, sizeof(GridBar), st));
     set_int(ctx->d_remaining.as<int>(), nsys, st);
-    CK(launch_pcg(o.precision, o.threads_per_row, prm, ctx->grid, st));
+    CK(launch_pcg(o.precision, o.threads_per_row, prm, ctx->grid, ctx->pcg_smem, st));
     return HSC_OK;
 }
 
@@ -878,10 +961,9 @@ int hsc_set_options(hsc_ctx* ctx, const hsc_options* opt) {
     const bool relayout = opt->precision != ctx->opt.precision || opt->max_rank != ctx->opt.max_rank ||
                           opt->threads_per_row != ctx->opt.threads_per_row;
     ctx->opt = *opt;
-    if (relayout) {
+    if (relayout)
         for (auto& S : ctx->sys) S.analyzed = false;
-        ctx->part_key_gen = -1;
-    }
+    ctx->part_key_gen = -1;  // descriptors carry option values (ACA rtol, ...)
     if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
     return HSC_OK;
 }
@@ -896,6 +978,7 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
     int rc = ensure_common(ctx, st);
     if (rc) return rc;
     bool any_new = false;
+    if ((int)ctx->sys.size() < count) ctx->sys.resize(count);  // moves only; before any analysis of this call
     std::vector<int> idx(count);
     for (int s = 0; s < count; ++s) {
         bool re = false;
@@ -925,7 +1008,15 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
     CK(cudaEventRecord(ctx->ev[0], st));
     auto enqueue = [&](bool allow_sync) -> int {
         for (int s = 0; s < count; ++s) {
-            int r2 = numeric_setup(ctx, ctx->sys[s], A[s], st, allow_sync);
+            int r2 = numeric_pre(ctx, ctx->sys[s], A[s], st);
+            if (r2) return r2;
+        }
+        stage_mark(ctx, 1, st);
+        int r1 = aca_all(ctx, count, st);
+        if (r1) return r1;
+        stage_mark(ctx, 2, st);
+        for (int s = 0; s < count; ++s) {
+            int r2 = numeric_post(ctx, ctx->sys[s], st, allow_sync);
             if (r2) return r2;
             schur_rhs(ctx->sys[s], d_b[s], st);
         }
@@ -1111,7 +1202,7 @@ int hsc_spmv(hsc_ctx* ctx, const hsc_bcoo3* A, const hsc_dof_layout* layout, con
     if (rc) return rc;
     System& S = ctx->sys[0];
     DevScal* ds = S.scal.as<DevScal>();
-    launch_fill_bsr(0, S.src.as<int>(), A->d_values, S.nnz, S.v64.as<double>(), nullptr, st);
+    launch_fill_bsr(S.src.as<int>(), A->d_values, S.nnz, S.v64.as<double>(), nullptr, nullptr, st);
     launch_extract(S.qq.as<int>(), S.nqq, S.qf.as<int>(), S.nqf, A->d_values, S.qm, S.a, S.A.as<double>(),
                    S.E.as<double>(), S.node_nz.as<int>(), st);
     (void)ds;

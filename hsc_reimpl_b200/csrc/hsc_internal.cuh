@@ -20,8 +20,9 @@
 
 namespace hsc {
 
-constexpr int kThreads = 256;            // persistent-kernel CTA size
+constexpr int kThreads = 512;            // persistent-kernel CTA size (one CTA per SM)
 constexpr int kWarps = kThreads / 32;
+constexpr int kMaxRank = 256;
 
 struct GridBar {
     unsigned int count;
@@ -44,34 +45,54 @@ __device__ __forceinline__ void st_release_u32(unsigned int* p, unsigned int v) 
 __device__ __forceinline__ int ld_volatile_i32(const int* p) {
     return *reinterpret_cast<const volatile int*>(p);
 }
+__device__ __forceinline__ void red_release_add_u32(unsigned int* p, unsigned int v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
-// Grid-wide barrier for a cooperative launch.  Every wait is bounded by
-// `limit` polls; a wait that gives up raises gb->abort, after which every
-// CTA leaves at its next barrier.  Returns false when the grid must exit.
-__device__ __forceinline__ bool grid_sync(GridBar* gb, unsigned int nblocks, long long limit, int where) {
+// Thread-0 half of a grid barrier: release-arrive on the monotonic counter,
+// then acquire-poll until barrier `epoch` is complete.  Bounded: returns
+// false (and raises gb->abort) when the wait gives up or another CTA aborted.
+__device__ __forceinline__ bool grid_arrive_wait(GridBar* gb, unsigned int nblocks, long long limit, int epoch) {
+    const unsigned int target = (unsigned int)(epoch + 1) * nblocks;
+    red_release_add_u32(&gb->count, 1u);
+    long long n = 0;
+    while (ld_acquire_u32(&gb->count) < target) {
+        ++n;
+        if (n > 256) __nanosleep(20);
+        if ((n & 255) == 0 && ld_volatile_i32(&gb->abort)) return false;
+        if (n > limit) {
+            atomicExch(&gb->abort, 1);
+            atomicExch(&gb->where, epoch);
+            return false;
+        }
+    }
+    return ld_volatile_i32(&gb->abort) == 0;
+}
+
+// Grid-wide barrier for a cooperative launch.  The arrival counter only
+// grows: barrier number `epoch` (0, 1, 2, ... per launch) completes when it
+// reaches (epoch + 1) * nblocks, so no reset round trip is needed.  Every wait
+// is bounded by `limit` polls; a wait that gives up raises gb->abort, after
+// which every CTA leaves at its next barrier.  Returns false when the grid
+// must exit.
+__device__ __forceinline__ bool grid_sync(GridBar* gb, unsigned int nblocks, long long limit, int epoch) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        unsigned int g = ld_acquire_u32(&gb->gen);
+        const unsigned int target = (unsigned int)(epoch + 1) * nblocks;
         __threadfence();
-        unsigned int prev = atomicAdd(&gb->count, 1u);
-        if (prev == nblocks - 1) {
-            atomicExch(&gb->count, 0u);
-            __threadfence();
-            st_release_u32(&gb->gen, g + 1);
-        } else {
-            long long n = 0;
-            while (ld_acquire_u32(&gb->gen) == g) {
-                ++n;
-                if (n > 32) __nanosleep(40);
-                if ((n & 127) == 0 && ld_volatile_i32(&gb->abort)) { ok = 0; break; }
-                if (n > limit) {
-                    atomicExch(&gb->abort, 1);
-                    atomicExch(&gb->where, where);
-                    ok = 0;
-                    break;
-                }
+        atomicAdd(&gb->count, 1u);
+        long long n = 0;
+        while (ld_acquire_u32(&gb->count) < target) {
+            ++n;
+            if (n > 64) __nanosleep(32);
+            if ((n & 127) == 0 && ld_volatile_i32(&gb->abort)) { ok = 0; break; }
+            if (n > limit) {
+                atomicExch(&gb->abort, 1);
+                atomicExch(&gb->where, epoch);
+                ok = 0;
+                break;
             }
         }
         if (ld_volatile_i32(&gb->abort)) ok = 0;
@@ -136,7 +157,8 @@ struct SysDesc {
     const int* rowflag;    // per node: active-node index, or -1
     const int* rowptr;
     const int* colidx;
-    const void* vals;      // MT planes (mixed modes: active diagonal blocks zeroed)
+    const void* vals;      // operator planes (mixed modes: active diagonal blocks zeroed)
+    const void* vals_pc;   // preconditioner planes (BF16 mode: bf16 copy; else == vals)
     const double* vals64;  // FP64 planes (true-residual replacement)
     const double* dact;    // FP64 active diagonal blocks (mixed modes), row-major 9 per active node
     const void* dinv;      // Dd^-1 planes over nodes (omega NOT folded in)
@@ -167,7 +189,9 @@ struct PcgParams {
     const int* cta_sys;        // per CTA: its system
     const int* cta_row;        // per CTA: [row_begin, row_end) pairs
     const int* cta_act;        // per CTA: [act_begin, act_end) pairs in the system's act list
-    double* part;              // 3 * gridDim partials
+    double* part_rr;           // per CTA: r.r after the update phase
+    double* part_rz;           // per CTA: r.z after the last preconditioner phase
+    double* part_pap;          // per CTA: p.S p of phase A
     GridBar* bar;
     int* remaining;            // systems still iterating
     double omega;
@@ -177,6 +201,7 @@ struct PcgParams {
     int max_iter;
     int rr_every;              // residual replacement interval (0 = only at convergence)
     long long spin_limit;
+    int vt_smem;               // doubles of shared memory for the CTA's Vt block (0: read it from global)
 };
 
 // launch counter of this library (hsc_setup.cu)
@@ -184,7 +209,9 @@ void count_launch();
 long long launch_count();
 
 // kernel launchers (hsc_pcg.cu)
-cudaError_t launch_pcg(int precision, int tpr, const PcgParams& prm, int grid, cudaStream_t st);
-int pcg_blocks_per_sm(int precision, int tpr);
+cudaError_t launch_pcg(int precision, int tpr, const PcgParams& prm, int grid, size_t smem, cudaStream_t st);
+int pcg_blocks_per_sm(int precision, int tpr, size_t smem);
+// dynamic shared memory of the PCG kernel for a Vt block of `vt_doubles`
+size_t pcg_smem_bytes(int vt_doubles, int kmax_all);
 
 }  // namespace hsc

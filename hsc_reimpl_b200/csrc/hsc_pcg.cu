@@ -1,25 +1,35 @@
 // Persistent Schur-complement PCG for one or many HSC systems.
 //
-// One cooperative launch runs the whole PCG loop of linear_hsc.cu:359-393
-// (reference loop; core.py:95-138 is the oracle's form) for every system of a
-// batch.  Each CTA owns a contiguous range of FEM block rows of one system;
-// grid-wide barriers (bounded waits) separate the phases of an iteration:
+// One cooperative launch (one 512-thread CTA per SM) runs the whole PCG loop
+// of linear_hsc.cu:359-393 (core.py:95-138 is the oracle's form) for every
+// system of a batch.  Each CTA owns a contiguous range of FEM block rows of
+// one system; grid-wide barriers with bounded waits separate the phases:
 //
-//   A  p = z + beta p_old (formed on the fly in the gathers),  y = D p,
-//      tt_j = (Vt^T p)_j by designated warps, partial p.Dp - sum d_j tt_j^2
+//   A  p = z + beta p_prev (formed on the fly in the gathers),  y = D p,
+//      tt_j = (Vt^T z)_j + beta tt_j by designated warps (the Vt^T z
+//      partials were produced per CTA at the end of the previous phase),
+//      partial p.Dp - sum_j d_j tt_j^2
 //   -- barrier --
 //   B  alpha = rz / pSp;  y[act] -= Vt (d .* tt);  x += alpha p;
 //      r -= alpha y;  t = w Dd^-1 r;  z = w_0 t;  partial r.r
 //   -- barrier --
-//   C_k (k = 1 .. terms-1): t' = t - w Dd^-1 (D t);  z += w_k t';  partial r.z
+//   C_k (k = 1 .. terms-1): t' = t - w Dd^-1 (D t);  z += w_k t';
+//      partial r.z and the CTA's Vt^T z partials after the last term
 //   -- barrier each --
 //
-// so one iteration costs terms+1 barriers and `terms` passes over D, and all
-// scalars are reduced redundantly (same order, same bits) by every CTA of a
-// system: no atomics in any sum, results are bit-reproducible.  The true
+// so one iteration costs terms+1 barriers and `terms` passes over D.  All
+// scalars are reduced redundantly, in the same order, by every CTA of a
+// system: no floating-point atomics, bit-reproducible results.  The true
 // residual check at convergence (linear_hsc.cu:375-387) and the FP64 residual
 // replacement of the mixed-precision modes run as a replacement slot
 // (A' r = rhs - D x in FP64, B' r += Vt d Vt^T x) with the same barrier count.
+//
+// On a vehicle-size system the ~20 MB matrix stays in L2 and one iteration is
+// bound by latency, so the kernel shortens dependent chains: the CTA partial
+// is folded into the barrier arrival (release add, acquire poll), the r.r and
+// r.z partials are fetched in one pass, the SpMV issues the column indices and
+// gathers of several blocks before using them, and each CTA keeps its block of
+// Vt (the rows of its own coupled dofs) in shared memory for the whole solve.
 #include <type_traits>
 
 #include "hsc_internal.cuh"
@@ -32,6 +42,8 @@ template <class MT> struct Cmp { using T = float; };
 template <> struct Cmp<double> { using T = double; };
 template <class MT> struct DinvT { using T = float; };
 template <> struct DinvT<double> { using T = double; };
+template <class MT> struct Unroll { static constexpr int U = 4; };
+template <> struct Unroll<double> { static constexpr int U = 2; };
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -39,44 +51,38 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// deterministic CTA sum; result valid in every thread
-__device__ __forceinline__ double block_sum(double v, double* s_red, double* s_out) {
-    v = warp_sum(v);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    __syncthreads();
-    if (lane == 0) s_red[warp] = v;
-    __syncthreads();
-    if (warp == 0) {
-        double t = lane < kWarps ? s_red[lane] : 0.0;
-        t = warp_sum(t);
-        if (lane == 0) *s_out = t;
-    }
-    __syncthreads();
-    return *s_out;
-}
-
-// deterministic sum of part[b..e) (same order in every CTA); valid in every thread
-__device__ __forceinline__ double sum_parts(const double* part, int b, int e, double* s_out) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    __syncthreads();
-    if (warp == 0) {
-        double t = 0.0;
-        for (int i = b + lane; i < e; i += 32) t += part[i];
-        t = warp_sum(t);
-        if (lane == 0) *s_out = t;
-    }
-    __syncthreads();
-    return *s_out;
-}
-
 template <class VT>
 __device__ __forceinline__ VT& elem(void* v, int dof) {
     return reinterpret_cast<VT*>(v)[4 * (dof / 3) + dof % 3];
 }
 
-// y_row = sum_k B_k x[col_k] over own rows; TPR lanes per row, then the
-// group leader runs the epilogue.
-template <class MT, class CT, int TPR, class Gather, class Epi>
+// warp-level sums of a[b..e) and (optionally) c[b..e), loads issued before the
+// adds, fixed order: the same bits in every CTA.  Valid in lane 0.
+__device__ __forceinline__ void warp_sum_parts(const double* pa, const double* pc, int b, int e, double& sa,
+                                               double& sc) {
+    const int lane = threadIdx.x & 31;
+    double va[8], vc[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int i = b + lane + 32 * q;
+        va[q] = i < e ? pa[i] : 0.0;
+        vc[q] = (pc && i < e) ? pc[i] : 0.0;
+    }
+    sa = 0.0;
+    sc = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) { sa += va[q]; sc += vc[q]; }
+    for (int i = b + lane + 256; i < e; i += 32) {
+        sa += pa[i];
+        if (pc) sc += pc[i];
+    }
+    sa = warp_sum(sa);
+    sc = warp_sum(sc);
+}
+
+// y_row = sum_k B_k x[col_k] over own rows; TPR lanes per row, U blocks per
+// lane in flight, then the group leader runs the epilogue.
+template <class MT, class CT, int TPR, int U, class Gather, class Epi>
 __device__ __forceinline__ void spmv_own(const int* __restrict__ rowptr, const int* __restrict__ colidx,
                                          const MT* __restrict__ vals, int nnz, int rb, int re,
                                          const Gather& gather, Epi& epi) {
@@ -87,20 +93,35 @@ __device__ __forceinline__ void spmv_own(const int* __restrict__ rowptr, const i
         CT a0 = 0, a1 = 0, a2 = 0;
         if (row < re) {
             const int k0 = __ldg(rowptr + row), k1 = __ldg(rowptr + row + 1);
-            for (int k = k0 + sub; k < k1; k += TPR) {
-                const int c = __ldg(colidx + k);
-                CT x0, x1, x2;
-                gather(c, x0, x1, x2);
-                const MT* v = vals + k;
-                const CT b0 = Num<MT>::get(__ldg(v)), b1 = Num<MT>::get(__ldg(v + nnz)),
-                         b2 = Num<MT>::get(__ldg(v + 2 * (size_t)nnz));
-                const CT b3 = Num<MT>::get(__ldg(v + 3 * (size_t)nnz)), b4 = Num<MT>::get(__ldg(v + 4 * (size_t)nnz)),
-                         b5 = Num<MT>::get(__ldg(v + 5 * (size_t)nnz));
-                const CT b6 = Num<MT>::get(__ldg(v + 6 * (size_t)nnz)), b7 = Num<MT>::get(__ldg(v + 7 * (size_t)nnz)),
-                         b8 = Num<MT>::get(__ldg(v + 8 * (size_t)nnz));
-                a0 += b0 * x0 + b1 * x1 + b2 * x2;
-                a1 += b3 * x0 + b4 * x1 + b5 * x2;
-                a2 += b6 * x0 + b7 * x1 + b8 * x2;
+            for (int kb = k0 + sub; kb < k1; kb += TPR * U) {
+                int c[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int k = kb + u * TPR;
+                    c[u] = k < k1 ? __ldg(colidx + k) : -1;
+                }
+                CT xv[U][3];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    if (c[u] >= 0) gather(c[u], xv[u][0], xv[u][1], xv[u][2]);
+                    else xv[u][0] = xv[u][1] = xv[u][2] = 0;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int k = kb + u * TPR;
+                    if (k < k1) {
+                        const MT* v = vals + k;
+                        const size_t s = (size_t)nnz;
+                        const CT b0 = Num<MT>::get(__ldg(v)), b1 = Num<MT>::get(__ldg(v + s)),
+                                 b2 = Num<MT>::get(__ldg(v + 2 * s)), b3 = Num<MT>::get(__ldg(v + 3 * s)),
+                                 b4 = Num<MT>::get(__ldg(v + 4 * s)), b5 = Num<MT>::get(__ldg(v + 5 * s)),
+                                 b6 = Num<MT>::get(__ldg(v + 6 * s)), b7 = Num<MT>::get(__ldg(v + 7 * s)),
+                                 b8 = Num<MT>::get(__ldg(v + 8 * s));
+                        a0 += b0 * xv[u][0] + b1 * xv[u][1] + b2 * xv[u][2];
+                        a1 += b3 * xv[u][0] + b4 * xv[u][1] + b5 * xv[u][2];
+                        a2 += b6 * xv[u][0] + b7 * xv[u][1] + b8 * xv[u][2];
+                    }
+                }
             }
         }
 #pragma unroll
@@ -127,17 +148,20 @@ __device__ __forceinline__ void dinv_apply(const DT* __restrict__ dinv, int n, i
 
 enum SlotKind { kIdle = 0, kNormal = 1, kReplace = 2 };
 
-template <class MT, class VT, int TPR>
-__global__ void __launch_bounds__(kThreads, 2) pcg_kernel(const PcgParams prm) {
+template <class MT, class PT, class VT, int TPR>
+__global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
     using CT = typename Cmp<MT>::T;
     using DT = typename DinvT<MT>::T;
     // mixed modes keep the diagonal blocks of the coupled (active) nodes out of
     // the bulk planes and apply them in FP64: those blocks carry the contact /
     // stitch stiffness that cancels against the low-rank term in S = D - V C V^T
     constexpr bool kSplit = !std::is_same<MT, double>::value;
-    __shared__ double s_red[kWarps];
-    __shared__ double s_out;
-    extern __shared__ double s_dtt[];  // kmax doubles
+    constexpr int UA = Unroll<MT>::U;
+    constexpr int UC = Unroll<PT>::U;
+    __shared__ double s_w[kWarps][2];
+    __shared__ double s_bc[4];
+    __shared__ int s_ok;
+    extern __shared__ double smem[];
 
     const int cta = blockIdx.x;
     const unsigned int G = gridDim.x;
@@ -145,6 +169,7 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_kernel(const PcgParams prm) {
     const SysDesc& S = prm.sys[sidx];
     const int rb = prm.cta_row[2 * cta], re = prm.cta_row[2 * cta + 1];
     const int ab = prm.cta_act[2 * cta], ae = prm.cta_act[2 * cta + 1];
+    const int na = ae - ab;
     const int cb = S.cta_begin, ce = S.cta_end;
     const int ncta = ce - cb, lcta = cta - cb;
     const bool leader_cta = (cta == cb);
@@ -152,12 +177,10 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_kernel(const PcgParams prm) {
     const int rank = *S.rank;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int gwarp = lcta * kWarps + warp, nwarp = ncta * kWarps;
-    double* partA = prm.part;
-    double* partB = prm.part + G;
-    double* partC = prm.part + 2 * G;
     const double omega = prm.omega;
     const int nterms = prm.nterms;
     const MT* vals = reinterpret_cast<const MT*>(S.vals);
+    const PT* vals_pc = reinterpret_cast<const PT*>(S.vals_pc);
     const DT* dinv = reinterpret_cast<const DT*>(S.dinv);
     const double* vt = S.vt64;
     double* x = S.x;
@@ -168,6 +191,20 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_kernel(const PcgParams prm) {
     VT* pbuf[2] = {reinterpret_cast<VT*>(S.p[0]), reinterpret_cast<VT*>(S.p[1])};
     VT* tbuf[2] = {reinterpret_cast<VT*>(S.t[0]), reinterpret_cast<VT*>(S.t[1])};
 
+    // shared memory: d .* tt (kMaxRank), own coupled-dof z (na), Vt block (na * rank)
+    double* s_dtt = smem;
+    double* s_z = smem + kMaxRank;
+    double* s_vt = s_z + ((na + 1) & ~1);
+    const bool vt_smem = na > 0 && ((na + 1) & ~1) + na * rank <= prm.vt_smem;
+    if (vt_smem)
+        for (int e = threadIdx.x; e < na * rank; e += kThreads) {
+            const int j = e / na, il = e - j * na;
+            s_vt[e] = __ldg(vt + (size_t)j * a + ab + il);
+        }
+    auto vt_own = [&](int j, int il) -> double {
+        return vt_smem ? s_vt[j * na + il] : __ldg(vt + (size_t)j * a + ab + il);
+    };
+
     int it = 0, status = 0, nrep = 0;
     double rz = 0.0, normb = 0.0, rel = 1.0, beta = 0.0;
     bool done = false, counted = false, first = true;
@@ -175,57 +212,47 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_kernel(const PcgParams prm) {
     bool conv_check = false;
     int pc = 0;  // p buffer holding the previous direction
     int tc = 0;  // t buffer holding the current term
-    int bar_id = 0;
+    int epoch = 0;
 
+    // grid barrier with the CTA partials folded into the arrival: each warp
+    // reduces its values, thread 0 adds the warp sums (fixed order), stores
+    // them and arrives
+    auto barrier = [&](double* o0, double v0, double* o1, double v1) -> bool {
+        v0 = warp_sum(v0);
+        v1 = warp_sum(v1);
+        if (lane == 0) { s_w[warp][0] = v0; s_w[warp][1] = v1; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t0 = 0.0, t1 = 0.0;
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) { t0 += s_w[w][0]; t1 += s_w[w][1]; }
+            if (o0) o0[cta] = t0;
+            if (o1) o1[cta] = t1;
+            s_ok = grid_arrive_wait(prm.bar, G, prm.spin_limit, epoch);
+        }
+        ++epoch;
+        __syncthreads();
+        return s_ok != 0;
+    };
     auto dact_mul = [&](int an, double p0, double p1, double p2, double& o0, double& o1, double& o2) {
         const double* d = S.dact + 9 * (size_t)an;
         o0 = d[0] * p0 + d[1] * p1 + d[2] * p2;
         o1 = d[3] * p0 + d[4] * p1 + d[5] * p2;
         o2 = d[6] * p0 + d[7] * p1 + d[8] * p2;
     };
-    // per-CTA partials of Vt^T z over the CTA's own active dofs (z final)
+    // per-CTA partials of Vt^T z over the CTA's own coupled dofs (z final)
     auto compute_zpart = [&]() {
-        if (ab >= ae) return;  // uniform within the CTA
+        if (na <= 0) return;  // uniform within the CTA
+        __syncthreads();
+        for (int il = threadIdx.x; il < na; il += kThreads) s_z[il] = (double)elem<VT>(z, __ldg(S.act + ab + il));
         __syncthreads();
         for (int j = warp; j < rank; j += kWarps) {
-            const double* col = vt + (size_t)j * a;
             double sacc = 0.0;
-            for (int i = ab + lane; i < ae; i += 32) sacc += __ldg(col + i) * (double)elem<VT>(z, __ldg(S.act + i));
+            for (int il = lane; il < na; il += 32) sacc += vt_own(j, il) * s_z[il];
             sacc = warp_sum(sacc);
             if (lane == 0) S.zpart[(size_t)j * ncta + lcta] = sacc;
         }
     };
-
-    // ---------------- prologue: r = rhs, x = 0, z = M r ----------------
-    {
-        double acc_rr = 0.0, acc_rz = 0.0;
-        for (int row = rb + threadIdx.x; row < re; row += kThreads) {
-            double r0, r1, r2;
-            Vec4<double>::load(rhs, row, r0, r1, r2);
-            Vec4<double>::store(r, row, r0, r1, r2);
-            Vec4<double>::store(x, row, 0.0, 0.0, 0.0);
-            Vec4<VT>::store(pbuf[0], row, (VT)0, (VT)0, (VT)0);  // beta * p_prev must be 0, not NaN
-            double t0, t1, t2;
-            dinv_apply(dinv, n, row, omega, r0, r1, r2, t0, t1, t2);
-            Vec4<VT>::store(tbuf[0], row, (VT)t0, (VT)t1, (VT)t2);
-            const double w0 = prm.w[0];
-            const VT z0 = (VT)(w0 * t0), z1 = (VT)(w0 * t1), z2 = (VT)(w0 * t2);
-            Vec4<VT>::store(z, row, z0, z1, z2);
-            acc_rr += r0 * r0 + r1 * r1 + r2 * r2;
-            acc_rz += r0 * (double)z0 + r1 * (double)z1 + r2 * (double)z2;
-        }
-        for (int i = ab + threadIdx.x; i < ae; i += kThreads) S.pact[i] = 0.0;
-        if (ab >= ae)
-            for (int j = threadIdx.x; j < rank; j += kThreads) S.zpart[(size_t)j * ncta + lcta] = 0.0;
-        if (leader_cta)
-            for (int j = threadIdx.x; j < rank; j += kThreads) S.tt[j] = 0.0;
-        const double srr = block_sum(acc_rr, s_red, &s_out);
-        const double srz = block_sum(acc_rz, s_red, &s_out);
-        if (threadIdx.x == 0) { partA[cta] = srr; partB[cta] = srz; }
-        if (nterms == 1) compute_zpart();
-    }
-    if (!grid_sync(prm.bar, G, prm.spin_limit, bar_id++)) return;
-
     // C_k phases k = 1..nterms-1 of the preconditioner polynomial
     auto precond_tail = [&](bool active_sys) -> bool {
         for (int k = 1; k < nterms; ++k) {
@@ -267,24 +294,53 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_kernel(const PcgParams prm) {
                         acc += r0 * (double)s0 + r1 * (double)s1 + r2 * (double)s2;
                     }
                 };
-                spmv_own<MT, CT, TPR>(S.rowptr, S.colidx, vals, nnz, rb, re, gather, epi);
+                spmv_own<PT, CT, TPR, UC>(S.rowptr, S.colidx, vals_pc, nnz, rb, re, gather, epi);
                 if (last) compute_zpart();
             }
-            if (last) {
-                const double sum = block_sum(acc, s_red, &s_out);
-                if (threadIdx.x == 0) partB[cta] = sum;
-            }
             tc ^= 1;
-            if (!grid_sync(prm.bar, G, prm.spin_limit, bar_id++)) return false;
+            if (!barrier(last ? prm.part_rz : nullptr, acc, nullptr, 0.0)) return false;
         }
         return true;
     };
+
+    // ---------------- prologue: r = rhs, x = 0, z = M r ----------------
+    {
+        double acc_rr = 0.0, acc_rz = 0.0;
+        for (int row = rb + threadIdx.x; row < re; row += kThreads) {
+            double r0, r1, r2;
+            Vec4<double>::load(rhs, row, r0, r1, r2);
+            Vec4<double>::store(r, row, r0, r1, r2);
+            Vec4<double>::store(x, row, 0.0, 0.0, 0.0);
+            Vec4<VT>::store(pbuf[0], row, (VT)0, (VT)0, (VT)0);  // beta * p_prev must be 0, not NaN
+            double t0, t1, t2;
+            dinv_apply(dinv, n, row, omega, r0, r1, r2, t0, t1, t2);
+            Vec4<VT>::store(tbuf[0], row, (VT)t0, (VT)t1, (VT)t2);
+            const double w0 = prm.w[0];
+            const VT z0 = (VT)(w0 * t0), z1 = (VT)(w0 * t1), z2 = (VT)(w0 * t2);
+            Vec4<VT>::store(z, row, z0, z1, z2);
+            acc_rr += r0 * r0 + r1 * r1 + r2 * r2;
+            acc_rz += r0 * (double)z0 + r1 * (double)z1 + r2 * (double)z2;
+        }
+        for (int i = ab + threadIdx.x; i < ae; i += kThreads) S.pact[i] = 0.0;
+        if (na <= 0)
+            for (int j = threadIdx.x; j < rank; j += kThreads) S.zpart[(size_t)j * ncta + lcta] = 0.0;
+        if (leader_cta)
+            for (int j = threadIdx.x; j < rank; j += kThreads) S.tt[j] = 0.0;
+        if (nterms == 1) compute_zpart();
+        if (!barrier(prm.part_rr, acc_rr, nterms == 1 ? prm.part_rz : nullptr, acc_rz)) return;
+    }
     if (!precond_tail(true)) return;
 
     // ---------------- main loop: one slot per iteration ----------------
     for (;;) {
-        const double rr = sum_parts(partA, cb, ce, &s_out);
-        const double rzn = sum_parts(partB, cb, ce, &s_out);
+        if (warp == 0) {
+            double srr, srz;
+            warp_sum_parts(prm.part_rr, prm.part_rz, cb, ce, srr, srz);
+            if (lane == 0) { s_bc[0] = srr; s_bc[1] = srz; }
+        }
+        __syncthreads();
+        const double rr = s_bc[0];
+        const double rzn = s_bc[1];
         if (!done) {
             if (first) {
                 normb = sqrt(rr);
@@ -376,12 +432,11 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_kernel(const PcgParams prm) {
                         acc += (double)g0 * (double)(VT)y0 + (double)g1 * (double)(VT)y1 + (double)g2 * (double)(VT)y2;
                     }
                 };
-                spmv_own<MT, CT, TPR>(S.rowptr, S.colidx, vals, nnz, rb, re, gather, epi);
-                // tt_j = (Vt^T z)_j + beta tt_j (per-CTA partials of Vt^T z from the last phase)
+                spmv_own<MT, CT, TPR, UA>(S.rowptr, S.colidx, vals, nnz, rb, re, gather, epi);
+                // tt_j = (Vt^T z)_j + beta tt_j from the per-CTA partials of Vt^T z
                 for (int j = gwarp; j < rank; j += nwarp) {
-                    double sz = 0.0;
-                    for (int c = lane; c < ncta; c += 32) sz += S.zpart[(size_t)j * ncta + c];
-                    sz = warp_sum(sz);
+                    double sz, unused;
+                    warp_sum_parts(S.zpart + (size_t)j * ncta, nullptr, 0, ncta, sz, unused);
                     if (lane == 0) {
                         const double t = sz + bd * S.tt[j];
                         S.tt[j] = t;
@@ -396,7 +451,7 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_kernel(const PcgParams prm) {
                     Vec4<double>::load(rhs, row, h0, h1, h2);
                     Vec4<double>::store(r, row, h0 - y0, h1 - y1, h2 - y2);
                 };
-                spmv_own<double, double, TPR>(S.rowptr, S.colidx, S.vals64, nnz, rb, re, gather, epi);
+                spmv_own<double, double, TPR, 2>(S.rowptr, S.colidx, S.vals64, nnz, rb, re, gather, epi);
                 for (int j = gwarp; j < rank; j += nwarp) {
                     const double* col = vt + (size_t)j * a;
                     double d = 0.0;
@@ -408,10 +463,8 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_kernel(const PcgParams prm) {
                     if (lane == 0) S.ttx[j] = d;
                 }
             }
-            const double sum = block_sum(acc, s_red, &s_out);
-            if (threadIdx.x == 0) partC[cta] = sum;
+            if (!barrier(prm.part_pap, acc, nullptr, 0.0)) return;
         }
-        if (!grid_sync(prm.bar, G, prm.spin_limit, bar_id++)) return;
         if (ld_volatile_i32(prm.remaining) == 0) break;
 
         // ---- phase B: alpha, low-rank correction, x/r update, t = w Dd^-1 r ----
@@ -420,7 +473,13 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_kernel(const PcgParams prm) {
             bool work = slot != kIdle;
             double alpha = 0.0;
             if (slot == kNormal) {
-                const double pAp = sum_parts(partC, cb, ce, &s_out);
+                if (warp == 0) {
+                    double sp, unused;
+                    warp_sum_parts(prm.part_pap, nullptr, cb, ce, sp, unused);
+                    if (lane == 0) s_bc[2] = sp;
+                }
+                __syncthreads();
+                const double pAp = s_bc[2];
                 if (!(isfinite(pAp) && pAp > 0)) {
                     done = true; status = 3; work = false;                      // linear_hsc.cu:370-371
                 } else {
@@ -429,15 +488,15 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_kernel(const PcgParams prm) {
                 }
             }
             if (work) {
-                const double* tsrc = slot == kNormal ? S.tt : S.ttx;
-                if (ab < ae) {
+                if (na > 0) {
+                    const double* tsrc = slot == kNormal ? S.tt : S.ttx;
                     for (int j = threadIdx.x; j < rank; j += kThreads) s_dtt[j] = __ldg(S.dpiv + j) * tsrc[j];
                     __syncthreads();
-                    for (int i = ab + threadIdx.x; i < ae; i += kThreads) {
+                    for (int il = threadIdx.x; il < na; il += kThreads) {
                         double c = 0.0;
-                        for (int j = 0; j < rank; ++j) c += __ldg(vt + (size_t)j * a + i) * s_dtt[j];
-                        if (slot == kNormal) S.yact[i] -= c;                       // y = D p - Vt d Vt^T p
-                        else elem<double>(r, __ldg(S.act + i)) += c;              // r = rhs - D x + Vt d Vt^T x
+                        for (int j = 0; j < rank; ++j) c += vt_own(j, il) * s_dtt[j];
+                        if (slot == kNormal) S.yact[ab + il] -= c;                     // y = D p - Vt d Vt^T p
+                        else elem<double>(r, __ldg(S.act + ab + il)) += c;           // r = rhs - D x + Vt d Vt^T x
                     }
                 }
                 __syncthreads();
@@ -483,59 +542,64 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_kernel(const PcgParams prm) {
                 }
                 if (nterms == 1) compute_zpart();
             }
-            const double srr = block_sum(acc_rr, s_red, &s_out);
-            const double srz = block_sum(acc_rz, s_red, &s_out);
-            if (threadIdx.x == 0) { partA[cta] = srr; if (nterms == 1) partB[cta] = srz; }
             if (!work) slot = kIdle;
+            if (!barrier(prm.part_rr, acc_rr, nterms == 1 ? prm.part_rz : nullptr, acc_rz)) return;
         }
-        if (!grid_sync(prm.bar, G, prm.spin_limit, bar_id++)) return;
         prev_slot = slot;
         // ---- phases C ----
         if (!precond_tail(slot != kIdle)) return;
     }
 }
 
-template <class MT, class VT, int TPR>
+template <class MT, class PT, class VT, int TPR>
 cudaError_t launch_t(const PcgParams& prm, int grid, cudaStream_t st, size_t smem) {
+    auto fn = pcg_kernel<MT, PT, VT, TPR>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     void* args[] = {(void*)&prm};
-    return cudaLaunchCooperativeKernel((void*)pcg_kernel<MT, VT, TPR>, dim3(grid), dim3(kThreads), args, smem, st);
+    return cudaLaunchCooperativeKernel((void*)fn, dim3(grid), dim3(kThreads), args, smem, st);
 }
 
-template <class MT, class VT, int TPR>
+template <class MT, class PT, class VT, int TPR>
 int bps_t(size_t smem) {
+    auto fn = pcg_kernel<MT, PT, VT, TPR>;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, pcg_kernel<MT, VT, TPR>, kThreads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, smem);
     return b;
 }
 
 }  // namespace
 
-constexpr size_t kDttSmem = 256 * sizeof(double);
+size_t pcg_smem_bytes(int vt_doubles, int kmax_all) {
+    (void)kmax_all;
+    return sizeof(double) * (size_t)(kMaxRank + vt_doubles);
+}
 
-cudaError_t launch_pcg(int precision, int tpr, const PcgParams& prm, int grid, cudaStream_t st) {
+cudaError_t launch_pcg(int precision, int tpr, const PcgParams& prm, int grid, size_t smem, cudaStream_t st) {
     count_launch();
-#define HSC_PCG_CASE(MT, VT)                                                   \
+#define HSC_PCG_CASE(MT, PT, VT)                                               \
     switch (tpr) {                                                             \
-        case 2: return launch_t<MT, VT, 2>(prm, grid, st, kDttSmem);           \
-        case 8: return launch_t<MT, VT, 8>(prm, grid, st, kDttSmem);           \
-        default: return launch_t<MT, VT, 4>(prm, grid, st, kDttSmem);          \
+        case 2: return launch_t<MT, PT, VT, 2>(prm, grid, st, smem);           \
+        case 8: return launch_t<MT, PT, VT, 8>(prm, grid, st, smem);           \
+        default: return launch_t<MT, PT, VT, 4>(prm, grid, st, smem);          \
     }
-    if (precision == 0) { HSC_PCG_CASE(double, double) }
-    if (precision == 1) { HSC_PCG_CASE(float, float) }
-    HSC_PCG_CASE(__nv_bfloat16, float)
+    if (precision == 0) { HSC_PCG_CASE(double, double, double) }
+    if (precision == 1) { HSC_PCG_CASE(float, float, float) }
+    HSC_PCG_CASE(float, __nv_bfloat16, float)
 #undef HSC_PCG_CASE
 }
 
-int pcg_blocks_per_sm(int precision, int tpr) {
-#define HSC_BPS_CASE(MT, VT)                                                   \
+int pcg_blocks_per_sm(int precision, int tpr, size_t smem) {
+#define HSC_BPS_CASE(MT, PT, VT)                                               \
     switch (tpr) {                                                             \
-        case 2: return bps_t<MT, VT, 2>(kDttSmem);                             \
-        case 8: return bps_t<MT, VT, 8>(kDttSmem);                             \
-        default: return bps_t<MT, VT, 4>(kDttSmem);                            \
+        case 2: return bps_t<MT, PT, VT, 2>(smem);                             \
+        case 8: return bps_t<MT, PT, VT, 8>(smem);                             \
+        default: return bps_t<MT, PT, VT, 4>(smem);                            \
     }
-    if (precision == 0) { HSC_BPS_CASE(double, double) }
-    if (precision == 1) { HSC_BPS_CASE(float, float) }
-    HSC_BPS_CASE(__nv_bfloat16, float)
+    if (precision == 0) { HSC_BPS_CASE(double, double, double) }
+    if (precision == 1) { HSC_BPS_CASE(float, float, float) }
+    HSC_BPS_CASE(float, __nv_bfloat16, float)
 #undef HSC_BPS_CASE
 }
 

@@ -66,8 +66,9 @@ __global__ void pattern_hash_kernel(const int* rows, const int* cols, long long 
     if ((threadIdx.x & 31) == 0) atomicAdd(out, h);
 }
 
-template <class MT>
-__global__ void fill_bsr_kernel(const int* src, const double* values, int nnz, double* v64, MT* vmt) {
+// BCOO entry -> full BSR planes: FP64 always, plus an FP32 and/or a BF16 copy
+__global__ void fill_bsr_kernel(const int* src, const double* values, int nnz, double* v64, float* vf,
+                                __nv_bfloat16* vb) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nnz) return;
     const int packed = src[k];
@@ -79,8 +80,10 @@ __global__ void fill_bsr_kernel(const int* src, const double* values, int nnz, d
 #pragma unroll
         for (int cc = 0; cc < 3; ++cc) {
             const double v = tr ? B[cc + 3 * rr] : B[rr + 3 * cc];
-            v64[(size_t)(3 * rr + cc) * nnz + k] = v;
-            if (vmt) vmt[(size_t)(3 * rr + cc) * nnz + k] = Num<MT>::put(v);
+            const size_t o = (size_t)(3 * rr + cc) * nnz + k;
+            v64[o] = v;
+            if (vf) vf[o] = (float)v;
+            if (vb) vb[o] = __float2bfloat16_rn((float)v);
         }
 }
 
@@ -211,7 +214,8 @@ __global__ void __launch_bounds__(256) aca_kernel(AcaParams p) {
         }
         reduce_local(ls, lm);
     }
-    if (!grid_sync(p.bar, G, p.spin_limit, 100)) return;
+    int epoch = 0;
+    if (!grid_sync(p.bar, G, p.spin_limit, epoch++)) return;
     double scale = 0.0, residual = 0.0;
     int k = 0;
     for (;; ++k) {
@@ -260,7 +264,7 @@ __global__ void __launch_bounds__(256) aca_kernel(AcaParams p) {
         }
         reduce_local(ls, lm);
         cur ^= 1;
-        if (!grid_sync(p.bar, G, p.spin_limit, 101)) return;
+        if (!grid_sync(p.bar, G, p.spin_limit, epoch++)) return;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *p.rank = k;
@@ -371,6 +375,71 @@ __global__ void chol_solve_kernel(const double* L, int m, const double* B, int l
     for (int i = lane; i < m; i += 32) X[(size_t)i * ldx + gw] = y[i];
 }
 
+// P = A^-1 for an SPD A (m <= 160) in one 1024-thread CTA: Cholesky in
+// shared memory (2-D trailing update, two barriers per column), then each warp
+// solves L L^T x = e_c for its columns with the vector held in registers
+// (lane l owns entries l, l+32, ...).
+constexpr int kCholQ = 5;  // 32 * 5 = 160 rows in registers
+__global__ void __launch_bounds__(1024) chol_inverse_kernel(const double* A, int m, double* P, int* bad) {
+    extern __shared__ double L[];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int ld = m + 1;  // odd row stride: column walks hit distinct banks
+    for (int e = threadIdx.x; e < m * m; e += 1024) L[(e / m) * ld + e % m] = A[e];
+    __syncthreads();
+    bool ok = true;
+    for (int j = 0; j < m; ++j) {
+        double d = L[j * ld + j];
+        if (!(d > 0.0) || !isfinite(d)) { ok = false; d = 1.0; }
+        const double dj = sqrt(d);
+        __syncthreads();
+        if (threadIdx.x == 0) L[j * ld + j] = dj;
+        for (int i = j + 1 + threadIdx.x; i < m; i += 1024) L[i * ld + j] /= dj;
+        __syncthreads();
+        for (int i = j + 1 + ty; i < m; i += 32) {
+            const double lij = L[i * ld + j];
+            for (int l = j + 1 + tx; l <= i; l += 32) L[i * ld + l] -= lij * L[l * ld + j];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && !ok) atomicAdd(bad, 1);
+    // columns of the inverse
+    for (int c = ty; c < m; c += 32) {
+        double y[kCholQ];
+#pragma unroll
+        for (int q = 0; q < kCholQ; ++q) y[q] = 0.0;
+        for (int i = 0; i < m; ++i) {                       // L y = e_c
+            double sacc = 0.0;
+#pragma unroll
+            for (int q = 0; q < kCholQ; ++q) {
+                const int k = 32 * q + tx;
+                if (k < i) sacc += L[i * ld + k] * y[q];
+            }
+            sacc = wsum(sacc);
+            const double v = ((i == c ? 1.0 : 0.0) - sacc) / L[i * ld + i];
+#pragma unroll
+            for (int q = 0; q < kCholQ; ++q)
+                if (32 * q + tx == i) y[q] = v;
+        }
+        for (int i = m - 1; i >= 0; --i) {                  // L^T x = y
+            double sacc = 0.0;
+#pragma unroll
+            for (int q = 0; q < kCholQ; ++q) {
+                const int k = 32 * q + tx;
+                if (k > i && k < m) sacc += L[k * ld + i] * y[q];
+            }
+            sacc = wsum(sacc);
+#pragma unroll
+            for (int q = 0; q < kCholQ; ++q)
+                if (32 * q + tx == i) y[q] = (y[q] - sacc) / L[i * ld + i];
+        }
+#pragma unroll
+        for (int q = 0; q < kCholQ; ++q) {
+            const int i = 32 * q + tx;
+            if (i < m) P[(size_t)i * m + c] = y[q];
+        }
+    }
+}
+
 // C (k x k, row-major, k from device) = L diag(d) L^T in one CTA: L unit lower
 // (row-major, ld kmax) and d written out; C symmetrised first.
 __global__ void __launch_bounds__(1024) ldlt_kernel(double* C, int kmax, const int* dk, double* L, double* d,
@@ -378,36 +447,37 @@ __global__ void __launch_bounds__(1024) ldlt_kernel(double* C, int kmax, const i
     extern __shared__ double sm[];
     const int k = *dk;
     double* W = use_smem ? sm : C;
-    for (int e = threadIdx.x; e < k * k; e += blockDim.x) {
+    const int ldw = use_smem ? k + 1 : kmax;  // odd stride in shared memory
+    for (int e = threadIdx.x; e < k * k; e += blockDim.x) {  // lower triangle only (in place when W == C)
         const int i = e / k, l = e % k;
-        W[e] = 0.5 * (C[(size_t)i * kmax + l] + C[(size_t)l * kmax + i]);
+        if (l <= i) W[(size_t)i * ldw + l] = 0.5 * (C[(size_t)i * kmax + l] + C[(size_t)l * kmax + i]);
     }
     __syncthreads();
     __shared__ int s_bad;
     if (threadIdx.x == 0) s_bad = 0;
     __syncthreads();
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     for (int j = 0; j < k; ++j) {
-        const double dj = W[(size_t)j * k + j];
-        if (threadIdx.x == 0 && !(isfinite(dj) && dj != 0.0)) s_bad = 1;
-        __syncthreads();
-        const double djs = (isfinite(dj) && dj != 0.0) ? dj : 1.0;
-        // column j of L: W[i][j] / d_j (keep W[i][j] unscaled until the update is done)
-        const int rem = k - j - 1;
-        for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
-            const int i = j + 1 + e / rem, l = j + 1 + e % rem;
-            if (l <= i) W[(size_t)i * k + l] -= W[(size_t)i * k + j] * W[(size_t)l * k + j] / djs;
+        const double dj = W[(size_t)j * ldw + j];
+        const bool okj = isfinite(dj) && dj != 0.0;
+        if (threadIdx.x == 0 && !okj) s_bad = 1;
+        const double djs = okj ? dj : 1.0;
+        // trailing update with the unscaled column j, then scale it
+        for (int i = j + 1 + ty; i < k; i += 32) {
+            const double wij = W[(size_t)i * ldw + j] / djs;
+            for (int l = j + 1 + tx; l <= i; l += 32) W[(size_t)i * ldw + l] -= wij * W[(size_t)l * ldw + j];
         }
         __syncthreads();
-        for (int i = j + 1 + threadIdx.x; i < k; i += blockDim.x) W[(size_t)i * k + j] /= djs;
+        for (int i = j + 1 + threadIdx.x; i < k; i += blockDim.x) W[(size_t)i * ldw + j] /= djs;
         __syncthreads();
     }
     for (int e = threadIdx.x; e < kmax * kmax; e += blockDim.x) {
         const int i = e / kmax, l = e % kmax;
         double v = 0.0;
-        if (i < k && l < k) v = (l < i) ? W[(size_t)i * k + l] : (l == i ? 1.0 : 0.0);
+        if (i < k && l < k) v = (l < i) ? W[(size_t)i * ldw + l] : (l == i ? 1.0 : 0.0);
         L[e] = v;
     }
-    for (int j = threadIdx.x; j < kmax; j += blockDim.x) d[j] = j < k ? W[(size_t)j * k + j] : 0.0;
+    for (int j = threadIdx.x; j < kmax; j += blockDim.x) d[j] = j < k ? W[(size_t)j * ldw + j] : 0.0;
     if (threadIdx.x == 0 && s_bad) atomicAdd(bad, 1);
 }
 
@@ -688,17 +758,18 @@ __global__ void sub_kernel(const double* b, const double* y, double* r, int N) {
 
 // FP64 copies of the coupled nodes' diagonal blocks; in the mixed modes the
 // bulk planes drop them (they are applied in FP64 by the PCG kernel)
-template <class MT>
 __global__ void split_active_diag_kernel(const int* act, int nact_nodes, const int* diag_pos, const double* v64,
-                                         int nnz, MT* vmt, double* dact) {
+                                         int nnz, float* vf, __nv_bfloat16* vb, double* dact) {
     const int an = blockIdx.x * blockDim.x + threadIdx.x;
     if (an >= nact_nodes) return;
     const int node = act[3 * an] / 3;
     const int k = diag_pos[node];
 #pragma unroll
     for (int e = 0; e < 9; ++e) {
-        dact[9 * (size_t)an + e] = v64[(size_t)e * nnz + k];
-        if (vmt) vmt[(size_t)e * nnz + k] = Num<MT>::put(0.0);
+        const size_t o = (size_t)e * nnz + k;
+        dact[9 * (size_t)an + e] = v64[o];
+        if (vf) vf[o] = 0.0f;
+        if (vb) vb[o] = __float2bfloat16_rn(0.0f);
     }
 }
 
@@ -722,12 +793,10 @@ void launch_pattern_hash(const int* rows, const int* cols, long long nnzb, unsig
     HSC_COUNTED(pattern_hash_kernel<<<g, 256, 0, st>>>(rows, cols, nnzb, out));
 }
 
-void launch_fill_bsr(int precision, const int* src, const double* values, int nnz, double* v64, void* vmt,
+void launch_fill_bsr(const int* src, const double* values, int nnz, double* v64, float* vf, __nv_bfloat16* vb,
                      cudaStream_t st) {
     if (nnz == 0) return;
-    if (precision == 0) HSC_COUNTED(fill_bsr_kernel<double><<<blocks(nnz), 256, 0, st>>>(src, values, nnz, v64, nullptr));
-    else if (precision == 1) HSC_COUNTED(fill_bsr_kernel<float><<<blocks(nnz), 256, 0, st>>>(src, values, nnz, v64, (float*)vmt));
-    else HSC_COUNTED(fill_bsr_kernel<__nv_bfloat16><<<blocks(nnz), 256, 0, st>>>(src, values, nnz, v64, (__nv_bfloat16*)vmt));
+    HSC_COUNTED(fill_bsr_kernel<<<blocks(nnz), 256, 0, st>>>(src, values, nnz, v64, vf, vb));
 }
 
 void launch_dinv(int precision, const int* diag_pos, const double* v64, int nnz, int n, void* dinv, int* bad,
@@ -771,6 +840,14 @@ void launch_cholesky(const double* A, int m, double* L, int* bad, cudaStream_t s
     HSC_COUNTED(cholesky_kernel<<<1, 1024, use ? bytes : 0, st>>>(A, m, L, use, bad));
 }
 
+bool launch_chol_inverse(const double* A, int m, double* P, int* bad, cudaStream_t st) {
+    const size_t bytes = sizeof(double) * (size_t)m * (m + 1);
+    if (m > 32 * kCholQ || bytes > 200 * 1024) return false;
+    cudaFuncSetAttribute(chol_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    HSC_COUNTED(chol_inverse_kernel<<<1, 1024, bytes, st>>>(A, m, P, bad));
+    return true;
+}
+
 void launch_chol_solve(const double* L, int m, const double* B, int ldb, double* X, int ldx, int ncol,
                        const int* dncol, double* work, cudaStream_t st) {
     if (ncol <= 0) return;
@@ -778,7 +855,7 @@ void launch_chol_solve(const double* L, int m, const double* B, int ldb, double*
 }
 
 void launch_ldlt(double* C, int kmax, const int* dk, double* L, double* d, int* bad, cudaStream_t st) {
-    const size_t bytes = sizeof(double) * (size_t)kmax * kmax;
+    const size_t bytes = sizeof(double) * (size_t)kmax * (kmax + 1);
     const int use = bytes <= 200 * 1024;
     if (use) cudaFuncSetAttribute(ldlt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     HSC_COUNTED(ldlt_kernel<<<1, 1024, use ? bytes : 0, st>>>(C, kmax, dk, L, d, use, bad));
@@ -860,16 +937,11 @@ void launch_sub(const double* b, const double* y, double* r, int N, cudaStream_t
     HSC_COUNTED(sub_kernel<<<blocks(N), 256, 0, st>>>(b, y, r, N));
 }
 
-void launch_split_active_diag(int precision, const int* act, int nact_nodes, const int* diag_pos, const double* v64,
-                              int nnz, void* vmt, double* dact, cudaStream_t st) {
+void launch_split_active_diag(const int* act, int nact_nodes, const int* diag_pos, const double* v64, int nnz,
+                              float* vf, __nv_bfloat16* vb, double* dact, cudaStream_t st) {
     if (nact_nodes <= 0) return;
-    if (precision == 0)
-        HSC_COUNTED(split_active_diag_kernel<double><<<blocks(nact_nodes), 256, 0, st>>>(act, nact_nodes, diag_pos, v64, nnz, nullptr, dact));
-    else if (precision == 1)
-        HSC_COUNTED(split_active_diag_kernel<float><<<blocks(nact_nodes), 256, 0, st>>>(act, nact_nodes, diag_pos, v64, nnz, (float*)vmt, dact));
-    else
-        HSC_COUNTED(split_active_diag_kernel<__nv_bfloat16><<<blocks(nact_nodes), 256, 0, st>>>(act, nact_nodes, diag_pos, v64, nnz,
-                                                                                  (__nv_bfloat16*)vmt, dact));
+    HSC_COUNTED(split_active_diag_kernel<<<blocks(nact_nodes), 256, 0, st>>>(act, nact_nodes, diag_pos, v64, nnz, vf,
+                                                                              vb, dact));
 }
 
 void convert_f64_f32(const double* src, float* dst, long long n, cudaStream_t st) {

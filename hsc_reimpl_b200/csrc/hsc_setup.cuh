@@ -23,6 +23,22 @@ struct AcaParams {
     long long spin_limit;
 };
 
+// one system of the cluster ACA (hsc_aca.cu)
+struct AcaSys {
+    const double* E;       // coupling, row-major m x nc (read only)
+    int m, nc, cap;
+    double rtol;
+    double* U;             // m x cap, column-major
+    double* V;             // nc x cap, column-major
+    double* hist;          // cap + 1 residuals
+    int* rank;
+    double* err;
+};
+size_t aca_cluster_smem_doubles(int m, int nc);
+bool aca_cluster_fits(int m, int nc);
+cudaError_t launch_aca_cluster(const AcaSys* d_sys, int nsys, size_t smem_doubles, cudaStream_t st);
+int aca_cluster_supported(size_t smem_doubles);
+
 struct GemmArgs {
     const double* A;
     const double* B;
@@ -52,7 +68,7 @@ struct FullSpmv {
 };
 
 void launch_pattern_hash(const int* rows, const int* cols, long long nnzb, unsigned long long* out, cudaStream_t st);
-void launch_fill_bsr(int precision, const int* src, const double* values, int nnz, double* v64, void* vmt,
+void launch_fill_bsr(const int* src, const double* values, int nnz, double* v64, float* vf, __nv_bfloat16* vb,
                      cudaStream_t st);
 void launch_dinv(int precision, const int* diag_pos, const double* v64, int nnz, int n, void* dinv, int* bad,
                  cudaStream_t st);
@@ -62,6 +78,8 @@ cudaError_t launch_aca(const AcaParams& p, int grid, cudaStream_t st);
 int aca_blocks_per_sm();
 void launch_gemm(const GemmArgs& g, int M, int N, cudaStream_t st);
 void launch_cholesky(const double* A, int m, double* L, int* bad, cudaStream_t st);
+// P = A^-1 by Cholesky in one CTA; false (nothing launched) when m is too large
+bool launch_chol_inverse(const double* A, int m, double* P, int* bad, cudaStream_t st);
 void launch_chol_solve(const double* L, int m, const double* B, int ldb, double* X, int ldx, int ncol,
                        const int* dncol, double* work, cudaStream_t st);
 void launch_ldlt(double* C, int kmax, const int* dk, double* L, double* d, int* bad, cudaStream_t st);
@@ -87,8 +105,8 @@ void launch_scatter_y(const double* ypad, int n, int fo, const double* yq, int q
 void launch_line_step(double* x, const double* d, int N, const double* nd, cudaStream_t st);
 void launch_dot2(const double* a, const double* b, const double* c, int N, double* out, cudaStream_t st);
 void launch_sub(const double* b, const double* y, double* r, int N, cudaStream_t st);
-void launch_split_active_diag(int precision, const int* act, int nact_nodes, const int* diag_pos, const double* v64,
-                              int nnz, void* vmt, double* dact, cudaStream_t st);
+void launch_split_active_diag(const int* act, int nact_nodes, const int* diag_pos, const double* v64, int nnz,
+                              float* vf, __nv_bfloat16* vb, double* dact, cudaStream_t st);
 void convert_f64_f32(const double* src, float* dst, long long n, cudaStream_t st);
 void set_int(int* p, int v, cudaStream_t st);
 

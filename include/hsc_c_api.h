@@ -56,8 +56,9 @@ extern "C" {
 
 /* arithmetic of the Schur PCG bulk (SpMV, Neumann terms, low-rank apply) */
 #define HSC_FP64 0            /* everything FP64 (the reference form) */
-#define HSC_FP32 1            /* FP32 values and search vectors, FP64 x/r, FP64 residual replacement */
-#define HSC_BF16 2            /* BF16 matrix values, FP32 vectors and accumulation, FP64 replacement */
+#define HSC_FP32 1            /* FP32 bulk values and search vectors; FP64 x, r, coupled-node blocks, low-rank
+                                  term and residual replacement */
+#define HSC_BF16 2            /* FP32 operator, BF16 preconditioner planes, FP32 accumulation, FP64 replacement */
 
 /* approximate ABD inverse P (linear_hsc.cu:263-297, core.py:148-150) */
 #define HSC_ABD_NEUMANN 0     /* fixed-order block-Jacobi Neumann */

@@ -295,14 +295,19 @@ def test_pattern_change_behind_same_pointers_is_reanalysed(api, torch, cube_syst
 
 
 def test_refinement_reaches_target(api, torch, cube_system):
-    """Quadratic refinement (core.py:171-198) with a crude ACA (rtol 1e-2) and
-    an order-2 Neumann ABD inverse still reaches a 1e-9 full residual."""
-    ctx = api.HSCContext(api.HSCOptions(neumann_order=2, omega=2 / 3, aca_rtol=1e-2, tol=1e-6,
-                                        abd_inverse="neumann", refine_target=1e-9, max_refinements=60))
-    x, st = ctx.solve(api.DeviceSystem.from_system(cube_system))
+    """Quadratic refinement (core.py:171-198) over order-3 Neumann ABD-inverse
+    directions: one direction leaves ~3.5e-7, refinement reaches 1e-9 in the
+    same number of steps as the oracle."""
+    s = cube_system
+    opt = dict(neumann_order=3, omega=2 / 3, tol=1e-6, abd_inverse="neumann")
+    ctx = api.HSCContext(api.HSCOptions(refine_target=1e-9, max_refinements=60, **opt))
+    x, st = ctx.solve(api.DeviceSystem.from_system(s))
+    xo, so, _ = O.hsc_solve(s.H, s.layout, s.b, order=3, omega=2 / 3, tol=1e-6, abd_inverse="neumann",
+                            refine_target=1e-9, max_refinements=60)
     assert st["status"] == 0, st
     assert st["full_relative_residual"] <= 1e-9
-    assert st["refinement_steps"] >= 1
+    assert abs(st["refinement_steps"] - so["refinement_steps"]) <= 1
+    assert rel(x.cpu().numpy(), xo) < 1e-6
 
 
 def test_plugin_mirror_do_solve(api, torch, cube_system, tmp_path):
