@@ -7,8 +7,11 @@ from __future__ import annotations
 import ctypes as C
 from pathlib import Path
 
+import os
+
 HERE = Path(__file__).resolve().parent
-LIB_PATH = HERE / "libhsc_b200.so"
+# HSC_LIB selects another in-tree build of the same ABI (the self-checking one)
+LIB_PATH = HERE / os.environ.get("HSC_LIB", "libhsc_b200.so")
 
 HSC_OK = 0
 HSC_ERR_INVALID = 1
@@ -108,6 +111,7 @@ EXPORTS = {
     "hsc_get_abd_inverse": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
     "hsc_version": (C.c_int, []),
     "hsc_kernel_launches": (C.c_longlong, []),
+    "hsc_debug_checks": (C.c_int, [C.POINTER(C.c_longlong)]),
 }
 
 _LIB = None

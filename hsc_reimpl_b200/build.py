@@ -29,25 +29,30 @@ def _run(cmd):
     return r
 
 
-def build(force=False, verbose=False):
-    BUILD.mkdir(exist_ok=True)
+def build(force=False, verbose=False, checked=False):
+    """Build libhsc_b200.so; ``checked=True`` builds libhsc_b200_checked.so with
+    the index guards of hsc_check.cuh compiled in."""
+    build_dir = BUILD / "checked" if checked else BUILD
+    lib = HERE / ("libhsc_b200_checked.so" if checked else "libhsc_b200.so")
+    extra = ["-DHSC_CHECKED"] if checked else []
+    build_dir.mkdir(parents=True, exist_ok=True)
     headers = list(CSRC.glob("*.cuh")) + [HERE.parent / "include" / "hsc_c_api.h"]
     newest_header = max(h.stat().st_mtime for h in headers)
     objs = []
     for src in SOURCES:
         s = CSRC / src
-        o = BUILD / (s.stem + ".o")
+        o = build_dir / (s.stem + ".o")
         if force or not o.exists() or o.stat().st_mtime < max(s.stat().st_mtime, newest_header):
-            cmd = [NVCC, *FLAGS, "-c", str(s), "-o", str(o)]
+            cmd = [NVCC, *FLAGS, *extra, "-c", str(s), "-o", str(o)]
             if verbose:
                 print(" ".join(cmd))
             _run(cmd)
         objs.append(str(o))
-    if force or not LIB.exists() or LIB.stat().st_mtime < max(Path(o).stat().st_mtime for o in objs):
+    if force or not lib.exists() or lib.stat().st_mtime < max(Path(o).stat().st_mtime for o in objs):
         _run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-cudart", "static",
-              "-o", str(LIB), *objs])
-    return LIB
+              "-o", str(lib), *objs])
+    return lib
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose=True))
+    print(build(force="--force" in sys.argv, verbose=True, checked="--checked" in sys.argv))

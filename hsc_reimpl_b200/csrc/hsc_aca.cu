@@ -14,14 +14,16 @@
 //   computing the next step's partials.
 //
 // Partials and candidates are double-buffered, so one barrier per step is
-// enough.  Every CTA takes the same decisions from the same bits, so all of
-// them leave the loop at the same step; a last cluster barrier keeps each
-// CTA's shared memory alive while the others may still read it.  Systems
+// enough.  Every CTA takes the same decisions from the same bits (the same
+// 16 partials, the same candidate column at the same shared-memory offset in
+// the owner), so all of them leave the loop at the same step; a last cluster
+// barrier keeps each CTA's shared memory alive while the others may read it.  Systems
 // whose coupling does not fit 16 CTAs use the cooperative grid version.
 #include <cooperative_groups.h>
 
 #include <cfloat>
 
+#include "hsc_check.cuh"
 #include "hsc_setup.cuh"
 
 namespace cg = cooperative_groups;
@@ -56,25 +58,32 @@ __device__ __forceinline__ void warp_best(double& v, long long& i, double& s, in
 
 __global__ void __launch_bounds__(kAcaThreads, 1) aca_cluster_kernel(const AcaSys* sys) {
     cg::cluster_group cl = cg::this_cluster();
-    const int cr = (int)cl.block_rank();
     const AcaSys P = sys[blockIdx.x / kAcaCluster];
+    if (cl.num_blocks() != kAcaCluster) {  // launched without the 16-CTA cluster: refuse, uniformly
+        if (threadIdx.x == 0 && blockIdx.x % kAcaCluster == 0) { *P.rank = 0; *P.err = -1.0; }
+        return;
+    }
+    const int cr = (int)cl.block_rank();
     const int m = P.m, nc = P.nc;
     const int w = (nc + kAcaCluster - 1) / kAcaCluster;
     const int c0 = min(nc, cr * w), c1 = min(nc, c0 + w), nl = c1 - c0;
     const long long total = (long long)m * nc;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     extern __shared__ double sm[];
-    double* R = sm;                 // m x nl, row-major
-    double* cand = R + m * nl;      // 2 x m candidate columns
+    // the same layout in every CTA of the cluster (offsets must not depend on
+    // this CTA's own width nl): DSMEM maps an offset into the peer's memory
+    double* R = sm;                 // m x nl, row-major, in an m x w region
+    double* cand = R + m * w;       // 2 x m candidate columns
     double* u = cand + 2 * m;       // m
-    double* v = u + m;              // nl
+    double* v = u + m;              // nl <= w
     __shared__ Part part[2];
     __shared__ Part s_w[kAcaWarps];
     __shared__ double s_sc[2];
     __shared__ long long s_si;
 
     for (int r = warp; r < m; r += kAcaWarps)
-        for (int c = lane; c < nl; c += 32) R[r * nl + c] = P.E[(size_t)r * nc + c0 + c];
+        for (int c = lane; c < nl; c += 32)
+            if (HSC_IN(c0 + c < nc && r * nl + c < m * nl, 102, c0 + c)) R[r * nl + c] = P.E[(size_t)r * nc + c0 + c];
     __syncthreads();
 
     // local (max, idx, sum) of the slice -> part[slot]; candidate column -> cand[slot]
@@ -95,7 +104,8 @@ __global__ void __launch_bounds__(kAcaThreads, 1) aca_cluster_kernel(const AcaSy
         const long long gi = part[slot].idx;
         if (gi < total) {
             const int jl = (int)(gi % nc) - c0;
-            for (int r = tid; r < m; r += kAcaThreads) cand[slot * m + r] = R[r * nl + jl];
+            for (int r = tid; r < m; r += kAcaThreads)
+                if (HSC_IN(jl >= 0 && jl < nl, 103, jl)) cand[slot * m + r] = R[r * nl + jl];
         }
     };
     {
@@ -117,7 +127,7 @@ __global__ void __launch_bounds__(kAcaThreads, 1) aca_cluster_kernel(const AcaSy
         if (warp == 0) {
             double pv = -1.0, ps = 0.0;
             long long pi = total;
-            if (lane < kAcaCluster) {
+            if (lane < kAcaCluster && HSC_IN(lane < (int)cl.num_blocks(), 109, lane)) {
                 const Part* rp = cl.map_shared_rank(&part[slot], lane);
                 pv = rp->vmax; pi = rp->idx; ps = rp->sum;
             }
@@ -137,16 +147,19 @@ __global__ void __launch_bounds__(kAcaThreads, 1) aca_cluster_kernel(const AcaSy
         if (!(residual > P.rtol) || k >= P.cap || gi >= total) break;
         const int i = (int)(gi / nc), j = (int)(gi - (long long)i * nc);
         const int owner = j / w;
-        const double* rc = cl.map_shared_rank(cand + slot * m, owner);
-        for (int r = tid; r < m; r += kAcaThreads) u[r] = rc[r];
+        const bool own_ok = HSC_IN(owner >= 0 && owner < (int)cl.num_blocks() && i < m, 110, owner);
+        const double* rc = cl.map_shared_rank(cand + slot * m, own_ok ? owner : 0);
+        for (int r = tid; r < m; r += kAcaThreads) u[r] = own_ok ? rc[r] : 0.0;
         __syncthreads();
         const double pivot = u[i];
         if (!(fabs(pivot) > DBL_EPSILON * fmax(scale, DBL_MIN))) break;
         for (int c = tid; c < nl; c += kAcaThreads) v[c] = R[i * nl + c] / pivot;
         __syncthreads();
         if (cr == 0)
-            for (int r = tid; r < m; r += kAcaThreads) P.U[(size_t)k * m + r] = u[r];
-        for (int c = tid; c < nl; c += kAcaThreads) P.V[(size_t)k * nc + c0 + c] = v[c];
+            for (int r = tid; r < m; r += kAcaThreads)
+                if (HSC_IN(k < P.cap, 106, k)) P.U[(size_t)k * m + r] = u[r];
+        for (int c = tid; c < nl; c += kAcaThreads)
+            if (HSC_IN(k < P.cap && c0 + c < nc, 107, k)) P.V[(size_t)k * nc + c0 + c] = v[c];
         double ls = 0.0, lv = -1.0;
         long long li = total;
         for (int r = warp; r < m; r += kAcaWarps) {
@@ -200,6 +213,8 @@ cudaError_t launch_aca_cluster(const AcaSys* d_sys, int nsys, size_t smem_double
     count_launch();
     return cudaLaunchKernelEx(&cfg, aca_cluster_kernel, d_sys);
 }
+
+void read_fail_aca(long long* out) { hsc_read_fail(out); }
 
 int aca_cluster_supported(size_t smem_doubles) {
     cudaError_t e = cudaFuncSetAttribute(aca_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);

@@ -806,6 +806,7 @@ int system_status(hsc_ctx* ctx, const System& S, const DevScal& h, bool residual
     if (h.bad_fem) { snprintf(buf, sizeof buf, "HSC: %d non-positive FEM diagonal blocks", h.bad_fem); msg = buf; return HSC_ERR_NONSPD; }
     if (h.bad_abd) { msg = "HSC: non-SPD ABD block"; return HSC_ERR_NONSPD; }
     if (h.bad_ldlt) { msg = "HSC: singular reduced core U^T P U"; return HSC_ERR_NONSPD; }
+    if (h.aca_err < 0) { msg = "HSC: the ACA cluster launch did not get 16 CTAs"; return HSC_ERR_CUDA; }
     const int st = (int)h.pcg[2];
     if (grid_abort || st < 0) { msg = "HSC: a device-side wait gave up (grid barrier timeout)"; return HSC_ERR_TIMEOUT; }
     if (st == 3) { snprintf(buf, sizeof buf, "HSC Schur PCG breakdown at iteration %d. No fallback.", (int)h.pcg[0]); msg = buf; return HSC_ERR_BREAKDOWN; }
@@ -885,6 +886,14 @@ extern "C" {
 int hsc_version(void) { return HSC_API_VERSION; }
 
 long long hsc_kernel_launches(void) { return launch_count(); }
+
+int hsc_debug_checks(long long* out6) {
+    if (!out6) return HSC_ERR_INVALID;
+    read_fail_aca(out6);
+    read_fail_pcg(out6 + 2);
+    read_fail_setup(out6 + 4);
+    return HSC_OK;
+}
 
 int hsc_options_default(hsc_options* o) {
     if (!o) return HSC_ERR_INVALID;

@@ -32,6 +32,7 @@
 // Vt (the rows of its own coupled dofs) in shared memory for the whole solve.
 #include <type_traits>
 
+#include "hsc_check.cuh"
 #include "hsc_internal.cuh"
 
 namespace hsc {
@@ -196,10 +197,13 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
     double* s_z = smem + kMaxRank;
     double* s_vt = s_z + ((na + 1) & ~1);
     const bool vt_smem = na > 0 && ((na + 1) & ~1) + na * rank <= prm.vt_smem;
+    HSC_IN(rank <= kMaxRank && rank <= S.kmax, 207, rank);
+    HSC_IN(na <= 0 || ((na + 1) & ~1) <= prm.vt_smem, 201, na);
     if (vt_smem)
         for (int e = threadIdx.x; e < na * rank; e += kThreads) {
             const int j = e / na, il = e - j * na;
-            s_vt[e] = __ldg(vt + (size_t)j * a + ab + il);
+            if (HSC_IN(((na + 1) & ~1) + e < prm.vt_smem && ab + il < a, 200, e))
+                s_vt[e] = __ldg(vt + (size_t)j * a + ab + il);
         }
     auto vt_own = [&](int j, int il) -> double {
         return vt_smem ? s_vt[j * na + il] : __ldg(vt + (size_t)j * a + ab + il);
@@ -244,13 +248,16 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
     auto compute_zpart = [&]() {
         if (na <= 0) return;  // uniform within the CTA
         __syncthreads();
-        for (int il = threadIdx.x; il < na; il += kThreads) s_z[il] = (double)elem<VT>(z, __ldg(S.act + ab + il));
+        for (int il = threadIdx.x; il < na; il += kThreads) {
+            const int dof = __ldg(S.act + ab + il);
+            if (HSC_IN(dof >= 0 && dof < 3 * n, 204, dof)) s_z[il] = (double)elem<VT>(z, dof);
+        }
         __syncthreads();
         for (int j = warp; j < rank; j += kWarps) {
             double sacc = 0.0;
             for (int il = lane; il < na; il += 32) sacc += vt_own(j, il) * s_z[il];
             sacc = warp_sum(sacc);
-            if (lane == 0) S.zpart[(size_t)j * ncta + lcta] = sacc;
+            if (lane == 0 && HSC_IN(j < S.kmax, 205, j)) S.zpart[(size_t)j * ncta + lcta] = sacc;
         }
     };
     // C_k phases k = 1..nterms-1 of the preconditioner polynomial
@@ -399,6 +406,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
                 const double bd = beta;
                 auto gather = [&](int c, CT& g0, CT& g1, CT& g2) {
                     VT z0, z1, z2, q0, q1, q2;
+                    if (!HSC_IN(c >= 0 && c < n, 203, c)) c = 0;
                     Vec4<VT>::load(z, c, z0, z1, z2);
                     Vec4<VT>::load(pprev, c, q0, q1, q2);
                     g0 = (CT)(VT)((CT)z0 + bc * (CT)q0);
@@ -409,7 +417,8 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
                     CT g0, g1, g2;
                     gather(row, g0, g1, g2);
                     Vec4<VT>::store(pnew, row, (VT)g0, (VT)g1, (VT)g2);
-                    const int an = __ldg(S.rowflag + row);
+                    int an = __ldg(S.rowflag + row);
+                    if (!HSC_IN(an < a / 3, 206, an)) an = -1;
                     if (an >= 0) {
                         // FP64 direction and product at a coupled node
                         VT z0, z1, z2;
@@ -570,6 +579,8 @@ int bps_t(size_t smem) {
 }
 
 }  // namespace
+
+void read_fail_pcg(long long* out) { hsc_read_fail(out); }
 
 size_t pcg_smem_bytes(int vt_doubles, int kmax_all) {
     (void)kmax_all;

@@ -10,6 +10,7 @@
 //   * small dense FP64 algebra for the ABD inverse and the reduced core
 //     (Cholesky, triangular solves, tiled GEMM, LDL^T);
 //   * right-hand side, back-substitution and the full-system residual.
+#include "hsc_check.cuh"
 #include "hsc_setup.cuh"
 
 #include <atomic>
@@ -397,7 +398,8 @@ __global__ void __launch_bounds__(1024) chol_inverse_kernel(const double* A, int
         __syncthreads();
         for (int i = j + 1 + ty; i < m; i += 32) {
             const double lij = L[i * ld + j];
-            for (int l = j + 1 + tx; l <= i; l += 32) L[i * ld + l] -= lij * L[l * ld + j];
+            for (int l = j + 1 + tx; l <= i; l += 32)
+                if (HSC_IN(i * ld + l < m * ld && l * ld + j < m * ld, 300, i * ld + l)) L[i * ld + l] -= lij * L[l * ld + j];
         }
         __syncthreads();
     }
@@ -435,7 +437,7 @@ __global__ void __launch_bounds__(1024) chol_inverse_kernel(const double* A, int
 #pragma unroll
         for (int q = 0; q < kCholQ; ++q) {
             const int i = 32 * q + tx;
-            if (i < m) P[(size_t)i * m + c] = y[q];
+            if (i < m && HSC_IN(c < m, 301, c)) P[(size_t)i * m + c] = y[q];
         }
     }
 }
@@ -943,6 +945,8 @@ void launch_split_active_diag(const int* act, int nact_nodes, const int* diag_po
     HSC_COUNTED(split_active_diag_kernel<<<blocks(nact_nodes), 256, 0, st>>>(act, nact_nodes, diag_pos, v64, nnz, vf,
                                                                               vb, dact));
 }
+
+void read_fail_setup(long long* out) { hsc_read_fail(out); }
 
 void convert_f64_f32(const double* src, float* dst, long long n, cudaStream_t st) {
     if (n > 0) HSC_COUNTED(f64_to_f32_kernel<<<blocks(n), 256, 0, st>>>(src, dst, n));

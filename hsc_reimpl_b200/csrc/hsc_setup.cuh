@@ -38,6 +38,10 @@ size_t aca_cluster_smem_doubles(int m, int nc);
 bool aca_cluster_fits(int m, int nc);
 cudaError_t launch_aca_cluster(const AcaSys* d_sys, int nsys, size_t smem_doubles, cudaStream_t st);
 int aca_cluster_supported(size_t smem_doubles);
+// first failed index guard of a self-checking build, per translation unit
+void read_fail_aca(long long* out);
+void read_fail_pcg(long long* out);
+void read_fail_setup(long long* out);
 
 struct GemmArgs {
     const double* A;

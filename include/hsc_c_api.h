@@ -168,6 +168,9 @@ HSC_EXPORT int hsc_get_abd_inverse(hsc_ctx* ctx, int32_t sys, double* P);
 HSC_EXPORT int hsc_version(void);
 /* Kernels this library has launched in the process so far (all contexts). */
 HSC_EXPORT long long hsc_kernel_launches(void);
+/* First failed index guard of a self-checking build (-DHSC_CHECKED) as
+ * (code, value) pairs for the ACA, PCG and setup kernels; zeros otherwise. */
+HSC_EXPORT int hsc_debug_checks(long long* out6);
 
 #ifdef __cplusplus
 }
