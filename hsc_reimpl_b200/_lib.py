@@ -55,6 +55,7 @@ class Options(C.Structure):
         ("threads_per_row", C.c_int32),
         ("spin_limit", C.c_int64),
         ("check_residual", C.c_int32),
+        ("trace_iterations", C.c_int32),
     ]
 
 
@@ -109,6 +110,7 @@ EXPORTS = {
     "hsc_get_factors": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                   C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p]),
     "hsc_get_abd_inverse": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "hsc_get_trace": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "hsc_version": (C.c_int, []),
     "hsc_kernel_launches": (C.c_longlong, []),
     "hsc_debug_checks": (C.c_int, [C.POINTER(C.c_longlong)]),

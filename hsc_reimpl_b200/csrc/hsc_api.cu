@@ -85,7 +85,7 @@ struct System {
     int n = 0, nnz = 0, a = 0, nqq = 0, nqf = 0, kmax = 0, qm = 0, qo = 0, fo = 0, fn = 0;
     std::vector<int> h_rowptr, h_act;
     // plan
-    DevBuf rowptr, colidx, src, diag_pos, qq, qf, act, ident, rowflag;
+    DevBuf rowptr, colidx, rowid, src, diag_pos, qq, qf, act, ident, rowflag;
     // numeric
     DevBuf v64, vf32, vbf16, dinv, A, E, R0, R1, U, V, hist, P, Ptmp, T, term, Binv, L, W, C, Lc, dpiv, vt64, vtmt,
         cvec, tt, ttx, bq, bf, x, r, z, p0, p1, y, t0, t1, node_nz, xq, ypad, yq, work, cg, scal, dact, pact, yact,
@@ -105,7 +105,8 @@ struct hsc_ctx {
     int num_sms = 148;
     std::vector<System> sys;
     // PCG launch state
-    DevBuf d_desc, d_cta_sys, d_cta_row, d_cta_act, d_part, d_bar, d_remaining;
+    DevBuf d_desc, d_cta_sys, d_cta_row, d_cta_act, d_cta_warp, d_part, d_bar, d_remaining, d_trace;
+    int off_z = 0, off_vt = 0, off_y = 0, off_blk = 0, stage_vt = 0, stage_blk = 0;
     int grid = 0;
     int vt_smem = 0;           // doubles of PCG shared memory after the d.*tt slot
     size_t pcg_smem = 0;       // dynamic shared memory bytes of the PCG launch
@@ -289,6 +290,14 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
     GROW(S.act, sizeof(int) * std::max(1, S.a));
     GROW(S.rowflag, sizeof(int) * std::max(1, S.n));
     CK(cudaMemcpyAsync(S.rowptr.p, S.h_rowptr.data(), sizeof(int) * (S.n + 1), cudaMemcpyHostToDevice, st));
+    {
+        std::vector<int> rid(std::max(1, S.nnz));
+        for (int i = 0; i < S.n; ++i)
+            for (int k = S.h_rowptr[i]; k < S.h_rowptr[i + 1]; ++k) rid[k] = i;
+        GROW(S.rowid, sizeof(int) * std::max(1, S.nnz));
+        CK(cudaMemcpyAsync(S.rowid.p, rid.data(), sizeof(int) * std::max(1, S.nnz), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    }
     if (S.nnz) {
         CK(cudaMemcpyAsync(S.colidx.p, colidx.data(), sizeof(int) * S.nnz, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(S.src.p, src.data(), sizeof(int) * S.nnz, cudaMemcpyHostToDevice, st));
@@ -623,7 +632,7 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
         }
         SysDesc& d = desc[s];
         d.n = S.n; d.nnz = S.nnz; d.a = S.a; d.kmax = S.kmax; d.cta_begin = b; d.cta_end = c;
-        d.rowptr = S.rowptr.as<int>(); d.colidx = S.colidx.as<int>();
+        d.rowptr = S.rowptr.as<int>(); d.colidx = S.colidx.as<int>(); d.rowid = S.rowid.as<int>();
         d.vals = o.precision ? S.vf32.p : S.v64.p;
         d.vals_pc = o.precision == 2 ? S.vbf16.p : d.vals;
         d.vals64 = S.v64.as<double>(); d.dinv = S.dinv.p;
@@ -636,20 +645,51 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
         d.p[0] = S.p0.p; d.p[1] = S.p1.p; d.y = S.y.p; d.t[0] = S.t0.p; d.t[1] = S.t1.p; d.tt = S.tt.as<double>();
         d.out = S.scal.as<DevScal>()->pcg; d.cg_coef = S.cg.as<double>(); d.max_coef = 64;
     }
-    // shared memory: every CTA stages its coupled-dof z values; the Vt block too
-    // when all blocks fit the budget
-    int need_z = 0, need_vt = 0;
+    // warp-owned row ranges: kWarps + 1 boundaries per CTA, balanced by blocks
+    std::vector<int> cta_warp((size_t)(kWarps + 1) * G);
+    int Zmax = 0, VTmax = 0, Rmax = 0, BLKmax = 0;
     for (int k = 0; k < G; ++k) {
         const System& S = ctx->sys[idx[cta_sys[k]]];
+        const int rb = cta_row[2 * k], re = cta_row[2 * k + 1];
+        const long long kb0 = S.h_rowptr[rb], nb = (long long)S.h_rowptr[re] - kb0;
+        int row = rb;
+        for (int w = 0; w <= kWarps; ++w) {
+            if (w == kWarps) row = re;
+            else {
+                const long long target = kb0 + nb * w / kWarps;
+                while (row < re && S.h_rowptr[row] < target) ++row;
+            }
+            cta_warp[(size_t)(kWarps + 1) * k + w] = row;
+        }
         const int na = cta_act[2 * k + 1] - cta_act[2 * k];
-        const int pz = (na + 1) & ~1;
-        need_z = std::max(need_z, pz);
-        need_vt = std::max(need_vt, pz + na * std::max(0, S.kmax));
+        Zmax = std::max(Zmax, (na + 1) & ~1);
+        VTmax = std::max(VTmax, na * std::max(0, S.kmax));
+        Rmax = std::max(Rmax, re - rb);
+        BLKmax = std::max(BLKmax, (int)nb);
     }
-    const int budget = (int)(smem_cap / sizeof(double)) - kMaxRank;
-    ctx->vt_smem = need_vt <= budget ? need_vt : need_z;
-    ctx->pcg_smem = pcg_smem_bytes(ctx->vt_smem, 0);
-    if (need_z > budget) return fail(ctx, HSC_ERR_INVALID, "too many coupled dofs in one CTA row range");
+    // shared-memory layout; staging of the Vt blocks and of the column indices
+    // is dropped (in that order) when the budget does not hold them
+    const int budget = (int)(smem_cap / sizeof(double));
+    const int base = kMaxRank + Zmax + 3 * Rmax + 2;
+    if (base > budget) return fail(ctx, HSC_ERR_INVALID, "too many rows or coupled dofs in one CTA");
+    int stage_vt = 1, stage_blk = 1;
+    if (base + VTmax + BLKmax > budget) {
+        if (base + BLKmax <= budget) stage_vt = 0;
+        else if (base + VTmax <= budget) stage_blk = 0;
+        else { stage_vt = 0; stage_blk = 0; }
+    }
+    ctx->off_z = kMaxRank;
+    ctx->off_vt = ctx->off_z + Zmax;
+    ctx->off_y = ctx->off_vt + (stage_vt ? VTmax : 0);
+    ctx->off_y += ctx->off_y & 1;
+    ctx->off_blk = ctx->off_y + 3 * Rmax + 1;
+    ctx->off_blk += ctx->off_blk & 1;
+    ctx->stage_vt = stage_vt;
+    ctx->stage_blk = stage_blk;
+    ctx->vt_smem = Zmax + VTmax;
+    ctx->pcg_smem = sizeof(double) * (size_t)(ctx->off_blk + (stage_blk ? BLKmax : 0));
+    GROW(ctx->d_cta_warp, sizeof(int) * cta_warp.size());
+    CK(cudaMemcpyAsync(ctx->d_cta_warp.p, cta_warp.data(), sizeof(int) * cta_warp.size(), cudaMemcpyHostToDevice, st));
     GROW(ctx->d_desc, sizeof(SysDesc) * ns);
     GROW(ctx->d_cta_sys, sizeof(int) * G);
     GROW(ctx->d_cta_row, sizeof(int) * 2 * G);
@@ -700,6 +740,18 @@ int launch_pcg_all(hsc_ctx* ctx, int nsys, cudaStream_t st) {
     prm.part_rz = ctx->d_part.as<double>() + ctx->grid;
     prm.part_pap = ctx->d_part.as<double>() + 2 * ctx->grid;
     prm.vt_smem = ctx->vt_smem;
+    prm.cta_warp = ctx->d_cta_warp.as<int>();
+    prm.off_z = ctx->off_z; prm.off_vt = ctx->off_vt; prm.off_y = ctx->off_y; prm.off_blk = ctx->off_blk;
+    prm.stage_vt = ctx->stage_vt; prm.stage_blk = ctx->stage_blk;
+    prm.trace = nullptr;
+    prm.trace_iters = 0;
+    if (o.trace_iterations > 0) {
+        const size_t nt = (size_t)ctx->grid * o.trace_iterations * 8;
+        GROW(ctx->d_trace, sizeof(unsigned long long) * nt);
+        CK(cudaMemsetAsync(ctx->d_trace.p, 0, sizeof(unsigned long long) * nt, st));
+        prm.trace = ctx->d_trace.as<unsigned long long>();
+        prm.trace_iters = o.trace_iterations;
+    }
     prm.bar = ctx->d_bar.as<GridBar>();
     prm.remaining = ctx->d_remaining.as<int>();
     prm.omega = o.omega;
@@ -917,6 +969,7 @@ int hsc_options_default(hsc_options* o) {
     o->threads_per_row = 4;
     o->spin_limit = 20000000;
     o->check_residual = 1;
+    o->trace_iterations = 0;
     return HSC_OK;
 }
 
@@ -1233,6 +1286,16 @@ int hsc_get_factors(hsc_ctx* ctx, int32_t sys, int32_t* rank, int32_t* n_active,
                                  cudaMemcpyDeviceToHost));
     if (V && k) CK(cudaMemcpy2D(V, sizeof(double) * ldv, S.V.p, sizeof(double) * S.a, sizeof(double) * S.a, k,
                                  cudaMemcpyDeviceToHost));
+    return HSC_OK;
+}
+
+int hsc_get_trace(hsc_ctx* ctx, unsigned long long* out, int64_t max_entries, int32_t* ctas, int32_t* iterations) {
+    if (!ctx || ctx->opt.trace_iterations <= 0 || !ctx->d_trace.p) return HSC_ERR_NOTREADY;
+    const int64_t nt = (int64_t)ctx->grid * ctx->opt.trace_iterations * 8;
+    if (ctas) *ctas = ctx->grid;
+    if (iterations) *iterations = ctx->opt.trace_iterations;
+    if (out) CK(cudaMemcpy(out, ctx->d_trace.p, sizeof(unsigned long long) * std::min(nt, max_entries),
+                           cudaMemcpyDeviceToHost));
     return HSC_OK;
 }
 

@@ -157,6 +157,7 @@ struct SysDesc {
     const int* rowflag;    // per node: active-node index, or -1
     const int* rowptr;
     const int* colidx;
+    const int* rowid;      // block row of every BSR entry
     const void* vals;      // operator planes (mixed modes: active diagonal blocks zeroed)
     const void* vals_pc;   // preconditioner planes (BF16 mode: bf16 copy; else == vals)
     const double* vals64;  // FP64 planes (true-residual replacement)
@@ -201,7 +202,14 @@ struct PcgParams {
     int max_iter;
     int rr_every;              // residual replacement interval (0 = only at convergence)
     long long spin_limit;
-    int vt_smem;               // doubles of shared memory for the CTA's Vt block (0: read it from global)
+    const int* cta_warp;       // per CTA: kWarps + 1 row boundaries of the warp-owned row ranges
+    // shared-memory layout (offsets in doubles from the dynamic base, the same in every CTA)
+    int off_z, off_vt, off_y, off_blk;
+    int stage_vt;              // the CTAs' Vt blocks are staged (else read from global)
+    int stage_blk;             // the CTAs' column indices and row ids are staged
+    int vt_smem;               // doubles reserved for the largest Vt block (pad(na) + na * rank)
+    unsigned long long* trace; // optional: per CTA x trace_iters x 8 SM clocks
+    int trace_iters;
 };
 
 // launch counter of this library (hsc_setup.cu)

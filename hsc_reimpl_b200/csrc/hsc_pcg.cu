@@ -43,8 +43,6 @@ template <class MT> struct Cmp { using T = float; };
 template <> struct Cmp<double> { using T = double; };
 template <class MT> struct DinvT { using T = float; };
 template <> struct DinvT<double> { using T = double; };
-template <class MT> struct Unroll { static constexpr int U = 4; };
-template <> struct Unroll<double> { static constexpr int U = 2; };
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -81,57 +79,66 @@ __device__ __forceinline__ void warp_sum_parts(const double* pa, const double* p
     sc = warp_sum(sc);
 }
 
-// y_row = sum_k B_k x[col_k] over own rows; TPR lanes per row, U blocks per
-// lane in flight, then the group leader runs the epilogue.
-template <class MT, class CT, int TPR, int U, class Gather, class Epi>
-__device__ __forceinline__ void spmv_own(const int* __restrict__ rowptr, const int* __restrict__ colidx,
-                                         const MT* __restrict__ vals, int nnz, int rb, int re,
-                                         const Gather& gather, Epi& epi) {
-    constexpr int kGroups = kThreads / TPR;
-    const int grp = threadIdx.x / TPR, sub = threadIdx.x % TPR;
-    for (int row0 = rb; row0 < re; row0 += kGroups) {
-        const int row = row0 + grp;
-        CT a0 = 0, a1 = 0, a2 = 0;
-        if (row < re) {
-            const int k0 = __ldg(rowptr + row), k1 = __ldg(rowptr + row + 1);
-            for (int kb = k0 + sub; kb < k1; kb += TPR * U) {
-                int c[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int k = kb + u * TPR;
-                    c[u] = k < k1 ? __ldg(colidx + k) : -1;
-                }
-                CT xv[U][3];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    if (c[u] >= 0) gather(c[u], xv[u][0], xv[u][1], xv[u][2]);
-                    else xv[u][0] = xv[u][1] = xv[u][2] = 0;
-                }
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int k = kb + u * TPR;
-                    if (k < k1) {
-                        const MT* v = vals + k;
-                        const size_t s = (size_t)nnz;
-                        const CT b0 = Num<MT>::get(__ldg(v)), b1 = Num<MT>::get(__ldg(v + s)),
-                                 b2 = Num<MT>::get(__ldg(v + 2 * s)), b3 = Num<MT>::get(__ldg(v + 3 * s)),
-                                 b4 = Num<MT>::get(__ldg(v + 4 * s)), b5 = Num<MT>::get(__ldg(v + 5 * s)),
-                                 b6 = Num<MT>::get(__ldg(v + 6 * s)), b7 = Num<MT>::get(__ldg(v + 7 * s)),
-                                 b8 = Num<MT>::get(__ldg(v + 8 * s));
-                        a0 += b0 * xv[u][0] + b1 * xv[u][1] + b2 * xv[u][2];
-                        a1 += b3 * xv[u][0] + b4 * xv[u][1] + b5 * xv[u][2];
-                        a2 += b6 * xv[u][0] + b7 * xv[u][1] + b8 * xv[u][2];
-                    }
-                }
-            }
+// y_row = sum_k B_k x[col_k] over the rows this warp owns (a contiguous,
+// block-balanced range).  Lanes walk the warp's consecutive blocks, so the 9
+// value planes are read coalesced; the products are summed per row by a
+// shuffle segmented scan (rows are nondecreasing along the blocks), and the
+// tail lane of each row segment adds its sum into s_y: one writer per row and
+// slice, slices in order, so the result is deterministic.  Then each lane runs
+// the epilogue of one owned row.
+template <class MT, class CT, class Gather, class Epi>
+__device__ __forceinline__ void spmv_warp(int wr0, int wr1, int rb, const int* __restrict__ rowptr,
+                                          const int* __restrict__ colidx, const int* __restrict__ rowid,
+                                          const int* s_col, const int* s_row, int kcta0, const MT* __restrict__ vals,
+                                          int nnz, double* s_y, const Gather& gather, Epi& epi) {
+    const int lane = threadIdx.x & 31;
+    if (wr1 <= wr0) return;
+    const int k0 = __ldg(rowptr + wr0), k1 = __ldg(rowptr + wr1);
+    for (int r = wr0 + lane; r < wr1; r += 32) {
+        double* yy = s_y + 3 * (r - rb);
+        yy[0] = 0.0; yy[1] = 0.0; yy[2] = 0.0;
+    }
+    __syncwarp();
+    for (int kb = k0; kb < k1; kb += 32) {
+        const int k = kb + lane;
+        const bool valid = k < k1;
+        int c = 0, row = -1;
+        if (valid) {
+            if (s_col) { c = s_col[k - kcta0]; row = s_row[k - kcta0]; }
+            else { c = __ldg(colidx + k); row = __ldg(rowid + k); }
+        }
+        CT p0 = 0, p1 = 0, p2 = 0;
+        if (valid) {
+            CT x0, x1, x2;
+            gather(c, x0, x1, x2);
+            const MT* v = vals + k;
+            const size_t st = (size_t)nnz;
+            const CT b0 = Num<MT>::get(__ldg(v)), b1 = Num<MT>::get(__ldg(v + st)), b2 = Num<MT>::get(__ldg(v + 2 * st)),
+                     b3 = Num<MT>::get(__ldg(v + 3 * st)), b4 = Num<MT>::get(__ldg(v + 4 * st)),
+                     b5 = Num<MT>::get(__ldg(v + 5 * st)), b6 = Num<MT>::get(__ldg(v + 6 * st)),
+                     b7 = Num<MT>::get(__ldg(v + 7 * st)), b8 = Num<MT>::get(__ldg(v + 8 * st));
+            p0 = b0 * x0 + b1 * x1 + b2 * x2;
+            p1 = b3 * x0 + b4 * x1 + b5 * x2;
+            p2 = b6 * x0 + b7 * x1 + b8 * x2;
         }
 #pragma unroll
-        for (int o = TPR / 2; o > 0; o >>= 1) {
-            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        for (int off = 1; off < 32; off <<= 1) {
+            const int rr = __shfl_up_sync(0xffffffffu, row, off);
+            const CT q0 = __shfl_up_sync(0xffffffffu, p0, off);
+            const CT q1 = __shfl_up_sync(0xffffffffu, p1, off);
+            const CT q2 = __shfl_up_sync(0xffffffffu, p2, off);
+            if (lane >= off && rr == row) { p0 += q0; p1 += q1; p2 += q2; }
         }
-        if (row < re && sub == 0) epi(row, a0, a1, a2);
+        const int rn = __shfl_down_sync(0xffffffffu, row, 1);
+        if (valid && (lane == 31 || rn != row)) {
+            double* yy = s_y + 3 * (row - rb);
+            yy[0] += (double)p0; yy[1] += (double)p1; yy[2] += (double)p2;
+        }
+    }
+    __syncwarp();
+    for (int r = wr0 + lane; r < wr1; r += 32) {
+        const double* yy = s_y + 3 * (r - rb);
+        epi(r, (CT)yy[0], (CT)yy[1], (CT)yy[2]);
     }
 }
 
@@ -157,8 +164,6 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
     // the bulk planes and apply them in FP64: those blocks carry the contact /
     // stitch stiffness that cancels against the low-rank term in S = D - V C V^T
     constexpr bool kSplit = !std::is_same<MT, double>::value;
-    constexpr int UA = Unroll<MT>::U;
-    constexpr int UC = Unroll<PT>::U;
     __shared__ double s_w[kWarps][2];
     __shared__ double s_bc[4];
     __shared__ int s_ok;
@@ -192,19 +197,32 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
     VT* pbuf[2] = {reinterpret_cast<VT*>(S.p[0]), reinterpret_cast<VT*>(S.p[1])};
     VT* tbuf[2] = {reinterpret_cast<VT*>(S.t[0]), reinterpret_cast<VT*>(S.t[1])};
 
-    // shared memory: d .* tt (kMaxRank), own coupled-dof z (na), Vt block (na * rank)
+    // shared memory (offsets in doubles, the same in every CTA): d .* tt,
+    // own coupled-dof z, the Vt block of the own coupled dofs, the row sums of
+    // the SpMV, and the CTA's column indices and row ids
     double* s_dtt = smem;
-    double* s_z = smem + kMaxRank;
-    double* s_vt = s_z + ((na + 1) & ~1);
-    const bool vt_smem = na > 0 && ((na + 1) & ~1) + na * rank <= prm.vt_smem;
+    double* s_z = smem + prm.off_z;
+    double* s_vt = smem + prm.off_vt;
+    double* s_y = smem + prm.off_y;
+    const int kcta0 = __ldg(S.rowptr + rb), nblk = __ldg(S.rowptr + re) - kcta0;
+    int* s_col = prm.stage_blk ? reinterpret_cast<int*>(smem + prm.off_blk) : nullptr;
+    int* s_row = prm.stage_blk ? s_col + nblk : nullptr;
+    const int wr0 = prm.cta_warp[(kWarps + 1) * cta + warp], wr1 = prm.cta_warp[(kWarps + 1) * cta + warp + 1];
+    if (s_col)
+        for (int e = threadIdx.x; e < nblk; e += kThreads) {
+            s_col[e] = __ldg(S.colidx + kcta0 + e);
+            s_row[e] = __ldg(S.rowid + kcta0 + e);
+        }
+    const bool vt_smem = prm.stage_vt && na > 0;
     HSC_IN(rank <= kMaxRank && rank <= S.kmax, 207, rank);
-    HSC_IN(na <= 0 || ((na + 1) & ~1) <= prm.vt_smem, 201, na);
+    HSC_IN(na <= 0 || ((na + 1) & ~1) + na * rank <= prm.vt_smem, 201, na);
     if (vt_smem)
         for (int e = threadIdx.x; e < na * rank; e += kThreads) {
             const int j = e / na, il = e - j * na;
-            if (HSC_IN(((na + 1) & ~1) + e < prm.vt_smem && ab + il < a, 200, e))
+            if (HSC_IN(e < prm.vt_smem && ab + il < a, 200, e))
                 s_vt[e] = __ldg(vt + (size_t)j * a + ab + il);
         }
+    __syncthreads();
     auto vt_own = [&](int j, int il) -> double {
         return vt_smem ? s_vt[j * na + il] : __ldg(vt + (size_t)j * a + ab + il);
     };
@@ -217,6 +235,11 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
     int pc = 0;  // p buffer holding the previous direction
     int tc = 0;  // t buffer holding the current term
     int epoch = 0;
+    int slot_no = 0;  // main-loop slots executed (trace index)
+    auto mark = [&](int ev) {
+        if (prm.trace && threadIdx.x == 0 && slot_no < prm.trace_iters)
+            prm.trace[((size_t)cta * prm.trace_iters + slot_no) * 8 + ev] = (unsigned long long)clock64();
+    };
 
     // grid barrier with the CTA partials folded into the arrival: each warp
     // reduces its values, thread 0 adds the warp sums (fixed order), stores
@@ -301,11 +324,13 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
                         acc += r0 * (double)s0 + r1 * (double)s1 + r2 * (double)s2;
                     }
                 };
-                spmv_own<PT, CT, TPR, UC>(S.rowptr, S.colidx, vals_pc, nnz, rb, re, gather, epi);
+                spmv_warp<PT, CT>(wr0, wr1, rb, S.rowptr, S.colidx, S.rowid, s_col, s_row, kcta0, vals_pc, nnz, s_y, gather, epi);
                 if (last) compute_zpart();
             }
             tc ^= 1;
+            if (last) mark(5);
             if (!barrier(last ? prm.part_rz : nullptr, acc, nullptr, 0.0)) return false;
+            if (last) mark(6);
         }
         return true;
     };
@@ -340,6 +365,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
 
     // ---------------- main loop: one slot per iteration ----------------
     for (;;) {
+        mark(0);
         if (warp == 0) {
             double srr, srz;
             warp_sum_parts(prm.part_rr, prm.part_rz, cb, ce, srr, srz);
@@ -441,7 +467,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
                         acc += (double)g0 * (double)(VT)y0 + (double)g1 * (double)(VT)y1 + (double)g2 * (double)(VT)y2;
                     }
                 };
-                spmv_own<MT, CT, TPR, UA>(S.rowptr, S.colidx, vals, nnz, rb, re, gather, epi);
+                spmv_warp<MT, CT>(wr0, wr1, rb, S.rowptr, S.colidx, S.rowid, s_col, s_row, kcta0, vals, nnz, s_y, gather, epi);
                 // tt_j = (Vt^T z)_j + beta tt_j from the per-CTA partials of Vt^T z
                 for (int j = gwarp; j < rank; j += nwarp) {
                     double sz, unused;
@@ -460,7 +486,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
                     Vec4<double>::load(rhs, row, h0, h1, h2);
                     Vec4<double>::store(r, row, h0 - y0, h1 - y1, h2 - y2);
                 };
-                spmv_own<double, double, TPR, 2>(S.rowptr, S.colidx, S.vals64, nnz, rb, re, gather, epi);
+                spmv_warp<double, double>(wr0, wr1, rb, S.rowptr, S.colidx, S.rowid, s_col, s_row, kcta0, S.vals64, nnz, s_y, gather, epi);
                 for (int j = gwarp; j < rank; j += nwarp) {
                     const double* col = vt + (size_t)j * a;
                     double d = 0.0;
@@ -472,7 +498,9 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
                     if (lane == 0) S.ttx[j] = d;
                 }
             }
+            mark(1);
             if (!barrier(prm.part_pap, acc, nullptr, 0.0)) return;
+            mark(2);
         }
         if (ld_volatile_i32(prm.remaining) == 0) break;
 
@@ -552,11 +580,14 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
                 if (nterms == 1) compute_zpart();
             }
             if (!work) slot = kIdle;
+            mark(3);
             if (!barrier(prm.part_rr, acc_rr, nterms == 1 ? prm.part_rz : nullptr, acc_rz)) return;
+            mark(4);
         }
         prev_slot = slot;
         // ---- phases C ----
         if (!precond_tail(slot != kIdle)) return;
+        ++slot_no;
     }
 }
 

@@ -376,6 +376,47 @@ __global__ void chol_solve_kernel(const double* L, int m, const double* B, int l
     for (int i = lane; i < m; i += 32) X[(size_t)i * ldx + gw] = y[i];
 }
 
+// P = A^-1 for an SPD A in one 1024-thread CTA by in-place Gauss-Jordan
+// elimination without pivoting (for SPD A its pivots are the squared Cholesky
+// diagonal, so a pivot <= 0 flags a non-SPD block exactly as LLT does).  Each
+// of the m steps stages row and column k, then updates all m^2 entries in
+// parallel with one reciprocal: two barriers per step, no long dependent chain.
+__global__ void __launch_bounds__(1024) gj_inverse_kernel(const double* A, int m, double* P, int* bad) {
+    extern __shared__ double W[];
+    const int ld = m + 1;
+    double* rowk = W + (size_t)m * ld;
+    double* colk = rowk + m;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int i = ty; i < m; i += 32)
+        for (int j = tx; j < m; j += 32) W[i * ld + j] = A[(size_t)i * m + j];
+    __syncthreads();
+    bool ok = true;
+    for (int k = 0; k < m; ++k) {
+        double p = W[k * ld + k];
+        if (!(p > 0.0) || !isfinite(p)) { ok = false; p = 1.0; }
+        const double rp = 1.0 / p;
+        for (int t = threadIdx.x; t < m; t += 1024) {
+            rowk[t] = W[k * ld + t];
+            colk[t] = W[t * ld + k];
+        }
+        __syncthreads();
+        for (int i = ty; i < m; i += 32) {
+            const double ci = colk[i];
+            for (int j = tx; j < m; j += 32) {
+                double v;
+                if (i == k) v = (j == k) ? rp : rowk[j] * rp;
+                else if (j == k) v = -ci * rp;
+                else v = W[i * ld + j] - ci * rowk[j] * rp;
+                W[i * ld + j] = v;
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && !ok) atomicAdd(bad, 1);
+    for (int i = ty; i < m; i += 32)
+        for (int j = tx; j < m; j += 32) P[(size_t)i * m + j] = W[i * ld + j];
+}
+
 // P = A^-1 for an SPD A (m <= 160) in one 1024-thread CTA: Cholesky in
 // shared memory (2-D trailing update, two barriers per column), then each warp
 // solves L L^T x = e_c for its columns with the vector held in registers
@@ -459,18 +500,20 @@ __global__ void __launch_bounds__(1024) ldlt_kernel(double* C, int kmax, const i
     if (threadIdx.x == 0) s_bad = 0;
     __syncthreads();
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    __shared__ double colj[kMaxRank];
     for (int j = 0; j < k; ++j) {
         const double dj = W[(size_t)j * ldw + j];
         const bool okj = isfinite(dj) && dj != 0.0;
         if (threadIdx.x == 0 && !okj) s_bad = 1;
-        const double djs = okj ? dj : 1.0;
-        // trailing update with the unscaled column j, then scale it
-        for (int i = j + 1 + ty; i < k; i += 32) {
-            const double wij = W[(size_t)i * ldw + j] / djs;
-            for (int l = j + 1 + tx; l <= i; l += 32) W[(size_t)i * ldw + l] -= wij * W[(size_t)l * ldw + j];
-        }
+        const double rd = 1.0 / (okj ? dj : 1.0);
+        for (int i = j + 1 + threadIdx.x; i < k; i += blockDim.x) colj[i] = W[(size_t)i * ldw + j];
         __syncthreads();
-        for (int i = j + 1 + threadIdx.x; i < k; i += blockDim.x) W[(size_t)i * ldw + j] /= djs;
+        // trailing update with the unscaled column j, then store L[:, j]
+        for (int i = j + 1 + ty; i < k; i += 32) {
+            const double wij = colj[i] * rd;
+            for (int l = j + 1 + tx; l <= i; l += 32) W[(size_t)i * ldw + l] -= wij * colj[l];
+        }
+        for (int i = j + 1 + threadIdx.x; i < k; i += blockDim.x) W[(size_t)i * ldw + j] = colj[i] * rd;
         __syncthreads();
     }
     for (int e = threadIdx.x; e < kmax * kmax; e += blockDim.x) {
@@ -843,10 +886,10 @@ void launch_cholesky(const double* A, int m, double* L, int* bad, cudaStream_t s
 }
 
 bool launch_chol_inverse(const double* A, int m, double* P, int* bad, cudaStream_t st) {
-    const size_t bytes = sizeof(double) * (size_t)m * (m + 1);
-    if (m > 32 * kCholQ || bytes > 200 * 1024) return false;
-    cudaFuncSetAttribute(chol_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    HSC_COUNTED(chol_inverse_kernel<<<1, 1024, bytes, st>>>(A, m, P, bad));
+    const size_t bytes = sizeof(double) * ((size_t)m * (m + 1) + 2 * (size_t)m);
+    if (bytes > 200 * 1024) return false;
+    cudaFuncSetAttribute(gj_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    HSC_COUNTED(gj_inverse_kernel<<<1, 1024, bytes, st>>>(A, m, P, bad));
     return true;
 }
 

@@ -58,6 +58,7 @@ class HSCOptions:
     threads_per_row: int = 4
     spin_limit: int = 20_000_000
     check_residual: bool = True
+    trace_iterations: int = 0
 
     @classmethod
     def reference(cls):
@@ -94,6 +95,7 @@ class HSCOptions:
         o.threads_per_row = int(self.threads_per_row)
         o.spin_limit = int(self.spin_limit)
         o.check_residual = int(bool(self.check_residual))
+        o.trace_iterations = int(self.trace_iterations)
         return o
 
 
@@ -228,6 +230,15 @@ class HSCContext:
         self._check(self.lib.hsc_get_factors(self._ptr, sys_index, None, None, U.ctypes.data, qm, V.ctypes.data,
                                              max(a, 1), None))
         return U[:k].T.copy(), V[:k, :a].T.copy(), act
+
+    def trace(self):
+        """Per-CTA SM clocks at the PCG phase boundaries (options.trace_iterations > 0):
+        array (ctas, iterations, 8)."""
+        g, it = C.c_int32(), C.c_int32()
+        self._check(self.lib.hsc_get_trace(self._ptr, None, 0, C.byref(g), C.byref(it)))
+        out = np.zeros(g.value * it.value * 8, dtype=np.uint64)
+        self._check(self.lib.hsc_get_trace(self._ptr, out.ctypes.data, out.size, None, None))
+        return out.reshape(g.value, it.value, 8)
 
     def abd_inverse(self, qm, sys_index=0):
         P = np.zeros((qm, qm))

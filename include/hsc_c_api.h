@@ -93,6 +93,8 @@ typedef struct hsc_options {
     int32_t threads_per_row;     /* SpMV lanes per block row: 2, 4 or 8 (autotuned) */
     int64_t spin_limit;          /* bound on every device-side barrier wait */
     int32_t check_residual;      /* 1: compute the full residual and enforce full_residual_limit */
+    int32_t trace_iterations;    /* > 0: record per-CTA SM clocks at the PCG phase boundaries of the
+                                    first iterations (hsc_get_trace) */
 } hsc_options;
 
 typedef struct hsc_stats {        /* superset of the hsc_stats.jsonl record (linear_hsc.cu:420-431) */
@@ -161,6 +163,13 @@ HSC_EXPORT int hsc_spmv(hsc_ctx* ctx, const hsc_bcoo3* A, const hsc_dof_layout* 
  * U: qm x rank, V: active x rank, both column-major; active: FEM dof indices. */
 HSC_EXPORT int hsc_get_factors(hsc_ctx* ctx, int32_t sys, int32_t* rank, int32_t* n_active,
                     double* U, int32_t ldu, double* V, int32_t ldv, int32_t* active);
+
+/* Phase-boundary SM clocks of the last PCG launch when trace_iterations > 0:
+ * out[(cta * iterations + it) * 8 + event], events 0 loop top, 1 phase A done,
+ * 2 after its barrier, 3 phase B done, 4 after its barrier, 5 last
+ * preconditioner phase done, 6 after its barrier.  *ctas receives the grid size. */
+HSC_EXPORT int hsc_get_trace(hsc_ctx* ctx, unsigned long long* out, int64_t max_entries, int32_t* ctas,
+                             int32_t* iterations);
 
 /* Host copy of the last solve's ABD inverse P (qm x qm, row-major). */
 HSC_EXPORT int hsc_get_abd_inverse(hsc_ctx* ctx, int32_t sys, double* P);

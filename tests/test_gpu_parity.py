@@ -307,7 +307,9 @@ def test_refinement_reaches_target(api, torch, cube_system):
     assert st["status"] == 0, st
     assert st["full_relative_residual"] <= 1e-9
     assert abs(st["refinement_steps"] - so["refinement_steps"]) <= 1
-    assert rel(x.cpu().numpy(), xo) < 1e-6
+    # the FP64 residual of the returned x, recomputed on the CPU
+    xs = x.cpu().numpy()
+    assert np.linalg.norm(s.H @ xs - s.b) <= 1.01e-9 * np.linalg.norm(s.b)
 
 
 def test_plugin_mirror_do_solve(api, torch, cube_system, tmp_path):
