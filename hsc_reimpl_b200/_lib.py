@@ -107,6 +107,7 @@ EXPORTS = {
                                   C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int32, C.c_void_p,
                                   C.POINTER(Stats)]),
     "hsc_spmv": (C.c_int, [C.c_void_p, C.POINTER(BCOO3), C.POINTER(Layout), C.c_void_p, C.c_void_p, C.c_void_p]),
+    "hsc_spmv_noalloc": (C.c_int, [C.POINTER(BCOO3), C.c_void_p, C.c_void_p, C.c_void_p]),
     "hsc_get_factors": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                   C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p]),
     "hsc_get_abd_inverse": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),

@@ -159,6 +159,16 @@ HSC_EXPORT int hsc_solve_batch(hsc_ctx* ctx, int32_t count, const hsc_bcoo3* A, 
 HSC_EXPORT int hsc_spmv(hsc_ctx* ctx, const hsc_bcoo3* A, const hsc_dof_layout* layout,
              const double* d_x, double* d_y, void* stream);
 
+/* y = H x like hsc_spmv, but with no context and no device allocation, for
+ * callers that cannot allocate when they need the product (a fixed up-front
+ * memory pool, or a loop that must not take cudaFree's device-wide sync).  It
+ * accumulates in a static 8 MiB device array of this library, so at most
+ * 1,048,576 dofs (3 * nblock); larger systems get HSC_ERR_INVALID.  Calls that
+ * overlap on the GPU share that array and race; the first call on a device
+ * looks up the array's address and should come before any stream capture.
+ * y may alias x.  This entry point has no counterpart in the reference. */
+HSC_EXPORT int hsc_spmv_noalloc(const hsc_bcoo3* A, const double* d_x, double* d_y, void* stream);
+
 /* Host copies of the last solve's coupling factors (tests / diagnostics).
  * U: qm x rank, V: active x rank, both column-major; active: FEM dof indices. */
 HSC_EXPORT int hsc_get_factors(hsc_ctx* ctx, int32_t sys, int32_t* rank, int32_t* n_active,
