@@ -37,9 +37,9 @@ sys.path.insert(0, HERE)
 METRIC = "HSC solves/s & PCG iters to rel-res 1e-6: learned/FP32 vs plain FP64, 1 B200"
 UNIT = "solves/s"
 TARGET = 1e-6
-# DRAM bytes of one PCG launch on the vehicle workload from an ncu capture
-# (profiles/pcg_kernel_vehicle.md); null until captured
-NCU_TRAFFIC_PER_ITER = None
+# DRAM bytes per PCG iteration on the vehicle workload from an ncu capture
+# (profiles/pcg_kernel_vehicle.md: 21.75 MB read + 0.99 MB written over 204 iterations)
+NCU_TRAFFIC_PER_ITER = (21.747456e6 + 0.990976e6) / 204
 
 
 def parse():
@@ -60,6 +60,20 @@ def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return ws, rank, local
+
+
+def max_over_ranks(ms, dist, device):
+    """The slowest rank's device time (every rank takes this same collective)."""
+    import torch
+    el = torch.tensor([ms], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(el, op=dist.ReduceOp.MAX)
+    return float(el.item())
+
+
+def replica_throughput(steps, ws, max_ms):
+    """Whole-job solves/s: every rank solved `steps` systems within `max_ms`."""
+    return ws * steps / (max_ms / 1000.0)
 
 
 def workload_config(s):
@@ -272,10 +286,7 @@ def run_gpu(args):
             clocks = sampler.stop()
         if mi == 0:
             launches = lib.hsc_kernel_launches() - l0
-        el = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        if dist is not None:
-            dist.all_reduce(el, op=dist.ReduceOp.MAX)
-        total_ms = float(el.item())
+        total_ms = max_over_ranks(total_ms, dist, dev)
         last = stats_all[-1]
         xs = x.cpu().numpy()
         ok = all(t["status"] == 0 and t["full_relative_residual"] <= TARGET for t in stats_all)
@@ -283,7 +294,7 @@ def run_gpu(args):
         bytes_iter = pcg_bytes_per_iteration(last, s, mode, 2)
         pcg_launch_ms = pcg_ms / args.steps
         modes[mode] = {
-            "solves_per_s": ws * args.steps / (total_ms / 1000.0),
+            "solves_per_s": replica_throughput(args.steps, ws, total_ms),
             "ms_per_solve": total_ms / args.steps,
             "pcg_iterations": iters,
             "full_relative_residual": max(t["full_relative_residual"] for t in stats_all),
@@ -348,11 +359,8 @@ def run_gpu(args):
             ev1.record()
             torch.cuda.synchronize()
             tot += ev0.elapsed_time(ev1)
-        el = torch.tensor([tot], dtype=torch.float64, device=dev)
-        if dist is not None:
-            dist.all_reduce(el, op=dist.ReduceOp.MAX)
-        tot = float(el.item())
-        e2e = {"value": ws * args.steps / (tot / 1000.0), "unit": UNIT,
+        tot = max_over_ranks(tot, dist, dev)
+        e2e = {"value": replica_throughput(args.steps, ws, tot), "unit": UNIT,
                "h2d_bytes_per_step": int(vals_h.numel() * 8 + b_h.numel() * 8),
                "d2h_bytes_per_step": int(x_h.numel() * 8), "mode": flag}
     cpu = None

@@ -249,8 +249,9 @@ class HSCContext:
 # ----------------------------------------------------------------------------
 # the plugin mirror
 # ----------------------------------------------------------------------------
-CONFIG_DEFAULTS = {                         # integration.patch:33-54
-    "linear_system/solver": "linear_hsc",
+# integration.patch:33-54.  "linear_system/solver" has no default here: the
+# plugin is selected only by an explicit "linear_hsc" (linear_hsc.cu:174-176).
+CONFIG_DEFAULTS = {
     "linear_system/tol_rate": 1e-4,
     "linear_system/hsc/max_rank": 128,
     "linear_system/hsc/neumann_order": 5,

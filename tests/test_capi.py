@@ -80,3 +80,7 @@ def test_plugin_selection_mirrors_do_build():
     from hsc_reimpl_b200.solver import LinearHSC, SimSystemException
     with pytest.raises(SimSystemException):
         LinearHSC().do_build({"linear_system/solver": "fused_pcg"})
+    with pytest.raises(SimSystemException):
+        LinearHSC().do_build({})                       # no solver key: not selected
+    with pytest.raises(ValueError, match="Invalid HSC parameters"):
+        LinearHSC().do_build({"linear_system/solver": "linear_hsc", "linear_system/hsc/omega": 1.5})
