@@ -80,19 +80,25 @@ class LinearHSC final : public IterativeSolver {
 
     void append_record(int rc) {
         std::ofstream out(workspace() + "/hsc_stats.jsonl", std::ios::app);
-        char buf[1024];
+        char buf[2048];
         std::snprintf(buf, sizeof buf,
                       "{\"frame\":%zu,\"newton\":%zu,\"fem_dofs\":%d,\"abd_dofs\":%d,\"active_fem_dofs\":%d,"
                       "\"rank\":%d,\"aca_relative_error\":%.17g,\"pcg_iterations\":%d,"
                       "\"schur_relative_residual\":%.17g,\"full_relative_residual\":%.17g,\"setup_ms\":%.6g,"
                       "\"total_ms\":%.6g,\"active_mesh_contacts\":0,\"active_ground_contacts\":0,"
                       "\"adaptive_abd_inverse\":%s,\"neumann_doublings\":%d,\"abd_inverse_residual\":%.17g,"
-                      "\"full_residual_limit\":%.17g,\"accepted\":%s,\"solver\":\"linear_hsc\",\"fallback\":false}\n",
+                      "\"full_residual_limit\":%.17g,\"accepted\":%s,\"solver\":\"linear_hsc\",\"fallback\":%s,"
+                      "\"precision_mode\":\"%s\",\"preconditioner\":\"%s\",\"refinement_steps\":%d,"
+                      "\"pcg_ms\":%.6g,\"lanczos_min\":%.17g,\"lanczos_max\":%.17g}\n",
                       engine().frame, engine().newton, stats.fem_dofs, stats.abd_dofs, stats.active_fem_dofs,
                       stats.rank, stats.aca_relative_error, stats.pcg_iterations, stats.schur_relative_residual,
                       stats.full_relative_residual, stats.setup_ms, stats.total_ms,
                       opt.abd_inverse == HSC_ABD_ADAPTIVE ? "true" : "false", stats.neumann_doublings,
-                      stats.abd_inverse_residual, opt.full_residual_limit, rc == HSC_OK ? "true" : "false");
+                      stats.abd_inverse_residual, opt.full_residual_limit, rc == HSC_OK ? "true" : "false",
+                      stats.fallback ? "true" : "false",
+                      stats.precision == HSC_BF16 ? "bf16" : stats.precision == HSC_FP32 ? "fp32" : "fp64",
+                      stats.preconditioner == HSC_PRECOND_POLY ? "polynomial" : "neumann", stats.refinement_steps,
+                      stats.pcg_ms, stats.lanczos_min, stats.lanczos_max);
         out << buf;
     }
 };
