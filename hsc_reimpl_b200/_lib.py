@@ -29,8 +29,9 @@ STATUS_NAMES = {0: "ok", 1: "invalid", 2: "nonspd", 3: "breakdown", 4: "noconv",
 
 HSC_FP64, HSC_FP32, HSC_BF16 = 0, 1, 2
 HSC_ABD_NEUMANN, HSC_ABD_ADAPTIVE, HSC_ABD_EXACT = 0, 1, 2
-HSC_PRECOND_NEUMANN, HSC_PRECOND_POLY = 0, 1
+HSC_PRECOND_NEUMANN, HSC_PRECOND_POLY, HSC_PRECOND_SCHUR_POLY, HSC_PRECOND_LEARNED = 0, 1, 2, 3
 HSC_MAX_POLY = 16
+HSC_FEATURES, HSC_MLP_HIDDEN, HSC_MLP_OUT, HSC_MLP_PARAMS = 16, 64, 8, 5768
 
 
 class Options(C.Structure):
@@ -115,6 +116,18 @@ EXPORTS = {
     "hsc_version": (C.c_int, []),
     "hsc_kernel_launches": (C.c_longlong, []),
     "hsc_debug_checks": (C.c_int, [C.POINTER(C.c_longlong)]),
+    "hsc_set_learned_model": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "hsc_get_features": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "hsc_get_poly_weights": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
+    "hsc_get_lanczos": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
+    "hsc_mlp_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_void_p]),
+    "hsc_mlp_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "hsc_poly_ls_loss": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_float,
+                                   C.c_void_p, C.c_void_p, C.c_void_p]),
+    "hsc_adam_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_float,
+                                C.c_float, C.c_float, C.c_float, C.c_float, C.c_int32, C.c_void_p]),
 }
 
 _LIB = None

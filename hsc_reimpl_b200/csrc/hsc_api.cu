@@ -12,6 +12,7 @@
 //   one D2H copy of the per-system scalars, then the status checks of
 //   linear_hsc.cu:394-435.
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -20,6 +21,7 @@
 #include <vector>
 
 #include "../../include/hsc_c_api.h"
+#include "hsc_learned.cuh"
 #include "hsc_setup.cuh"
 
 using namespace hsc;
@@ -69,6 +71,9 @@ struct DevScal {
     int bad_abd;              // non-SPD ABD blocks
     int bad_ldlt;             // zero / non-finite reduced-core pivot
     int pad[4];
+    double prev[kPrev];       // record of the previous solve (learned-model features)
+    double wl[16];            // learned polynomial weights of this solve
+    float feat[kFeat];        // features of this solve
 };
 
 struct System {
@@ -89,8 +94,11 @@ struct System {
     // numeric
     DevBuf v64, vf32, vbf16, dinv, A, E, R0, R1, U, V, hist, P, Ptmp, T, term, Binv, L, W, C, Lc, dpiv, vt64, vtmt,
         cvec, tt, ttx, bq, bf, x, r, z, p0, p1, y, t0, t1, node_nz, xq, ypad, yq, work, cg, scal, dact, pact, yact,
-        zpart;
+        zpart, tpart;
     DevBuf dvec[4];           // contiguous-N scratch for refinement
+    double h_last[kPrev] = {};   // record of the last solve: 1, lanczos min, max, iterations, q(0)
+    double h_prevrec[kPrev] = {};// record the features of the current solve see
+    double h_cg[2 * kMaxCoef] = {};
     DevScal h_scal{};
     std::vector<int> h_node_nz;
     bool aca_on_cluster = false;
@@ -119,6 +127,8 @@ struct hsc_ctx {
     size_t aca_cluster_smem = 0;
     int aca_cluster_ok = -1;   // the device can schedule a 16-CTA cluster of the ACA kernel
     DevBuf res_part;
+    DevBuf mlp, feat_part;     // learned model (BF16 parameters), feature partials
+    bool has_model = false;
     cudaEvent_t ev[9] = {};
     bool stage_events = false;  // record the per-stage events (single system, no graph)
     // graph cache (batch)
@@ -162,7 +172,12 @@ int validate_options(const hsc_options* o, std::string& why) {
     if (!(o->tol >= 0)) { why = "tol must be >= 0"; return 0; }
     if (o->precision < 0 || o->precision > 2) { why = "unknown precision"; return 0; }
     if (o->abd_inverse < 0 || o->abd_inverse > 2) { why = "unknown abd_inverse"; return 0; }
-    if (o->preconditioner == HSC_PRECOND_POLY && (o->poly_degree < 1 || o->poly_degree > HSC_MAX_POLY)) {
+    if (o->preconditioner < HSC_PRECOND_NEUMANN || o->preconditioner > HSC_PRECOND_LEARNED) {
+        why = "unknown preconditioner";
+        return 0;
+    }
+    if ((o->preconditioner == HSC_PRECOND_POLY || o->preconditioner == HSC_PRECOND_SCHUR_POLY) &&
+        (o->poly_degree < 1 || o->poly_degree > HSC_MAX_POLY)) {
         why = "poly_degree must be in [1, 16]";
         return 0;
     }
@@ -353,9 +368,11 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
     GROW(S.ypad, sizeof(double) * n4);
     GROW(S.yq, sizeof(double) * qm);
     GROW(S.work, sizeof(double) * qm * qm);
-    GROW(S.cg, sizeof(double) * 2 * 64);
+    GROW(S.cg, sizeof(double) * 2 * kMaxCoef);
     GROW(S.scal, sizeof(DevScal));
-    const size_t N = 3 * (size_t)M.nblock;
+    // contiguous-N vectors; dvec[3] also holds the node-padded x (4 doubles per
+    // node) that full_spmv_contig gathers, which is longer than N when n > qm
+    const size_t N = std::max(3 * (size_t)M.nblock, n4);
     for (auto& d : S.dvec) GROW(d, sizeof(double) * N);
     if (S.qm) {
         std::vector<double> I((size_t)S.qm * S.qm, 0.0);
@@ -466,7 +483,7 @@ int numeric_pre(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, cudaStream_t st) {
     const int P = ctx->opt.precision;
     DevScal* ds = S.scal.as<DevScal>();
     S.h_scal.pcg[7] = 0;
-    CK(cudaMemsetAsync(ds, 0, sizeof(DevScal), st));
+    CK(cudaMemsetAsync(ds, 0, offsetof(DevScal, prev), st));  // the previous-solve record stays
     launch_pattern_hash(M.d_rows, M.d_cols, M.nnzb, &ds->hash, st);
     float* vf = P ? S.vf32.as<float>() : nullptr;
     __nv_bfloat16* vb = P == 2 ? S.vbf16.as<__nv_bfloat16>() : nullptr;
@@ -641,9 +658,12 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
         d.pact = S.pact.as<double>(); d.yact = S.yact.as<double>(); d.ttx = S.ttx.as<double>();
         GROW(S.zpart, sizeof(double) * std::max(1, S.kmax) * (size_t)(c - b));
         d.zpart = S.zpart.as<double>();
+        GROW(S.tpart, sizeof(double) * 2 * std::max(1, S.kmax) * (size_t)(c - b));
+        d.tpart = S.tpart.as<double>();
+        d.wdev = o.preconditioner == HSC_PRECOND_LEARNED ? S.scal.as<DevScal>()->wl : nullptr;
         d.x = S.x.as<double>(); d.r = S.r.as<double>(); d.rhs = S.bf.as<double>(); d.z = S.z.p;
         d.p[0] = S.p0.p; d.p[1] = S.p1.p; d.y = S.y.p; d.t[0] = S.t0.p; d.t[1] = S.t1.p; d.tt = S.tt.as<double>();
-        d.out = S.scal.as<DevScal>()->pcg; d.cg_coef = S.cg.as<double>(); d.max_coef = 64;
+        d.out = S.scal.as<DevScal>()->pcg; d.cg_coef = S.cg.as<double>(); d.max_coef = kMaxCoef;
     }
     // warp-owned row ranges: kWarps + 1 boundaries per CTA, balanced by blocks
     std::vector<int> cta_warp((size_t)(kWarps + 1) * G);
@@ -755,9 +775,13 @@ int launch_pcg_all(hsc_ctx* ctx, int nsys, cudaStream_t st) {
     prm.bar = ctx->d_bar.as<GridBar>();
     prm.remaining = ctx->d_remaining.as<int>();
     prm.omega = o.omega;
-    if (o.preconditioner == HSC_PRECOND_POLY) {
+    prm.schur_basis = o.preconditioner == HSC_PRECOND_SCHUR_POLY || o.preconditioner == HSC_PRECOND_LEARNED;
+    if (o.preconditioner == HSC_PRECOND_POLY || o.preconditioner == HSC_PRECOND_SCHUR_POLY) {
         prm.nterms = o.poly_degree;
         for (int k = 0; k < o.poly_degree; ++k) prm.w[k] = o.poly_weights[k];
+    } else if (o.preconditioner == HSC_PRECOND_LEARNED) {
+        prm.nterms = kPolyOut;                 // weights from the device (SysDesc::wdev)
+        for (int k = 0; k < kPolyOut; ++k) prm.w[k] = 1.0;
     } else {
         prm.nterms = o.neumann_order;
         for (int k = 0; k < o.neumann_order; ++k) prm.w[k] = 1.0;
@@ -882,6 +906,7 @@ int ensure_common(hsc_ctx* ctx, cudaStream_t st) {
     GROW(ctx->aca_pidx, sizeof(long long) * 4096);
     GROW(ctx->aca_bar, sizeof(GridBar));
     GROW(ctx->res_part, sizeof(double) * 3 * kResParts);
+    GROW(ctx->feat_part, sizeof(double) * kFeatParts * 2 * std::max(1, ctx->num_sms));
     if (!ctx->aca_grid) ctx->aca_grid = std::min(4096, std::max(1, aca_blocks_per_sm()) * ctx->num_sms);
     if (!ctx->ev[0])
         for (auto& e : ctx->ev) CK(cudaEventCreate(&e));
@@ -905,6 +930,7 @@ int read_scalars(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st, int
         System& S = ctx->sys[idx[s]];
         S.h_node_nz.resize(S.a / 3);
         if (S.a) CK(cudaMemcpyAsync(S.h_node_nz.data(), S.node_nz.p, sizeof(int) * (S.a / 3), cudaMemcpyDeviceToHost, st));
+        if (S.cg.p) CK(cudaMemcpyAsync(S.h_cg, S.cg.p, sizeof(double) * 2 * kMaxCoef, cudaMemcpyDeviceToHost, st));
     }
     CK(cudaStreamSynchronize(st));
     grid_abort = gb.abort | ga.abort;
@@ -914,6 +940,32 @@ int read_scalars(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st, int
         ctx->sys[idx[s]].h_scal.pcg[7] = d7;
     }
     return HSC_OK;
+}
+
+FeatArgs feat_args(hsc_ctx* ctx, System& S, bool with_model) {
+    DevScal* ds = S.scal.as<DevScal>();
+    FeatArgs f{};
+    f.n = S.n; f.nnz = S.nnz; f.a = S.a; f.kmax = S.kmax;
+    f.rowptr = S.rowptr.as<int>(); f.colidx = S.colidx.as<int>(); f.diag_pos = S.diag_pos.as<int>();
+    f.rowflag = S.rowflag.as<int>(); f.v64 = S.v64.as<double>(); f.rank = &ds->rank;
+    f.vt64 = S.vt64.as<double>(); f.dpiv = S.dpiv.as<double>(); f.prev = ds->prev;
+    f.mlp = with_model ? ctx->mlp.as<uint16_t>() : nullptr;
+    f.feat = ds->feat; f.w = ds->wl;
+    f.part = ctx->feat_part.as<double>();
+    f.nparts = std::max(1, std::min(2 * ctx->num_sms, (S.n + 255) / 256));
+    return f;
+}
+
+// sum of the polynomial weights the current options use for system S (q(0))
+double weight_sum(const hsc_options& o, const System& S) {
+    double w = 0.0;
+    if (o.preconditioner == HSC_PRECOND_LEARNED)
+        for (int k = 0; k < kPolyOut; ++k) w += S.h_scal.wl[k];
+    else if (o.preconditioner == HSC_PRECOND_POLY || o.preconditioner == HSC_PRECOND_SCHUR_POLY)
+        for (int k = 0; k < o.poly_degree; ++k) w += o.poly_weights[k];
+    else
+        w = o.neumann_order;
+    return w;
 }
 
 int prepare_system(hsc_ctx* ctx, int s, const hsc_bcoo3& M, const hsc_dof_layout& L, cudaStream_t st, bool& reanalyzed) {
@@ -1057,6 +1109,14 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
     }
     const bool refine = o.refine_target > 0 && count == 1;
     const bool residual = o.check_residual || refine;
+    const bool learned = o.preconditioner == HSC_PRECOND_LEARNED;
+    if (learned && !ctx->has_model) return fail(ctx, HSC_ERR_INVALID, "HSC_PRECOND_LEARNED without a model (hsc_set_learned_model)");
+    // the features of this solve see the record of the previous solve of the same system
+    for (int s = 0; s < count; ++s) {
+        System& S = ctx->sys[s];
+        if (S.h_last[0] > 0.5) std::memcpy(S.h_prevrec, S.h_last, sizeof S.h_prevrec);
+        CK(cudaMemcpyAsync(S.scal.as<DevScal>()->prev, S.h_prevrec, sizeof S.h_prevrec, cudaMemcpyHostToDevice, st));
+    }
     // graph key: every pointer the numeric phase touches
     std::vector<const void*> key;
     for (int s = 0; s < count; ++s) {
@@ -1082,6 +1142,8 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
             if (r2) return r2;
             schur_rhs(ctx->sys[s], d_b[s], st);
         }
+        if (learned)
+            for (int s = 0; s < count; ++s) CK(launch_features(feat_args(ctx, ctx->sys[s], true), st));
         CK(cudaEventRecord(ctx->ev[5], st));
         int r3 = launch_pcg_all(ctx, count, st);
         if (r3) return r3;
@@ -1224,16 +1286,31 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
             for (int i = 0; i < 8; ++i) out[s].stage_ms[i] = ms_stage[i];
             out[s].accepted = st_s == HSC_OK;
             out[s].fallback = 0;
-            double lo = 0, hi = 0;
-            std::vector<double> coef(128);
-            if (cudaMemcpy(coef.data(), S.cg.p, sizeof(double) * 128, cudaMemcpyDeviceToHost) == cudaSuccess) {
-                const int m = std::min(64, std::max(0, (int)S.h_scal.pcg[0]));
-                lanczos_extremes(coef.data(), m, lo, hi);
-            }
-            out[s].lanczos_min = lo;
-            out[s].lanczos_max = hi;
+        }
+        // Lanczos extremes of this solve; they become the next solve's record
+        const int m = std::min(kMaxCoef, std::max(0, (int)S.h_scal.pcg[0]));
+        double lo = 0, hi = 0;
+        lanczos_extremes(S.h_cg, m, lo, hi);
+        if (out) { out[s].lanczos_min = lo; out[s].lanczos_max = hi; }
+        if (m > 0 && lo > 0) {
+            S.h_last[0] = 1.0; S.h_last[1] = lo; S.h_last[2] = hi; S.h_last[3] = S.h_scal.pcg[0];
+            S.h_last[4] = weight_sum(o, S);
         }
         if (st_s && !worst) { worst = st_s; ctx->err = msg; }
+    }
+    // a stalled polynomial / learned preconditioner: redo with the plain Neumann series
+    if (count == 1 && !refine && depth == 0 && o.fallback_on_stall && o.preconditioner != HSC_PRECOND_NEUMANN &&
+        (worst == HSC_ERR_BREAKDOWN || worst == HSC_ERR_NOCONV)) {
+        const hsc_options saved = ctx->opt;
+        ctx->opt.preconditioner = HSC_PRECOND_NEUMANN;
+        ctx->part_key_gen = -1;
+        const int iters_first = out ? out[0].pcg_iterations : 0;
+        const int r = solve_impl(ctx, count, A, lay, d_b, d_x, use_graph, st, out, depth + 1);
+        ctx->opt = saved;
+        ctx->part_key_gen = -1;
+        if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+        if (out) { out[0].fallback = 1; out[0].pcg_iterations += iters_first; }
+        return r;
     }
     return worst;
 }
@@ -1296,6 +1373,50 @@ int hsc_get_trace(hsc_ctx* ctx, unsigned long long* out, int64_t max_entries, in
     if (iterations) *iterations = ctx->opt.trace_iterations;
     if (out) CK(cudaMemcpy(out, ctx->d_trace.p, sizeof(unsigned long long) * std::min(nt, max_entries),
                            cudaMemcpyDeviceToHost));
+    return HSC_OK;
+}
+
+int hsc_set_learned_model(hsc_ctx* ctx, const uint16_t* params_bf16) {
+    if (!ctx || !params_bf16) return HSC_ERR_INVALID;
+    GROW(ctx->mlp, sizeof(uint16_t) * kParams);
+    CK(cudaMemcpy(ctx->mlp.p, params_bf16, sizeof(uint16_t) * kParams, cudaMemcpyHostToDevice));
+    ctx->has_model = true;
+    if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+    return HSC_OK;
+}
+
+int hsc_get_features(hsc_ctx* ctx, int32_t sys, float* out) {
+    if (!ctx || !out || sys < 0 || sys >= (int)ctx->sys.size() || !ctx->sys[sys].analyzed) return HSC_ERR_NOTREADY;
+    System& S = ctx->sys[sys];
+    int rc = ensure_common(ctx, nullptr);
+    if (rc) return rc;
+    CK(launch_features(feat_args(ctx, S, false), nullptr));
+    CK(cudaMemcpy(out, S.scal.as<DevScal>()->feat, sizeof(float) * kFeat, cudaMemcpyDeviceToHost));
+    return HSC_OK;
+}
+
+int hsc_get_poly_weights(hsc_ctx* ctx, int32_t sys, double* out, int32_t max, int32_t* degree) {
+    if (!ctx || sys < 0 || sys >= (int)ctx->sys.size() || !ctx->sys[sys].analyzed) return HSC_ERR_NOTREADY;
+    const hsc_options& o = ctx->opt;
+    const System& S = ctx->sys[sys];
+    std::vector<double> w;
+    if (o.preconditioner == HSC_PRECOND_LEARNED) w.assign(S.h_scal.wl, S.h_scal.wl + kPolyOut);
+    else if (o.preconditioner == HSC_PRECOND_POLY || o.preconditioner == HSC_PRECOND_SCHUR_POLY)
+        w.assign(o.poly_weights, o.poly_weights + o.poly_degree);
+    else w.assign(o.neumann_order, 1.0);
+    if (degree) *degree = (int)w.size();
+    if (out)
+        for (int k = 0; k < std::min<int>(max, (int)w.size()); ++k) out[k] = w[k];
+    return HSC_OK;
+}
+
+int hsc_get_lanczos(hsc_ctx* ctx, int32_t sys, double* coef, int32_t max_pairs, int32_t* pairs) {
+    if (!ctx || sys < 0 || sys >= (int)ctx->sys.size() || !ctx->sys[sys].analyzed) return HSC_ERR_NOTREADY;
+    const System& S = ctx->sys[sys];
+    const int m = std::min(kMaxCoef, std::max(0, (int)S.h_scal.pcg[0]));
+    const int k = std::min<int>(m, std::max(0, max_pairs));
+    if (pairs) *pairs = k;
+    if (coef) std::memcpy(coef, S.h_cg, sizeof(double) * 2 * k);
     return HSC_OK;
 }
 

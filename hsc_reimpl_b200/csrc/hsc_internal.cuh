@@ -177,12 +177,16 @@ struct SysDesc {
     double* pact;          // FP64 direction at the active dofs (a)
     double* yact;          // FP64 S p at the active dofs (a)
     double* zpart;         // kmax x ncta: per-CTA partials of Vt^T z (own active dofs)
+    double* tpart;         // 2 x kmax x ncta: per-CTA partials of Vt^T t_k (Schur-basis terms), by term parity
+    const double* wdev;    // device polynomial weights of this system (learned), or null: PcgParams::w
     double* tt;            // kmax: Vt^T p (recurrence Vt^T z + beta Vt^T p_prev)
     double* ttx;           // kmax: Vt^T x (true-residual slot)
     double* out;           // per-system results [0]=iters [1]=rel [2]=status [3]=normb [4]=replacements
     double* cg_coef;       // 2*max_coef: alpha_k, beta_k for the Lanczos estimate
     int max_coef;
 };
+
+constexpr int kMaxCoef = 256;  // CG coefficients kept per solve for the Lanczos estimates
 
 struct PcgParams {
     const SysDesc* sys;
@@ -198,6 +202,7 @@ struct PcgParams {
     double omega;
     int nterms;                // polynomial terms (Neumann order or poly degree)
     double w[16];              // polynomial weights
+    int schur_basis;           // terms t_k = (I - w Dd^-1 S)^k t_0 on the Schur operator (else on D)
     double tol;
     int max_iter;
     int rr_every;              // residual replacement interval (0 = only at convergence)
@@ -215,6 +220,8 @@ struct PcgParams {
 // launch counter of this library (hsc_setup.cu)
 void count_launch();
 long long launch_count();
+// with HSC_SYNC_CHECK set: synchronise and report the first failing launch
+void debug_sync(const char* what);
 
 // kernel launchers (hsc_pcg.cu)
 cudaError_t launch_pcg(int precision, int tpr, const PcgParams& prm, int grid, size_t smem, cudaStream_t st);

@@ -17,6 +17,12 @@
 //      partial r.z and the CTA's Vt^T z partials after the last term
 //   -- barrier each --
 //
+// With the Schur basis (the learned polynomial) the terms run on S instead of
+// D: t' = t - w Dd^-1 (D t - Vt d Vt^T t).  Every phase that writes a term
+// also leaves the CTA's partials of Vt^T t (ping-pong by term parity), and
+// the next C phase sums them before its SpMV and subtracts the low-rank part
+// at its coupled rows; the barrier count stays the same.
+//
 // so one iteration costs terms+1 barriers and `terms` passes over D.  All
 // scalars are reduced redundantly, in the same order, by every CTA of a
 // system: no floating-point atomics, bit-reproducible results.  The true
@@ -157,7 +163,10 @@ __device__ __forceinline__ void dinv_apply(const DT* __restrict__ dinv, int n, i
 enum SlotKind { kIdle = 0, kNormal = 1, kReplace = 2 };
 
 template <class MT, class PT, class VT, int TPR>
-__global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
+__global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_arg) {
+    // a local copy: the lambdas below capture it by reference, and a reference
+    // to a kernel parameter would be a parameter-space address
+    const PcgParams prm = prm_arg;
     using CT = typename Cmp<MT>::T;
     using DT = typename DinvT<MT>::T;
     // mixed modes keep the diagonal blocks of the coupled (active) nodes out of
@@ -267,22 +276,27 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
         o1 = d[3] * p0 + d[4] * p1 + d[5] * p2;
         o2 = d[6] * p0 + d[7] * p1 + d[8] * p2;
     };
-    // per-CTA partials of Vt^T z over the CTA's own coupled dofs (z final)
-    auto compute_zpart = [&]() {
+    // per-CTA partials of Vt^T v over the CTA's own coupled dofs (v final)
+    auto compute_part = [&](void* v, double* dst) {
         if (na <= 0) return;  // uniform within the CTA
         __syncthreads();
         for (int il = threadIdx.x; il < na; il += kThreads) {
             const int dof = __ldg(S.act + ab + il);
-            if (HSC_IN(dof >= 0 && dof < 3 * n, 204, dof)) s_z[il] = (double)elem<VT>(z, dof);
+            if (HSC_IN(dof >= 0 && dof < 3 * n, 204, dof)) s_z[il] = (double)elem<VT>(v, dof);
         }
         __syncthreads();
         for (int j = warp; j < rank; j += kWarps) {
             double sacc = 0.0;
             for (int il = lane; il < na; il += 32) sacc += vt_own(j, il) * s_z[il];
             sacc = warp_sum(sacc);
-            if (lane == 0 && HSC_IN(j < S.kmax, 205, j)) S.zpart[(size_t)j * ncta + lcta] = sacc;
+            if (lane == 0 && HSC_IN(j < S.kmax, 205, j)) dst[(size_t)j * ncta + lcta] = sacc;
         }
     };
+    auto compute_zpart = [&]() { compute_part(z, S.zpart); };
+    const bool schur = prm.schur_basis != 0;
+    auto tpart_half = [&](int h) { return S.tpart + (size_t)h * S.kmax * ncta; };
+    const double* wdev = S.wdev;
+    auto weight = [&](int k) -> double { return wdev ? wdev[k] : prm.w[k]; };
     // C_k phases k = 1..nterms-1 of the preconditioner polynomial
     auto precond_tail = [&](bool active_sys) -> bool {
         for (int k = 1; k < nterms; ++k) {
@@ -291,7 +305,24 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
             if (active_sys) {
                 const VT* tcur = tbuf[tc];
                 VT* tnew = tbuf[tc ^ 1];
-                const double wk = prm.w[k];
+                const double wk = weight(k);
+                // Schur basis: low-rank part Vt d Vt^T t of S t at the own coupled dofs
+                const bool corr = schur && na > 0;
+                if (corr) {
+                    const double* tp = tpart_half((k - 1) & 1);
+                    for (int j = warp; j < rank; j += kWarps) {
+                        double sv, unused;
+                        warp_sum_parts(tp + (size_t)j * ncta, nullptr, 0, ncta, sv, unused);
+                        if (lane == 0) s_dtt[j] = __ldg(S.dpiv + j) * sv;
+                    }
+                    __syncthreads();
+                    for (int il = threadIdx.x; il < na; il += kThreads) {
+                        double c = 0.0;
+                        for (int j = 0; j < rank; ++j) c += vt_own(j, il) * s_dtt[j];
+                        s_z[il] = c;
+                    }
+                    __syncthreads();
+                }
                 auto gather = [&](int c, CT& g0, CT& g1, CT& g2) {
                     VT u0, u1, u2;
                     Vec4<VT>::load(tcur, c, u0, u1, u2);
@@ -307,6 +338,15 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
                             double d0, d1, d2;
                             dact_mul(an, (double)c0, (double)c1, (double)c2, d0, d1, d2);
                             v0 += d0; v1 += d1; v2 += d2;
+                        }
+                    }
+                    if (corr) {
+                        const int an = __ldg(S.rowflag + row);
+                        if (an >= 0) {
+                            const int il = 3 * an - ab;
+                            if (HSC_IN(il >= 0 && il + 2 < na, 208, il)) {
+                                v0 -= s_z[il]; v1 -= s_z[il + 1]; v2 -= s_z[il + 2];
+                            }
                         }
                     }
                     double e0, e1, e2;
@@ -326,6 +366,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
                 };
                 spmv_warp<PT, CT>(wr0, wr1, rb, S.rowptr, S.colidx, S.rowid, s_col, s_row, kcta0, vals_pc, nnz, s_y, gather, epi);
                 if (last) compute_zpart();
+                else if (schur) compute_part(tnew, tpart_half(k & 1));
             }
             tc ^= 1;
             if (last) mark(5);
@@ -347,7 +388,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
             double t0, t1, t2;
             dinv_apply(dinv, n, row, omega, r0, r1, r2, t0, t1, t2);
             Vec4<VT>::store(tbuf[0], row, (VT)t0, (VT)t1, (VT)t2);
-            const double w0 = prm.w[0];
+            const double w0 = weight(0);
             const VT z0 = (VT)(w0 * t0), z1 = (VT)(w0 * t1), z2 = (VT)(w0 * t2);
             Vec4<VT>::store(z, row, z0, z1, z2);
             acc_rr += r0 * r0 + r1 * r1 + r2 * r2;
@@ -355,7 +396,11 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
         }
         for (int i = ab + threadIdx.x; i < ae; i += kThreads) S.pact[i] = 0.0;
         if (na <= 0)
-            for (int j = threadIdx.x; j < rank; j += kThreads) S.zpart[(size_t)j * ncta + lcta] = 0.0;
+            for (int j = threadIdx.x; j < rank; j += kThreads) {
+                S.zpart[(size_t)j * ncta + lcta] = 0.0;
+                if (schur) { tpart_half(0)[(size_t)j * ncta + lcta] = 0.0; tpart_half(1)[(size_t)j * ncta + lcta] = 0.0; }
+            }
+        if (schur && nterms > 1) compute_part(tbuf[0], tpart_half(0));
         if (leader_cta)
             for (int j = threadIdx.x; j < rank; j += kThreads) S.tt[j] = 0.0;
         if (nterms == 1) compute_zpart();
@@ -538,7 +583,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
                 }
                 __syncthreads();
                 const VT* pnew = pbuf[pc ^ 1];
-                const double w0 = prm.w[0];
+                const double w0 = weight(0);
                 for (int row = rb + threadIdx.x; row < re; row += kThreads) {
                     double r0, r1, r2;
                     if (slot == kNormal) {
@@ -578,6 +623,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm) {
                     pc ^= 1;
                 }
                 if (nterms == 1) compute_zpart();
+                else if (schur) compute_part(tbuf[tc], tpart_half(0));
             }
             if (!work) slot = kIdle;
             mark(3);
@@ -597,7 +643,9 @@ cudaError_t launch_t(const PcgParams& prm, int grid, cudaStream_t st, size_t sme
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     void* args[] = {(void*)&prm};
-    return cudaLaunchCooperativeKernel((void*)fn, dim3(grid), dim3(kThreads), args, smem, st);
+    e = cudaLaunchCooperativeKernel((void*)fn, dim3(grid), dim3(kThreads), args, smem, st);
+    debug_sync("pcg_kernel");
+    return e;
 }
 
 template <class MT, class PT, class VT, int TPR>

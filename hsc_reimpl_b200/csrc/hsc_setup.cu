@@ -14,6 +14,8 @@
 #include "hsc_setup.cuh"
 
 #include <atomic>
+#include <cstdio>
+#include <cstdlib>
 #include <cfloat>
 
 namespace hsc {
@@ -22,10 +24,23 @@ namespace hsc {
 static std::atomic<long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+// HSC_SYNC_CHECK=1 (debugging, no graph capture): synchronise after every
+// launch of this library and name the first launch that left an error
+void debug_sync(const char* what) {
+    static int on = -1;
+    if (on < 0) {
+        const char* e = std::getenv("HSC_SYNC_CHECK");
+        on = (e && *e && *e != '0') ? 1 : 0;
+    }
+    if (!on) return;
+    const cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) std::fprintf(stderr, "HSC_SYNC_CHECK: %s after %s\n", cudaGetErrorString(e), what);
+}
 #define HSC_COUNTED(...)      \
     do {                      \
         ::hsc::count_launch(); \
         __VA_ARGS__;          \
+        ::hsc::debug_sync(#__VA_ARGS__); \
     } while (0)
 
 namespace {

@@ -50,7 +50,9 @@ class HSCOptions:
     abd_inverse_tol: float = 1e-5
     full_residual_limit: float = 0.1
     precision: str = "fp64"
-    poly_weights: tuple | None = None      # set -> HSC_PRECOND_POLY
+    poly_weights: tuple | None = None      # set -> polynomial preconditioner with these weights
+    poly_basis: str = "fem"                # "fem": terms on D (HSC_PRECOND_POLY); "schur": on S
+    learned: bool = False                  # HSC_PRECOND_LEARNED (needs HSCContext.set_learned_model)
     residual_replacement: int = 0
     refine_target: float = 0.0
     max_refinements: int = 20
@@ -78,11 +80,15 @@ class HSCOptions:
         o.abd_inverse_tol = float(self.abd_inverse_tol)
         o.full_residual_limit = float(self.full_residual_limit)
         o.precision = PRECISIONS[self.precision]
-        if self.poly_weights is not None:
+        if self.learned:
+            o.preconditioner = _lib.HSC_PRECOND_LEARNED
+        elif self.poly_weights is not None:
             w = [float(v) for v in self.poly_weights]
             if not 1 <= len(w) <= _lib.HSC_MAX_POLY:
                 raise ValueError("1..16 polynomial weights")
-            o.preconditioner = _lib.HSC_PRECOND_POLY
+            if self.poly_basis not in ("fem", "schur"):
+                raise ValueError("poly_basis is 'fem' or 'schur'")
+            o.preconditioner = _lib.HSC_PRECOND_SCHUR_POLY if self.poly_basis == "schur" else _lib.HSC_PRECOND_POLY
             o.poly_degree = len(w)
             for i, v in enumerate(w):
                 o.poly_weights[i] = v
@@ -244,6 +250,34 @@ class HSCContext:
         P = np.zeros((qm, qm))
         self._check(self.lib.hsc_get_abd_inverse(self._ptr, sys_index, P.ctypes.data))
         return P
+
+    # -- learned preconditioner -------------------------------------------------
+    def set_learned_model(self, params_bf16):
+        """Load the 5768 BF16 parameters (uint16 bit patterns) of the learned model."""
+        p = np.ascontiguousarray(params_bf16, dtype=np.uint16)
+        if p.size != _lib.HSC_MLP_PARAMS:
+            raise ValueError(f"expected {_lib.HSC_MLP_PARAMS} parameters, got {p.size}")
+        self._check(self.lib.hsc_set_learned_model(self._ptr, p.ctypes.data))
+
+    def features(self, sys_index=0):
+        """The 16 learned-model features of system `sys_index` after a solve."""
+        out = np.zeros(_lib.HSC_FEATURES, dtype=np.float32)
+        self._check(self.lib.hsc_get_features(self._ptr, sys_index, out.ctypes.data))
+        return out
+
+    def poly_weights(self, sys_index=0):
+        """Polynomial weights the last solve used."""
+        out = np.zeros(_lib.HSC_MAX_POLY)
+        deg = C.c_int32()
+        self._check(self.lib.hsc_get_poly_weights(self._ptr, sys_index, out.ctypes.data, out.size, C.byref(deg)))
+        return out[:deg.value].copy()
+
+    def lanczos(self, sys_index=0, max_pairs=256):
+        """CG coefficients (alpha_k, beta_k) of the last solve, shape (pairs, 2)."""
+        out = np.zeros((max_pairs, 2))
+        n = C.c_int32()
+        self._check(self.lib.hsc_get_lanczos(self._ptr, sys_index, out.ctypes.data, max_pairs, C.byref(n)))
+        return out[:n.value].copy()
 
 
 # ----------------------------------------------------------------------------

@@ -67,7 +67,21 @@ extern "C" {
 
 /* FEM preconditioner polynomial z = sum_k w_k (I - w Dd^-1 D)^k w Dd^-1 r */
 #define HSC_PRECOND_NEUMANN 0 /* w_k = 1, k < neumann_order (linear_hsc.cu:330-343) */
-#define HSC_PRECOND_POLY 1    /* caller-supplied w_k (e.g. from the learned model) */
+#define HSC_PRECOND_POLY 1    /* caller-supplied w_k on the same D-basis terms */
+/* Schur basis: z = sum_k w_k (I - w Dd^-1 S)^k w Dd^-1 r, S = D - V C V^T.  For an eigenvalue mu of
+   w Dd^-1 S the preconditioned operator has the eigenvalue mu * sum_k w_k (1 - mu)^k, so the weights
+   shape the spectrum of the operator PCG actually iterates on.  No reference counterpart. */
+#define HSC_PRECOND_SCHUR_POLY 2 /* caller-supplied w_k (poly_degree of them) */
+#define HSC_PRECOND_LEARNED 3    /* 8 weights per system from the context's learned model
+                                    (hsc_set_learned_model), computed on the device from the
+                                    system's features; falls back to plain Neumann on a stall */
+
+/* learned model: 16 features -> 64 -> 64 -> 8 positive weights (ReLU, softplus), BF16 parameters,
+   flat row-major (out x in): W1[64][16], b1[64], W2[64][64], b2[64], W3[8][64], b3[8] */
+#define HSC_FEATURES 16
+#define HSC_MLP_HIDDEN 64
+#define HSC_MLP_OUT 8
+#define HSC_MLP_PARAMS 5768
 
 #define HSC_MAX_POLY 16
 
@@ -83,13 +97,14 @@ typedef struct hsc_options {
     double full_residual_limit;  /* linear_system/hsc/full_residual_limit (0.1) */
     int32_t precision;           /* HSC_FP64 / HSC_FP32 / HSC_BF16 */
     int32_t preconditioner;      /* HSC_PRECOND_* */
-    int32_t poly_degree;         /* number of weights used with HSC_PRECOND_POLY */
+    int32_t poly_degree;         /* number of weights used with HSC_PRECOND_POLY / _SCHUR_POLY */
     double poly_weights[HSC_MAX_POLY];
     int32_t residual_replacement;/* iterations between FP64 true-residual replacements; 0 = only at convergence */
     double refine_target;        /* > 0: repeat HSC directions with exact line search until
                                     |b - H x|/|b| <= target (core.py:171-198) */
     int32_t max_refinements;
-    int32_t fallback_on_stall;   /* with HSC_PRECOND_POLY: redo with plain Neumann when PCG breaks down or stalls */
+    int32_t fallback_on_stall;   /* polynomial / learned preconditioners: redo a single-system solve with plain
+                                    Neumann (neumann_order) when PCG breaks down or hits max_iter */
     int32_t threads_per_row;     /* SpMV lanes per block row: 2, 4 or 8 (autotuned) */
     int64_t spin_limit;          /* bound on every device-side barrier wait */
     int32_t check_residual;      /* 1: compute the full residual and enforce full_residual_limit */
@@ -183,6 +198,40 @@ HSC_EXPORT int hsc_get_trace(hsc_ctx* ctx, unsigned long long* out, int64_t max_
 
 /* Host copy of the last solve's ABD inverse P (qm x qm, row-major). */
 HSC_EXPORT int hsc_get_abd_inverse(hsc_ctx* ctx, int32_t sys, double* P);
+
+/* ---------------------------------------------------------------------------
+ * Learned polynomial preconditioner (no reference counterpart; the reference
+ * fixes the Neumann weights to 1, linear_hsc.cu:330-343).
+ * ------------------------------------------------------------------------- */
+/* Load the model used by HSC_PRECOND_LEARNED: HSC_MLP_PARAMS BF16 values (host memory). */
+HSC_EXPORT int hsc_set_learned_model(hsc_ctx* ctx, const uint16_t* params_bf16);
+/* The HSC_FEATURES features of system `sys` as the learned model sees them: statistics of the
+ * current numeric system plus the record of the solve before the last one.  Call after a solve. */
+HSC_EXPORT int hsc_get_features(hsc_ctx* ctx, int32_t sys, float* out);
+/* Polynomial weights the last solve of `sys` used (learned: the model's output). */
+HSC_EXPORT int hsc_get_poly_weights(hsc_ctx* ctx, int32_t sys, double* out, int32_t max, int32_t* degree);
+/* CG coefficients (alpha_k, beta_k) of the last solve of `sys`, up to max_pairs pairs; they define
+ * the Lanczos tridiagonal of the preconditioned Schur operator seen from the right-hand side. */
+HSC_EXPORT int hsc_get_lanczos(hsc_ctx* ctx, int32_t sys, double* coef, int32_t max_pairs, int32_t* pairs);
+
+/* Training kernels of the model (device pointers, the caller's stream).  batch samples, row-major.
+ * forward: x (batch x 16) -> h1, h2 (batch x 64, after ReLU), o (batch x 8, before softplus),
+ * w = softplus(o); any of h1, h2, o, w may be NULL. */
+HSC_EXPORT int hsc_mlp_forward(const uint16_t* d_params, const float* d_x, int32_t batch, float* d_h1,
+                               float* d_h2, float* d_o, float* d_w, void* stream);
+/* backward: gradient of the parameters (HSC_MLP_PARAMS floats, summed over the batch in sample order)
+ * from gw = dL/dw (batch x 8); d_scratch holds batch * (8 + 64 + 64) floats. */
+HSC_EXPORT int hsc_mlp_backward(const uint16_t* d_params, const float* d_x, const float* d_h1, const float* d_h2,
+                                const float* d_o, const float* d_gw, int32_t batch, float* d_scratch,
+                                float* d_grad, void* stream);
+/* least-squares residual-polynomial loss of each sample and its gradient in w:
+ * L = scale * sum_i tau_i (1 - theta_i sum_k w_k (1 - theta_i)^k)^2, theta and tau batch x m. */
+HSC_EXPORT int hsc_poly_ls_loss(const float* d_w, const float* d_theta, const float* d_tau, int32_t batch,
+                                int32_t m, float scale, float* d_loss, float* d_gw, void* stream);
+/* one Adam step on FP32 master parameters, writing their BF16 copy. */
+HSC_EXPORT int hsc_adam_step(float* d_master, uint16_t* d_params, const float* d_grad, float* d_m, float* d_v,
+                             int32_t n, float lr, float beta1, float beta2, float eps, float weight_decay,
+                             int32_t step, void* stream);
 
 HSC_EXPORT int hsc_version(void);
 /* Kernels this library has launched in the process so far (all contexts). */

@@ -176,6 +176,20 @@ def neumann_apply(D, Dinv, r, order=5, omega=0.7, weights=None):
     return z
 
 
+def schur_poly_apply(schur, Dinv, r, order=5, omega=0.7, weights=None):
+    """The Schur-basis polynomial of the learned preconditioner (no reference
+    counterpart): the Neumann recursion of ``neumann_apply`` with the Schur
+    operator S = D - V C V^T in place of D,
+    z = sum_k w_k t_k,  t_0 = w B^-1 r,  t_k = t_{k-1} - w B^-1 S t_{k-1}."""
+    w = neumann_weights(order, weights)
+    term = omega * block_diag_apply(Dinv, r)
+    z = w[0] * term
+    for k in range(1, w.size):
+        term = term - omega * block_diag_apply(Dinv, schur(term))
+        z = z + w[k] * term
+    return z
+
+
 def neumann_dense(A, bs, order, omega):
     """Explicit P = sum_{k<order} T^k w B^-1 with T = I - w B^-1 A,
     symmetrised (``linear_hsc.cu:263-275``; ``core.py:74-88`` applied to I)."""
@@ -283,7 +297,7 @@ def pcg_schur(matvec, rhs, precond, tol, max_iter, history=None):
 
 
 DEFAULTS = dict(max_rank=128, aca_rtol=None, order=5, omega=0.7, tol=1e-4, max_iter=2000,
-                abd_inverse="adaptive", abd_inverse_tol=1e-5, weights=None,
+                abd_inverse="adaptive", abd_inverse_tol=1e-5, weights=None, basis="fem",
                 full_residual_limit=0.1, refine_target=None, max_refinements=20)
 
 
@@ -322,6 +336,8 @@ class HSCOracle:
 
     def precond(self, r):
         o = self.o
+        if o["basis"] == "schur":
+            return schur_poly_apply(self.schur, self.Dinv, r, o["order"], o["omega"], o["weights"])
         return neumann_apply(self.D, self.Dinv, r, o["order"], o["omega"], o["weights"])
 
     def solve_once(self, b, history=None):
