@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--modes", default="fp64,fp32")
+    ap.add_argument("--modes", default="fp64,fp32,learned64,learned32")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -195,7 +195,7 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def pcg_bytes_per_iteration(ctx_stats, s, prec, order):
+def pcg_bytes_per_iteration(ctx_stats, s, prec, order, schur=False):
     """Algorithmic bytes one PCG iteration moves in this layout:
     `order` passes over the full BSR D (values + column indices + row pointers),
     the node-padded vector traffic of the phases and Dd^-1 planes; the low-rank
@@ -219,6 +219,8 @@ def pcg_bytes_per_iteration(ctx_stats, s, prec, order):
     a = ctx_stats["active_fem_dofs"]
     k = ctx_stats["rank"]
     lowrank = 3 * a * k * 8
+    if schur:  # Schur-basis terms: Vt^T t partials and the low-rank correction in every C phase
+        lowrank += (order - 1) * 2 * a * k * 8
     return order * spmv + a_vec + b_vec + c_vec + lowrank
 
 
@@ -247,14 +249,21 @@ def run_gpu(args):
         "fp64": HSCOptions(neumann_order=2, omega=0.7, tol=1e-6, abd_inverse="exact", precision="fp64"),
         "fp32": HSCOptions(neumann_order=2, omega=0.7, tol=1e-6, abd_inverse="exact", precision="fp32",
                            residual_replacement=50),
+        "learned64": HSCOptions(learned=True, omega=0.7, tol=1e-6, abd_inverse="exact", precision="fp64"),
+        "learned32": HSCOptions(learned=True, omega=0.7, tol=1e-6, abd_inverse="exact", precision="fp32",
+                                residual_replacement=50),
     }
-    want = [m for m in args.modes.split(",") if m in mode_opts]
+    from hsc_reimpl_b200 import learned as L
+    model = L.load_model()[0] if L.MODEL_PATH.exists() else None
+    want = [m for m in args.modes.split(",") if m in mode_opts and (model is not None or "learned" not in m)]
     ctx = None
     clocks = None
     launches = None
     for mi, mode in enumerate(want):
         opt = mode_opts[mode]
         ctx = HSCContext(opt) if ctx is None else ctx
+        if model is not None:
+            ctx.set_learned_model(model)
         ctx.set_options(opt)
         x = torch.empty_like(ds.b)
         for _ in range(args.warmup):
@@ -291,7 +300,9 @@ def run_gpu(args):
         xs = x.cpu().numpy()
         ok = all(t["status"] == 0 and t["full_relative_residual"] <= TARGET for t in stats_all)
         iters = last["pcg_iterations"]
-        bytes_iter = pcg_bytes_per_iteration(last, s, mode, 2)
+        terms = 8 if "learned" in mode else 2
+        bytes_iter = pcg_bytes_per_iteration(last, s, "fp64" if mode.endswith("64") else "fp32", terms,
+                                             schur="learned" in mode)
         pcg_launch_ms = pcg_ms / args.steps
         modes[mode] = {
             "solves_per_s": replica_throughput(args.steps, ws, total_ms),

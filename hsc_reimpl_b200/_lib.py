@@ -57,6 +57,7 @@ class Options(C.Structure):
         ("spin_limit", C.c_int64),
         ("check_residual", C.c_int32),
         ("trace_iterations", C.c_int32),
+        ("resident", C.c_int32),
     ]
 
 

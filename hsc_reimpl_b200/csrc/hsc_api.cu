@@ -88,19 +88,20 @@ struct System {
     unsigned long long hash = 0;
     // sizes
     int n = 0, nnz = 0, a = 0, nqq = 0, nqf = 0, kmax = 0, qm = 0, qo = 0, fo = 0, fn = 0;
-    std::vector<int> h_rowptr, h_act;
+    std::vector<int> h_rowptr, h_act, h_colidx;
     // plan
     DevBuf rowptr, colidx, rowid, src, diag_pos, qq, qf, act, ident, rowflag;
     // numeric
     DevBuf v64, vf32, vbf16, dinv, A, E, R0, R1, U, V, hist, P, Ptmp, T, term, Binv, L, W, C, Lc, dpiv, vt64, vtmt,
         cvec, tt, ttx, bq, bf, x, r, z, p0, p1, y, t0, t1, node_nz, xq, ypad, yq, work, cg, scal, dact, pact, yact,
-        zpart, tpart;
+        zpart, tpart, lcol;
     DevBuf dvec[4];           // contiguous-N scratch for refinement
     double h_last[kPrev] = {};   // record of the last solve: 1, lanczos min, max, iterations, q(0)
     double h_prevrec[kPrev] = {};// record the features of the current solve see
     double h_cg[2 * kMaxCoef] = {};
     DevScal h_scal{};
     std::vector<int> h_node_nz;
+    std::vector<unsigned short> h_lcol;
     bool aca_on_cluster = false;
 };
 
@@ -113,8 +114,10 @@ struct hsc_ctx {
     int num_sms = 148;
     std::vector<System> sys;
     // PCG launch state
-    DevBuf d_desc, d_cta_sys, d_cta_row, d_cta_act, d_cta_warp, d_part, d_bar, d_remaining, d_trace;
+    DevBuf d_desc, d_cta_sys, d_cta_row, d_cta_act, d_cta_aidx, d_cta_warp, d_part, d_bar, d_remaining, d_trace;
+    DevBuf d_win_off, d_win_nodes, d_win_own;
     int off_z = 0, off_vt = 0, off_y = 0, off_blk = 0, stage_vt = 0, stage_blk = 0;
+    int resident = 0, off_wn = 0, off_win = 0, off_val = 0, off_vpc = 0, off_lidx = 0;
     int grid = 0;
     int vt_smem = 0;           // doubles of PCG shared memory after the d.*tt slot
     size_t pcg_smem = 0;       // dynamic shared memory bytes of the PCG launch
@@ -315,6 +318,7 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
     }
     if (S.nnz) {
         CK(cudaMemcpyAsync(S.colidx.p, colidx.data(), sizeof(int) * S.nnz, cudaMemcpyHostToDevice, st));
+        S.h_colidx = colidx;
         CK(cudaMemcpyAsync(S.src.p, src.data(), sizeof(int) * S.nnz, cudaMemcpyHostToDevice, st));
     }
     CK(cudaMemcpyAsync(S.diag_pos.p, diag.data(), sizeof(int) * S.n, cudaMemcpyHostToDevice, st));
@@ -627,7 +631,7 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
         nc[big]--; used--;
     }
     G = used;
-    std::vector<int> cta_sys(G), cta_row(2 * G), cta_act(2 * G);
+    std::vector<int> cta_sys(G), cta_row(2 * G), cta_act(2 * G), cta_aidx(G, -1);
     std::vector<SysDesc> desc(ns);
     int c = 0;
     for (int s = 0; s < ns; ++s) {
@@ -658,7 +662,11 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
         d.pact = S.pact.as<double>(); d.yact = S.yact.as<double>(); d.ttx = S.ttx.as<double>();
         GROW(S.zpart, sizeof(double) * std::max(1, S.kmax) * (size_t)(c - b));
         d.zpart = S.zpart.as<double>();
-        GROW(S.tpart, sizeof(double) * 2 * std::max(1, S.kmax) * (size_t)(c - b));
+        int nact = 0;
+        for (int k = b; k < c; ++k)
+            if (cta_act[2 * k + 1] > cta_act[2 * k]) cta_aidx[k] = nact++;
+        d.nact_cta = nact;
+        GROW(S.tpart, sizeof(double) * 2 * std::max(1, S.kmax) * (size_t)std::max(1, nact));
         d.tpart = S.tpart.as<double>();
         d.wdev = o.preconditioner == HSC_PRECOND_LEARNED ? S.scal.as<DevScal>()->wl : nullptr;
         d.x = S.x.as<double>(); d.r = S.r.as<double>(); d.rhs = S.bf.as<double>(); d.z = S.z.p;
@@ -687,13 +695,54 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
         Rmax = std::max(Rmax, re - rb);
         BLKmax = std::max(BLKmax, (int)nb);
     }
-    // shared-memory layout; staging of the Vt blocks and of the column indices
-    // is dropped (in that order) when the budget does not hold them
+    // vector windows (resident mode): the sorted nodes each CTA's blocks read,
+    // and per BSR entry the window position of its column
+    std::vector<int> win_off(G + 1, 0), win_nodes, win_own(G, 0);
+    int Wmax = 0;
+    bool win_ok = o.resident != 0;
+    {
+        std::vector<int> stamp, pos;
+        for (int k = 0; k < G && win_ok; ++k) {
+            System& S = ctx->sys[idx[cta_sys[k]]];
+            if ((int)stamp.size() < S.n) { stamp.assign(S.n, -1); pos.assign(S.n, 0); }
+            const int rb = cta_row[2 * k], re = cta_row[2 * k + 1];
+            const int kb0 = S.h_rowptr[rb], kb1 = S.h_rowptr[re];
+            std::vector<int> w;
+            for (int e = kb0; e < kb1; ++e) {
+                const int c = S.h_colidx[e];
+                if (stamp[c] != k) { stamp[c] = k; w.push_back(c); }
+            }
+            std::sort(w.begin(), w.end());
+            for (int i = 0; i < (int)w.size(); ++i) pos[w[i]] = i;
+            if (w.size() > 65535 || re - rb > 65535) { win_ok = false; break; }
+            if (S.h_lcol.size() != (size_t)S.nnz) S.h_lcol.assign(S.nnz, 0);
+            for (int e = kb0; e < kb1; ++e) S.h_lcol[e] = (unsigned short)pos[S.h_colidx[e]];
+            win_own[k] = rb < re ? pos[rb] : 0;
+            win_off[k + 1] = win_off[k] + (int)w.size();
+            win_nodes.insert(win_nodes.end(), w.begin(), w.end());
+            Wmax = std::max(Wmax, (int)w.size());
+        }
+    }
+    // shared-memory layout (doubles).  Resident when the BSR slice, its indices
+    // and the window fit next to the rest; otherwise staging of the Vt blocks
+    // and of the column indices is dropped (in that order) when the budget does
+    // not hold them
     const int budget = (int)(smem_cap / sizeof(double));
+    const int res_budget = (int)((227 * 1024 - 1024) / sizeof(double));
     const int base = kMaxRank + Zmax + 3 * Rmax + 2;
     if (base > budget) return fail(ctx, HSC_ERR_INVALID, "too many rows or coupled dofs in one CTA");
-    int stage_vt = 1, stage_blk = 1;
-    if (base + VTmax + BLKmax > budget) {
+    const size_t vtb = vt_bytes(o.precision), mtb = o.precision == 0 ? 8 : 4;
+    auto dbl = [](size_t bytes) { return (int)((bytes + 15) / 16 * 2); };  // 16-byte aligned, in doubles
+    const int W_wn = dbl(sizeof(int) * (size_t)Wmax), W_win = dbl(4 * vtb * (size_t)Wmax);
+    const int W_val = dbl(9 * mtb * (size_t)BLKmax), W_vpc = o.precision == 2 ? dbl(9 * 2 * (size_t)BLKmax) : 0;
+    const int W_lidx = dbl(4 * (size_t)BLKmax);
+    const int res_need = base + 4 + W_wn + W_win + W_val + W_vpc + W_lidx;
+    int stage_vt = 1, stage_blk = 1, resident = 0;
+    if (win_ok && res_need <= res_budget) {
+        resident = 1;
+        stage_blk = 0;
+        stage_vt = res_need + VTmax <= res_budget ? 1 : 0;
+    } else if (base + VTmax + BLKmax > budget) {
         if (base + BLKmax <= budget) stage_vt = 0;
         else if (base + VTmax <= budget) stage_blk = 0;
         else { stage_vt = 0; stage_blk = 0; }
@@ -707,13 +756,39 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
     ctx->stage_vt = stage_vt;
     ctx->stage_blk = stage_blk;
     ctx->vt_smem = Zmax + VTmax;
-    ctx->pcg_smem = sizeof(double) * (size_t)(ctx->off_blk + (stage_blk ? BLKmax : 0));
+    ctx->resident = resident;
+    if (resident) {
+        ctx->off_wn = ctx->off_blk;
+        ctx->off_win = ctx->off_wn + W_wn;
+        ctx->off_val = ctx->off_win + W_win;
+        ctx->off_vpc = ctx->off_val + W_val;
+        ctx->off_lidx = ctx->off_vpc + W_vpc;
+        ctx->pcg_smem = sizeof(double) * (size_t)(ctx->off_lidx + W_lidx);
+        GROW(ctx->d_win_off, sizeof(int) * (G + 1));
+        GROW(ctx->d_win_nodes, sizeof(int) * std::max<size_t>(1, win_nodes.size()));
+        GROW(ctx->d_win_own, sizeof(int) * G);
+        CK(cudaMemcpyAsync(ctx->d_win_off.p, win_off.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice, st));
+        if (!win_nodes.empty())
+            CK(cudaMemcpyAsync(ctx->d_win_nodes.p, win_nodes.data(), sizeof(int) * win_nodes.size(),
+                               cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->d_win_own.p, win_own.data(), sizeof(int) * G, cudaMemcpyHostToDevice, st));
+        for (int s2 = 0; s2 < ns; ++s2) {
+            System& S = ctx->sys[idx[s2]];
+            GROW(S.lcol, sizeof(unsigned short) * (size_t)std::max(1, S.nnz));
+            if (S.nnz)
+                CK(cudaMemcpyAsync(S.lcol.p, S.h_lcol.data(), sizeof(unsigned short) * S.nnz, cudaMemcpyHostToDevice, st));
+            desc[s2].lcol = S.lcol.as<unsigned short>();
+        }
+    } else {
+        ctx->pcg_smem = sizeof(double) * (size_t)(ctx->off_blk + (stage_blk ? BLKmax : 0));
+    }
     GROW(ctx->d_cta_warp, sizeof(int) * cta_warp.size());
     CK(cudaMemcpyAsync(ctx->d_cta_warp.p, cta_warp.data(), sizeof(int) * cta_warp.size(), cudaMemcpyHostToDevice, st));
     GROW(ctx->d_desc, sizeof(SysDesc) * ns);
     GROW(ctx->d_cta_sys, sizeof(int) * G);
     GROW(ctx->d_cta_row, sizeof(int) * 2 * G);
     GROW(ctx->d_cta_act, sizeof(int) * 2 * G);
+    GROW(ctx->d_cta_aidx, sizeof(int) * G);
     GROW(ctx->d_part, sizeof(double) * 3 * G);
     GROW(ctx->d_bar, sizeof(GridBar));
     GROW(ctx->d_remaining, sizeof(int));
@@ -721,6 +796,7 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
     CK(cudaMemcpyAsync(ctx->d_cta_sys.p, cta_sys.data(), sizeof(int) * G, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->d_cta_row.p, cta_row.data(), sizeof(int) * 2 * G, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->d_cta_act.p, cta_act.data(), sizeof(int) * 2 * G, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->d_cta_aidx.p, cta_aidx.data(), sizeof(int) * G, cudaMemcpyHostToDevice, st));
     // cluster-ACA descriptors (pointers only: valid for every numeric pass of this analysis)
     std::vector<AcaSys> aca;
     size_t aca_smem = 0;
@@ -756,6 +832,7 @@ int launch_pcg_all(hsc_ctx* ctx, int nsys, cudaStream_t st) {
     prm.cta_sys = ctx->d_cta_sys.as<int>();
     prm.cta_row = ctx->d_cta_row.as<int>();
     prm.cta_act = ctx->d_cta_act.as<int>();
+    prm.cta_aidx = ctx->d_cta_aidx.as<int>();
     prm.part_rr = ctx->d_part.as<double>();
     prm.part_rz = ctx->d_part.as<double>() + ctx->grid;
     prm.part_pap = ctx->d_part.as<double>() + 2 * ctx->grid;
@@ -763,6 +840,10 @@ int launch_pcg_all(hsc_ctx* ctx, int nsys, cudaStream_t st) {
     prm.cta_warp = ctx->d_cta_warp.as<int>();
     prm.off_z = ctx->off_z; prm.off_vt = ctx->off_vt; prm.off_y = ctx->off_y; prm.off_blk = ctx->off_blk;
     prm.stage_vt = ctx->stage_vt; prm.stage_blk = ctx->stage_blk;
+    prm.resident = ctx->resident;
+    prm.win_off = ctx->d_win_off.as<int>(); prm.win_nodes = ctx->d_win_nodes.as<int>(); prm.win_own = ctx->d_win_own.as<int>();
+    prm.off_wn = ctx->off_wn; prm.off_win = ctx->off_win; prm.off_val = ctx->off_val; prm.off_vpc = ctx->off_vpc;
+    prm.off_lidx = ctx->off_lidx;
     prm.trace = nullptr;
     prm.trace_iters = 0;
     if (o.trace_iterations > 0) {
@@ -1022,6 +1103,7 @@ int hsc_options_default(hsc_options* o) {
     o->spin_limit = 20000000;
     o->check_residual = 1;
     o->trace_iterations = 0;
+    o->resident = 1;
     return HSC_OK;
 }
 

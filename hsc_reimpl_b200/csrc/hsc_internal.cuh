@@ -177,7 +177,10 @@ struct SysDesc {
     double* pact;          // FP64 direction at the active dofs (a)
     double* yact;          // FP64 S p at the active dofs (a)
     double* zpart;         // kmax x ncta: per-CTA partials of Vt^T z (own active dofs)
-    double* tpart;         // 2 x kmax x ncta: per-CTA partials of Vt^T t_k (Schur-basis terms), by term parity
+    double* tpart;         // 2 x kmax x nact_cta: partials of Vt^T t_k of the CTAs with coupled dofs
+                           // (Schur-basis terms), by term parity
+    int nact_cta;          // CTAs of this system that own coupled dofs
+    const unsigned short* lcol;  // resident mode: per BSR entry, window position of its column
     const double* wdev;    // device polynomial weights of this system (learned), or null: PcgParams::w
     double* tt;            // kmax: Vt^T p (recurrence Vt^T z + beta Vt^T p_prev)
     double* ttx;           // kmax: Vt^T x (true-residual slot)
@@ -194,6 +197,7 @@ struct PcgParams {
     const int* cta_sys;        // per CTA: its system
     const int* cta_row;        // per CTA: [row_begin, row_end) pairs
     const int* cta_act;        // per CTA: [act_begin, act_end) pairs in the system's act list
+    const int* cta_aidx;       // per CTA: its index among the system's CTAs with coupled dofs, or -1
     double* part_rr;           // per CTA: r.r after the update phase
     double* part_rz;           // per CTA: r.z after the last preconditioner phase
     double* part_pap;          // per CTA: p.S p of phase A
@@ -215,6 +219,14 @@ struct PcgParams {
     int vt_smem;               // doubles reserved for the largest Vt block (pad(na) + na * rank)
     unsigned long long* trace; // optional: per CTA x trace_iters x 8 SM clocks
     int trace_iters;
+    // resident mode: each CTA keeps its BSR slice (operator and preconditioner
+    // planes), local indices and the window of vector nodes its blocks read in
+    // shared memory; a phase stages the window once and runs the SpMV from there
+    int resident;
+    const int* win_off;        // per CTA: G + 1 offsets into win_nodes
+    const int* win_nodes;      // sorted global node ids of each CTA's window
+    const int* win_own;        // per CTA: window position of its first row
+    int off_wn, off_win, off_val, off_vpc, off_lidx;  // shared-memory offsets (doubles)
 };
 
 // launch counter of this library (hsc_setup.cu)

@@ -92,7 +92,11 @@ __device__ __forceinline__ void warp_sum_parts(const double* pa, const double* p
 // tail lane of each row segment adds its sum into s_y: one writer per row and
 // slice, slices in order, so the result is deterministic.  Then each lane runs
 // the epilogue of one owned row.
-template <class MT, class CT, class Gather, class Epi>
+//
+// The warp loads NB slices of 32 blocks (indices, gathers and values) before
+// it scans the first one, so one round trip to L2 serves NB slices: the loop
+// is bound by load latency, not bandwidth, on an L2-resident matrix.
+template <int NB, class MT, class CT, class Gather, class Epi>
 __device__ __forceinline__ void spmv_warp(int wr0, int wr1, int rb, const int* __restrict__ rowptr,
                                           const int* __restrict__ colidx, const int* __restrict__ rowid,
                                           const int* s_col, const int* s_row, int kcta0, const MT* __restrict__ vals,
@@ -105,40 +109,119 @@ __device__ __forceinline__ void spmv_warp(int wr0, int wr1, int rb, const int* _
         yy[0] = 0.0; yy[1] = 0.0; yy[2] = 0.0;
     }
     __syncwarp();
-    for (int kb = k0; kb < k1; kb += 32) {
-        const int k = kb + lane;
-        const bool valid = k < k1;
-        int c = 0, row = -1;
-        if (valid) {
-            if (s_col) { c = s_col[k - kcta0]; row = s_row[k - kcta0]; }
-            else { c = __ldg(colidx + k); row = __ldg(rowid + k); }
-        }
-        CT p0 = 0, p1 = 0, p2 = 0;
-        if (valid) {
-            CT x0, x1, x2;
-            gather(c, x0, x1, x2);
-            const MT* v = vals + k;
-            const size_t st = (size_t)nnz;
-            const CT b0 = Num<MT>::get(__ldg(v)), b1 = Num<MT>::get(__ldg(v + st)), b2 = Num<MT>::get(__ldg(v + 2 * st)),
-                     b3 = Num<MT>::get(__ldg(v + 3 * st)), b4 = Num<MT>::get(__ldg(v + 4 * st)),
-                     b5 = Num<MT>::get(__ldg(v + 5 * st)), b6 = Num<MT>::get(__ldg(v + 6 * st)),
-                     b7 = Num<MT>::get(__ldg(v + 7 * st)), b8 = Num<MT>::get(__ldg(v + 8 * st));
-            p0 = b0 * x0 + b1 * x1 + b2 * x2;
-            p1 = b3 * x0 + b4 * x1 + b5 * x2;
-            p2 = b6 * x0 + b7 * x1 + b8 * x2;
+    const size_t st = (size_t)nnz;
+    for (int kb = k0; kb < k1; kb += 32 * NB) {
+        CT p0[NB], p1[NB], p2[NB];
+        int row[NB];
+#pragma unroll
+        for (int h = 0; h < NB; ++h) {
+            const int k = kb + 32 * h + lane;
+            const bool valid = k < k1;
+            int c = 0;
+            row[h] = -1;
+            if (valid) {
+                if (s_col) { c = s_col[k - kcta0]; row[h] = s_row[k - kcta0]; }
+                else { c = __ldg(colidx + k); row[h] = __ldg(rowid + k); }
+            }
+            p0[h] = 0; p1[h] = 0; p2[h] = 0;
+            if (valid) {
+                CT x0, x1, x2;
+                gather(c, x0, x1, x2);
+                const MT* v = vals + k;
+                const CT b0 = Num<MT>::get(__ldg(v)), b1 = Num<MT>::get(__ldg(v + st)),
+                         b2 = Num<MT>::get(__ldg(v + 2 * st)), b3 = Num<MT>::get(__ldg(v + 3 * st)),
+                         b4 = Num<MT>::get(__ldg(v + 4 * st)), b5 = Num<MT>::get(__ldg(v + 5 * st)),
+                         b6 = Num<MT>::get(__ldg(v + 6 * st)), b7 = Num<MT>::get(__ldg(v + 7 * st)),
+                         b8 = Num<MT>::get(__ldg(v + 8 * st));
+                p0[h] = b0 * x0 + b1 * x1 + b2 * x2;
+                p1[h] = b3 * x0 + b4 * x1 + b5 * x2;
+                p2[h] = b6 * x0 + b7 * x1 + b8 * x2;
+            }
         }
 #pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            const int rr = __shfl_up_sync(0xffffffffu, row, off);
-            const CT q0 = __shfl_up_sync(0xffffffffu, p0, off);
-            const CT q1 = __shfl_up_sync(0xffffffffu, p1, off);
-            const CT q2 = __shfl_up_sync(0xffffffffu, p2, off);
-            if (lane >= off && rr == row) { p0 += q0; p1 += q1; p2 += q2; }
+        for (int h = 0; h < NB; ++h) {
+            CT a0 = p0[h], a1 = p1[h], a2 = p2[h];
+            const int rw = row[h];
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int rr = __shfl_up_sync(0xffffffffu, rw, off);
+                const CT q0 = __shfl_up_sync(0xffffffffu, a0, off);
+                const CT q1 = __shfl_up_sync(0xffffffffu, a1, off);
+                const CT q2 = __shfl_up_sync(0xffffffffu, a2, off);
+                if (lane >= off && rr == rw) { a0 += q0; a1 += q1; a2 += q2; }
+            }
+            const int rn = __shfl_down_sync(0xffffffffu, rw, 1);
+            if (rw >= 0 && (lane == 31 || rn != rw)) {
+                double* yy = s_y + 3 * (rw - rb);
+                yy[0] += (double)a0; yy[1] += (double)a1; yy[2] += (double)a2;
+            }
+            __syncwarp();
         }
-        const int rn = __shfl_down_sync(0xffffffffu, row, 1);
-        if (valid && (lane == 31 || rn != row)) {
-            double* yy = s_y + 3 * (row - rb);
-            yy[0] += (double)p0; yy[1] += (double)p1; yy[2] += (double)p2;
+    }
+    __syncwarp();
+    for (int r = wr0 + lane; r < wr1; r += 32) {
+        const double* yy = s_y + 3 * (r - rb);
+        epi(r, (CT)yy[0], (CT)yy[1], (CT)yy[2]);
+    }
+}
+
+// spmv_warp over the CTA's shared-memory copy: value planes s_val[e * nblk +
+// kl], window positions of the columns (s_lc) and local rows (s_lr) of the
+// CTA's blocks, and the staged vector window s_win (4 entries per node).
+// Same slices, scan and summation order as spmv_warp.
+template <int NB, class MT, class CT, class VT, class Epi>
+__device__ __forceinline__ void spmv_warp_res(int wr0, int wr1, int rb, const int* __restrict__ rowptr, int kcta0,
+                                              int nblk, const MT* s_val, const unsigned short* s_lc,
+                                              const unsigned short* s_lr, const VT* s_win, double* s_y, Epi& epi) {
+    const int lane = threadIdx.x & 31;
+    if (wr1 <= wr0) return;
+    const int k0 = __ldg(rowptr + wr0) - kcta0, k1 = __ldg(rowptr + wr1) - kcta0;
+    for (int r = wr0 + lane; r < wr1; r += 32) {
+        double* yy = s_y + 3 * (r - rb);
+        yy[0] = 0.0; yy[1] = 0.0; yy[2] = 0.0;
+    }
+    __syncwarp();
+    for (int kb = k0; kb < k1; kb += 32 * NB) {
+        CT p0[NB], p1[NB], p2[NB];
+        int row[NB];
+#pragma unroll
+        for (int h = 0; h < NB; ++h) {
+            const int k = kb + 32 * h + lane;
+            row[h] = -1;
+            p0[h] = 0; p1[h] = 0; p2[h] = 0;
+            if (k < k1) {
+                row[h] = s_lr[k];
+                VT u0, u1, u2;
+                Vec4<VT>::load(s_win, s_lc[k], u0, u1, u2);
+                const CT x0 = (CT)u0, x1 = (CT)u1, x2 = (CT)u2;
+                const MT* v = s_val + k;
+                const CT b0 = Num<MT>::get(v[0]), b1 = Num<MT>::get(v[nblk]), b2 = Num<MT>::get(v[2 * nblk]),
+                         b3 = Num<MT>::get(v[3 * nblk]), b4 = Num<MT>::get(v[4 * nblk]),
+                         b5 = Num<MT>::get(v[5 * nblk]), b6 = Num<MT>::get(v[6 * nblk]),
+                         b7 = Num<MT>::get(v[7 * nblk]), b8 = Num<MT>::get(v[8 * nblk]);
+                p0[h] = b0 * x0 + b1 * x1 + b2 * x2;
+                p1[h] = b3 * x0 + b4 * x1 + b5 * x2;
+                p2[h] = b6 * x0 + b7 * x1 + b8 * x2;
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < NB; ++h) {
+            CT a0 = p0[h], a1 = p1[h], a2 = p2[h];
+            const int rw = row[h];
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int rr = __shfl_up_sync(0xffffffffu, rw, off);
+                const CT q0 = __shfl_up_sync(0xffffffffu, a0, off);
+                const CT q1 = __shfl_up_sync(0xffffffffu, a1, off);
+                const CT q2 = __shfl_up_sync(0xffffffffu, a2, off);
+                if (lane >= off && rr == rw) { a0 += q0; a1 += q1; a2 += q2; }
+            }
+            const int rn = __shfl_down_sync(0xffffffffu, rw, 1);
+            if (rw >= 0 && (lane == 31 || rn != rw)) {
+                double* yy = s_y + 3 * rw;
+                yy[0] += (double)a0; yy[1] += (double)a1; yy[2] += (double)a2;
+            }
+            __syncwarp();
         }
     }
     __syncwarp();
@@ -169,6 +252,9 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
     const PcgParams prm = prm_arg;
     using CT = typename Cmp<MT>::T;
     using DT = typename DinvT<MT>::T;
+    // 32-block slices a warp loads per round trip in the SpMV (the "tile width" the
+    // autotuner picks through threads_per_row: 2 -> 1, 4 -> 2, 8 -> 4)
+    constexpr int kNB = TPR / 2;
     // mixed modes keep the diagonal blocks of the coupled (active) nodes out of
     // the bulk planes and apply them in FP64: those blocks carry the contact /
     // stitch stiffness that cancels against the low-rank term in S = D - V C V^T
@@ -176,7 +262,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
     __shared__ double s_w[kWarps][2];
     __shared__ double s_bc[4];
     __shared__ int s_ok;
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) double smem[];
 
     const int cta = blockIdx.x;
     const unsigned int G = gridDim.x;
@@ -184,6 +270,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
     const SysDesc& S = prm.sys[sidx];
     const int rb = prm.cta_row[2 * cta], re = prm.cta_row[2 * cta + 1];
     const int ab = prm.cta_act[2 * cta], ae = prm.cta_act[2 * cta + 1];
+    const int aidx = prm.cta_aidx[cta];
     const int na = ae - ab;
     const int cb = S.cta_begin, ce = S.cta_end;
     const int ncta = ce - cb, lcta = cta - cb;
@@ -222,6 +309,28 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
             s_col[e] = __ldg(S.colidx + kcta0 + e);
             s_row[e] = __ldg(S.rowid + kcta0 + e);
         }
+    // resident mode: the CTA's value planes, local indices and window node list
+    const bool res = prm.resident != 0;
+    const int wn0 = res ? prm.win_off[cta] : 0, nwin = res ? prm.win_off[cta + 1] - wn0 : 0;
+    const int wown = res ? prm.win_own[cta] : 0;
+    int* s_wn = reinterpret_cast<int*>(smem + prm.off_wn);
+    VT* s_win = reinterpret_cast<VT*>(smem + prm.off_win);
+    MT* s_val = reinterpret_cast<MT*>(smem + prm.off_val);
+    PT* s_vpc = std::is_same<MT, PT>::value ? reinterpret_cast<PT*>(s_val) : reinterpret_cast<PT*>(smem + prm.off_vpc);
+    unsigned short* s_lc = reinterpret_cast<unsigned short*>(smem + prm.off_lidx);
+    unsigned short* s_lr = s_lc + nblk;
+    if (res) {
+        for (int e = threadIdx.x; e < 9 * nblk; e += kThreads) {
+            const int pl = e / nblk, kl = e - pl * nblk;
+            s_val[e] = vals[(size_t)pl * nnz + kcta0 + kl];
+            if (!std::is_same<MT, PT>::value) s_vpc[e] = vals_pc[(size_t)pl * nnz + kcta0 + kl];
+        }
+        for (int e = threadIdx.x; e < nblk; e += kThreads) {
+            s_lc[e] = S.lcol[kcta0 + e];
+            s_lr[e] = (unsigned short)(__ldg(S.rowid + kcta0 + e) - rb);
+        }
+        for (int e = threadIdx.x; e < nwin; e += kThreads) s_wn[e] = prm.win_nodes[wn0 + e];
+    }
     const bool vt_smem = prm.stage_vt && na > 0;
     HSC_IN(rank <= kMaxRank && rank <= S.kmax, 207, rank);
     HSC_IN(na <= 0 || ((na + 1) & ~1) + na * rank <= prm.vt_smem, 201, na);
@@ -276,8 +385,9 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
         o1 = d[3] * p0 + d[4] * p1 + d[5] * p2;
         o2 = d[6] * p0 + d[7] * p1 + d[8] * p2;
     };
-    // per-CTA partials of Vt^T v over the CTA's own coupled dofs (v final)
-    auto compute_part = [&](void* v, double* dst) {
+    // per-CTA partials of Vt^T v over the CTA's own coupled dofs (v final),
+    // written to dst[j * stride]
+    auto compute_part = [&](void* v, double* dst, int stride) {
         if (na <= 0) return;  // uniform within the CTA
         __syncthreads();
         for (int il = threadIdx.x; il < na; il += kThreads) {
@@ -289,12 +399,46 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
             double sacc = 0.0;
             for (int il = lane; il < na; il += 32) sacc += vt_own(j, il) * s_z[il];
             sacc = warp_sum(sacc);
-            if (lane == 0 && HSC_IN(j < S.kmax, 205, j)) dst[(size_t)j * ncta + lcta] = sacc;
+            if (lane == 0 && HSC_IN(j < S.kmax, 205, j)) dst[(size_t)j * stride] = sacc;
         }
     };
-    auto compute_zpart = [&]() { compute_part(z, S.zpart); };
+    auto compute_zpart = [&]() { compute_part(z, S.zpart + lcta, ncta); };
     const bool schur = prm.schur_basis != 0;
-    auto tpart_half = [&](int h) { return S.tpart + (size_t)h * S.kmax * ncta; };
+    const int nact = S.nact_cta;
+    auto tpart_half = [&](int h) { return S.tpart + (size_t)h * S.kmax * nact; };
+    // s_dtt[j] = d_j * sum_c P[j * nact + c] for j < rank: the partials of the
+    // coupled CTAs, JW rows per warp with all their loads issued together,
+    // summed in the same order in every CTA
+    auto sum_tparts = [&](const double* P) {
+        constexpr int JW = 8;
+        for (int j0 = warp * JW; j0 < rank; j0 += kWarps * JW) {
+            double v[JW];
+#pragma unroll
+            for (int q = 0; q < JW; ++q) v[q] = 0.0;
+            for (int c = lane; c < nact; c += 32)
+#pragma unroll
+                for (int q = 0; q < JW; ++q)
+                    if (j0 + q < rank) v[q] += P[(size_t)(j0 + q) * nact + c];
+#pragma unroll
+            for (int q = 0; q < JW; ++q) {
+                const double t = warp_sum(v[q]);
+                if (lane == 0 && j0 + q < rank) s_dtt[j0 + q] = __ldg(S.dpiv + j0 + q) * t;
+            }
+        }
+    };
+    // out[il] = sum_j Vt[own il, j] s_dtt[j] for il < na: four threads per row
+    // (j interleaved), combined by shuffles in a fixed order
+    auto lowrank_rows = [&](double* out) {
+        for (int base = 0; base < na; base += kThreads / 4) {
+            const int il = base + (threadIdx.x >> 2), q = threadIdx.x & 3;
+            double c = 0.0;
+            if (il < na)
+                for (int j = q; j < rank; j += 4) c += vt_own(j, il) * s_dtt[j];
+            c += __shfl_xor_sync(0xffffffffu, c, 1);
+            c += __shfl_xor_sync(0xffffffffu, c, 2);
+            if (il < na && q == 0) out[il] = c;
+        }
+    };
     const double* wdev = S.wdev;
     auto weight = [&](int k) -> double { return wdev ? wdev[k] : prm.w[k]; };
     // C_k phases k = 1..nterms-1 of the preconditioner polynomial
@@ -309,18 +453,9 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                 // Schur basis: low-rank part Vt d Vt^T t of S t at the own coupled dofs
                 const bool corr = schur && na > 0;
                 if (corr) {
-                    const double* tp = tpart_half((k - 1) & 1);
-                    for (int j = warp; j < rank; j += kWarps) {
-                        double sv, unused;
-                        warp_sum_parts(tp + (size_t)j * ncta, nullptr, 0, ncta, sv, unused);
-                        if (lane == 0) s_dtt[j] = __ldg(S.dpiv + j) * sv;
-                    }
+                    sum_tparts(tpart_half((k - 1) & 1));
                     __syncthreads();
-                    for (int il = threadIdx.x; il < na; il += kThreads) {
-                        double c = 0.0;
-                        for (int j = 0; j < rank; ++j) c += vt_own(j, il) * s_dtt[j];
-                        s_z[il] = c;
-                    }
+                    lowrank_rows(s_z);
                     __syncthreads();
                 }
                 auto gather = [&](int c, CT& g0, CT& g1, CT& g2) {
@@ -330,7 +465,8 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                 };
                 auto epi = [&](int row, CT w0, CT w1, CT w2) {
                     VT c0, c1, c2;
-                    Vec4<VT>::load(tcur, row, c0, c1, c2);
+                    if (res) Vec4<VT>::load(s_win, wown + row - rb, c0, c1, c2);
+                    else Vec4<VT>::load(tcur, row, c0, c1, c2);
                     double v0 = w0, v1 = w1, v2 = w2;
                     if (kSplit) {
                         const int an = __ldg(S.rowflag + row);
@@ -364,9 +500,21 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                         acc += r0 * (double)s0 + r1 * (double)s1 + r2 * (double)s2;
                     }
                 };
-                spmv_warp<PT, CT>(wr0, wr1, rb, S.rowptr, S.colidx, S.rowid, s_col, s_row, kcta0, vals_pc, nnz, s_y, gather, epi);
+                if (res) {
+                    for (int i = threadIdx.x; i < nwin; i += kThreads) {
+                        VT u0, u1, u2;
+                        Vec4<VT>::load(tcur, s_wn[i], u0, u1, u2);
+                        Vec4<VT>::store(s_win, i, u0, u1, u2);
+                    }
+                    __syncthreads();
+                    spmv_warp_res<kNB, PT, CT, VT>(wr0, wr1, rb, S.rowptr, kcta0, nblk, s_vpc, s_lc, s_lr, s_win, s_y, epi);
+                    __syncthreads();
+                } else {
+                    spmv_warp<kNB, PT, CT>(wr0, wr1, rb, S.rowptr, S.colidx, S.rowid, s_col, s_row, kcta0, vals_pc, nnz, s_y,
+                                      gather, epi);
+                }
                 if (last) compute_zpart();
-                else if (schur) compute_part(tnew, tpart_half(k & 1));
+                else if (schur) compute_part(tnew, tpart_half(k & 1) + aidx, nact);
             }
             tc ^= 1;
             if (last) mark(5);
@@ -396,11 +544,8 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
         }
         for (int i = ab + threadIdx.x; i < ae; i += kThreads) S.pact[i] = 0.0;
         if (na <= 0)
-            for (int j = threadIdx.x; j < rank; j += kThreads) {
-                S.zpart[(size_t)j * ncta + lcta] = 0.0;
-                if (schur) { tpart_half(0)[(size_t)j * ncta + lcta] = 0.0; tpart_half(1)[(size_t)j * ncta + lcta] = 0.0; }
-            }
-        if (schur && nterms > 1) compute_part(tbuf[0], tpart_half(0));
+            for (int j = threadIdx.x; j < rank; j += kThreads) S.zpart[(size_t)j * ncta + lcta] = 0.0;
+        if (schur && nterms > 1) compute_part(tbuf[0], tpart_half(0) + aidx, nact);
         if (leader_cta)
             for (int j = threadIdx.x; j < rank; j += kThreads) S.tt[j] = 0.0;
         if (nterms == 1) compute_zpart();
@@ -486,7 +631,13 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                 };
                 auto epi = [&](int row, CT y0, CT y1, CT y2) {
                     CT g0, g1, g2;
-                    gather(row, g0, g1, g2);
+                    if (res) {
+                        VT u0, u1, u2;
+                        Vec4<VT>::load(s_win, wown + row - rb, u0, u1, u2);
+                        g0 = (CT)u0; g1 = (CT)u1; g2 = (CT)u2;
+                    } else {
+                        gather(row, g0, g1, g2);
+                    }
                     Vec4<VT>::store(pnew, row, (VT)g0, (VT)g1, (VT)g2);
                     int an = __ldg(S.rowflag + row);
                     if (!HSC_IN(an < a / 3, 206, an)) an = -1;
@@ -512,7 +663,20 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                         acc += (double)g0 * (double)(VT)y0 + (double)g1 * (double)(VT)y1 + (double)g2 * (double)(VT)y2;
                     }
                 };
-                spmv_warp<MT, CT>(wr0, wr1, rb, S.rowptr, S.colidx, S.rowid, s_col, s_row, kcta0, vals, nnz, s_y, gather, epi);
+                if (res) {
+                    // stage p = z + beta p_prev over the window, then the SpMV from shared memory
+                    for (int i = threadIdx.x; i < nwin; i += kThreads) {
+                        CT g0, g1, g2;
+                        gather(s_wn[i], g0, g1, g2);
+                        Vec4<VT>::store(s_win, i, (VT)g0, (VT)g1, (VT)g2);
+                    }
+                    __syncthreads();
+                    spmv_warp_res<kNB, MT, CT, VT>(wr0, wr1, rb, S.rowptr, kcta0, nblk, s_val, s_lc, s_lr, s_win, s_y, epi);
+                    __syncthreads();
+                } else {
+                    spmv_warp<kNB, MT, CT>(wr0, wr1, rb, S.rowptr, S.colidx, S.rowid, s_col, s_row, kcta0, vals, nnz, s_y,
+                                      gather, epi);
+                }
                 // tt_j = (Vt^T z)_j + beta tt_j from the per-CTA partials of Vt^T z
                 for (int j = gwarp; j < rank; j += nwarp) {
                     double sz, unused;
@@ -531,7 +695,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                     Vec4<double>::load(rhs, row, h0, h1, h2);
                     Vec4<double>::store(r, row, h0 - y0, h1 - y1, h2 - y2);
                 };
-                spmv_warp<double, double>(wr0, wr1, rb, S.rowptr, S.colidx, S.rowid, s_col, s_row, kcta0, S.vals64, nnz, s_y, gather, epi);
+                spmv_warp<kNB, double, double>(wr0, wr1, rb, S.rowptr, S.colidx, S.rowid, s_col, s_row, kcta0, S.vals64, nnz, s_y, gather, epi);
                 for (int j = gwarp; j < rank; j += nwarp) {
                     const double* col = vt + (size_t)j * a;
                     double d = 0.0;
@@ -574,9 +738,10 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                     const double* tsrc = slot == kNormal ? S.tt : S.ttx;
                     for (int j = threadIdx.x; j < rank; j += kThreads) s_dtt[j] = __ldg(S.dpiv + j) * tsrc[j];
                     __syncthreads();
+                    lowrank_rows(s_z);
+                    __syncthreads();
                     for (int il = threadIdx.x; il < na; il += kThreads) {
-                        double c = 0.0;
-                        for (int j = 0; j < rank; ++j) c += vt_own(j, il) * s_dtt[j];
+                        const double c = s_z[il];
                         if (slot == kNormal) S.yact[ab + il] -= c;                     // y = D p - Vt d Vt^T p
                         else elem<double>(r, __ldg(S.act + ab + il)) += c;           // r = rhs - D x + Vt d Vt^T x
                     }
@@ -623,7 +788,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                     pc ^= 1;
                 }
                 if (nterms == 1) compute_zpart();
-                else if (schur) compute_part(tbuf[tc], tpart_half(0));
+                else if (schur) compute_part(tbuf[tc], tpart_half(0) + aidx, nact);
             }
             if (!work) slot = kIdle;
             mark(3);

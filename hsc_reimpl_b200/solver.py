@@ -61,6 +61,7 @@ class HSCOptions:
     spin_limit: int = 20_000_000
     check_residual: bool = True
     trace_iterations: int = 0
+    resident: bool = True                  # BSR slices + vector windows in shared memory when they fit
 
     @classmethod
     def reference(cls):
@@ -102,6 +103,7 @@ class HSCOptions:
         o.spin_limit = int(self.spin_limit)
         o.check_residual = int(bool(self.check_residual))
         o.trace_iterations = int(self.trace_iterations)
+        o.resident = int(bool(self.resident))
         return o
 
 

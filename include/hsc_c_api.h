@@ -105,11 +105,14 @@ typedef struct hsc_options {
     int32_t max_refinements;
     int32_t fallback_on_stall;   /* polynomial / learned preconditioners: redo a single-system solve with plain
                                     Neumann (neumann_order) when PCG breaks down or hits max_iter */
-    int32_t threads_per_row;     /* SpMV lanes per block row: 2, 4 or 8 (autotuned) */
+    int32_t threads_per_row;     /* SpMV tile width: 2, 4 or 8 -> 1, 2 or 4 slices of 32 blocks loaded per
+                                    warp round trip (autotuned, default 4) */
     int64_t spin_limit;          /* bound on every device-side barrier wait */
     int32_t check_residual;      /* 1: compute the full residual and enforce full_residual_limit */
     int32_t trace_iterations;    /* > 0: record per-CTA SM clocks at the PCG phase boundaries of the
                                     first iterations (hsc_get_trace) */
+    int32_t resident;            /* 1: each PCG CTA keeps its BSR slice and vector window in shared memory
+                                    when they fit (else they stream from L2); 0: always stream */
 } hsc_options;
 
 typedef struct hsc_stats {        /* superset of the hsc_stats.jsonl record (linear_hsc.cu:420-431) */
