@@ -58,6 +58,7 @@ class Options(C.Structure):
         ("check_residual", C.c_int32),
         ("trace_iterations", C.c_int32),
         ("resident", C.c_int32),
+        ("fuse_update", C.c_int32),
     ]
 
 

@@ -6,7 +6,11 @@ candidate (``threads_per_row`` -> slices of 32 blocks a warp loads per round
 trip, ``max_rank`` -> ACA rank cap) with CUDA events and keeps the fastest one
 whose every system still meets the FP64-verified full-system residual target.
 A rank cap below what the coupling needs leaves an ACA error that no PCG
-tolerance can remove, so the residual test is what bounds the rank from below.
+tolerance can remove -- and can make the approximate Schur complement
+indefinite, which PCG reports as a breakdown -- so the status and residual
+tests are what bound the rank from below.  The default relaxation is
+omega = 0.6: block-Jacobi-scaled cube and torus operators reach
+lambda_max(Dd^-1 D) = 2.9, where the order-2 series needs omega < 2 / 2.9.
 """
 from __future__ import annotations
 
@@ -19,7 +23,7 @@ import numpy as np
 from .solver import DeviceSystem, HSCContext, HSCOptions
 
 TILES = (2, 4, 8)
-RANKS = (4, 8, 16, 32)
+RANKS = (4, 8, 16, 32, 64, 128)
 
 
 def time_batch(ctx, systems, xs, reps=3, warmup=1, use_graph=True):
@@ -45,7 +49,7 @@ def autotune(systems, base: HSCOptions | None = None, tiles=TILES, ranks=RANKS, 
              use_graph=True, log=None):
     """Returns (best options, table of every candidate)."""
     import torch
-    base = base or HSCOptions(precision="fp32", residual_replacement=50)
+    base = base or HSCOptions(precision="fp32", residual_replacement=50, omega=0.6)
     devs = [s if isinstance(s, DeviceSystem) else DeviceSystem.from_system(s) for s in systems]
     xs = [torch.empty_like(d.b) for d in devs]
     table = []

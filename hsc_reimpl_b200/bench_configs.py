@@ -5,7 +5,7 @@
 c1  the 1,331-node cube with one affine plate (error against a sparse direct solve)
 c3  64 uneven systems in one persistent launch replayed as a CUDA graph, FP32
     values with FP64 residual replacement every 50 iterations, after the
-    autotuner (tile width x ACA rank cap 4-32)
+    autotuner (tile width x ACA rank cap 4-128; omega 0.6)
 c4  the learned polynomial preconditioner on held-out vehicle trajectories:
     PCG iterations and time to 1e-6 against plain order-2 Neumann (FP64 and FP32)
 c5  the 1 M-tet torus (12 bodies, 30 % contact-active tread): FP64 / FP32 /
@@ -77,7 +77,7 @@ def c3(flush, count=64):
     systems = make_batch_systems(seed=0, count=count)
     gen_s = time.time() - t
     devs = [DeviceSystem.from_system(s) for s in systems]
-    base = HSCOptions(precision="fp32", residual_replacement=50)
+    base = HSCOptions(precision="fp32", residual_replacement=50, omega=0.6)
     best, table = autotune(devs, base=base, log=log)
     out = {"workload": f"batch_{count}_uneven", "systems": count, "generation_s": gen_s,
            "tets": [int(s.meta["tets"]) for s in systems], "bodies": [int(s.meta["bodies"]) for s in systems],

@@ -88,10 +88,11 @@ struct System {
     unsigned long long hash = 0;
     // sizes
     int n = 0, nnz = 0, a = 0, nqq = 0, nqf = 0, kmax = 0, qm = 0, qo = 0, fo = 0, fn = 0;
-    std::vector<int> h_rowptr, h_act, h_colidx;
+    std::vector<int> h_rowptr, h_act, h_colidx, h_rowflag;
     // plan
     DevBuf rowptr, colidx, rowid, src, diag_pos, qq, qf, act, ident, rowflag;
     // numeric
+    DevBuf r2;
     DevBuf v64, vf32, vbf16, dinv, A, E, R0, R1, U, V, hist, P, Ptmp, T, term, Binv, L, W, C, Lc, dpiv, vt64, vtmt,
         cvec, tt, ttx, bq, bf, x, r, z, p0, p1, y, t0, t1, node_nz, xq, ypad, yq, work, cg, scal, dact, pact, yact,
         zpart, tpart, lcol;
@@ -115,9 +116,10 @@ struct hsc_ctx {
     std::vector<System> sys;
     // PCG launch state
     DevBuf d_desc, d_cta_sys, d_cta_row, d_cta_act, d_cta_aidx, d_cta_warp, d_part, d_bar, d_remaining, d_trace;
-    DevBuf d_win_off, d_win_nodes, d_win_own;
+    DevBuf d_win_off, d_win_nodes, d_win_own, d_win_flag, d_win_act_off, d_win_act;
     int off_z = 0, off_vt = 0, off_y = 0, off_blk = 0, stage_vt = 0, stage_blk = 0;
-    int resident = 0, off_wn = 0, off_win = 0, off_val = 0, off_vpc = 0, off_lidx = 0;
+    int resident = 0, stage_vals = 0, off_wn = 0, off_win = 0, off_val = 0, off_vpc = 0, off_lidx = 0, off_dinv = 0, off_rf = 0;
+    int off_own = 0, off_act = 0, own_rows = 0, own_act = 0, off_wflag = 0, off_wact = 0, off_wcorr = 0, wact_max = 0;
     int grid = 0;
     int vt_smem = 0;           // doubles of PCG shared memory after the d.*tt slot
     size_t pcg_smem = 0;       // dynamic shared memory bytes of the PCG launch
@@ -284,6 +286,7 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
             for (int c = 0; c < 3; ++c) S.h_act[3 * act_index[i] + c] = 3 * i + c;
     std::vector<int> rowflag(S.n, -1);
     for (int i = 0; i < S.n; ++i) rowflag[i] = act_index[i];
+    S.h_rowflag = rowflag;
     std::vector<int> qf;
     qf.reserve(qfraw.size());
     {
@@ -361,6 +364,7 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
     GROW(S.bf, sizeof(double) * n4);
     GROW(S.x, sizeof(double) * n4);
     GROW(S.r, sizeof(double) * n4);
+    GROW(S.r2, sizeof(double) * n4);
     GROW(S.z, vt_bytes(P) * n4);
     GROW(S.p0, vt_bytes(P) * n4);
     GROW(S.p1, vt_bytes(P) * n4);
@@ -669,7 +673,7 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
         GROW(S.tpart, sizeof(double) * 2 * std::max(1, S.kmax) * (size_t)std::max(1, nact));
         d.tpart = S.tpart.as<double>();
         d.wdev = o.preconditioner == HSC_PRECOND_LEARNED ? S.scal.as<DevScal>()->wl : nullptr;
-        d.x = S.x.as<double>(); d.r = S.r.as<double>(); d.rhs = S.bf.as<double>(); d.z = S.z.p;
+        d.x = S.x.as<double>(); d.r = S.r.as<double>(); d.r2 = S.r2.as<double>(); d.rhs = S.bf.as<double>(); d.z = S.z.p;
         d.p[0] = S.p0.p; d.p[1] = S.p1.p; d.y = S.y.p; d.t[0] = S.t0.p; d.t[1] = S.t1.p; d.tt = S.tt.as<double>();
         d.out = S.scal.as<DevScal>()->pcg; d.cg_coef = S.cg.as<double>(); d.max_coef = kMaxCoef;
     }
@@ -697,8 +701,8 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
     }
     // vector windows (resident mode): the sorted nodes each CTA's blocks read,
     // and per BSR entry the window position of its column
-    std::vector<int> win_off(G + 1, 0), win_nodes, win_own(G, 0);
-    int Wmax = 0;
+    std::vector<int> win_off(G + 1, 0), win_nodes, win_own(G, 0), win_flag, win_act_off(G + 1, 0), win_act;
+    int Wmax = 0, WAmax = 0;
     bool win_ok = o.resident != 0;
     {
         std::vector<int> stamp, pos;
@@ -720,6 +724,14 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
             win_own[k] = rb < re ? pos[rb] : 0;
             win_off[k + 1] = win_off[k] + (int)w.size();
             win_nodes.insert(win_nodes.end(), w.begin(), w.end());
+            int nwa = 0;
+            for (int c : w) {
+                const int an = S.h_rowflag[c];
+                win_flag.push_back(an >= 0 ? nwa : -1);
+                if (an >= 0) { win_act.push_back(an); ++nwa; }
+            }
+            win_act_off[k + 1] = win_act_off[k] + nwa;
+            WAmax = std::max(WAmax, nwa);
             Wmax = std::max(Wmax, (int)w.size());
         }
     }
@@ -736,12 +748,24 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
     const int W_wn = dbl(sizeof(int) * (size_t)Wmax), W_win = dbl(4 * vtb * (size_t)Wmax);
     const int W_val = dbl(9 * mtb * (size_t)BLKmax), W_vpc = o.precision == 2 ? dbl(9 * 2 * (size_t)BLKmax) : 0;
     const int W_lidx = dbl(4 * (size_t)BLKmax);
-    const int res_need = base + 4 + W_wn + W_win + W_val + W_vpc + W_lidx;
-    int stage_vt = 1, stage_blk = 1, resident = 0;
-    if (win_ok && res_need <= res_budget) {
+    const int W_dinv = dbl(9 * mtb * (size_t)Rmax), W_rf = dbl(sizeof(int) * (2 * (size_t)Rmax + 1));
+    const int W_own = dbl(2 * 3 * 8 * (size_t)Rmax + 4 * 3 * vtb * (size_t)Rmax);
+    const int W_act = dbl(2 * 8 * (size_t)Zmax + sizeof(int) * (size_t)Zmax);
+    const int W_wflag = dbl(sizeof(int) * (size_t)Wmax), W_wact = dbl(sizeof(int) * (size_t)WAmax);
+    const int W_wcorr = dbl(3 * 8 * (size_t)WAmax);
+    const int res_need = base + 4 + W_wn + W_win + W_val + W_vpc + W_lidx + W_dinv + W_rf + W_own + W_act + W_wflag +
+                         W_wact + W_wcorr;
+    // resident: Vt blocks first (they sit on the critical path of the coupled
+    // CTAs), then the value planes; without room for the planes they stream
+    const int need_novals = res_need - W_val - W_vpc;
+    int stage_vt = 1, stage_blk = 1, resident = 0, stage_vals = 0;
+    if (win_ok && need_novals <= res_budget) {
         resident = 1;
         stage_blk = 0;
-        stage_vt = res_need + VTmax <= res_budget ? 1 : 0;
+        if (res_need + VTmax <= res_budget) { stage_vt = 1; stage_vals = 1; }
+        else if (need_novals + VTmax <= res_budget) { stage_vt = 1; stage_vals = 0; }
+        else if (res_need <= res_budget) { stage_vt = 0; stage_vals = 1; }
+        else { stage_vt = 0; stage_vals = 0; }
     } else if (base + VTmax + BLKmax > budget) {
         if (base + BLKmax <= budget) stage_vt = 0;
         else if (base + VTmax <= budget) stage_blk = 0;
@@ -757,13 +781,32 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
     ctx->stage_blk = stage_blk;
     ctx->vt_smem = Zmax + VTmax;
     ctx->resident = resident;
+    ctx->stage_vals = stage_vals;
     if (resident) {
         ctx->off_wn = ctx->off_blk;
         ctx->off_win = ctx->off_wn + W_wn;
         ctx->off_val = ctx->off_win + W_win;
-        ctx->off_vpc = ctx->off_val + W_val;
-        ctx->off_lidx = ctx->off_vpc + W_vpc;
-        ctx->pcg_smem = sizeof(double) * (size_t)(ctx->off_lidx + W_lidx);
+        ctx->off_vpc = ctx->off_val + (stage_vals ? W_val : 0);
+        ctx->off_lidx = ctx->off_vpc + (stage_vals ? W_vpc : 0);
+        ctx->off_dinv = ctx->off_lidx + W_lidx;
+        ctx->off_rf = ctx->off_dinv + W_dinv;
+        ctx->off_own = ctx->off_rf + W_rf;
+        ctx->off_act = ctx->off_own + W_own;
+        ctx->own_rows = Rmax;
+        ctx->own_act = Zmax;
+        ctx->off_wflag = ctx->off_act + W_act;
+        ctx->off_wact = ctx->off_wflag + W_wflag;
+        ctx->off_wcorr = ctx->off_wact + W_wact;
+        ctx->wact_max = WAmax;
+        ctx->pcg_smem = sizeof(double) * (size_t)(ctx->off_wcorr + W_wcorr);
+        GROW(ctx->d_win_flag, sizeof(int) * std::max<size_t>(1, win_flag.size()));
+        GROW(ctx->d_win_act_off, sizeof(int) * (G + 1));
+        GROW(ctx->d_win_act, sizeof(int) * std::max<size_t>(1, win_act.size()));
+        if (!win_flag.empty())
+            CK(cudaMemcpyAsync(ctx->d_win_flag.p, win_flag.data(), sizeof(int) * win_flag.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->d_win_act_off.p, win_act_off.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice, st));
+        if (!win_act.empty())
+            CK(cudaMemcpyAsync(ctx->d_win_act.p, win_act.data(), sizeof(int) * win_act.size(), cudaMemcpyHostToDevice, st));
         GROW(ctx->d_win_off, sizeof(int) * (G + 1));
         GROW(ctx->d_win_nodes, sizeof(int) * std::max<size_t>(1, win_nodes.size()));
         GROW(ctx->d_win_own, sizeof(int) * G);
@@ -790,7 +833,10 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
     GROW(ctx->d_cta_act, sizeof(int) * 2 * G);
     GROW(ctx->d_cta_aidx, sizeof(int) * G);
     GROW(ctx->d_part, sizeof(double) * 3 * G);
-    GROW(ctx->d_bar, sizeof(GridBar));
+    if (!ctx->d_bar.p) {
+        GROW(ctx->d_bar, sizeof(GridBar));
+        CK(cudaMemsetAsync(ctx->d_bar.p, 0, sizeof(GridBar), st));
+    }
     GROW(ctx->d_remaining, sizeof(int));
     CK(cudaMemcpyAsync(ctx->d_desc.p, desc.data(), sizeof(SysDesc) * ns, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->d_cta_sys.p, cta_sys.data(), sizeof(int) * G, cudaMemcpyHostToDevice, st));
@@ -841,13 +887,20 @@ int launch_pcg_all(hsc_ctx* ctx, int nsys, cudaStream_t st) {
     prm.off_z = ctx->off_z; prm.off_vt = ctx->off_vt; prm.off_y = ctx->off_y; prm.off_blk = ctx->off_blk;
     prm.stage_vt = ctx->stage_vt; prm.stage_blk = ctx->stage_blk;
     prm.resident = ctx->resident;
+    prm.stage_vals = ctx->stage_vals;
     prm.win_off = ctx->d_win_off.as<int>(); prm.win_nodes = ctx->d_win_nodes.as<int>(); prm.win_own = ctx->d_win_own.as<int>();
     prm.off_wn = ctx->off_wn; prm.off_win = ctx->off_win; prm.off_val = ctx->off_val; prm.off_vpc = ctx->off_vpc;
     prm.off_lidx = ctx->off_lidx;
+    prm.off_dinv = ctx->off_dinv; prm.off_rf = ctx->off_rf;
+    prm.off_own = ctx->off_own; prm.off_act = ctx->off_act; prm.own_rows = ctx->own_rows; prm.own_act = ctx->own_act;
+    prm.win_flag = ctx->d_win_flag.as<int>(); prm.win_act_off = ctx->d_win_act_off.as<int>();
+    prm.win_act = ctx->d_win_act.as<int>();
+    prm.off_wflag = ctx->off_wflag; prm.off_wact = ctx->off_wact; prm.off_wcorr = ctx->off_wcorr;
+    prm.wact_max = ctx->wact_max;
     prm.trace = nullptr;
     prm.trace_iters = 0;
     if (o.trace_iterations > 0) {
-        const size_t nt = (size_t)ctx->grid * o.trace_iterations * 8;
+        const size_t nt = (size_t)ctx->grid * o.trace_iterations * kTraceEvents;
         GROW(ctx->d_trace, sizeof(unsigned long long) * nt);
         CK(cudaMemsetAsync(ctx->d_trace.p, 0, sizeof(unsigned long long) * nt, st));
         prm.trace = ctx->d_trace.as<unsigned long long>();
@@ -867,6 +920,7 @@ int launch_pcg_all(hsc_ctx* ctx, int nsys, cudaStream_t st) {
         prm.nterms = o.neumann_order;
         for (int k = 0; k < o.neumann_order; ++k) prm.w[k] = 1.0;
     }
+    prm.fuse = ctx->resident && o.fuse_update && !prm.schur_basis && prm.nterms >= 2;
     prm.tol = o.tol;
     prm.max_iter = o.max_iter;
     prm.rr_every = o.residual_replacement;
@@ -985,7 +1039,10 @@ int ensure_common(hsc_ctx* ctx, cudaStream_t st) {
     GROW(ctx->aca_psum, sizeof(double) * 4096);
     GROW(ctx->aca_pmax, sizeof(double) * 4096);
     GROW(ctx->aca_pidx, sizeof(long long) * 4096);
-    GROW(ctx->aca_bar, sizeof(GridBar));
+    if (!ctx->aca_bar.p) {
+        GROW(ctx->aca_bar, sizeof(GridBar));
+        CK(cudaMemsetAsync(ctx->aca_bar.p, 0, sizeof(GridBar), st));  // read back even when no grid ACA ran
+    }
     GROW(ctx->res_part, sizeof(double) * 3 * kResParts);
     GROW(ctx->feat_part, sizeof(double) * kFeatParts * 2 * std::max(1, ctx->num_sms));
     if (!ctx->aca_grid) ctx->aca_grid = std::min(4096, std::max(1, aca_blocks_per_sm()) * ctx->num_sms);
@@ -1103,7 +1160,8 @@ int hsc_options_default(hsc_options* o) {
     o->spin_limit = 20000000;
     o->check_residual = 1;
     o->trace_iterations = 0;
-    o->resident = 1;
+    o->resident = 0;
+    o->fuse_update = 0;
     return HSC_OK;
 }
 
@@ -1450,7 +1508,7 @@ int hsc_get_factors(hsc_ctx* ctx, int32_t sys, int32_t* rank, int32_t* n_active,
 
 int hsc_get_trace(hsc_ctx* ctx, unsigned long long* out, int64_t max_entries, int32_t* ctas, int32_t* iterations) {
     if (!ctx || ctx->opt.trace_iterations <= 0 || !ctx->d_trace.p) return HSC_ERR_NOTREADY;
-    const int64_t nt = (int64_t)ctx->grid * ctx->opt.trace_iterations * 8;
+    const int64_t nt = (int64_t)ctx->grid * ctx->opt.trace_iterations * kTraceEvents;
     if (ctas) *ctas = ctx->grid;
     if (iterations) *iterations = ctx->opt.trace_iterations;
     if (out) CK(cudaMemcpy(out, ctx->d_trace.p, sizeof(unsigned long long) * std::min(nt, max_entries),

@@ -169,6 +169,7 @@ struct SysDesc {
     const int* rank;       // device scalar
     double* x;             // FP64 node-padded
     double* r;             // FP64 node-padded
+    double* r2;            // second residual buffer (fused update: neighbours read the old r)
     const double* rhs;     // FP64 node-padded
     void* z;               // VT node-padded
     void* p[2];            // VT node-padded ping-pong
@@ -189,6 +190,7 @@ struct SysDesc {
     int max_coef;
 };
 
+constexpr int kTraceEvents = 16;  // clock slots per CTA and iteration in trace mode
 constexpr int kMaxCoef = 256;  // CG coefficients kept per solve for the Lanczos estimates
 
 struct PcgParams {
@@ -223,10 +225,22 @@ struct PcgParams {
     // planes), local indices and the window of vector nodes its blocks read in
     // shared memory; a phase stages the window once and runs the SpMV from there
     int resident;
+    int stage_vals;            // resident mode: the value planes are copied too (else read from L2)
     const int* win_off;        // per CTA: G + 1 offsets into win_nodes
     const int* win_nodes;      // sorted global node ids of each CTA's window
     const int* win_own;        // per CTA: window position of its first row
     int off_wn, off_win, off_val, off_vpc, off_lidx;  // shared-memory offsets (doubles)
+    int off_dinv, off_rf;      // the CTA's rows' Dd^-1 planes and row flags (resident mode)
+    int off_own, off_act;      // own-row vectors (x, r, z, p, y, t) and coupled-dof values / list
+    // fused update (resident mode, FEM-basis polynomial, normal slots): after the
+    // alpha barrier every CTA forms t0 = w Dd^-1 (r - alpha y) over its window
+    // itself, so the update and the first preconditioner phase share a barrier
+    int fuse;
+    const int* win_flag;       // per window entry: position in the CTA's coupled-window list, or -1
+    const int* win_act_off;    // per CTA: G + 1 offsets into win_act
+    const int* win_act;        // active-node index (rowflag) of each coupled window node
+    int off_wflag, off_wact, off_wcorr, wact_max;
+    int own_rows, own_act;     // rows and coupled dofs the own-row regions hold (the maxima over CTAs)
 };
 
 // launch counter of this library (hsc_setup.cu)

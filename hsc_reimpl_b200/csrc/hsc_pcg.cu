@@ -50,6 +50,15 @@ template <> struct Cmp<double> { using T = double; };
 template <class MT> struct DinvT { using T = float; };
 template <> struct DinvT<double> { using T = double; };
 
+// b0 x0 + b1 x1 + b2 x2 with explicit fused multiply-adds, so the rounding
+// does not depend on how the compiler contracts the surrounding code
+__device__ __forceinline__ float dot3(float b0, float b1, float b2, float x0, float x1, float x2) {
+    return __fmaf_rn(b2, x2, __fmaf_rn(b1, x1, b0 * x0));
+}
+__device__ __forceinline__ double dot3(double b0, double b1, double b2, double x0, double x1, double x2) {
+    return __fma_rn(b2, x2, __fma_rn(b1, x1, b0 * x0));
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -133,9 +142,9 @@ __device__ __forceinline__ void spmv_warp(int wr0, int wr1, int rb, const int* _
                          b4 = Num<MT>::get(__ldg(v + 4 * st)), b5 = Num<MT>::get(__ldg(v + 5 * st)),
                          b6 = Num<MT>::get(__ldg(v + 6 * st)), b7 = Num<MT>::get(__ldg(v + 7 * st)),
                          b8 = Num<MT>::get(__ldg(v + 8 * st));
-                p0[h] = b0 * x0 + b1 * x1 + b2 * x2;
-                p1[h] = b3 * x0 + b4 * x1 + b5 * x2;
-                p2[h] = b6 * x0 + b7 * x1 + b8 * x2;
+                p0[h] = dot3(b0, b1, b2, x0, x1, x2);
+                p1[h] = dot3(b3, b4, b5, x0, x1, x2);
+                p2[h] = dot3(b6, b7, b8, x0, x1, x2);
             }
         }
 #pragma unroll
@@ -199,9 +208,9 @@ __device__ __forceinline__ void spmv_warp_res(int wr0, int wr1, int rb, const in
                          b3 = Num<MT>::get(v[3 * nblk]), b4 = Num<MT>::get(v[4 * nblk]),
                          b5 = Num<MT>::get(v[5 * nblk]), b6 = Num<MT>::get(v[6 * nblk]),
                          b7 = Num<MT>::get(v[7 * nblk]), b8 = Num<MT>::get(v[8 * nblk]);
-                p0[h] = b0 * x0 + b1 * x1 + b2 * x2;
-                p1[h] = b3 * x0 + b4 * x1 + b5 * x2;
-                p2[h] = b6 * x0 + b7 * x1 + b8 * x2;
+                p0[h] = dot3(b0, b1, b2, x0, x1, x2);
+                p1[h] = dot3(b3, b4, b5, x0, x1, x2);
+                p2[h] = dot3(b6, b7, b8, x0, x1, x2);
             }
         }
 #pragma unroll
@@ -231,6 +240,43 @@ __device__ __forceinline__ void spmv_warp_res(int wr0, int wr1, int rb, const in
     }
 }
 
+// y_row = sum_k B_k x[col_k] from the CTA's shared-memory copy, four threads
+// per row: each sums its blocks k = first + sub, + 4, ... in order, then a
+// fixed butterfly adds the four partial sums; the sub == 0 thread runs the
+// epilogue.  No scan: in shared memory the load pattern needs no warp-wide
+// coalescing, and a row has ~12 blocks.
+template <bool kGlobalVals, class MT, class CT, class VT, class Epi>
+__device__ __forceinline__ void spmv_rows_res(int rb, int nrow, const int* s_rp, size_t pstride, const MT* val,
+                                              const unsigned short* s_lc, const VT* s_win, Epi& epi) {
+    // value planes: shared memory (val = the CTA's copy, pstride = its block
+    // count) or global memory (val = the CTA's first block, pstride = nnz)
+    auto ld = [&](const MT* p) -> CT { return (CT)Num<MT>::get(kGlobalVals ? __ldg(p) : *p); };
+    const int sub = threadIdx.x & 3;
+    for (int lr0 = 0; lr0 < nrow; lr0 += kThreads / 4) {
+        const int lr = lr0 + (threadIdx.x >> 2);
+        CT a0 = 0, a1 = 0, a2 = 0;
+        if (lr < nrow) {
+            const int k1 = s_rp[lr + 1];
+            for (int k = s_rp[lr] + sub; k < k1; k += 4) {
+                VT u0, u1, u2;
+                Vec4<VT>::load(s_win, s_lc[k], u0, u1, u2);
+                const CT x0 = (CT)u0, x1 = (CT)u1, x2 = (CT)u2;
+                const MT* v = val + k;
+                a0 += dot3(ld(v), ld(v + pstride), ld(v + 2 * pstride), x0, x1, x2);
+                a1 += dot3(ld(v + 3 * pstride), ld(v + 4 * pstride), ld(v + 5 * pstride), x0, x1, x2);
+                a2 += dot3(ld(v + 6 * pstride), ld(v + 7 * pstride), ld(v + 8 * pstride), x0, x1, x2);
+            }
+        }
+        a0 += __shfl_xor_sync(0xffffffffu, a0, 1);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, 1);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, 1);
+        a0 += __shfl_xor_sync(0xffffffffu, a0, 2);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, 2);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, 2);
+        if (lr < nrow && sub == 0) epi(rb + lr, a0, a1, a2);
+    }
+}
+
 template <class DT>
 __device__ __forceinline__ void dinv_apply(const DT* __restrict__ dinv, int n, int row, double s,
                                            double r0, double r1, double r2, double& o0, double& o1, double& o2) {
@@ -238,6 +284,18 @@ __device__ __forceinline__ void dinv_apply(const DT* __restrict__ dinv, int n, i
     const double d0 = __ldg(d), d1 = __ldg(d + n), d2 = __ldg(d + 2 * (size_t)n);
     const double d3 = __ldg(d + 3 * (size_t)n), d4 = __ldg(d + 4 * (size_t)n), d5 = __ldg(d + 5 * (size_t)n);
     const double d6 = __ldg(d + 6 * (size_t)n), d7 = __ldg(d + 7 * (size_t)n), d8 = __ldg(d + 8 * (size_t)n);
+    o0 = s * (d0 * r0 + d1 * r1 + d2 * r2);
+    o1 = s * (d3 * r0 + d4 * r1 + d5 * r2);
+    o2 = s * (d6 * r0 + d7 * r1 + d8 * r2);
+}
+
+// dinv_apply on the CTA's shared-memory copy of its rows' planes (stride = its row count)
+template <class DT>
+__device__ __forceinline__ void dinv_apply_s(const DT* sd, int stride, int lr, double s, double r0, double r1,
+                                             double r2, double& o0, double& o1, double& o2) {
+    const DT* d = sd + lr;
+    const double d0 = d[0], d1 = d[stride], d2 = d[2 * stride], d3 = d[3 * stride], d4 = d[4 * stride];
+    const double d5 = d[5 * stride], d6 = d[6 * stride], d7 = d[7 * stride], d8 = d[8 * stride];
     o0 = s * (d0 * r0 + d1 * r1 + d2 * r2);
     o1 = s * (d3 * r0 + d4 * r1 + d5 * r2);
     o2 = s * (d6 * r0 + d7 * r1 + d8 * r2);
@@ -319,18 +377,134 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
     PT* s_vpc = std::is_same<MT, PT>::value ? reinterpret_cast<PT*>(s_val) : reinterpret_cast<PT*>(smem + prm.off_vpc);
     unsigned short* s_lc = reinterpret_cast<unsigned short*>(smem + prm.off_lidx);
     unsigned short* s_lr = s_lc + nblk;
+    const int nrow = re - rb;
+    const int Rown = prm.own_rows, Zown = prm.own_act;
+    DT* s_dinv = reinterpret_cast<DT*>(smem + prm.off_dinv);
+    int* s_rf = reinterpret_cast<int*>(smem + prm.off_rf);
+    int* s_rp = s_rf + Rown;   // the CTA's row pointers, local to its first block (nrow + 1)
     if (res) {
-        for (int e = threadIdx.x; e < 9 * nblk; e += kThreads) {
-            const int pl = e / nblk, kl = e - pl * nblk;
-            s_val[e] = vals[(size_t)pl * nnz + kcta0 + kl];
-            if (!std::is_same<MT, PT>::value) s_vpc[e] = vals_pc[(size_t)pl * nnz + kcta0 + kl];
-        }
+        if (prm.stage_vals)
+            for (int e = threadIdx.x; e < 9 * nblk; e += kThreads) {
+                const int pl = e / nblk, kl = e - pl * nblk;
+                s_val[e] = vals[(size_t)pl * nnz + kcta0 + kl];
+                if (!std::is_same<MT, PT>::value) s_vpc[e] = vals_pc[(size_t)pl * nnz + kcta0 + kl];
+            }
         for (int e = threadIdx.x; e < nblk; e += kThreads) {
             s_lc[e] = S.lcol[kcta0 + e];
             s_lr[e] = (unsigned short)(__ldg(S.rowid + kcta0 + e) - rb);
         }
         for (int e = threadIdx.x; e < nwin; e += kThreads) s_wn[e] = prm.win_nodes[wn0 + e];
+        for (int e = threadIdx.x; e < 9 * nrow; e += kThreads) {
+            const int pl = e / nrow, lr = e - pl * nrow;
+            s_dinv[e] = dinv[(size_t)pl * n + rb + lr];
+        }
+        for (int e = threadIdx.x; e < nrow; e += kThreads) s_rf[e] = __ldg(S.rowflag + rb + e);
+        for (int e = threadIdx.x; e <= nrow; e += kThreads) s_rp[e] = __ldg(S.rowptr + rb + e) - kcta0;
     }
+    // own-row vectors (resident mode): x, r, z, the new direction p, y = S p and
+    // the current term t of the CTA's rows live in shared memory, 3 entries per
+    // row; x, z, p and t are also written through to global memory, where the
+    // neighbours' windows read them.  r and y never leave the CTA.
+    double* s_xo = reinterpret_cast<double*>(smem + prm.off_own);
+    double* s_ro = s_xo + 3 * Rown;
+    VT* s_zo = reinterpret_cast<VT*>(s_ro + 3 * Rown);
+    VT* s_po = s_zo + 3 * Rown;
+    VT* s_yo = s_po + 3 * Rown;
+    VT* s_to = s_yo + 3 * Rown;
+    double* s_pa = reinterpret_cast<double*>(smem + prm.off_act);
+    double* s_ya = s_pa + Zown;
+    int* s_act = reinterpret_cast<int*>(s_ya + Zown);
+    if (res)
+        for (int e = threadIdx.x; e < na; e += kThreads) s_act[e] = __ldg(S.act + ab + e);
+    // fused update: window flags, the coupled window nodes and their corrections
+    const bool fuse = res && prm.fuse != 0;
+    int* s_wflag = reinterpret_cast<int*>(smem + prm.off_wflag);
+    int* s_wan = reinterpret_cast<int*>(smem + prm.off_wact);
+    double* s_wcorr = smem + prm.off_wcorr;
+    const int wa0 = fuse ? prm.win_act_off[cta] : 0, nwa = fuse ? prm.win_act_off[cta + 1] - wa0 : 0;
+    if (fuse) {
+        for (int e = threadIdx.x; e < nwin; e += kThreads) s_wflag[e] = prm.win_flag[wn0 + e];
+        for (int e = threadIdx.x; e < nwa; e += kThreads) s_wan[e] = prm.win_act[wa0 + e];
+    }
+    double* rbuf[2] = {S.r, S.r2};
+    int rcur = 0;      // residual buffer the neighbours read (fused update)
+    int tail_k0 = 1;   // first preconditioner phase the next precond_tail runs
+    auto ld_z = [&](int row, VT& a0, VT& a1, VT& a2) {
+        if (res) { const VT* q = s_zo + 3 * (row - rb); a0 = q[0]; a1 = q[1]; a2 = q[2]; }
+        else Vec4<VT>::load(z, row, a0, a1, a2);
+    };
+    auto st_z = [&](int row, VT a0, VT a1, VT a2) {
+        Vec4<VT>::store(z, row, a0, a1, a2);
+        if (res) { VT* q = s_zo + 3 * (row - rb); q[0] = a0; q[1] = a1; q[2] = a2; }
+    };
+    auto ld_r = [&](int row, double& a0, double& a1, double& a2) {
+        if (res) { const double* q = s_ro + 3 * (row - rb); a0 = q[0]; a1 = q[1]; a2 = q[2]; }
+        else Vec4<double>::load(r, row, a0, a1, a2);
+    };
+    auto st_r = [&](int row, double a0, double a1, double a2) {
+        if (res) {
+            double* q = s_ro + 3 * (row - rb); q[0] = a0; q[1] = a1; q[2] = a2;
+            if (fuse) Vec4<double>::store(rbuf[rcur], row, a0, a1, a2);
+        } else {
+            Vec4<double>::store(r, row, a0, a1, a2);
+        }
+    };
+    auto ld_x = [&](int row, double& a0, double& a1, double& a2) {
+        if (res) { const double* q = s_xo + 3 * (row - rb); a0 = q[0]; a1 = q[1]; a2 = q[2]; }
+        else Vec4<double>::load(x, row, a0, a1, a2);
+    };
+    auto st_x = [&](int row, double a0, double a1, double a2) {
+        Vec4<double>::store(x, row, a0, a1, a2);
+        if (res) { double* q = s_xo + 3 * (row - rb); q[0] = a0; q[1] = a1; q[2] = a2; }
+    };
+    auto ld_p = [&](const VT* pg, int row, VT& a0, VT& a1, VT& a2) {
+        if (res) { const VT* q = s_po + 3 * (row - rb); a0 = q[0]; a1 = q[1]; a2 = q[2]; }
+        else Vec4<VT>::load(pg, row, a0, a1, a2);
+    };
+    auto st_p = [&](VT* pg, int row, VT a0, VT a1, VT a2) {
+        Vec4<VT>::store(pg, row, a0, a1, a2);
+        if (res) { VT* q = s_po + 3 * (row - rb); q[0] = a0; q[1] = a1; q[2] = a2; }
+    };
+    auto ld_y = [&](int row, VT& a0, VT& a1, VT& a2) {
+        if (res) { const VT* q = s_yo + 3 * (row - rb); a0 = q[0]; a1 = q[1]; a2 = q[2]; }
+        else Vec4<VT>::load(y, row, a0, a1, a2);
+    };
+    auto st_y = [&](int row, VT a0, VT a1, VT a2) {
+        if (res) { VT* q = s_yo + 3 * (row - rb); q[0] = a0; q[1] = a1; q[2] = a2; }
+        if (!res || fuse) Vec4<VT>::store(y, row, a0, a1, a2);
+    };
+    auto st_t = [&](VT* tg, int row, VT a0, VT a1, VT a2) {
+        Vec4<VT>::store(tg, row, a0, a1, a2);
+        if (res) { VT* q = s_to + 3 * (row - rb); q[0] = a0; q[1] = a1; q[2] = a2; }
+    };
+    // direction / product at the coupled dofs (index i in the system's act list)
+    auto pact_ref = [&](int i) -> double& { return res ? s_pa[i - ab] : S.pact[i]; };
+    auto yact_ref = [&](int i) -> double& { return res ? s_ya[i - ab] : S.yact[i]; };
+    // rowflag / Dd^-1 of an own row: shared-memory copies in resident mode
+    auto rowflag_of = [&](int row) -> int { return res ? s_rf[row - rb] : __ldg(S.rowflag + row); };
+    auto dinv_row = [&](int row, double r0, double r1, double r2, double& o0, double& o1, double& o2) {
+        if (res) dinv_apply_s(s_dinv, nrow, row - rb, omega, r0, r1, r2, o0, o1, o2);
+        else dinv_apply(dinv, n, row, omega, r0, r1, r2, o0, o1, o2);
+    };
+    // stage node values into the window: every thread issues the loads of up
+    // to four (FP64: two) nodes before it stores any, so the window costs one
+    // round trip
+    auto stage_window = [&](auto&& load_node) {
+        constexpr int SQ = sizeof(VT) == 8 ? 2 : 4;
+        for (int i0 = threadIdx.x; i0 < nwin; i0 += SQ * kThreads) {
+            VT v[SQ][3];
+#pragma unroll
+            for (int q = 0; q < SQ; ++q) {
+                const int i = i0 + q * kThreads;
+                if (i < nwin) load_node(s_wn[i], v[q][0], v[q][1], v[q][2]);
+            }
+#pragma unroll
+            for (int q = 0; q < SQ; ++q) {
+                const int i = i0 + q * kThreads;
+                if (i < nwin) Vec4<VT>::store(s_win, i, v[q][0], v[q][1], v[q][2]);
+            }
+        }
+    };
     const bool vt_smem = prm.stage_vt && na > 0;
     HSC_IN(rank <= kMaxRank && rank <= S.kmax, 207, rank);
     HSC_IN(na <= 0 || ((na + 1) & ~1) + na * rank <= prm.vt_smem, 201, na);
@@ -356,7 +530,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
     int slot_no = 0;  // main-loop slots executed (trace index)
     auto mark = [&](int ev) {
         if (prm.trace && threadIdx.x == 0 && slot_no < prm.trace_iters)
-            prm.trace[((size_t)cta * prm.trace_iters + slot_no) * 8 + ev] = (unsigned long long)clock64();
+            prm.trace[((size_t)cta * prm.trace_iters + slot_no) * kTraceEvents + ev] = (unsigned long long)clock64();
     };
 
     // grid barrier with the CTA partials folded into the arrival: each warp
@@ -387,22 +561,50 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
     };
     // per-CTA partials of Vt^T v over the CTA's own coupled dofs (v final),
     // written to dst[j * stride]
-    auto compute_part = [&](void* v, double* dst, int stride) {
+    auto compute_part = [&](void* v, const VT* vown, double* dst, int stride) {
         if (na <= 0) return;  // uniform within the CTA
         __syncthreads();
         for (int il = threadIdx.x; il < na; il += kThreads) {
-            const int dof = __ldg(S.act + ab + il);
-            if (HSC_IN(dof >= 0 && dof < 3 * n, 204, dof)) s_z[il] = (double)elem<VT>(v, dof);
+            if (res) {
+                s_z[il] = (double)vown[s_act[il] - 3 * rb];
+            } else {
+                const int dof = __ldg(S.act + ab + il);
+                if (HSC_IN(dof >= 0 && dof < 3 * n, 204, dof)) s_z[il] = (double)elem<VT>(v, dof);
+            }
         }
         __syncthreads();
-        for (int j = warp; j < rank; j += kWarps) {
-            double sacc = 0.0;
-            for (int il = lane; il < na; il += 32) sacc += vt_own(j, il) * s_z[il];
-            sacc = warp_sum(sacc);
-            if (lane == 0 && HSC_IN(j < S.kmax, 205, j)) dst[(size_t)j * stride] = sacc;
+        // JW columns per warp, the first 128 coupled dofs fully unrolled so every
+        // Vt load of the warp is in flight at once (one round trip when Vt is
+        // read from L2); the summation order per column is il = lane, +32, ...
+        constexpr int JW = 6;
+        for (int j0 = warp * JW; j0 < rank; j0 += kWarps * JW) {
+            double sacc[JW];
+#pragma unroll
+            for (int q = 0; q < JW; ++q) sacc[q] = 0.0;
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const int il = lane + 32 * m;
+                if (il < na) {
+                    const double zv = s_z[il];
+#pragma unroll
+                    for (int q = 0; q < JW; ++q)
+                        if (j0 + q < rank) sacc[q] += vt_own(j0 + q, il) * zv;
+                }
+            }
+            for (int il = lane + 128; il < na; il += 32) {
+                const double zv = s_z[il];
+#pragma unroll
+                for (int q = 0; q < JW; ++q)
+                    if (j0 + q < rank) sacc[q] += vt_own(j0 + q, il) * zv;
+            }
+#pragma unroll
+            for (int q = 0; q < JW; ++q) {
+                const double t = warp_sum(sacc[q]);
+                if (lane == 0 && j0 + q < rank && HSC_IN(j0 + q < S.kmax, 205, j0 + q)) dst[(size_t)(j0 + q) * stride] = t;
+            }
         }
     };
-    auto compute_zpart = [&]() { compute_part(z, S.zpart + lcta, ncta); };
+    auto compute_zpart = [&]() { compute_part(z, s_zo, S.zpart + lcta, ncta); };
     const bool schur = prm.schur_basis != 0;
     const int nact = S.nact_cta;
     auto tpart_half = [&](int h) { return S.tpart + (size_t)h * S.kmax * nact; };
@@ -426,16 +628,24 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
             }
         }
     };
-    // out[il] = sum_j Vt[own il, j] s_dtt[j] for il < na: four threads per row
-    // (j interleaved), combined by shuffles in a fixed order
+    // out[il] = sum_j Vt[own il, j] s_dtt[j] for il < na: eight threads per
+    // row (j interleaved; the first 128 columns fully unrolled so all loads are
+    // in flight at once), combined by shuffles in a fixed order
     auto lowrank_rows = [&](double* out) {
-        for (int base = 0; base < na; base += kThreads / 4) {
-            const int il = base + (threadIdx.x >> 2), q = threadIdx.x & 3;
+        for (int base = 0; base < na; base += kThreads / 8) {
+            const int il = base + (threadIdx.x >> 3), q = threadIdx.x & 7;
             double c = 0.0;
-            if (il < na)
-                for (int j = q; j < rank; j += 4) c += vt_own(j, il) * s_dtt[j];
+            if (il < na) {
+#pragma unroll
+                for (int m = 0; m < 16; ++m) {
+                    const int j = q + 8 * m;
+                    if (j < rank) c += vt_own(j, il) * s_dtt[j];
+                }
+                for (int j = q + 128; j < rank; j += 8) c += vt_own(j, il) * s_dtt[j];
+            }
             c += __shfl_xor_sync(0xffffffffu, c, 1);
             c += __shfl_xor_sync(0xffffffffu, c, 2);
+            c += __shfl_xor_sync(0xffffffffu, c, 4);
             if (il < na && q == 0) out[il] = c;
         }
     };
@@ -443,7 +653,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
     auto weight = [&](int k) -> double { return wdev ? wdev[k] : prm.w[k]; };
     // C_k phases k = 1..nterms-1 of the preconditioner polynomial
     auto precond_tail = [&](bool active_sys) -> bool {
-        for (int k = 1; k < nterms; ++k) {
+        for (int k = tail_k0; k < nterms; ++k) {
             double acc = 0.0;
             const bool last = (k == nterms - 1);
             if (active_sys) {
@@ -469,7 +679,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                     else Vec4<VT>::load(tcur, row, c0, c1, c2);
                     double v0 = w0, v1 = w1, v2 = w2;
                     if (kSplit) {
-                        const int an = __ldg(S.rowflag + row);
+                        const int an = rowflag_of(row);
                         if (an >= 0) {
                             double d0, d1, d2;
                             dact_mul(an, (double)c0, (double)c1, (double)c2, d0, d1, d2);
@@ -477,7 +687,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                         }
                     }
                     if (corr) {
-                        const int an = __ldg(S.rowflag + row);
+                        const int an = rowflag_of(row);
                         if (an >= 0) {
                             const int il = 3 * an - ab;
                             if (HSC_IN(il >= 0 && il + 2 < na, 208, il)) {
@@ -486,35 +696,35 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                         }
                     }
                     double e0, e1, e2;
-                    dinv_apply(dinv, n, row, omega, v0, v1, v2, e0, e1, e2);
+                    dinv_row(row, v0, v1, v2, e0, e1, e2);
                     const double n0 = (double)c0 - e0, n1 = (double)c1 - e1, n2 = (double)c2 - e2;
-                    Vec4<VT>::store(tnew, row, (VT)n0, (VT)n1, (VT)n2);
+                    st_t(tnew, row, (VT)n0, (VT)n1, (VT)n2);
                     VT q0, q1, q2;
-                    Vec4<VT>::load(z, row, q0, q1, q2);
+                    ld_z(row, q0, q1, q2);
                     const VT s0 = (VT)((double)q0 + wk * n0), s1 = (VT)((double)q1 + wk * n1),
                              s2 = (VT)((double)q2 + wk * n2);
-                    Vec4<VT>::store(z, row, s0, s1, s2);
+                    st_z(row, s0, s1, s2);
                     if (last) {
                         double r0, r1, r2;
-                        Vec4<double>::load(r, row, r0, r1, r2);
+                        ld_r(row, r0, r1, r2);
                         acc += r0 * (double)s0 + r1 * (double)s1 + r2 * (double)s2;
                     }
                 };
                 if (res) {
-                    for (int i = threadIdx.x; i < nwin; i += kThreads) {
-                        VT u0, u1, u2;
-                        Vec4<VT>::load(tcur, s_wn[i], u0, u1, u2);
-                        Vec4<VT>::store(s_win, i, u0, u1, u2);
-                    }
+                    stage_window([&](int node, VT& u0, VT& u1, VT& u2) { Vec4<VT>::load(tcur, node, u0, u1, u2); });
                     __syncthreads();
-                    spmv_warp_res<kNB, PT, CT, VT>(wr0, wr1, rb, S.rowptr, kcta0, nblk, s_vpc, s_lc, s_lr, s_win, s_y, epi);
-                    __syncthreads();
+                    if (last) mark(7);
+                    if (prm.stage_vals) spmv_rows_res<false, PT, CT, VT>(rb, nrow, s_rp, nblk, s_vpc, s_lc, s_win, epi);
+                    else spmv_rows_res<true, PT, CT, VT>(rb, nrow, s_rp, (size_t)nnz, vals_pc + kcta0, s_lc, s_win, epi);
                 } else {
+                    if (last) mark(7);
                     spmv_warp<kNB, PT, CT>(wr0, wr1, rb, S.rowptr, S.colidx, S.rowid, s_col, s_row, kcta0, vals_pc, nnz, s_y,
                                       gather, epi);
                 }
+                __syncthreads();
+                if (last) mark(8);
                 if (last) compute_zpart();
-                else if (schur) compute_part(tnew, tpart_half(k & 1) + aidx, nact);
+                else if (schur) compute_part(tnew, s_to, tpart_half(k & 1) + aidx, nact);
             }
             tc ^= 1;
             if (last) mark(5);
@@ -530,31 +740,34 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
         for (int row = rb + threadIdx.x; row < re; row += kThreads) {
             double r0, r1, r2;
             Vec4<double>::load(rhs, row, r0, r1, r2);
-            Vec4<double>::store(r, row, r0, r1, r2);
-            Vec4<double>::store(x, row, 0.0, 0.0, 0.0);
+            st_r(row, r0, r1, r2);
+            st_x(row, 0.0, 0.0, 0.0);
             Vec4<VT>::store(pbuf[0], row, (VT)0, (VT)0, (VT)0);  // beta * p_prev must be 0, not NaN
             double t0, t1, t2;
-            dinv_apply(dinv, n, row, omega, r0, r1, r2, t0, t1, t2);
-            Vec4<VT>::store(tbuf[0], row, (VT)t0, (VT)t1, (VT)t2);
+            dinv_row(row, r0, r1, r2, t0, t1, t2);
+            st_t(tbuf[0], row, (VT)t0, (VT)t1, (VT)t2);
             const double w0 = weight(0);
             const VT z0 = (VT)(w0 * t0), z1 = (VT)(w0 * t1), z2 = (VT)(w0 * t2);
-            Vec4<VT>::store(z, row, z0, z1, z2);
+            st_z(row, z0, z1, z2);
             acc_rr += r0 * r0 + r1 * r1 + r2 * r2;
             acc_rz += r0 * (double)z0 + r1 * (double)z1 + r2 * (double)z2;
         }
-        for (int i = ab + threadIdx.x; i < ae; i += kThreads) S.pact[i] = 0.0;
+        for (int i = ab + threadIdx.x; i < ae; i += kThreads) pact_ref(i) = 0.0;
         if (na <= 0)
             for (int j = threadIdx.x; j < rank; j += kThreads) S.zpart[(size_t)j * ncta + lcta] = 0.0;
-        if (schur && nterms > 1) compute_part(tbuf[0], tpart_half(0) + aidx, nact);
+        if (schur && nterms > 1) compute_part(tbuf[0], s_to, tpart_half(0) + aidx, nact);
         if (leader_cta)
             for (int j = threadIdx.x; j < rank; j += kThreads) S.tt[j] = 0.0;
         if (nterms == 1) compute_zpart();
         if (!barrier(prm.part_rr, acc_rr, nterms == 1 ? prm.part_rz : nullptr, acc_rz)) return;
     }
-    if (!precond_tail(true)) return;
-
     // ---------------- main loop: one slot per iteration ----------------
+    // The preconditioner phases of a slot run at the top of the next loop pass
+    // (the first pass: those of the prologue), so precond_tail has one call
+    // site: the kernel stays small enough for the compiler to keep it inline.
+    bool tail_active = true;
     for (;;) {
+        if (!precond_tail(tail_active)) return;
         mark(0);
         if (warp == 0) {
             double srr, srz;
@@ -638,45 +851,50 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                     } else {
                         gather(row, g0, g1, g2);
                     }
-                    Vec4<VT>::store(pnew, row, (VT)g0, (VT)g1, (VT)g2);
-                    int an = __ldg(S.rowflag + row);
+                    st_p(pnew, row, (VT)g0, (VT)g1, (VT)g2);
+                    int an = rowflag_of(row);
                     if (!HSC_IN(an < a / 3, 206, an)) an = -1;
                     if (an >= 0) {
                         // FP64 direction and product at a coupled node
                         VT z0, z1, z2;
-                        Vec4<VT>::load(z, row, z0, z1, z2);
-                        double* pa = S.pact + 3 * (size_t)an;
-                        const double a0 = (double)z0 + bd * pa[0], a1 = (double)z1 + bd * pa[1],
-                                     a2 = (double)z2 + bd * pa[2];
-                        pa[0] = a0; pa[1] = a1; pa[2] = a2;
+                        ld_z(row, z0, z1, z2);
+                        double& pa0 = pact_ref(3 * an);
+                        double& pa1 = pact_ref(3 * an + 1);
+                        double& pa2 = pact_ref(3 * an + 2);
+                        const double a0 = (double)z0 + bd * pa0, a1 = (double)z1 + bd * pa1, a2 = (double)z2 + bd * pa2;
+                        pa0 = a0; pa1 = a1; pa2 = a2;
                         double v0 = y0, v1 = y1, v2 = y2;
                         if (kSplit) {
                             double d0, d1, d2;
                             dact_mul(an, a0, a1, a2, d0, d1, d2);
                             v0 += d0; v1 += d1; v2 += d2;
                         }
-                        double* ya = S.yact + 3 * (size_t)an;
-                        ya[0] = v0; ya[1] = v1; ya[2] = v2;
+                        yact_ref(3 * an) = v0; yact_ref(3 * an + 1) = v1; yact_ref(3 * an + 2) = v2;
+                        if (fuse) { double* yg = S.yact + 3 * (size_t)an; yg[0] = v0; yg[1] = v1; yg[2] = v2; }
                         acc += a0 * v0 + a1 * v1 + a2 * v2;
                     } else {
-                        Vec4<VT>::store(y, row, (VT)y0, (VT)y1, (VT)y2);
+                        st_y(row, (VT)y0, (VT)y1, (VT)y2);
                         acc += (double)g0 * (double)(VT)y0 + (double)g1 * (double)(VT)y1 + (double)g2 * (double)(VT)y2;
                     }
                 };
                 if (res) {
                     // stage p = z + beta p_prev over the window, then the SpMV from shared memory
-                    for (int i = threadIdx.x; i < nwin; i += kThreads) {
+                    stage_window([&](int node, VT& u0, VT& u1, VT& u2) {
                         CT g0, g1, g2;
-                        gather(s_wn[i], g0, g1, g2);
-                        Vec4<VT>::store(s_win, i, (VT)g0, (VT)g1, (VT)g2);
-                    }
+                        gather(node, g0, g1, g2);
+                        u0 = (VT)g0; u1 = (VT)g1; u2 = (VT)g2;
+                    });
                     __syncthreads();
-                    spmv_warp_res<kNB, MT, CT, VT>(wr0, wr1, rb, S.rowptr, kcta0, nblk, s_val, s_lc, s_lr, s_win, s_y, epi);
-                    __syncthreads();
+                    mark(9);
+                    if (prm.stage_vals) spmv_rows_res<false, MT, CT, VT>(rb, nrow, s_rp, nblk, s_val, s_lc, s_win, epi);
+                    else spmv_rows_res<true, MT, CT, VT>(rb, nrow, s_rp, (size_t)nnz, vals + kcta0, s_lc, s_win, epi);
                 } else {
+                    mark(9);
                     spmv_warp<kNB, MT, CT>(wr0, wr1, rb, S.rowptr, S.colidx, S.rowid, s_col, s_row, kcta0, vals, nnz, s_y,
                                       gather, epi);
                 }
+                __syncthreads();
+                mark(10);
                 // tt_j = (Vt^T z)_j + beta tt_j from the per-CTA partials of Vt^T z
                 for (int j = gwarp; j < rank; j += nwarp) {
                     double sz, unused;
@@ -693,7 +911,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                 auto epi = [&](int row, double y0, double y1, double y2) {
                     double h0, h1, h2;
                     Vec4<double>::load(rhs, row, h0, h1, h2);
-                    Vec4<double>::store(r, row, h0 - y0, h1 - y1, h2 - y2);
+                    st_r(row, h0 - y0, h1 - y1, h2 - y2);
                 };
                 spmv_warp<kNB, double, double>(wr0, wr1, rb, S.rowptr, S.colidx, S.rowid, s_col, s_row, kcta0, S.vals64, nnz, s_y, gather, epi);
                 for (int j = gwarp; j < rank; j += nwarp) {
@@ -718,6 +936,13 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
             double acc_rr = 0.0, acc_rz = 0.0;
             bool work = slot != kIdle;
             double alpha = 0.0;
+            // the coupled-dof CTAs read d .* tt (or d .* ttx) while warp 0 sums the partials
+            const bool fused_slot = fuse && slot == kNormal;
+            if (slot != kIdle && (na > 0 || (fused_slot && nwa > 0))) {
+                const double* tsrc = slot == kNormal ? S.tt : S.ttx;
+                for (int j = (int)threadIdx.x - 32; j < rank; j += kThreads - 32)
+                    if (j >= 0) s_dtt[j] = __ldg(S.dpiv + j) * tsrc[j];
+            }
             if (slot == kNormal) {
                 if (warp == 0) {
                     double sp, unused;
@@ -725,6 +950,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                     if (lane == 0) s_bc[2] = sp;
                 }
                 __syncthreads();
+                mark(11);
                 const double pAp = s_bc[2];
                 if (!(isfinite(pAp) && pAp > 0)) {
                     done = true; status = 3; work = false;                      // linear_hsc.cu:370-371
@@ -733,17 +959,126 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                     if (leader_cta && threadIdx.x == 0 && it < S.max_coef) S.cg_coef[2 * it] = alpha;
                 }
             }
-            if (work) {
+            if (work && fused_slot) {
+                // ---- fused update + first preconditioner phase ----
+                const VT* pnew = pbuf[pc ^ 1];
+                const double W0 = weight(0), W1 = weight(1);
+                const bool last1 = nterms == 2;
+                const double* rold = rbuf[rcur];
+                double* rnew = rbuf[rcur ^ 1];
+                VT* t1buf = tbuf[tc ^ 1];
+                __syncthreads();  // s_dtt filled above
+                // low-rank part of y at the coupled window dofs: 8 threads per dof
+                // (the order of lowrank_rows), Vt rows read from L2
+                for (int base = 0; base < 3 * nwa; base += kThreads / 8) {
+                    const int e = base + (threadIdx.x >> 3), q = threadIdx.x & 7;
+                    double c = 0.0;
+                    if (e < 3 * nwa) {
+                        const double* vrow = vt + 3 * s_wan[e / 3] + e % 3;
+#pragma unroll
+                        for (int m = 0; m < 16; ++m) {
+                            const int j = q + 8 * m;
+                            if (j < rank) c += __ldg(vrow + (size_t)j * a) * s_dtt[j];
+                        }
+                        for (int j = q + 128; j < rank; j += 8) c += __ldg(vrow + (size_t)j * a) * s_dtt[j];
+                    }
+                    c += __shfl_xor_sync(0xffffffffu, c, 1);
+                    c += __shfl_xor_sync(0xffffffffu, c, 2);
+                    c += __shfl_xor_sync(0xffffffffu, c, 4);
+                    if (e < 3 * nwa && q == 0) s_wcorr[e] = c;
+                }
+                __syncthreads();
+                mark(12);
+                // y_full at a window node (S p with the low-rank term)
+                auto y_full = [&](int wi, int node, double& y0, double& y1, double& y2) {
+                    const int k = s_wflag[wi];
+                    if (k >= 0) {
+                        const double* yg = S.yact + 3 * (size_t)s_wan[k];
+                        y0 = yg[0] - s_wcorr[3 * k]; y1 = yg[1] - s_wcorr[3 * k + 1]; y2 = yg[2] - s_wcorr[3 * k + 2];
+                    } else {
+                        VT u0, u1, u2;
+                        Vec4<VT>::load(y, node, u0, u1, u2);
+                        y0 = u0; y1 = u1; y2 = u2;
+                    }
+                };
+                // t0 = w Dd^-1 (r - alpha y) over the window, the same arithmetic in every CTA
+                for (int wi = threadIdx.x; wi < nwin; wi += kThreads) {
+                    const int node = s_wn[wi];
+                    double y0, y1, y2, r0, r1, r2, t0, t1, t2;
+                    y_full(wi, node, y0, y1, y2);
+                    Vec4<double>::load(rold, node, r0, r1, r2);
+                    r0 -= alpha * y0; r1 -= alpha * y1; r2 -= alpha * y2;
+                    dinv_apply(dinv, n, node, omega, r0, r1, r2, t0, t1, t2);
+                    Vec4<VT>::store(s_win, wi, (VT)t0, (VT)t1, (VT)t2);
+                }
+                __syncthreads();
+                double acc_rr2 = 0.0, acc_rz2 = 0.0;
+                auto epi = [&](int row, CT w0, CT w1, CT w2) {
+                    const int lr = row - rb;
+                    double y0, y1, y2, p0, p1, p2;
+                    y_full(wown + lr, row, y0, y1, y2);
+                    const int an = rowflag_of(row);
+                    if (an >= 0) {
+                        p0 = pact_ref(3 * an); p1 = pact_ref(3 * an + 1); p2 = pact_ref(3 * an + 2);
+                    } else {
+                        VT q0, q1, q2;
+                        ld_p(pnew, row, q0, q1, q2);
+                        p0 = q0; p1 = q1; p2 = q2;
+                    }
+                    double x0, x1, x2, r0, r1, r2;
+                    ld_x(row, x0, x1, x2);
+                    Vec4<double>::load(rold, row, r0, r1, r2);
+                    x0 += alpha * p0; x1 += alpha * p1; x2 += alpha * p2;
+                    r0 -= alpha * y0; r1 -= alpha * y1; r2 -= alpha * y2;
+                    st_x(row, x0, x1, x2);
+                    { double* q = s_ro + 3 * lr; q[0] = r0; q[1] = r1; q[2] = r2; }
+                    Vec4<double>::store(rnew, row, r0, r1, r2);
+                    double d0, d1, d2;
+                    dinv_row(row, r0, r1, r2, d0, d1, d2);                 // t0 in FP64
+                    const VT c0 = (VT)d0, c1 = (VT)d1, c2 = (VT)d2;        // == the window copy
+                    const VT zb0 = (VT)(W0 * d0), zb1 = (VT)(W0 * d1), zb2 = (VT)(W0 * d2);
+                    double v0 = w0, v1 = w1, v2 = w2;
+                    if (kSplit && an >= 0) {
+                        double e0, e1, e2;
+                        dact_mul(an, (double)c0, (double)c1, (double)c2, e0, e1, e2);
+                        v0 += e0; v1 += e1; v2 += e2;
+                    }
+                    double e0, e1, e2;
+                    dinv_row(row, v0, v1, v2, e0, e1, e2);
+                    const double n0 = (double)c0 - e0, n1 = (double)c1 - e1, n2 = (double)c2 - e2;
+                    st_t(t1buf, row, (VT)n0, (VT)n1, (VT)n2);
+                    const VT s0 = (VT)((double)zb0 + W1 * n0), s1 = (VT)((double)zb1 + W1 * n1),
+                             s2 = (VT)((double)zb2 + W1 * n2);
+                    st_z(row, s0, s1, s2);
+                    acc_rr2 += r0 * r0 + r1 * r1 + r2 * r2;
+                    if (last1) acc_rz2 += r0 * (double)s0 + r1 * (double)s1 + r2 * (double)s2;
+                };
+                if (prm.stage_vals) spmv_rows_res<false, PT, CT, VT>(rb, nrow, s_rp, nblk, s_vpc, s_lc, s_win, epi);
+                else spmv_rows_res<true, PT, CT, VT>(rb, nrow, s_rp, (size_t)nnz, vals_pc + kcta0, s_lc, s_win, epi);
+                __syncthreads();
+                mark(13);
+                if (last1) compute_zpart();
+                acc_rr = acc_rr2;
+                acc_rz = acc_rz2;
+                ++it;
+                pc ^= 1;
+                rcur ^= 1;
+                tc ^= 1;
+            } else if (work) {
                 if (na > 0) {
-                    const double* tsrc = slot == kNormal ? S.tt : S.ttx;
-                    for (int j = threadIdx.x; j < rank; j += kThreads) s_dtt[j] = __ldg(S.dpiv + j) * tsrc[j];
-                    __syncthreads();
+                    __syncthreads();  // s_dtt filled above
                     lowrank_rows(s_z);
                     __syncthreads();
+                    mark(12);
                     for (int il = threadIdx.x; il < na; il += kThreads) {
                         const double c = s_z[il];
-                        if (slot == kNormal) S.yact[ab + il] -= c;                     // y = D p - Vt d Vt^T p
-                        else elem<double>(r, __ldg(S.act + ab + il)) += c;           // r = rhs - D x + Vt d Vt^T x
+                        if (slot == kNormal) yact_ref(ab + il) -= c;                   // y = D p - Vt d Vt^T p
+                        else if (res) {                                                // r = rhs - D x + Vt d Vt^T x
+                            const int dl = s_act[il] - 3 * rb;
+                            s_ro[dl] += c;
+                            if (fuse) rbuf[rcur][4 * (s_act[il] / 3) + s_act[il] % 3] = s_ro[dl];
+                        }
+                        else elem<double>(r, __ldg(S.act + ab + il)) += c;
                     }
                 }
                 __syncthreads();
@@ -753,51 +1088,52 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                     double r0, r1, r2;
                     if (slot == kNormal) {
                         double p0, p1, p2, y0, y1, y2;
-                        const int an = __ldg(S.rowflag + row);
+                        const int an = rowflag_of(row);
                         if (an >= 0) {
-                            const double* pa = S.pact + 3 * (size_t)an;
-                            const double* ya = S.yact + 3 * (size_t)an;
-                            p0 = pa[0]; p1 = pa[1]; p2 = pa[2];
-                            y0 = ya[0]; y1 = ya[1]; y2 = ya[2];
+                            p0 = pact_ref(3 * an); p1 = pact_ref(3 * an + 1); p2 = pact_ref(3 * an + 2);
+                            y0 = yact_ref(3 * an); y1 = yact_ref(3 * an + 1); y2 = yact_ref(3 * an + 2);
                         } else {
                             VT q0, q1, q2, u0, u1, u2;
-                            Vec4<VT>::load(pnew, row, q0, q1, q2);
-                            Vec4<VT>::load(y, row, u0, u1, u2);
+                            ld_p(pnew, row, q0, q1, q2);
+                            ld_y(row, u0, u1, u2);
                             p0 = q0; p1 = q1; p2 = q2; y0 = u0; y1 = u1; y2 = u2;
                         }
                         double x0, x1, x2;
-                        Vec4<double>::load(x, row, x0, x1, x2);
-                        Vec4<double>::load(r, row, r0, r1, r2);
+                        ld_x(row, x0, x1, x2);
+                        ld_r(row, r0, r1, r2);
                         x0 += alpha * p0; x1 += alpha * p1; x2 += alpha * p2;
                         r0 -= alpha * y0; r1 -= alpha * y1; r2 -= alpha * y2;
-                        Vec4<double>::store(x, row, x0, x1, x2);
-                        Vec4<double>::store(r, row, r0, r1, r2);
+                        st_x(row, x0, x1, x2);
+                        st_r(row, r0, r1, r2);
                     } else {
-                        Vec4<double>::load(r, row, r0, r1, r2);
+                        ld_r(row, r0, r1, r2);
                     }
                     double t0, t1, t2;
-                    dinv_apply(dinv, n, row, omega, r0, r1, r2, t0, t1, t2);
-                    Vec4<VT>::store(tbuf[tc], row, (VT)t0, (VT)t1, (VT)t2);
+                    dinv_row(row, r0, r1, r2, t0, t1, t2);
+                    st_t(tbuf[tc], row, (VT)t0, (VT)t1, (VT)t2);
                     const VT z0 = (VT)(w0 * t0), z1 = (VT)(w0 * t1), z2 = (VT)(w0 * t2);
-                    Vec4<VT>::store(z, row, z0, z1, z2);
+                    st_z(row, z0, z1, z2);
                     acc_rr += r0 * r0 + r1 * r1 + r2 * r2;
                     acc_rz += r0 * (double)z0 + r1 * (double)z1 + r2 * (double)z2;
                 }
+                mark(13);
                 if (slot == kNormal) {
                     ++it;
                     pc ^= 1;
                 }
                 if (nterms == 1) compute_zpart();
-                else if (schur) compute_part(tbuf[tc], tpart_half(0) + aidx, nact);
+                else if (schur) compute_part(tbuf[tc], s_to, tpart_half(0) + aidx, nact);
             }
             if (!work) slot = kIdle;
+            tail_k0 = (work && fused_slot) ? 2 : 1;
             mark(3);
-            if (!barrier(prm.part_rr, acc_rr, nterms == 1 ? prm.part_rz : nullptr, acc_rz)) return;
+            const bool rz_here = nterms == 1 || (work && fused_slot && nterms == 2);
+            if (!barrier(prm.part_rr, acc_rr, rz_here ? prm.part_rz : nullptr, acc_rz)) return;
             mark(4);
         }
         prev_slot = slot;
         // ---- phases C ----
-        if (!precond_tail(slot != kIdle)) return;
+        tail_active = slot != kIdle;
         ++slot_no;
     }
 }

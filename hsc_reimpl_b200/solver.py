@@ -61,7 +61,8 @@ class HSCOptions:
     spin_limit: int = 20_000_000
     check_residual: bool = True
     trace_iterations: int = 0
-    resident: bool = True                  # BSR slices + vector windows in shared memory when they fit
+    resident: bool = False                 # BSR slices + vector windows in shared memory when they fit
+    fuse_update: bool = False              # resident mode: one grid barrier fewer per iteration
 
     @classmethod
     def reference(cls):
@@ -104,6 +105,7 @@ class HSCOptions:
         o.check_residual = int(bool(self.check_residual))
         o.trace_iterations = int(self.trace_iterations)
         o.resident = int(bool(self.resident))
+        o.fuse_update = int(bool(self.fuse_update))
         return o
 
 
@@ -241,12 +243,12 @@ class HSCContext:
 
     def trace(self):
         """Per-CTA SM clocks at the PCG phase boundaries (options.trace_iterations > 0):
-        array (ctas, iterations, 8)."""
+        array (ctas, iterations, 16)."""
         g, it = C.c_int32(), C.c_int32()
         self._check(self.lib.hsc_get_trace(self._ptr, None, 0, C.byref(g), C.byref(it)))
-        out = np.zeros(g.value * it.value * 8, dtype=np.uint64)
+        out = np.zeros(g.value * it.value * 16, dtype=np.uint64)
         self._check(self.lib.hsc_get_trace(self._ptr, out.ctypes.data, out.size, None, None))
-        return out.reshape(g.value, it.value, 8)
+        return out.reshape(g.value, it.value, 16)
 
     def abd_inverse(self, qm, sys_index=0):
         P = np.zeros((qm, qm))

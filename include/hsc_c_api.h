@@ -111,8 +111,14 @@ typedef struct hsc_options {
     int32_t check_residual;      /* 1: compute the full residual and enforce full_residual_limit */
     int32_t trace_iterations;    /* > 0: record per-CTA SM clocks at the PCG phase boundaries of the
                                     first iterations (hsc_get_trace) */
-    int32_t resident;            /* 1: each PCG CTA keeps its BSR slice and vector window in shared memory
-                                    when they fit (else they stream from L2); 0: always stream */
+    int32_t resident;            /* 1: each PCG CTA keeps its BSR slice, vector window and own-row vectors
+                                    in shared memory when they fit; 0 (default): stream them from L2, which
+                                    leaves room to keep the Vt blocks in shared memory and measured as fast */
+    int32_t fuse_update;         /* resident mode, FEM-basis polynomial of 2+ terms: 1 folds the x/r update
+                                    into the first preconditioner phase (each CTA forms
+                                    t0 = w Dd^-1 (r - alpha S p) over its own window), one grid barrier
+                                    fewer per iteration; 0 (default): separate update phase, which measured
+                                    as fast on the vehicle system (the window-wide t0 costs what the barrier did) */
 } hsc_options;
 
 typedef struct hsc_stats {        /* superset of the hsc_stats.jsonl record (linear_hsc.cu:420-431) */
@@ -193,9 +199,13 @@ HSC_EXPORT int hsc_get_factors(hsc_ctx* ctx, int32_t sys, int32_t* rank, int32_t
                     double* U, int32_t ldu, double* V, int32_t ldv, int32_t* active);
 
 /* Phase-boundary SM clocks of the last PCG launch when trace_iterations > 0:
- * out[(cta * iterations + it) * 8 + event], events 0 loop top, 1 phase A done,
+ * out[(cta * iterations + it) * 16 + event], events 0 loop top, 1 phase A done,
  * 2 after its barrier, 3 phase B done, 4 after its barrier, 5 last
- * preconditioner phase done, 6 after its barrier.  *ctas receives the grid size. */
+ * preconditioner phase done, 6 after its barrier; resident mode also records
+ * 7 / 8 the last preconditioner phase's window staged / SpMV done, 9 / 10 the
+ * same for phase A, 11 phase B's alpha known, 12 its low-rank correction done,
+ * 13 its row update done.  Events 5-8 of an iteration record the preconditioner
+ * phases that run just before its loop top (event 0).  *ctas receives the grid size. */
 HSC_EXPORT int hsc_get_trace(hsc_ctx* ctx, unsigned long long* out, int64_t max_entries, int32_t* ctas,
                              int32_t* iterations);
 
