@@ -59,6 +59,7 @@ class Options(C.Structure):
         ("trace_iterations", C.c_int32),
         ("resident", C.c_int32),
         ("fuse_update", C.c_int32),
+        ("aca_cluster", C.c_int32),
     ]
 
 

@@ -8,7 +8,8 @@ whose every system still meets the FP64-verified full-system residual target.
 A rank cap below what the coupling needs leaves an ACA error that no PCG
 tolerance can remove -- and can make the approximate Schur complement
 indefinite, which PCG reports as a breakdown -- so the status and residual
-tests are what bound the rank from below.  The default relaxation is
+tests are what bound the rank from below; with 12 bodies the coupling rank
+reaches 139, so the sweep ends at a cap (256) at or above every coupling rank.  The default relaxation is
 omega = 0.6: block-Jacobi-scaled cube and torus operators reach
 lambda_max(Dd^-1 D) = 2.9, where the order-2 series needs omega < 2 / 2.9.
 """
@@ -23,7 +24,7 @@ import numpy as np
 from .solver import DeviceSystem, HSCContext, HSCOptions
 
 TILES = (2, 4, 8)
-RANKS = (4, 8, 16, 32, 64, 128)
+RANKS = (4, 8, 16, 32, 64, 128, 256)
 
 
 def time_batch(ctx, systems, xs, reps=3, warmup=1, use_graph=True):

@@ -5,7 +5,7 @@
 c1  the 1,331-node cube with one affine plate (error against a sparse direct solve)
 c3  64 uneven systems in one persistent launch replayed as a CUDA graph, FP32
     values with FP64 residual replacement every 50 iterations, after the
-    autotuner (tile width x ACA rank cap 4-128; omega 0.6)
+    autotuner (tile width x ACA rank cap 4-256; omega 0.6)
 c4  the learned polynomial preconditioner on held-out vehicle trajectories:
     PCG iterations and time to 1e-6 against plain order-2 Neumann (FP64 and FP32)
 c5  the 1 M-tet torus (12 bodies, 30 % contact-active tread): FP64 / FP32 /
@@ -121,13 +121,16 @@ def c5(flush):
     out = {"workload": "stress_torus_1M_tets", "generation_s": time.time() - t, "meta": s.meta}
     ds = DeviceSystem.from_system(s)
     del s
-    ref_ctx = HSCContext(HSCOptions(neumann_order=2, tol=1e-10, max_rank=64))
+    # the coupling to 12 bodies has rank up to 144: caps below it leave an ACA
+    # error that makes the approximate Schur complement indefinite (the sweep
+    # below shows it), so the precision runs use an uncapped rank
+    ref_ctx = HSCContext(HSCOptions(neumann_order=2, tol=1e-10, max_rank=256, max_iter=50000))
     xr, sr = ref_ctx.solve(ds, raise_on_error=False)
     xr = xr.clone()
     out["reference"] = {"pcg_iterations": sr["pcg_iterations"], "full_relative_residual": sr["full_relative_residual"]}
     modes = {}
     for prec in ("fp64", "fp32", "bf16"):
-        o = HSCOptions(neumann_order=2, tol=1e-6, max_rank=64, precision=prec,
+        o = HSCOptions(neumann_order=2, tol=1e-6, max_rank=256, precision=prec,
                        residual_replacement=0 if prec == "fp64" else 50)
         ctx = HSCContext(o)
         ms, st, x = _timed_solves(ctx, ds, 3, flush)
@@ -138,7 +141,7 @@ def c5(flush):
         log(json.dumps({prec: modes[prec]}))
     out["precision"] = modes
     ranks = {}
-    for r in (8, 16, 32, 64):
+    for r in (8, 16, 32, 64, 256):
         ctx = HSCContext(HSCOptions(neumann_order=2, tol=1e-6, max_rank=r))
         ms, st, _ = _timed_solves(ctx, ds, 2, flush)
         ranks[r] = {"ms_per_solve": ms, "pcg_iterations": st["pcg_iterations"], "rank": st["rank"],
@@ -148,7 +151,7 @@ def c5(flush):
     out["rank_sweep"] = ranks
     orders = {}
     for k in (1, 2, 3, 4):
-        ctx = HSCContext(HSCOptions(neumann_order=k, tol=1e-6, max_rank=32))
+        ctx = HSCContext(HSCOptions(neumann_order=k, tol=1e-6, max_rank=256, omega=0.5))
         ms, st, _ = _timed_solves(ctx, ds, 2, flush)
         orders[k] = {"ms_per_solve": ms, "pcg_iterations": st["pcg_iterations"], "status": st["status"],
                      "pcg_us_per_iteration": 1000 * st["pcg_ms"] / max(1, st["pcg_iterations"])}

@@ -524,8 +524,7 @@ int aca_all(hsc_ctx* ctx, int count, cudaStream_t st) {
         ap.psum = ctx->aca_psum.as<double>(); ap.pmax = ctx->aca_pmax.as<double>(); ap.pidx = ctx->aca_pidx.as<long long>();
         ap.bar = ctx->aca_bar.as<GridBar>(); ap.spin_limit = o.spin_limit;
         CK(cudaMemsetAsync(ctx->aca_bar.p, 0, sizeof(GridBar), st));
-        const long long total = (long long)S.qm * S.a;
-        const int grid = (int)std::max<long long>(1, std::min<long long>(ctx->aca_grid, (total + 2047) / 2048));
+        const int grid = ctx->aca_grid;  // upper bound; launch_aca sizes the column strips
         CK(launch_aca(ap, grid, st));
     }
     return HSC_OK;
@@ -849,7 +848,7 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
     for (int s2 = 0; s2 < ns; ++s2) {
         System& S = ctx->sys[idx[s2]];
         S.aca_on_cluster = false;
-        if (S.kmax <= 0 || !aca_cluster_fits(S.qm, S.a)) continue;
+        if (S.kmax <= 0 || !o.aca_cluster || !aca_cluster_fits(S.qm, S.a)) continue;
         const size_t need = aca_cluster_smem_doubles(S.qm, S.a);
         if (ctx->aca_cluster_ok < 0) ctx->aca_cluster_ok = aca_cluster_supported(25600) > 0 ? 1 : 0;
         if (!ctx->aca_cluster_ok) continue;
@@ -1162,6 +1161,7 @@ int hsc_options_default(hsc_options* o) {
     o->trace_iterations = 0;
     o->resident = 0;
     o->fuse_update = 0;
+    o->aca_cluster = 1;
     return HSC_OK;
 }
 

@@ -190,17 +190,28 @@ __device__ __forceinline__ MaxIdx warp_best(MaxIdx m) {
     return m;
 }
 
+// Full-pivot ACA over the whole grid (couplings too large for the cluster
+// kernel).  Each CTA owns a strip of whole columns of R (all m rows, a
+// multiple of 32 columns): per rank step it forms v = R[i, strip] / pivot once
+// per column and u = R[:, j] once per row in shared memory, then updates its
+// strip (R - u v, no FMA, as numpy's R - outer(u, v)) with coalesced row
+// segments while it tracks the sum of squares and the row-major first
+// largest |R|; one grid barrier per step.
 __global__ void __launch_bounds__(256) aca_kernel(AcaParams p) {
     __shared__ double s_sum[8];
     __shared__ MaxIdx s_max[8];
     __shared__ double s_bc[4];
     __shared__ long long s_bi;
+    extern __shared__ double s_uv[];        // u (m rows) then v (strip columns)
     const int m = p.m, nc = p.nc;
     const long long total = (long long)m * nc;
     const unsigned G = gridDim.x;
-    const long long chunk = (total + G - 1) / G;
-    const long long f0 = min(total, (long long)blockIdx.x * chunk), f1 = min(total, f0 + chunk);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int strip = p.strip;                          // columns per CTA (a multiple of 32)
+    double* s_u = s_uv;
+    double* s_v = s_uv + m;
+    const int c0 = min(nc, (int)blockIdx.x * strip), c1 = min(nc, c0 + strip);
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int lane = tx, warp = ty;
     double* R[2] = {p.R0, p.R1};
     int cur = 0;
 
@@ -223,11 +234,13 @@ __global__ void __launch_bounds__(256) aca_kernel(AcaParams p) {
     {
         double ls = 0.0;
         MaxIdx lm{-1.0, (long long)total};
-        for (long long f = f0 + threadIdx.x; f < f1; f += blockDim.x) {
-            const double v = R[0][f];
-            ls += v * v;
-            lm = better(lm, MaxIdx{fabs(v), f});
-        }
+        for (int r = ty; r < m; r += 8)
+            for (int c = c0 + tx; c < c1; c += 32) {
+                const long long f = (long long)r * nc + c;
+                const double v = R[0][f];
+                ls += v * v;
+                lm = better(lm, MaxIdx{fabs(v), f});
+            }
         reduce_local(ls, lm);
     }
     int epoch = 0;
@@ -263,20 +276,28 @@ __global__ void __launch_bounds__(256) aca_kernel(AcaParams p) {
         double* Rn = R[cur ^ 1];
         const double pivot = Rc[gi];
         if (!(fabs(pivot) > DBL_EPSILON * fmax(scale, DBL_MIN))) break;
-        if (blockIdx.x == 0) {
-            for (int r = threadIdx.x; r < m; r += blockDim.x) p.U[(size_t)k * m + r] = Rc[(size_t)r * nc + j];
-            for (int c = threadIdx.x; c < nc; c += blockDim.x) p.V[(size_t)k * nc + c] = Rc[(size_t)i * nc + c] / pivot;
+        for (int r = threadIdx.x; r < m; r += blockDim.x) {
+            const double u = Rc[(size_t)r * nc + j];
+            s_u[r] = u;
+            if (blockIdx.x == 0) p.U[(size_t)k * m + r] = u;
         }
+        for (int c = c0 + (int)threadIdx.x; c < c1; c += blockDim.x) {
+            const double v = Rc[(size_t)i * nc + c] / pivot;
+            s_v[c - c0] = v;
+            p.V[(size_t)k * nc + c] = v;
+        }
+        __syncthreads();
         double ls = 0.0;
         MaxIdx lm{-1.0, (long long)total};
-        for (long long f = f0 + threadIdx.x; f < f1; f += blockDim.x) {
-            const int rr = (int)(f / nc), cc = (int)(f - (long long)rr * nc);
-            const double u = Rc[(size_t)rr * nc + j];
-            const double v = Rc[(size_t)i * nc + cc] / pivot;
-            const double val = __dsub_rn(Rc[f], __dmul_rn(u, v));  // numpy: R - outer(u, v), no FMA
-            Rn[f] = val;
-            ls += val * val;
-            lm = better(lm, MaxIdx{fabs(val), f});
+        for (int r = ty; r < m; r += 8) {
+            const double u = s_u[r];
+            for (int c = c0 + tx; c < c1; c += 32) {
+                const long long f = (long long)r * nc + c;
+                const double val = __dsub_rn(Rc[f], __dmul_rn(u, s_v[c - c0]));  // numpy: R - outer(u, v), no FMA
+                Rn[f] = val;
+                ls += val * val;
+                lm = better(lm, MaxIdx{fabs(val), f});
+            }
         }
         reduce_local(ls, lm);
         cur ^= 1;
@@ -876,9 +897,36 @@ void launch_extract(const int* qq, int nqq, const int* qf, int nqf, const double
 }
 
 cudaError_t launch_aca(const AcaParams& p, int grid, cudaStream_t st) {
+    // column strips: a multiple of 32 columns per CTA, as few CTAs as cover the columns
+    AcaParams q = p;
+    const int strips = (p.nc + 31) / 32;
+    // co-resident CTAs at this kernel's shared memory (m + a strip of doubles)
+    const size_t smem_max = sizeof(double) * ((size_t)p.m + 32 * (size_t)strips);
+    if (smem_max > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(aca_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)std::min<size_t>(smem_max, 227 * 1024));
+        if (e != cudaSuccess) return e;
+    }
+    int dev = 0, sms = 1, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int per = (strips + grid - 1) / grid;
+    size_t smem = sizeof(double) * ((size_t)p.m + 32 * (size_t)per);
+    for (;;) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, aca_kernel, 256, smem);
+        const int cap = per_sm * sms;
+        if (cap > 0 && (strips + per - 1) / per <= std::min(cap, grid)) break;
+        if (per >= strips) return cudaErrorInvalidConfiguration;
+        ++per;
+        smem = sizeof(double) * ((size_t)p.m + 32 * (size_t)per);
+    }
+    q.strip = 32 * per;
+    const int g = std::max(1, (p.nc + q.strip - 1) / q.strip);
     count_launch();
-    void* args[] = {(void*)&p};
-    return cudaLaunchCooperativeKernel((void*)aca_kernel, dim3(grid), dim3(256), args, 0, st);
+    void* args[] = {(void*)&q};
+    const cudaError_t e = cudaLaunchCooperativeKernel((void*)aca_kernel, dim3(g), dim3(256), args, smem, st);
+    debug_sync("aca_kernel");
+    return e;
 }
 
 int aca_blocks_per_sm() {

@@ -21,6 +21,7 @@ struct AcaParams {
     long long* pidx;
     GridBar* bar;
     long long spin_limit;
+    int strip;             // columns per CTA (set by launch_aca)
 };
 
 // one system of the cluster ACA (hsc_aca.cu)

@@ -63,6 +63,7 @@ class HSCOptions:
     trace_iterations: int = 0
     resident: bool = False                 # BSR slices + vector windows in shared memory when they fit
     fuse_update: bool = False              # resident mode: one grid barrier fewer per iteration
+    aca_cluster: bool = True               # cluster ACA when the coupling fits; False: the grid kernel
 
     @classmethod
     def reference(cls):
@@ -106,6 +107,7 @@ class HSCOptions:
         o.trace_iterations = int(self.trace_iterations)
         o.resident = int(bool(self.resident))
         o.fuse_update = int(bool(self.fuse_update))
+        o.aca_cluster = int(bool(self.aca_cluster))
         return o
 
 

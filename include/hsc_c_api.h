@@ -119,6 +119,9 @@ typedef struct hsc_options {
                                     t0 = w Dd^-1 (r - alpha S p) over its own window), one grid barrier
                                     fewer per iteration; 0 (default): separate update phase, which measured
                                     as fast on the vehicle system (the window-wide t0 costs what the barrier did) */
+    int32_t aca_cluster;         /* 1 (default): 16-CTA cluster ACA (distributed shared memory) when the
+                                    coupling fits it; 0: always the grid kernel (column strips, one grid
+                                    barrier per rank step), which also serves couplings too large for it */
 } hsc_options;
 
 typedef struct hsc_stats {        /* superset of the hsc_stats.jsonl record (linear_hsc.cu:420-431) */
