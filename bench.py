@@ -37,9 +37,10 @@ sys.path.insert(0, HERE)
 METRIC = "HSC solves/s & PCG iters to rel-res 1e-6: learned/FP32 vs plain FP64, 1 B200"
 UNIT = "solves/s"
 TARGET = 1e-6
-# DRAM bytes per PCG iteration on the vehicle workload from an ncu capture
-# (profiles/pcg_kernel_vehicle.md: 21.75 MB read + 0.99 MB written over 204 iterations)
-NCU_TRAFFIC_PER_ITER = (21.747456e6 + 0.990976e6) / 204
+# DRAM bytes per PCG iteration on the vehicle workload from an ncu capture of
+# the FP64 order-2 solve (profiles/pcg_kernel_vehicle.md: 24.23 MB read + 7.86 MB
+# written over 204 iterations)
+NCU_TRAFFIC_PER_ITER = (24.23e6 + 7.86e6) / 204
 
 
 def parse():

@@ -8,6 +8,7 @@ c3  64 uneven systems in one persistent launch replayed as a CUDA graph, FP32
     autotuner (tile width x ACA rank cap 4-256; omega 0.6)
 c4  the learned polynomial preconditioner on held-out vehicle trajectories:
     PCG iterations and time to 1e-6 against plain order-2 Neumann (FP64 and FP32)
+vehicle  two FP64 solves of the vehicle system (a short, fixed command for profilers)
 c5  the 1 M-tet torus (12 bodies, 30 % contact-active tread): FP64 / FP32 /
     BF16 solves with their error against a tight FP64 reference, ACA rank sweep
     8-64, Neumann order sweep 1-4, HBM GB/s of the full-H SpMV
@@ -182,6 +183,20 @@ def c5(flush):
     return out
 
 
+def vehicle(prec="fp64"):
+    from .solver import DeviceSystem, HSCContext, HSCOptions
+    from .systems import make_vehicle_system
+    s = make_vehicle_system(seed=0)
+    ds = DeviceSystem.from_system(s)
+    ctx = HSCContext(HSCOptions(neumann_order=2, precision=prec, residual_replacement=0 if prec == "fp64" else 50))
+    out = []
+    for _ in range(2):
+        _, st = ctx.solve(ds)
+        out.append({"status": st["status"], "pcg_iterations": st["pcg_iterations"], "pcg_ms": st["pcg_ms"],
+                    "total_ms": st["total_ms"]})
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--only", default="c1,c3,c4,c5")
@@ -192,6 +207,8 @@ def main(argv=None):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     want = a.only.split(",")
     rep = {}
+    if "vehicle" in want:
+        rep["vehicle"] = vehicle(); log(json.dumps({"vehicle": rep["vehicle"]}))
     if "c1" in want:
         rep["c1"] = c1(flush); log(json.dumps({"c1": rep["c1"]}))
     if "c3" in want:
