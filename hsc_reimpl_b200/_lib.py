@@ -131,6 +131,12 @@ EXPORTS = {
                                    C.c_void_p, C.c_void_p, C.c_void_p]),
     "hsc_adam_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_float,
                                 C.c_float, C.c_float, C.c_float, C.c_float, C.c_int32, C.c_void_p]),
+    "hsc_fem_assembler_create": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_double, C.c_double,
+                                           C.c_double, C.c_int32, C.POINTER(C.c_void_p)]),
+    "hsc_fem_assembler_destroy": (None, [C.c_void_p]),
+    "hsc_fem_pattern": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int64)]),
+    "hsc_fem_assemble": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32),
+                                   C.c_void_p]),
 }
 
 _LIB = None

@@ -1,0 +1,70 @@
+"""GPU assembly of the log-Neo-Hookean Tet4 Hessian into the solver's input form.
+
+``FemAssembler`` wraps ``hsc_fem_assembler_*`` / ``hsc_fem_assemble``
+(hsc_assemble.cu): the mesh analysis happens once, then every Newton step
+assembles the FEM block of the system on the device from the current node
+positions and per-tet Young's moduli, straight into a one-triangle BCOO the
+solver reads (log_neo_hookean_3d.cu:62-135, global_linear_system.cu:215-248).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import HSCError
+
+DT = 1.0 / 30.0
+
+
+class FemAssembler:
+    def __init__(self, tets, rest_x, rho=1000.0, nu=0.3, dt=DT, project=True):
+        import torch
+        self.torch = torch
+        self.lib = _lib.load()
+        tets = np.ascontiguousarray(tets, dtype=np.int32)
+        rest_x = np.ascontiguousarray(rest_x, dtype=np.float64)
+        self.ntet, self.nnode = tets.shape[0], rest_x.shape[0]
+        self._ptr = C.c_void_p()
+        rc = self.lib.hsc_fem_assembler_create(tets.ctypes.data, self.ntet, self.nnode, rest_x.ctypes.data, rho, nu,
+                                               dt, int(bool(project)), C.byref(self._ptr))
+        if rc != _lib.HSC_OK:
+            raise HSCError(rc, "hsc_fem_assembler_create failed")
+        n = C.c_int64()
+        self.lib.hsc_fem_pattern(self._ptr, None, None, C.byref(n))
+        self.nnzb = n.value
+        self.rows = torch.empty(self.nnzb, dtype=torch.int32, device="cuda")
+        self.cols = torch.empty(self.nnzb, dtype=torch.int32, device="cuda")
+        rc = self.lib.hsc_fem_pattern(self._ptr, C.c_void_p(self.rows.data_ptr()), C.c_void_p(self.cols.data_ptr()),
+                                      C.byref(n))
+        if rc != _lib.HSC_OK:
+            raise HSCError(rc, "hsc_fem_pattern failed")
+
+    def assemble(self, x, E, values=None, check=True):
+        """Values (nnzb, 9) column-major blocks at positions x (nnode, 3) with moduli E (ntet,)."""
+        torch = self.torch
+        x = torch.as_tensor(x, dtype=torch.float64, device="cuda").contiguous()
+        E = torch.as_tensor(E, dtype=torch.float64, device="cuda").contiguous()
+        if E.numel() == 1:
+            E = E.expand(self.ntet).contiguous()
+        if values is None:
+            values = torch.empty(self.nnzb, 9, dtype=torch.float64, device="cuda")
+        inv = C.c_int32(0)
+        stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        rc = self.lib.hsc_fem_assemble(self._ptr, C.c_void_p(x.data_ptr()), C.c_void_p(E.data_ptr()),
+                                       C.c_void_p(values.data_ptr()), C.byref(inv) if check else None, stream)
+        if rc != _lib.HSC_OK:
+            raise HSCError(rc, f"hsc_fem_assemble failed ({inv.value} inverted tets)")
+        return values
+
+    def close(self):
+        if self._ptr:
+            self.lib.hsc_fem_assembler_destroy(self._ptr)
+            self._ptr = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -9,6 +9,7 @@ c3  64 uneven systems in one persistent launch replayed as a CUDA graph, FP32
 c4  the learned polynomial preconditioner on held-out vehicle trajectories:
     PCG iterations and time to 1e-6 against plain order-2 Neumann (FP64 and FP32)
 vehicle  two FP64 solves of the vehicle system (a short, fixed command for profilers)
+assembly GPU assembly of the vehicle's 78,120-tet log-NH Hessian (hsc_fem_assemble) per call
 c5  the 1 M-tet torus (12 bodies, 30 % contact-active tread): FP64 / FP32 /
     BF16 solves with their error against a tight FP64 reference, ACA rank sweep
     8-64, Neumann order sweep 1-4, HBM GB/s of the full-H SpMV
@@ -183,6 +184,37 @@ def c5(flush):
     return out
 
 
+def assembly(reps=10):
+    import torch
+    from .assembly import FemAssembler
+    from .systems import annulus_mesh
+    xs, ts, off = [], [], 0
+    for t in range(7):
+        x, tets, _ = annulus_mesh(center=(1.2 * (t % 4), 0.5 * (t // 4), 0.0))
+        xs.append(x)
+        ts.append(tets + off)
+        off += len(x)
+    x = np.concatenate(xs)
+    tets = np.concatenate(ts)
+    rng = np.random.default_rng(0)
+    h = np.cbrt((np.abs(np.linalg.det(x[tets[:, 1:]] - x[tets[:, :1]])) / 6.0).mean())
+    xp = torch.from_numpy(x + 0.02 * h * rng.standard_normal(x.shape)).cuda()
+    E = torch.full((len(tets),), 1e8, dtype=torch.float64, device="cuda")
+    asm = FemAssembler(tets, x)
+    vals = asm.assemble(xp, E)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = []
+    for _ in range(reps):
+        e0.record()
+        asm.assemble(xp, E, values=vals, check=False)
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    m = statistics.median(ms)
+    return {"tets": int(len(tets)), "nodes": int(len(x)), "blocks": int(asm.nnzb), "ms": m,
+            "tets_per_s": len(tets) / (m / 1000)}
+
+
 def vehicle(prec="fp64"):
     from .solver import DeviceSystem, HSCContext, HSCOptions
     from .systems import make_vehicle_system
@@ -207,6 +239,8 @@ def main(argv=None):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     want = a.only.split(",")
     rep = {}
+    if "assembly" in want:
+        rep["assembly"] = assembly(); log(json.dumps({"assembly": rep["assembly"]}))
     if "vehicle" in want:
         rep["vehicle"] = vehicle(); log(json.dumps({"vehicle": rep["vehicle"]}))
     if "c1" in want:

@@ -216,6 +216,28 @@ HSC_EXPORT int hsc_get_trace(hsc_ctx* ctx, unsigned long long* out, int64_t max_
 HSC_EXPORT int hsc_get_abd_inverse(hsc_ctx* ctx, int32_t sys, double* P);
 
 /* ---------------------------------------------------------------------------
+ * GPU assembly of the log-Neo-Hookean Tet4 Hessian (the FEM block of a Newton
+ * system) into the solver's input form: one-triangle BCOO over nodes, sorted,
+ * unique, column-major 3x3 values; dt^2 V-scaled, SPD-projected per tet, plus
+ * the lumped mass.  Replaces log_neo_hookean_3d.cu:62-135 (per-tet Hessian,
+ * ddEddF_spd of log_neo_hookean_function.h:108-150) and the triplet-to-BCOO
+ * conversion of global_linear_system.cu:215-248 (ge2sym) for this block.
+ * ------------------------------------------------------------------------- */
+typedef struct hsc_fem_assembler hsc_fem_assembler;
+/* Mesh analysis (host arrays: tets ntet x 4 node ids, rest positions nnode x 3): rest shape
+ * matrices, volumes, lumped masses (rho V / 4 per tet corner) and the block pattern. */
+HSC_EXPORT int hsc_fem_assembler_create(const int32_t* tets, int32_t ntet, int32_t nnode, const double* rest_x,
+                                        double rho, double nu, double dt, int32_t project,
+                                        hsc_fem_assembler** out);
+HSC_EXPORT void hsc_fem_assembler_destroy(hsc_fem_assembler* a);
+/* The pattern: *nnzb blocks; d_rows / d_cols (device, may be NULL) receive the node indices. */
+HSC_EXPORT int hsc_fem_pattern(const hsc_fem_assembler* a, int32_t* d_rows, int32_t* d_cols, int64_t* nnzb);
+/* Numeric assembly at positions d_x (nnode x 3) with Young's moduli d_E (per tet) into d_values
+ * (nnzb x 9).  With `inverted` (host) set, waits and reports tets with det F <= 0 (HSC_ERR_NONSPD). */
+HSC_EXPORT int hsc_fem_assemble(hsc_fem_assembler* a, const double* d_x, const double* d_E, double* d_values,
+                                int32_t* inverted, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Learned polynomial preconditioner (no reference counterpart; the reference
  * fixes the Neumann weights to 1, linear_hsc.cu:330-343).
  * ------------------------------------------------------------------------- */
