@@ -137,6 +137,9 @@ EXPORTS = {
     "hsc_fem_pattern": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int64)]),
     "hsc_fem_assemble": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32),
                                    C.c_void_p]),
+    "hsc_fem_feasible_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int32,
+                                        C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                        C.c_void_p]),
 }
 
 _LIB = None

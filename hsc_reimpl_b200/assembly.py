@@ -58,6 +58,21 @@ class FemAssembler:
             raise HSCError(rc, f"hsc_fem_assemble failed ({inv.value} inverted tets)")
         return values
 
+    def feasible_step(self, x0, dx, alpha0=1.0, max_halvings=60):
+        """(alpha, halvings, limiting tets): the largest alpha0 * 2^-m whose segment keeps every
+        tet's det F above 1e-8 (the reference's line-search feasibility rule)."""
+        torch = self.torch
+        x0 = torch.as_tensor(x0, dtype=torch.float64, device="cuda").contiguous()
+        dx = torch.as_tensor(dx, dtype=torch.float64, device="cuda").contiguous()
+        alpha, m, lim = C.c_double(), C.c_int32(), C.c_int32()
+        stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        rc = self.lib.hsc_fem_feasible_step(self._ptr, C.c_void_p(x0.data_ptr()), C.c_void_p(dx.data_ptr()),
+                                            float(alpha0), int(max_halvings), C.byref(alpha), C.byref(m),
+                                            C.byref(lim), stream)
+        if rc not in (_lib.HSC_OK, _lib.HSC_ERR_NONSPD):
+            raise HSCError(rc, "hsc_fem_feasible_step failed")
+        return alpha.value, m.value, lim.value
+
     def close(self):
         if self._ptr:
             self.lib.hsc_fem_assembler_destroy(self._ptr)

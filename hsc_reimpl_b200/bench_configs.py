@@ -9,7 +9,8 @@ c3  64 uneven systems in one persistent launch replayed as a CUDA graph, FP32
 c4  the learned polynomial preconditioner on held-out vehicle trajectories:
     PCG iterations and time to 1e-6 against plain order-2 Neumann (FP64 and FP32)
 vehicle  two FP64 solves of the vehicle system (a short, fixed command for profilers)
-assembly GPU assembly of the vehicle's 78,120-tet log-NH Hessian (hsc_fem_assemble) per call
+assembly GPU assembly of the vehicle's 78,120-tet log-NH Hessian (hsc_fem_assemble) per call,
+         and the line-search feasible step of a rough direction (hsc_fem_feasible_step)
 c5  the 1 M-tet torus (12 bodies, 30 % contact-active tread): FP64 / FP32 /
     BF16 solves with their error against a tight FP64 reference, ACA rank sweep
     8-64, Neumann order sweep 1-4, HBM GB/s of the full-H SpMV
@@ -211,8 +212,20 @@ def assembly(reps=10):
         torch.cuda.synchronize()
         ms.append(e0.elapsed_time(e1))
     m = statistics.median(ms)
+    # line-search feasibility of a rough direction (about half the tets limit the step)
+    dx = torch.from_numpy(0.5 * h * rng.standard_normal(x.shape)).cuda()
+    feas = asm.feasible_step(xp, dx)
+    fs = []
+    for _ in range(reps):
+        e0.record()
+        asm.feasible_step(xp, dx)  # includes the read of (alpha, halvings) to the host
+        e1.record()
+        torch.cuda.synchronize()
+        fs.append(e0.elapsed_time(e1))
     return {"tets": int(len(tets)), "nodes": int(len(x)), "blocks": int(asm.nnzb), "ms": m,
-            "tets_per_s": len(tets) / (m / 1000)}
+            "tets_per_s": len(tets) / (m / 1000),
+            "feasible_step": {"alpha": feas[0], "halvings": feas[1], "limiting_tets": feas[2],
+                              "ms": statistics.median(fs)}}
 
 
 def vehicle(prec="fp64"):

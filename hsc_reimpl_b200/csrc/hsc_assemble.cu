@@ -171,6 +171,86 @@ __global__ void gather_blocks_kernel(const int* __restrict__ ptr, const int* __r
     for (int e = 0; e < 9; ++e) o[e] = acc[e];
 }
 
+// ---------------------------------------------------------------------------
+// line-search feasibility (reference: feasible_segment, log_neo_hookean_function.h:37-75,
+// applied per tet in the energy kernel, log_neo_hookean_3d.cu:45-52, so a trial
+// step whose segment inverts a tet has infinite energy and the search halves it)
+// ---------------------------------------------------------------------------
+constexpr double kMinJacobian = 1e-8;
+
+__device__ __forceinline__ double triple3(const double* A, int c0, const double* B, int c1, const double* C, int c2) {
+    // a . (b x c) for column c0 of A, c1 of B, c2 of C (row-major 3x3)
+    const double a0 = A[c0], a1 = A[3 + c0], a2 = A[6 + c0];
+    const double b0 = B[c1], b1 = B[3 + c1], b2 = B[6 + c1];
+    const double d0 = C[c2], d1 = C[3 + c2], d2 = C[6 + c2];
+    return a0 * (b1 * d2 - b2 * d1) + a1 * (b2 * d0 - b0 * d2) + a2 * (b0 * d1 - b1 * d0);
+}
+
+// det(A + s (E - A)) > min_jacobian for every s in [0, 1]: the endpoints and the
+// roots of the derivative of the cubic, which hold its interior minima
+__device__ bool segment_feasible(const double* A, const double* E) {
+    double B[9];
+    for (int e = 0; e < 9; ++e) B[e] = E[e] - A[e];
+    const double c0 = det3(A);
+    const double c1 = triple3(B, 0, A, 1, A, 2) + triple3(A, 0, B, 1, A, 2) + triple3(A, 0, A, 1, B, 2);
+    const double c2 = triple3(A, 0, B, 1, B, 2) + triple3(B, 0, A, 1, B, 2) + triple3(B, 0, B, 1, A, 2);
+    const double c3 = det3(B);
+    if (!(c0 > kMinJacobian && det3(E) > kMinJacobian)) return false;
+    const double a = 3.0 * c3, b = 2.0 * c2, c = c1;
+    double roots[2] = {-1.0, -1.0};
+    const double scale = fabs(a) + fabs(b) + fabs(c);
+    const double eps = 32.0 * 2.220446049250313e-16 * scale;
+    if (fabs(a) <= eps) {
+        if (fabs(b) > eps) roots[0] = -c / b;
+    } else {
+        const double disc = b * b - 4.0 * a * c;
+        if (disc >= 0.0) {
+            const double q = -0.5 * (b + copysign(sqrt(disc), b));
+            if (q == 0.0) roots[0] = -b / (2.0 * a);
+            else { roots[0] = q / a; roots[1] = c / q; }
+        }
+    }
+    for (int i = 0; i < 2; ++i) {
+        const double s = roots[i];
+        if (s > 0.0 && s < 1.0 && !(((c3 * s + c2) * s + c1) * s + c0 > kMinJacobian)) return false;
+    }
+    return true;
+}
+
+// per tet: the fewest halvings m of alpha0 whose trial segment is feasible
+// (max_halvings + 1 when none is); the step is set by the worst tet
+__global__ void feasible_step_kernel(const int* __restrict__ tets, int ntet, const double* __restrict__ x0,
+                                     const double* __restrict__ dx, const double* __restrict__ dminv, double alpha0,
+                                     int max_halvings, int* worst, int* count) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntet) return;
+    const int nd[4] = {tets[4 * t], tets[4 * t + 1], tets[4 * t + 2], tets[4 * t + 3]};
+    const double* Dm = dminv + 9 * (size_t)t;
+    auto defgrad = [&](double s, double* F) {  // F at x0 + s dx
+        double Ds[9];
+        for (int i = 0; i < 3; ++i)
+            for (int c = 0; c < 3; ++c) {
+                const size_t a = 3 * (size_t)nd[c + 1] + i, o = 3 * (size_t)nd[0] + i;
+                Ds[3 * i + c] = (x0[a] + s * dx[a]) - (x0[o] + s * dx[o]);
+            }
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                F[3 * i + j] = Ds[3 * i] * Dm[j] + Ds[3 * i + 1] * Dm[3 + j] + Ds[3 * i + 2] * Dm[6 + j];
+    };
+    double F0[9], F1[9];
+    defgrad(0.0, F0);
+    int m = 0;
+    double s = alpha0;
+    for (; m <= max_halvings; ++m, s *= 0.5) {
+        defgrad(s, F1);
+        if (segment_feasible(F0, F1)) break;
+    }
+    if (m > 0) {
+        atomicMax(worst, m);
+        atomicAdd(count, 1);
+    }
+}
+
 }  // namespace
 }  // namespace hsc
 
@@ -187,14 +267,15 @@ struct hsc_fem_assembler {
     int* ptr = nullptr;        // device nblk + 1
     int* src = nullptr;        // device ntet x 10
     double* stage = nullptr;   // device ntet x 10 x 9
-    int* bad = nullptr;        // device counter of inverted tets
+    int* bad = nullptr;        // device counter of inverted tets / worst halving count
+    int* aux = nullptr;        // device counter of tets that limit the step
 };
 
 namespace {
 void free_assembler(hsc_fem_assembler* a) {
     if (!a) return;
     cudaFree(a->tets); cudaFree(a->dminv); cudaFree(a->vol); cudaFree(a->mass); cudaFree(a->rows);
-    cudaFree(a->cols); cudaFree(a->ptr); cudaFree(a->src); cudaFree(a->stage); cudaFree(a->bad);
+    cudaFree(a->cols); cudaFree(a->ptr); cudaFree(a->src); cudaFree(a->stage); cudaFree(a->bad); cudaFree(a->aux);
     delete a;
 }
 template <class T> cudaError_t upload(T** d, const std::vector<T>& h) {
@@ -307,6 +388,29 @@ int hsc_fem_assemble(hsc_fem_assembler* a, const double* d_x, const double* d_E,
         if (cudaStreamSynchronize(st) != cudaSuccess) return HSC_ERR_CUDA;
         if (*inverted) return HSC_ERR_NONSPD;
     }
+    return HSC_OK;
+}
+
+int hsc_fem_feasible_step(hsc_fem_assembler* a, const double* d_x0, const double* d_dx, double alpha0,
+                          int32_t max_halvings, double* alpha, int32_t* halvings, int32_t* limited, void* stream) {
+    if (!a || !d_x0 || !d_dx || !alpha || !(alpha0 > 0) || max_halvings < 0 || max_halvings > 1000)
+        return HSC_ERR_INVALID;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemsetAsync(a->bad, 0, sizeof(int), st) != cudaSuccess) return HSC_ERR_CUDA;
+    if (!a->aux && cudaMalloc((void**)&a->aux, sizeof(int)) != cudaSuccess) return HSC_ERR_ALLOC;
+    if (cudaMemsetAsync(a->aux, 0, sizeof(int), st) != cudaSuccess) return HSC_ERR_CUDA;
+    hsc::count_launch();
+    hsc::feasible_step_kernel<<<(a->ntet + 127) / 128, 128, 0, st>>>(a->tets, a->ntet, d_x0, d_dx, a->dminv, alpha0,
+                                                                    max_halvings, a->bad, a->aux);
+    if (cudaGetLastError() != cudaSuccess) return HSC_ERR_CUDA;
+    int h[2] = {0, 0};
+    if (cudaMemcpyAsync(&h[0], a->bad, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return HSC_ERR_CUDA;
+    if (cudaMemcpyAsync(&h[1], a->aux, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return HSC_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return HSC_ERR_CUDA;
+    if (halvings) *halvings = h[0];
+    if (limited) *limited = h[1];
+    if (h[0] > max_halvings) { *alpha = 0.0; return HSC_ERR_NONSPD; }
+    *alpha = std::ldexp(alpha0, -h[0]);
     return HSC_OK;
 }
 

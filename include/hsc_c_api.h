@@ -236,6 +236,13 @@ HSC_EXPORT int hsc_fem_pattern(const hsc_fem_assembler* a, int32_t* d_rows, int3
  * (nnzb x 9).  With `inverted` (host) set, waits and reports tets with det F <= 0 (HSC_ERR_NONSPD). */
 HSC_EXPORT int hsc_fem_assemble(hsc_fem_assembler* a, const double* d_x, const double* d_E, double* d_values,
                                 int32_t* inverted, void* stream);
+/* Line-search feasibility of a Newton direction (feasible_segment, log_neo_hookean_function.h:37-75, as the
+ * energy kernel applies it, log_neo_hookean_3d.cu:45-52): the largest alpha = alpha0 * 2^-m, m <= max_halvings,
+ * such that det F(x0 + s dx) > 1e-8 on every tet for all s in [0, alpha].  *halvings = m, *limited = the tets
+ * that needed m > 0.  HSC_ERR_NONSPD (alpha = 0) when no such step exists or x0 itself is inverted. */
+HSC_EXPORT int hsc_fem_feasible_step(hsc_fem_assembler* a, const double* d_x0, const double* d_dx, double alpha0,
+                                     int32_t max_halvings, double* alpha, int32_t* halvings, int32_t* limited,
+                                     void* stream);
 
 /* ---------------------------------------------------------------------------
  * Learned polynomial preconditioner (no reference counterpart; the reference

@@ -83,3 +83,58 @@ def assemble(tets, rest_x, x, E, rho=1000.0, nu=0.3, dt=1.0 / 30.0, project=True
     keys = np.array(sorted(blocks))
     vals = np.array([np.asarray(blocks[k]).T.reshape(9) for k in keys])  # column-major
     return (keys // n).astype(np.int32), (keys % n).astype(np.int32), vals
+
+
+MIN_JACOBIAN = 1e-8
+
+
+def _triple(a, b, c):
+    return a @ np.cross(b, c)
+
+
+def segment_feasible(A, E):
+    """``feasible_segment`` (``log_neo_hookean_function.h:37-75``): det(A + s (E - A))
+    stays above 1e-8 on [0, 1] -- endpoints and the derivative roots of the cubic."""
+    B = E - A
+    c0 = np.linalg.det(A)
+    c1 = _triple(B[:, 0], A[:, 1], A[:, 2]) + _triple(A[:, 0], B[:, 1], A[:, 2]) + _triple(A[:, 0], A[:, 1], B[:, 2])
+    c2 = _triple(A[:, 0], B[:, 1], B[:, 2]) + _triple(B[:, 0], A[:, 1], B[:, 2]) + _triple(B[:, 0], B[:, 1], A[:, 2])
+    c3 = np.linalg.det(B)
+    if not (c0 > MIN_JACOBIAN and np.linalg.det(E) > MIN_JACOBIAN):
+        return False
+    a, b, c = 3 * c3, 2 * c2, c1
+    roots = []
+    scale = abs(a) + abs(b) + abs(c)
+    eps = 32 * 2.220446049250313e-16 * scale
+    if abs(a) <= eps:
+        if abs(b) > eps:
+            roots.append(-c / b)
+    else:
+        disc = b * b - 4 * a * c
+        if disc >= 0:
+            q = -0.5 * (b + np.copysign(np.sqrt(disc), b))
+            roots += [-b / (2 * a)] if q == 0 else [q / a, c / q]
+    return all(not (0 < s < 1) or ((c3 * s + c2) * s + c1) * s + c0 > MIN_JACOBIAN for s in roots)
+
+
+def feasible_step(tets, rest_x, x0, dx, alpha0=1.0, max_halvings=60):
+    """(alpha, halvings, limiting tets) of the backtracking rule: the fewest halvings of alpha0
+    that keep every tet's segment feasible."""
+    tets = np.asarray(tets)
+    Dminv = np.linalg.inv(np.transpose(rest_x[tets[:, 1:]] - rest_x[tets[:, :1]], (0, 2, 1)))
+    worst, limited = 0, 0
+    for t, nd in enumerate(tets):
+        F0 = np.transpose(x0[nd[1:]] - x0[nd[:1]]) @ Dminv[t]
+        s, m = alpha0, 0
+        while m <= max_halvings:
+            xs = x0[nd] + s * dx[nd]
+            F1 = np.transpose(xs[1:] - xs[:1]) @ Dminv[t]
+            if segment_feasible(F0, F1):
+                break
+            m += 1
+            s *= 0.5
+        worst = max(worst, m)
+        limited += m > 0
+    if worst > max_halvings:
+        return 0.0, worst, limited
+    return alpha0 * 2.0 ** -worst, worst, limited

@@ -121,3 +121,91 @@ def test_device_assembled_system_solves(torch):
     assert abs(st["pcg_iterations"] - so["pcg_iterations"]) <= 1
     assert np.linalg.norm(xg.cpu().numpy() - xo) <= 1e-6 * np.linalg.norm(xo)
     assert st["full_relative_residual"] <= 1e-7
+
+
+def test_oracle_feasibility_rule():
+    """A segment that passes through an inverted state between two positive
+    endpoints is infeasible (the reason for checking the derivative roots)."""
+    A = np.eye(3)
+    E = np.diag([1.0, 1.0, 1.0])
+    E[2, 2] = 1.0
+    assert F.segment_feasible(A, E)
+    # det(A + s B) = (1 - 2 s)^2 (1 + ...) dips to 0 at s = 0.5 while both ends are positive
+    A = np.diag([1.0, 1.0, 1.0])
+    E = np.diag([-1.0, -1.0, 1.0])
+    assert np.linalg.det(E) > 0
+    assert not F.segment_feasible(A, E)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scale", [0.05, 0.6, 3.0])
+def test_gpu_feasible_step_matches_oracle(torch, scale):
+    from hsc_reimpl_b200.assembly import FemAssembler
+    rng = np.random.default_rng(int(scale * 100))
+    x, tets = S.cube_mesh(5, 0.02)
+    dx = scale * 0.02 * rng.standard_normal(x.shape)
+    asm = FemAssembler(tets, x)
+    got = asm.feasible_step(x, dx, alpha0=1.0, max_halvings=40)
+    ref = F.feasible_step(tets, x, x, dx, alpha0=1.0, max_halvings=40)
+    assert got[1] == ref[1] and got[2] == ref[2]
+    assert got[0] == ref[0]
+    if scale < 0.1:
+        assert got == (1.0, 0, 0)
+    else:
+        assert got[1] > 0
+
+
+def test_oracle_feasible_step_is_tight():
+    """The returned step keeps every tet feasible and twice it does not."""
+    rng = np.random.default_rng(3)
+    x, tets = S.cube_mesh(2, 0.02)
+    dx = 0.04 * rng.standard_normal(x.shape)
+    alpha, m, lim = F.feasible_step(tets, x, x, dx, alpha0=1.0, max_halvings=40)
+    assert m > 0 and lim > 0 and alpha == 2.0 ** -m
+    a1, m1, _ = F.feasible_step(tets, x, x, alpha * dx, alpha0=1.0, max_halvings=40)
+    assert (a1, m1) == (1.0, 0)
+    _, m2, _ = F.feasible_step(tets, x, x, 2 * alpha * dx, alpha0=1.0, max_halvings=40)
+    assert m2 == 1
+
+
+@pytest.mark.gpu
+def test_gpu_feasible_step_rejects_inverted_start(torch):
+    from hsc_reimpl_b200.assembly import FemAssembler
+    x, tets = S.cube_mesh(3, 0.02)
+    asm = FemAssembler(tets, x)
+    xi = x.copy()
+    xi[:, 2] *= -1.0  # mirrored: every tet inverted at s = 0
+    alpha, m, lim = asm.feasible_step(xi, np.zeros_like(x), alpha0=1.0, max_halvings=8)
+    assert alpha == 0.0 and m == 9 and lim == len(tets)
+    assert F.feasible_step(tets, x, xi, np.zeros_like(x), 1.0, 8) == (0.0, 9, len(tets))
+    # a half step along a feasible direction
+    alpha, m, lim = asm.feasible_step(x, np.zeros_like(x), alpha0=0.5, max_halvings=8)
+    assert (alpha, m, lim) == (0.5, 0, 0)
+
+
+# The reference's native segment checks (reproduction/hsc_backend/check_log_nh.cpp:78-87):
+# (end matrix, feasible from the identity)
+def _segment_cases():
+    two_roots = np.eye(3); two_roots[0, 0] = -3; two_roots[1, 1] = -1     # det < 0 between 1/4 and 1/2
+    double_root = np.eye(3); double_root[0, 0] = -1; double_root[1, 1] = -1  # det touches 0 at 1/2
+    inverted_end = np.eye(3); inverted_end[2, 2] = -0.1
+    return [(two_roots, False), (double_root, False), (inverted_end, False), (0.25 * np.eye(3), True),
+            (np.eye(3), True)]
+
+
+def test_oracle_segment_known_answers():
+    for E, ok in _segment_cases():
+        assert F.segment_feasible(np.eye(3), E) == ok
+
+
+@pytest.mark.gpu
+def test_gpu_segment_known_answers(torch):
+    """One unit tet (Dm = I, so F = Ds): the step from the rest shape to F = E."""
+    from hsc_reimpl_b200.assembly import FemAssembler
+    rest = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], dtype=np.float64)
+    tets = np.array([[0, 1, 2, 3]], dtype=np.int32)
+    asm = FemAssembler(tets, rest)
+    for E, ok in _segment_cases():
+        end = np.vstack([np.zeros(3), E.T])  # node k = column k of F
+        got = asm.feasible_step(rest, end - rest, alpha0=1.0, max_halvings=0)
+        assert got == ((1.0, 0, 0) if ok else (0.0, 1, 1)), (E, got)
