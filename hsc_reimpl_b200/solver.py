@@ -335,8 +335,9 @@ class SolvingInfo:
 class LinearHSC:
     """Drop-in for the reference's ``LinearHSC : IterativeSolver``."""
 
-    def __init__(self, workspace: str | None = None):
+    def __init__(self, workspace: str | None = None, dump_systems: bool = False):
         self.workspace = workspace
+        self.dump_systems = dump_systems      # <workspace>/systems/f<frame>_n<newton>.npz per solve
         self.ctx: HSCContext | None = None
         self.options: HSCOptions | None = None
         self.frame = 0
@@ -371,6 +372,12 @@ class LinearHSC:
             os.makedirs(self.workspace, exist_ok=True)
             with open(os.path.join(self.workspace, "hsc_stats.jsonl"), "a") as f:
                 f.write(json.dumps(record) + "\n")
+            if self.dump_systems:
+                from .records import dump_system
+                d = os.path.join(self.workspace, "systems")
+                os.makedirs(d, exist_ok=True)
+                dump_system(os.path.join(d, f"f{self.frame:06d}_n{self.newton:04d}.npz"), info.A(),
+                            options=self.options, record=record, x=info.x())
         if stats["status"] != _lib.HSC_OK:
             raise HSCError(stats["status"], self.ctx.lib.hsc_last_error(self.ctx._ptr).decode())
         return stats
