@@ -140,6 +140,14 @@ EXPORTS = {
     "hsc_fem_feasible_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int32,
                                         C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                         C.c_void_p]),
+    "hsc_coupling_assembler_create": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32,
+                                                C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
+                                                C.POINTER(C.c_void_p)]),
+    "hsc_coupling_assembler_destroy": (C.c_int, [C.c_void_p]),
+    "hsc_coupling_assemble": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                        C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_void_p]),
+    "hsc_coupling_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p]),
 }
 
 _LIB = None

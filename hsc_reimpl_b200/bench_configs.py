@@ -10,7 +10,8 @@ c4  the learned polynomial preconditioner on held-out vehicle trajectories:
     PCG iterations and time to 1e-6 against plain order-2 Neumann (FP64 and FP32)
 vehicle  two FP64 solves of the vehicle system (a short, fixed command for profilers)
 assembly GPU assembly of the vehicle's 78,120-tet log-NH Hessian (hsc_fem_assemble) per call,
-         and the line-search feasible step of a rough direction (hsc_fem_feasible_step)
+         the line-search feasible step of a rough direction (hsc_fem_feasible_step) and the
+         ABD-FEM contact coupling with its E (hsc_coupling_assemble, 40,000 contacts)
 c5  the 1 M-tet torus (12 bodies, 30 % contact-active tread): FP64 / FP32 /
     BF16 solves with their error against a tight FP64 reference, ACA rank sweep
     8-64, Neumann order sweep 1-4, HBM GB/s of the full-H SpMV
@@ -222,8 +223,29 @@ def assembly(reps=10):
         e1.record()
         torch.cuda.synchronize()
         fs.append(e0.elapsed_time(e1))
+    # ABD-FEM contact coupling: 12 bodies x 400 vertices, 40,000 contacts on the 19,530 FEM nodes
+    from .assembly import CouplingAssembler
+    nb, nv, ncon = 12, 400, 40_000
+    v2b = np.repeat(np.arange(nb), nv).astype(np.int32)
+    xbar = rng.uniform(-1, 1, (nb * nv, 3))
+    av = rng.integers(0, nb * nv, ncon).astype(np.int32)
+    fv = rng.integers(0, len(x), ncon).astype(np.int32)
+    nrm = rng.standard_normal((ncon, 3))
+    Hc = -(nrm[:, :, None] * nrm[:, None, :]).reshape(-1, 9)
+    ca = CouplingAssembler(v2b, xbar, nb, len(x))
+    avd, fvd, Hd = (torch.from_numpy(a).cuda() for a in (av, fv, Hc))
+    cp = ca.assemble(avd, fvd, Hd)
+    cs = []
+    for _ in range(reps):
+        e0.record()
+        ca.assemble(avd, fvd, Hd)  # includes its one stream sync (sizes E) and the copies out
+        e1.record()
+        torch.cuda.synchronize()
+        cs.append(e0.elapsed_time(e1))
     return {"tets": int(len(tets)), "nodes": int(len(x)), "blocks": int(asm.nnzb), "ms": m,
             "tets_per_s": len(tets) / (m / 1000),
+            "coupling": {"bodies": nb, "contacts": ncon, "blocks": int(cp["rows"].numel()),
+                         "active_dofs": int(cp["active"].numel()), "ms": statistics.median(cs)},
             "feasible_step": {"alpha": feas[0], "halvings": feas[1], "limiting_tets": feas[2],
                               "ms": statistics.median(fs)}}
 

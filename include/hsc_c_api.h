@@ -240,6 +240,31 @@ HSC_EXPORT int hsc_fem_assemble(hsc_fem_assembler* a, const double* d_x, const d
  * energy kernel applies it, log_neo_hookean_3d.cu:45-52): the largest alpha = alpha0 * 2^-m, m <= max_halvings,
  * such that det F(x0 + s dx) > 1e-8 on every tet for all s in [0, alpha].  *halvings = m, *limited = the tets
  * that needed m > 0.  HSC_ERR_NONSPD (alpha = 0) when no such step exists or x0 itself is inverted. */
+/* ABD-FEM contact coupling, assembled on the device (reference: ABDFEMLinearSubsystem_assemble_kernel,
+ * abd_fem_linear_subsystem.cu:18-61) and fused with the solver's active-column and E extraction
+ * (linear_hsc.cu:205-247).  Per contact: H12x3 = J(xbar)^T H (zero when the body or the FEM node is fixed),
+ * summed per (body, node) pair in input order; output, sorted by (row, col): the upper-triangle blocks
+ * (abd_block_offset + 4 body + k, fem_block_offset + node), k = 0..3, of every pair with a nonzero block
+ * (column-major 3x3 values); the sorted global dofs 3 (fem_block_offset + node) + j of the nodes with a
+ * coupling block of nonzero squared norm; and E (12 nbody x nactive, row-major) over them.
+ * p_first = 1: body dofs (p, a1, a2, a3) with x = p + (a1.xbar, a2.xbar, a3.xbar) (libuipc's order);
+ * p_first = 0: (a1, a2, a3, p).  body_fixed / fem_fixed may be NULL. */
+typedef struct hsc_coupling_assembler hsc_coupling_assembler;
+HSC_EXPORT int hsc_coupling_assembler_create(int32_t n_abd_vertices, const int32_t* v2b, const double* x_bar,
+                                             int32_t nbody, const int32_t* body_fixed, int32_t nfem,
+                                             const int32_t* fem_fixed, int32_t abd_block_offset,
+                                             int32_t fem_block_offset, int32_t p_first, hsc_coupling_assembler** out);
+HSC_EXPORT int hsc_coupling_assembler_destroy(hsc_coupling_assembler* a);
+/* d_abd_vertex: ABD-local vertex per contact; d_fem_vertex: FEM-local node; d_H: 9 doubles per contact, the
+ * column-major 3x3 block (rows: the ABD vertex's dofs, columns: the FEM node's).  Synchronises the stream once
+ * to size E; *nblocks and *nactive are the output sizes.  HSC_ERR_INVALID on an index out of range. */
+HSC_EXPORT int hsc_coupling_assemble(hsc_coupling_assembler* a, const int32_t* d_abd_vertex,
+                                     const int32_t* d_fem_vertex, const double* d_H, int32_t ncontact,
+                                     int32_t* nblocks, int32_t* nactive, void* stream);
+/* Copies the last assembly's outputs (any pointer may be NULL): rows/cols [nblocks], values [9 nblocks],
+ * active [nactive], E [12 nbody x nactive]. */
+HSC_EXPORT int hsc_coupling_read(hsc_coupling_assembler* a, int32_t* d_rows, int32_t* d_cols, double* d_values,
+                                 int32_t* d_active, double* d_E, void* stream);
 HSC_EXPORT int hsc_fem_feasible_step(hsc_fem_assembler* a, const double* d_x0, const double* d_dx, double alpha0,
                                      int32_t max_halvings, double* alpha, int32_t* halvings, int32_t* limited,
                                      void* stream);
