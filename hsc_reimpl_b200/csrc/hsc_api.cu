@@ -12,6 +12,7 @@
 //   one D2H copy of the per-system scalars, then the status checks of
 //   linear_hsc.cu:394-435.
 #include <algorithm>
+#include <cstdlib>
 #include <cstddef>
 #include <cmath>
 #include <cstdio>
@@ -612,11 +613,27 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
     int G = bps * ctx->num_sms;
     const int ns = (int)idx.size();
     if (ns > G) return fail(ctx, HSC_ERR_INVALID, "more systems than co-resident CTAs");
+    // Work of a row range in block units: its blocks, one per row (vector updates), and for each node
+    // with coupled dofs the low-rank products of every preconditioner term (V^T t partial sums and the
+    // V c correction: 2 x 3 dofs x kmax multiply-adds, a block being 9), scaled by 0.5: the weight that
+    // measured fastest on the vehicle system among 0, 0.5, 1, 2, 4 (HSC_ACTIVE_ROW_WEIGHT overrides it).
+    double act_w = 0.5;
+    if (const char* e = std::getenv("HSC_ACTIVE_ROW_WEIGHT")) act_w = std::max(0.0, std::atof(e));
+    std::vector<std::vector<long long>> wpre(ns);  // per system: weighted prefix over rows
     long long tot = 0;
     std::vector<long long> w(ns);
     for (int s = 0; s < ns; ++s) {
         const System& S = ctx->sys[idx[s]];
-        w[s] = std::max<long long>(1, (long long)S.nnz + S.n);
+        const long long extra = (long long)std::llround(act_w * 6.0 * std::max(0, S.kmax) / 9.0);
+        auto& pre = wpre[s];
+        pre.assign(S.n + 1, 0);
+        long long nact_before = 0;
+        for (int i = 0; i < S.n; ++i) {
+            pre[i] = (long long)S.h_rowptr[i] + i + extra * nact_before;
+            if (S.h_rowflag[i] >= 0) ++nact_before;
+        }
+        pre[S.n] = (long long)S.h_rowptr[S.n] + S.n + extra * nact_before;
+        w[s] = std::max<long long>(1, pre[S.n]);
         tot += w[s];
     }
     // CTAs per system proportional to work, at least one, at most one per 16 rows
@@ -640,14 +657,15 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
     for (int s = 0; s < ns; ++s) {
         System& S = ctx->sys[idx[s]];
         const int b = c;
-        const long long rows_w = (long long)S.nnz + S.n;
+        const auto& pre = wpre[s];
+        const long long rows_w = pre[S.n];
         int row = 0;
         for (int k = 0; k < nc[s]; ++k, ++c) {
             const long long target = rows_w * (k + 1) / nc[s];
             const int rb = row;
             if (k == nc[s] - 1) row = S.n;
             else
-                while (row < S.n && (long long)S.h_rowptr[row] + row < target) ++row;
+                while (row < S.n && pre[row] < target) ++row;
             cta_sys[c] = s;
             cta_row[2 * c] = rb;
             cta_row[2 * c + 1] = row;
@@ -924,6 +942,10 @@ int launch_pcg_all(hsc_ctx* ctx, int nsys, cudaStream_t st) {
     prm.max_iter = o.max_iter;
     prm.rr_every = o.residual_replacement;
     prm.spin_limit = o.spin_limit;
+    // the barrier counter grows by one per CTA and grid barrier (at most nterms + 2 per iteration,
+    // one iteration more for the replacement slot) and keeps its top bit for the abort flag
+    if ((double)(o.max_iter + 2) * (prm.nterms + 3) * ctx->grid >= (double)kBarAbortBit)
+        return fail(ctx, HSC_ERR_INVALID, "max_iter too large for the grid barrier counter");
     CK(cudaMemsetAsync(ctx->d_bar.p, 0, sizeof(GridBar), st));
     set_int(ctx->d_remaining.as<int>(), nsys, st);
     CK(launch_pcg(o.precision, o.threads_per_row, prm, ctx->grid, ctx->pcg_smem, st));

@@ -52,21 +52,27 @@ __device__ __forceinline__ void red_release_add_u32(unsigned int* p, unsigned in
 // Thread-0 half of a grid barrier: release-arrive on the monotonic counter,
 // then acquire-poll until barrier `epoch` is complete.  Bounded: returns
 // false (and raises gb->abort) when the wait gives up or another CTA aborted.
+// A CTA that gives up also sets the counter's top bit, so every waiter's poll
+// sees the count reach its target and the abort in the same load: the barrier
+// costs no extra round trip for the abort check.  (The counter is reset before
+// each launch and stays below 2^31: epochs x CTAs per launch.)
+constexpr unsigned int kBarAbortBit = 0x80000000u;
 __device__ __forceinline__ bool grid_arrive_wait(GridBar* gb, unsigned int nblocks, long long limit, int epoch) {
     const unsigned int target = (unsigned int)(epoch + 1) * nblocks;
     red_release_add_u32(&gb->count, 1u);
     long long n = 0;
-    while (ld_acquire_u32(&gb->count) < target) {
+    unsigned int c;
+    while ((c = ld_acquire_u32(&gb->count)) < target) {
         ++n;
         if (n > 256) __nanosleep(20);
-        if ((n & 255) == 0 && ld_volatile_i32(&gb->abort)) return false;
         if (n > limit) {
             atomicExch(&gb->abort, 1);
             atomicExch(&gb->where, epoch);
+            atomicOr(&gb->count, kBarAbortBit);
             return false;
         }
     }
-    return ld_volatile_i32(&gb->abort) == 0;
+    return (c & kBarAbortBit) == 0;
 }
 
 // Grid-wide barrier for a cooperative launch.  The arrival counter only

@@ -305,9 +305,17 @@ enum SlotKind { kIdle = 0, kNormal = 1, kReplace = 2 };
 
 template <class MT, class PT, class VT, int TPR>
 __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_arg) {
-    // a local copy: the lambdas below capture it by reference, and a reference
-    // to a kernel parameter would be a parameter-space address
-    const PcgParams prm = prm_arg;
+    // The parameters and this CTA's system descriptor live in shared memory, one
+    // copy per CTA: the lambdas below capture them by reference (a reference to
+    // a kernel parameter would be a parameter-space address), and a per-thread
+    // local copy (440 B x 512 threads) does not stay in L1, so its loads went to
+    // L2 after every grid barrier.
+    __shared__ __align__(16) unsigned char s_prm_raw[sizeof(PcgParams)];
+    __shared__ __align__(16) unsigned char s_sys_raw[sizeof(SysDesc)];
+    PcgParams& prm_sh = *reinterpret_cast<PcgParams*>(s_prm_raw);
+    if (threadIdx.x == 0) prm_sh = prm_arg;
+    __syncthreads();
+    const PcgParams& prm = prm_sh;
     using CT = typename Cmp<MT>::T;
     using DT = typename DinvT<MT>::T;
     // 32-block slices a warp loads per round trip in the SpMV (the "tile width" the
@@ -325,7 +333,10 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
     const int cta = blockIdx.x;
     const unsigned int G = gridDim.x;
     const int sidx = prm.cta_sys[cta];
-    const SysDesc& S = prm.sys[sidx];
+    SysDesc& sys_sh = *reinterpret_cast<SysDesc*>(s_sys_raw);
+    if (threadIdx.x == 0) sys_sh = prm.sys[sidx];
+    __syncthreads();
+    const SysDesc& S = sys_sh;
     const int rb = prm.cta_row[2 * cta], re = prm.cta_row[2 * cta + 1];
     const int ab = prm.cta_act[2 * cta], ae = prm.cta_act[2 * cta + 1];
     const int aidx = prm.cta_aidx[cta];
@@ -348,8 +359,13 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
     const double* rhs = S.rhs;
     VT* z = reinterpret_cast<VT*>(S.z);
     VT* y = reinterpret_cast<VT*>(S.y);
-    VT* pbuf[2] = {reinterpret_cast<VT*>(S.p[0]), reinterpret_cast<VT*>(S.p[1])};
-    VT* tbuf[2] = {reinterpret_cast<VT*>(S.t[0]), reinterpret_cast<VT*>(S.t[1])};
+    // ping-pong buffers chosen by a select, not a runtime-indexed (local-memory) array
+    VT* const pbuf0 = reinterpret_cast<VT*>(S.p[0]);
+    VT* const pbuf1 = reinterpret_cast<VT*>(S.p[1]);
+    VT* const tbuf0 = reinterpret_cast<VT*>(S.t[0]);
+    VT* const tbuf1 = reinterpret_cast<VT*>(S.t[1]);
+    auto pbuf = [&](int i) { return i ? pbuf1 : pbuf0; };
+    auto tbuf = [&](int i) { return i ? tbuf1 : tbuf0; };
 
     // shared memory (offsets in doubles, the same in every CTA): d .* tt,
     // own coupled-dof z, the Vt block of the own coupled dofs, the row sums of
@@ -657,8 +673,8 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
             double acc = 0.0;
             const bool last = (k == nterms - 1);
             if (active_sys) {
-                const VT* tcur = tbuf[tc];
-                VT* tnew = tbuf[tc ^ 1];
+                const VT* tcur = tbuf(tc);
+                VT* tnew = tbuf(tc ^ 1);
                 const double wk = weight(k);
                 // Schur basis: low-rank part Vt d Vt^T t of S t at the own coupled dofs
                 const bool corr = schur && na > 0;
@@ -742,10 +758,10 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
             Vec4<double>::load(rhs, row, r0, r1, r2);
             st_r(row, r0, r1, r2);
             st_x(row, 0.0, 0.0, 0.0);
-            Vec4<VT>::store(pbuf[0], row, (VT)0, (VT)0, (VT)0);  // beta * p_prev must be 0, not NaN
+            Vec4<VT>::store(pbuf(0), row, (VT)0, (VT)0, (VT)0);  // beta * p_prev must be 0, not NaN
             double t0, t1, t2;
             dinv_row(row, r0, r1, r2, t0, t1, t2);
-            st_t(tbuf[0], row, (VT)t0, (VT)t1, (VT)t2);
+            st_t(tbuf(0), row, (VT)t0, (VT)t1, (VT)t2);
             const double w0 = weight(0);
             const VT z0 = (VT)(w0 * t0), z1 = (VT)(w0 * t1), z2 = (VT)(w0 * t2);
             st_z(row, z0, z1, z2);
@@ -755,7 +771,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
         for (int i = ab + threadIdx.x; i < ae; i += kThreads) pact_ref(i) = 0.0;
         if (na <= 0)
             for (int j = threadIdx.x; j < rank; j += kThreads) S.zpart[(size_t)j * ncta + lcta] = 0.0;
-        if (schur && nterms > 1) compute_part(tbuf[0], s_to, tpart_half(0) + aidx, nact);
+        if (schur && nterms > 1) compute_part(tbuf(0), s_to, tpart_half(0) + aidx, nact);
         if (leader_cta)
             for (int j = threadIdx.x; j < rank; j += kThreads) S.tt[j] = 0.0;
         if (nterms == 1) compute_zpart();
@@ -774,6 +790,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
             warp_sum_parts(prm.part_rr, prm.part_rz, cb, ce, srr, srz);
             if (lane == 0) { s_bc[0] = srr; s_bc[1] = srz; }
         }
+        mark(14);
         __syncthreads();
         const double rr = s_bc[0];
         const double rzn = s_bc[1];
@@ -825,12 +842,13 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
             }
         }
 
+        mark(15);
         // ---- phase A: y = D p (p = z + beta p_prev on the fly), tt = Vt^T p ----
         {
             double acc = 0.0;
             if (slot == kNormal) {
-                VT* pnew = pbuf[pc ^ 1];
-                const VT* pprev = pbuf[pc];
+                VT* pnew = pbuf(pc ^ 1);
+                const VT* pprev = pbuf(pc);
                 const CT bc = (CT)beta;
                 const double bd = beta;
                 auto gather = [&](int c, CT& g0, CT& g1, CT& g2) {
@@ -929,7 +947,9 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
             if (!barrier(prm.part_pap, acc, nullptr, 0.0)) return;
             mark(2);
         }
-        if (ld_volatile_i32(prm.remaining) == 0) break;
+        // every system finished: only possible once this CTA's own system is done, so the
+        // load stays off the critical path of the CTAs still iterating
+        if (done && ld_volatile_i32(prm.remaining) == 0) break;
 
         // ---- phase B: alpha, low-rank correction, x/r update, t = w Dd^-1 r ----
         {
@@ -961,12 +981,12 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
             }
             if (work && fused_slot) {
                 // ---- fused update + first preconditioner phase ----
-                const VT* pnew = pbuf[pc ^ 1];
+                const VT* pnew = pbuf(pc ^ 1);
                 const double W0 = weight(0), W1 = weight(1);
                 const bool last1 = nterms == 2;
                 const double* rold = rbuf[rcur];
                 double* rnew = rbuf[rcur ^ 1];
-                VT* t1buf = tbuf[tc ^ 1];
+                VT* t1buf = tbuf(tc ^ 1);
                 __syncthreads();  // s_dtt filled above
                 // low-rank part of y at the coupled window dofs: 8 threads per dof
                 // (the order of lowrank_rows), Vt rows read from L2
@@ -1082,7 +1102,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                     }
                 }
                 __syncthreads();
-                const VT* pnew = pbuf[pc ^ 1];
+                const VT* pnew = pbuf(pc ^ 1);
                 const double w0 = weight(0);
                 for (int row = rb + threadIdx.x; row < re; row += kThreads) {
                     double r0, r1, r2;
@@ -1110,7 +1130,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                     }
                     double t0, t1, t2;
                     dinv_row(row, r0, r1, r2, t0, t1, t2);
-                    st_t(tbuf[tc], row, (VT)t0, (VT)t1, (VT)t2);
+                    st_t(tbuf(tc), row, (VT)t0, (VT)t1, (VT)t2);
                     const VT z0 = (VT)(w0 * t0), z1 = (VT)(w0 * t1), z2 = (VT)(w0 * t2);
                     st_z(row, z0, z1, z2);
                     acc_rr += r0 * r0 + r1 * r1 + r2 * r2;
@@ -1122,7 +1142,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                     pc ^= 1;
                 }
                 if (nterms == 1) compute_zpart();
-                else if (schur) compute_part(tbuf[tc], s_to, tpart_half(0) + aidx, nact);
+                else if (schur) compute_part(tbuf(tc), s_to, tpart_half(0) + aidx, nact);
             }
             if (!work) slot = kIdle;
             tail_k0 = (work && fused_slot) ? 2 : 1;
