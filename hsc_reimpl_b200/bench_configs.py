@@ -8,7 +8,8 @@ c3  64 uneven systems in one persistent launch replayed as a CUDA graph, FP32
     autotuner (tile width x ACA rank cap 4-256; omega 0.6)
 c4  the learned polynomial preconditioner on held-out vehicle trajectories:
     PCG iterations and time to 1e-6 against plain order-2 Neumann (FP64 and FP32)
-vehicle  two FP64 solves of the vehicle system (a short, fixed command for profilers)
+vehicle  two solves of the vehicle system in --vehicle-precision (default FP64; a short, fixed command
+         for profilers)
 assembly GPU assembly of the vehicle's 78,120-tet log-NH Hessian (hsc_fem_assemble) per call,
          the line-search feasible step of a rough direction (hsc_fem_feasible_step) and the
          ABD-FEM contact coupling with its E (hsc_coupling_assemble, 40,000 contacts)
@@ -269,6 +270,7 @@ def main(argv=None):
     ap.add_argument("--only", default="c1,c3,c4,c5")
     ap.add_argument("--out", default=None)
     ap.add_argument("--batch-count", type=int, default=64)
+    ap.add_argument("--vehicle-precision", default="fp64", choices=("fp64", "fp32", "bf16"))
     a = ap.parse_args(argv)
     import torch
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
@@ -277,7 +279,7 @@ def main(argv=None):
     if "assembly" in want:
         rep["assembly"] = assembly(); log(json.dumps({"assembly": rep["assembly"]}))
     if "vehicle" in want:
-        rep["vehicle"] = vehicle(); log(json.dumps({"vehicle": rep["vehicle"]}))
+        rep["vehicle"] = vehicle(a.vehicle_precision); log(json.dumps({"vehicle": rep["vehicle"]}))
     if "c1" in want:
         rep["c1"] = c1(flush); log(json.dumps({"c1": rep["c1"]}))
     if "c3" in want:

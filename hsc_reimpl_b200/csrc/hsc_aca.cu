@@ -4,8 +4,9 @@
 // shared memory: CTA c of the cluster owns columns [c*w, (c+1)*w).  One ACA
 // step (core.py:22-50; linear_hsc.cu:248-262) is
 //
-//   every CTA publishes (max |R|, first row-major index of it, sum R^2) of its
-//   slice and the column of its local argmax (its candidate for u)
+//   every CTA pushes (max |R|, first row-major index of it, sum R^2) of its
+//   slice into every CTA's shared memory and keeps the column of its local
+//   argmax (its candidate for u)
 //   -- one hardware cluster barrier --
 //   every CTA reduces the 16 partials in the same fixed order, picks the
 //   pivot (i, j), reads u = R[:, j] from the owning CTA's candidate buffer
@@ -33,7 +34,7 @@ namespace hsc {
 namespace {
 
 constexpr int kAcaCluster = 16;
-constexpr int kAcaThreads = 512;
+constexpr int kAcaThreads = 1024;
 constexpr int kAcaWarps = kAcaThreads / 32;
 
 struct Part {
@@ -45,6 +46,21 @@ struct Part {
 
 __device__ __forceinline__ void better_into(double& v, long long& i, double qv, long long qi) {
     if (qv > v || (qv == v && qi < i)) { v = qv; i = qi; }
+}
+
+// the same order on a CTA-local row-major index (r * nl + c): within one CTA's
+// column slice it orders entries exactly as the global row-major index does
+__device__ __forceinline__ void better_into32(double& v, int& i, double qv, int qi) {
+    if (qv > v || (qv == v && qi < i)) { v = qv; i = qi; }
+}
+
+__device__ __forceinline__ void warp_best32(double& v, int& i, double& s) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const double qv = __shfl_xor_sync(0xffffffffu, v, o);
+        const int qi = __shfl_xor_sync(0xffffffffu, i, o);
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+        better_into32(v, i, qv, qi);
+    }
 }
 
 __device__ __forceinline__ void warp_best(double& v, long long& i, double& s, int width) {
@@ -77,45 +93,52 @@ __global__ void __launch_bounds__(kAcaThreads, 1) aca_cluster_kernel(const AcaSy
     double* u = cand + 2 * m;       // m
     double* v = u + m;              // nl <= w
     __shared__ Part part[2];
+    __shared__ Part parts[2][kAcaCluster];  // every CTA's step partial, pushed by its owner
     __shared__ Part s_w[kAcaWarps];
     __shared__ double s_sc[2];
     __shared__ long long s_si;
+    __shared__ int s_bl;  // this CTA's local argmax (publish)
 
     for (int r = warp; r < m; r += kAcaWarps)
         for (int c = lane; c < nl; c += 32)
             if (HSC_IN(c0 + c < nc && r * nl + c < m * nl, 102, c0 + c)) R[r * nl + c] = P.E[(size_t)r * nc + c0 + c];
-    __syncthreads();
+    cl.sync();  // every CTA of the cluster has started before the first push into its shared memory
 
-    // local (max, idx, sum) of the slice -> part[slot]; candidate column -> cand[slot]
-    auto publish = [&](int slot, double ls, double lv, long long li) {
-        warp_best(lv, li, ls, 32);
-        if (lane == 0) s_w[warp] = Part{lv, li, ls, 0.0};
+    // local (max, idx, sum) of the slice -> part[slot] (global index); candidate column -> cand[slot].
+    // The argmax runs on the CTA-local index; kNone marks an empty slice.
+    constexpr int kNone = 0x7fffffff;
+    auto publish = [&](int slot, double ls, double lv, int li) {
+        warp_best32(lv, li, ls);
+        if (lane == 0) { s_w[warp].vmax = lv; s_w[warp].idx = li; s_w[warp].sum = ls; }
         __syncthreads();
-        if (tid == 0) {
+        if (warp == 0) {
+            // the warp partials in a fixed tree order (the same bits in every run)
             double bv = -1.0, bs = 0.0;
-            long long bi = total;
-            for (int q = 0; q < kAcaWarps; ++q) {
-                bs += s_w[q].sum;
-                better_into(bv, bi, s_w[q].vmax, s_w[q].idx);
-            }
-            part[slot] = Part{bv, bi, bs, 0.0};
+            int bi = kNone;
+            if (lane < kAcaWarps) { bv = s_w[lane].vmax; bi = (int)s_w[lane].idx; bs = s_w[lane].sum; }
+            warp_best32(bv, bi, bs);
+            const long long gi = bi == kNone ? total : (long long)(bi / nl) * nc + c0 + bi % nl;
+            const Part pt{bv, gi, bs, 0.0};
+            if (lane == 0) { part[slot] = pt; s_bl = bi; }
+            // push it to every CTA of the cluster (the cluster barrier publishes it)
+            if (lane < kAcaCluster) *cl.map_shared_rank(&parts[slot][cr], lane) = pt;
         }
         __syncthreads();
-        const long long gi = part[slot].idx;
-        if (gi < total) {
-            const int jl = (int)(gi % nc) - c0;
+        const int bl = s_bl;
+        if (bl != kNone) {
+            const int jl = bl % nl;
             for (int r = tid; r < m; r += kAcaThreads)
                 if (HSC_IN(jl >= 0 && jl < nl, 103, jl)) cand[slot * m + r] = R[r * nl + jl];
         }
     };
     {
         double ls = 0.0, lv = -1.0;
-        long long li = total;
+        int li = kNone;
         for (int r = warp; r < m; r += kAcaWarps)
             for (int c = lane; c < nl; c += 32) {
                 const double x = R[r * nl + c];
                 ls += x * x;
-                better_into(lv, li, fabs(x), (long long)r * nc + c0 + c);
+                better_into32(lv, li, fabs(x), r * nl + c);
             }
         publish(0, ls, lv, li);
     }
@@ -128,8 +151,8 @@ __global__ void __launch_bounds__(kAcaThreads, 1) aca_cluster_kernel(const AcaSy
             double pv = -1.0, ps = 0.0;
             long long pi = total;
             if (lane < kAcaCluster && HSC_IN(lane < (int)cl.num_blocks(), 109, lane)) {
-                const Part* rp = cl.map_shared_rank(&part[slot], lane);
-                pv = rp->vmax; pi = rp->idx; ps = rp->sum;
+                const Part& rp = parts[slot][lane];
+                pv = rp.vmax; pi = rp.idx; ps = rp.sum;
             }
             warp_best(pv, pi, ps, 32);
             if (lane == 0) { s_sc[0] = ps; s_sc[1] = pv; s_si = pi; }
@@ -161,14 +184,14 @@ __global__ void __launch_bounds__(kAcaThreads, 1) aca_cluster_kernel(const AcaSy
         for (int c = tid; c < nl; c += kAcaThreads)
             if (HSC_IN(k < P.cap && c0 + c < nc, 107, k)) P.V[(size_t)k * nc + c0 + c] = v[c];
         double ls = 0.0, lv = -1.0;
-        long long li = total;
+        int li = kNone;
         for (int r = warp; r < m; r += kAcaWarps) {
             const double ur = u[r];
             for (int c = lane; c < nl; c += 32) {
                 const double x = __dsub_rn(R[r * nl + c], __dmul_rn(ur, v[c]));  // numpy: R - outer(u, v)
                 R[r * nl + c] = x;
                 ls += x * x;
-                better_into(lv, li, fabs(x), (long long)r * nc + c0 + c);
+                better_into32(lv, li, fabs(x), r * nl + c);
             }
         }
         publish(slot ^ 1, ls, lv, li);

@@ -1181,7 +1181,7 @@ int hsc_options_default(hsc_options* o) {
     o->spin_limit = 20000000;
     o->check_residual = 1;
     o->trace_iterations = 0;
-    o->resident = 0;
+    o->resident = 1;
     o->fuse_update = 0;
     o->aca_cluster = 1;
     return HSC_OK;

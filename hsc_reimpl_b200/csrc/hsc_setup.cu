@@ -453,6 +453,101 @@ __global__ void __launch_bounds__(1024) gj_inverse_kernel(const double* A, int m
         for (int j = tx; j < m; j += 32) P[(size_t)i * m + j] = W[i * ld + j];
 }
 
+// The same elimination for m <= 144 with the matrix held in registers: thread
+// (ty, tx) of a 16 x 32 grid owns rows ty + 16 r (r < 9) and columns tx + 32 c
+// (c < 5) for the whole inversion.  Step k: the owners of row k and column k
+// publish them (and the reciprocal pivot) in shared memory, one barrier, then
+// every thread updates its own entries.  The published row and column alternate
+// between two buffers, so one barrier per step keeps the next step's writers off
+// this step's readers.  Per step a thread reads 14 shared values instead of
+// streaming the whole matrix through shared memory.
+constexpr int kGjR = 9, kGjC = 5, kGjMax = 16 * kGjR;
+__global__ void __launch_bounds__(512) gj_inverse_reg_kernel(const double* A, int m, double* P, int* bad) {
+    __shared__ double s_row[2][32 * kGjC], s_col[2][kGjMax], s_rp[2];
+    __shared__ int s_bad;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    double w[kGjR][kGjC];
+#pragma unroll
+    for (int r = 0; r < kGjR; ++r)
+#pragma unroll
+        for (int c = 0; c < kGjC; ++c) {
+            const int i = ty + 16 * r, j = tx + 32 * c;
+            w[r][c] = (i < m && j < m) ? A[(size_t)i * m + j] : 0.0;
+        }
+    if (threadIdx.x == 0) s_bad = 0;
+    for (int k = 0; k < m; ++k) {
+        const int b = k & 1, kr = k >> 4, kc = k >> 5;
+        if (ty == (k & 15)) {
+#pragma unroll
+            for (int r = 0; r < kGjR; ++r)
+                if (r == kr)
+#pragma unroll
+                    for (int c = 0; c < kGjC; ++c) {
+                        const int j = tx + 32 * c;
+                        if (j < m) s_row[b][j] = w[r][c];
+                    }
+        }
+        if (tx == (k & 31)) {
+#pragma unroll
+            for (int c = 0; c < kGjC; ++c)
+                if (c == kc)
+#pragma unroll
+                    for (int r = 0; r < kGjR; ++r) {
+                        const int i = ty + 16 * r;
+                        if (i < m) s_col[b][i] = w[r][c];
+                        if (i == k) {
+                            double p = w[r][c];
+                            if (!(p > 0.0) || !isfinite(p)) { s_bad = 1; p = 1.0; }
+                            s_rp[b] = 1.0 / p;
+                        }
+                    }
+        }
+        __syncthreads();
+        const double rp = s_rp[b];
+        double rs[kGjC];
+#pragma unroll
+        for (int c = 0; c < kGjC; ++c) {
+            const int j = tx + 32 * c;
+            rs[c] = j < m ? s_row[b][j] * rp : 0.0;  // pivot row / pivot
+        }
+        // every entry: w_ij - c_i (row_j / p); then the owners of column k and row k overwrite
+        // theirs (-c_i / p, row_j / p, 1 / p) -- a warp-uniform branch for the row, one lane for the column
+#pragma unroll
+        for (int r = 0; r < kGjR; ++r) {
+            const int i = ty + 16 * r;
+            const double ci = i < m ? s_col[b][i] : 0.0;
+#pragma unroll
+            for (int c = 0; c < kGjC; ++c) w[r][c] = fma(-ci, rs[c], w[r][c]);
+        }
+        if (tx == (k & 31)) {
+#pragma unroll
+            for (int c = 0; c < kGjC; ++c)
+                if (c == kc)
+#pragma unroll
+                    for (int r = 0; r < kGjR; ++r) {
+                        const int i = ty + 16 * r;
+                        w[r][c] = i < m ? -s_col[b][i] * rp : 0.0;
+                    }
+        }
+        if (ty == (k & 15)) {
+#pragma unroll
+            for (int r = 0; r < kGjR; ++r)
+                if (r == kr)
+#pragma unroll
+                    for (int c = 0; c < kGjC; ++c) w[r][c] = (tx + 32 * c == k) ? rp : rs[c];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && s_bad) atomicAdd(bad, 1);
+#pragma unroll
+    for (int r = 0; r < kGjR; ++r)
+#pragma unroll
+        for (int c = 0; c < kGjC; ++c) {
+            const int i = ty + 16 * r, j = tx + 32 * c;
+            if (i < m && j < m) P[(size_t)i * m + j] = w[r][c];
+        }
+}
+
 // P = A^-1 for an SPD A (m <= 160) in one 1024-thread CTA: Cholesky in
 // shared memory (2-D trailing update, two barriers per column), then each warp
 // solves L L^T x = e_c for its columns with the vector held in registers
@@ -949,6 +1044,10 @@ void launch_cholesky(const double* A, int m, double* L, int* bad, cudaStream_t s
 }
 
 bool launch_chol_inverse(const double* A, int m, double* P, int* bad, cudaStream_t st) {
+    if (m <= kGjMax) {
+        HSC_COUNTED(gj_inverse_reg_kernel<<<1, 512, 0, st>>>(A, m, P, bad));
+        return true;
+    }
     const size_t bytes = sizeof(double) * ((size_t)m * (m + 1) + 2 * (size_t)m);
     if (bytes > 200 * 1024) return false;
     cudaFuncSetAttribute(gj_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);

@@ -61,7 +61,7 @@ class HSCOptions:
     spin_limit: int = 20_000_000
     check_residual: bool = True
     trace_iterations: int = 0
-    resident: bool = False                 # BSR slices + vector windows in shared memory when they fit
+    resident: bool = True                  # BSR slices + vector windows in shared memory when they fit
     fuse_update: bool = False              # resident mode: one grid barrier fewer per iteration
     aca_cluster: bool = True               # cluster ACA when the coupling fits; False: the grid kernel
 
