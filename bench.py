@@ -37,10 +37,12 @@ sys.path.insert(0, HERE)
 METRIC = "HSC solves/s & PCG iters to rel-res 1e-6: learned/FP32 vs plain FP64, 1 B200"
 UNIT = "solves/s"
 TARGET = 1e-6
-# DRAM bytes per PCG iteration on the vehicle workload from an ncu capture of
-# the FP64 order-2 solve (profiles/pcg_kernel_vehicle.md: 24.23 MB read + 7.86 MB
-# written over 204 iterations)
-NCU_TRAFFIC_PER_ITER = (24.23e6 + 7.86e6) / 204
+# DRAM bytes per PCG iteration on the vehicle workload, per mode, from ncu
+# captures of one order-2 solve on the default (shared-memory-resident) path
+# (profiles/pcg_kernel_vehicle.md): FP64 24.84 MB read + 1.11 MB written over
+# 204 iterations, FP32 32.17 MB + 0.51 MB over 245.  The learned modes run
+# the same kernel with eight Schur-basis terms and have no capture of their own.
+NCU_TRAFFIC_PER_ITER = {"fp64": (24.84e6 + 1.11e6) / 204, "fp32": (32.17e6 + 0.51e6) / 245}
 
 
 def parse():
@@ -332,7 +334,7 @@ def run_gpu(args):
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = F["pcg_bytes_per_iteration"] * F["pcg_iterations"] / (F["pcg_ms"] / 1000.0) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": (NCU_TRAFFIC_PER_ITER * F["pcg_iterations"]) if NCU_TRAFFIC_PER_ITER else None,
+                "traffic": (NCU_TRAFFIC_PER_ITER[flag] * F["pcg_iterations"]) if flag in NCU_TRAFFIC_PER_ITER else None,
                 "kernel": "hsc::pcg_kernel (persistent Schur PCG)",
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s",
                 "note": "the vehicle matrix (~20 MB FP64) stays L2-resident across iterations, so the "
