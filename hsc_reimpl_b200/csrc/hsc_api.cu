@@ -615,9 +615,16 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
     if (ns > G) return fail(ctx, HSC_ERR_INVALID, "more systems than co-resident CTAs");
     // Work of a row range in block units: its blocks, one per row (vector updates), and for each node
     // with coupled dofs the low-rank products of every preconditioner term (V^T t partial sums and the
-    // V c correction: 2 x 3 dofs x kmax multiply-adds, a block being 9), scaled by 0.5: the weight that
-    // measured fastest on the vehicle system among 0, 0.5, 1, 2, 4 (HSC_ACTIVE_ROW_WEIGHT overrides it).
-    double act_w = 0.5;
+    // V c correction: 2 x 3 dofs x kmax multiply-adds, a block being 9), scaled by a weight that depends
+    // on where the CTAs' Vt blocks will live: 0.5 when they fit shared memory (an average block of at most
+    // 48 KB; the fastest of 0, 0.5, 1, 2, 4 on the vehicle system), 2 when they stream from L2 (the
+    // fastest of 0, 0.5, 2, 3, 4, 8 on the 1 M-tet torus).  HSC_ACTIVE_ROW_WEIGHT overrides it.
+    double vt_doubles = 0.0;
+    for (int s = 0; s < ns; ++s) {
+        const System& S = ctx->sys[idx[s]];
+        vt_doubles += (double)S.a * std::max(0, S.kmax);
+    }
+    double act_w = vt_doubles * sizeof(double) / G <= 48.0 * 1024 ? 0.5 : 2.0;
     if (const char* e = std::getenv("HSC_ACTIVE_ROW_WEIGHT")) act_w = std::max(0.0, std::atof(e));
     std::vector<std::vector<long long>> wpre(ns);  // per system: weighted prefix over rows
     long long tot = 0;
