@@ -96,7 +96,7 @@ struct System {
     DevBuf r2;
     DevBuf v64, vf32, vbf16, dinv, A, E, R0, R1, U, V, hist, P, Ptmp, T, term, Binv, L, W, C, Lc, dpiv, vt64, vtmt,
         cvec, tt, ttx, bq, bf, x, r, z, p0, p1, y, t0, t1, node_nz, xq, ypad, yq, work, cg, scal, dact, pact, yact,
-        zpart, tpart, lcol;
+        zpart, tpart, lcol, rowpart;
     DevBuf dvec[4];           // contiguous-N scratch for refinement
     double h_last[kPrev] = {};   // record of the last solve: 1, lanczos min, max, iterations, q(0)
     double h_prevrec[kPrev] = {};// record the features of the current solve see
@@ -373,6 +373,7 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
     GROW(S.t0, vt_bytes(P) * n4);
     GROW(S.t1, vt_bytes(P) * n4);
     GROW(S.node_nz, sizeof(int) * std::max(1, S.a / 3));
+    GROW(S.rowpart, sizeof(double) * std::max(1, S.qm) * abd_row_chunks(S.a));
     GROW(S.xq, sizeof(double) * qm);
     GROW(S.ypad, sizeof(double) * n4);
     GROW(S.yq, sizeof(double) * qm);
@@ -582,6 +583,7 @@ void back_substitute(System& S, const double* b, double* x_out, bool residual, c
         FullSpmv f{S.rowptr.as<int>(), S.colidx.as<int>(), S.v64.as<double>(), S.nnz, S.n, S.A.as<double>(),
                    S.E.as<double>(), S.qm, S.a, S.act.as<int>(), S.xq.as<double>(), S.x.as<double>(),
                    S.ypad.as<double>(), S.yq.as<double>()};
+        f.rowpart = S.rowpart.as<double>();
         launch_full_spmv(f, st);
     }
 }
@@ -594,13 +596,15 @@ void residual_dots(hsc_ctx* ctx, System& S, cudaStream_t st) {
 }
 
 // y = H x for contiguous N vectors
-void full_spmv_contig(System& S, const double* x, double* y, cudaStream_t st) {
+void full_spmv_contig(System& S, const double* x, double* y, cudaStream_t st, const double* bcoo_values = nullptr) {
     double* xpad = S.dvec[3].as<double>();
     launch_gather_x(x, S.n, S.fo, xpad, st);
     if (S.qm) cudaMemcpyAsync(S.xq.p, x + S.qo, sizeof(double) * S.qm, cudaMemcpyDeviceToDevice, st);
     FullSpmv f{S.rowptr.as<int>(), S.colidx.as<int>(), S.v64.as<double>(), S.nnz, S.n, S.A.as<double>(),
                S.E.as<double>(), S.qm, S.a, S.act.as<int>(), S.xq.as<double>(), xpad, S.ypad.as<double>(),
                S.yq.as<double>()};
+    f.rowpart = S.rowpart.as<double>();
+    if (bcoo_values) { f.src = S.src.as<int>(); f.bcoo_values = bcoo_values; }
     launch_full_spmv(f, st);
     launch_scatter_y(S.ypad.as<double>(), S.n, S.fo, S.yq.as<double>(), S.qm, S.qo, y, st);
 }
@@ -1510,11 +1514,10 @@ int hsc_spmv(hsc_ctx* ctx, const hsc_bcoo3* A, const hsc_dof_layout* layout, con
     if (rc) return rc;
     System& S = ctx->sys[0];
     DevScal* ds = S.scal.as<DevScal>();
-    launch_fill_bsr(S.src.as<int>(), A->d_values, S.nnz, S.v64.as<double>(), nullptr, nullptr, st);
     launch_extract(S.qq.as<int>(), S.nqq, S.qf.as<int>(), S.nqf, A->d_values, S.qm, S.a, S.A.as<double>(),
                    S.E.as<double>(), S.node_nz.as<int>(), st);
     (void)ds;
-    full_spmv_contig(S, d_x, d_y, st);
+    full_spmv_contig(S, d_x, d_y, st, A->d_values);  // FEM blocks straight from the BCOO: no BSR refill
     CK(cudaStreamSynchronize(st));
     if (re) ctx->part_key_gen = -1;
     return HSC_OK;

@@ -841,14 +841,86 @@ __global__ void bsr_spmv64_kernel(const int* rowptr, const int* colidx, const do
     }
 }
 
+// The same product read straight from the caller's one-triangle BCOO through
+// the row-owner plan (src = 2 t + transposed), for a single SpMV with fresh
+// values: no refill of the BSR planes, each block read once per direction.
+__global__ void bcoo_row_spmv_kernel(const int* rowptr, const int* colidx, const int* src, const double* values, int n,
+                                     const double* xpad, double* ypad) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = tid >> 2, sub = tid & 3;
+    double a0 = 0, a1 = 0, a2 = 0;
+    if (row < n) {
+        for (int k = rowptr[row] + sub; k < rowptr[row + 1]; k += 4) {
+            const int c = colidx[k];
+            const int packed = src[k];
+            const double* B = values + 9 * (size_t)(packed >> 1);  // B(r, c) at r + 3 c
+            const double x0 = xpad[4 * (size_t)c], x1 = xpad[4 * (size_t)c + 1], x2 = xpad[4 * (size_t)c + 2];
+            double b[9];
+#pragma unroll
+            for (int e = 0; e < 9; ++e) b[e] = B[e];
+            if (packed & 1) {  // the mirrored block: B^T
+                a0 += b[0] * x0 + b[1] * x1 + b[2] * x2;
+                a1 += b[3] * x0 + b[4] * x1 + b[5] * x2;
+                a2 += b[6] * x0 + b[7] * x1 + b[8] * x2;
+            } else {
+                a0 += b[0] * x0 + b[3] * x1 + b[6] * x2;
+                a1 += b[1] * x0 + b[4] * x1 + b[7] * x2;
+                a2 += b[2] * x0 + b[5] * x1 + b[8] * x2;
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 2; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    }
+    if (row < n && sub == 0) {
+        ypad[4 * (size_t)row] = a0;
+        ypad[4 * (size_t)row + 1] = a1;
+        ypad[4 * (size_t)row + 2] = a2;
+        ypad[4 * (size_t)row + 3] = 0.0;
+    }
+}
+
 // y_f[act_c] += sum_r E[r, c] xq[r]   (one thread per active column)
 __global__ void et_xq_kernel(const double* E, int qm, int a, const int* act, const double* xq, double* ypad) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= a) return;
     double s = 0.0;
+#pragma unroll 8
     for (int r = 0; r < qm; ++r) s += E[(size_t)r * a + c] * xq[r];
     const int dof = act[c];
     ypad[4 * (size_t)(dof / 3) + dof % 3] += s;
+}
+
+// yq = A xq + E x_f[act] in two passes: one warp per (ABD row, chunk of
+// kRowChunk coupled columns) writes a partial (chunk 0 also takes the A row),
+// then one thread per row sums its partials in chunk order -- enough warps to
+// stream a wide E (144 x 25,518 on the 1 M-tet torus), deterministic sums.
+__global__ void abd_rows_part_kernel(const double* A, const double* E, int qm, int a, const int* act,
+                                     const double* xq, const double* xpad, int nchunk, double* part) {
+    const int r = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    const int chunk = blockIdx.x;
+    if (r >= qm || chunk >= nchunk) return;
+    double s = 0.0;
+    if (chunk == 0)
+        for (int j = lane; j < qm; j += 32) s += A[(size_t)r * qm + j] * xq[j];
+    const int c1 = min(a, (chunk + 1) * kRowChunk);
+    for (int c = chunk * kRowChunk + lane; c < c1; c += 32) {
+        const int dof = act[c];
+        s += E[(size_t)r * a + c] * xpad[4 * (size_t)(dof / 3) + dof % 3];
+    }
+    s = wsum(s);
+    if (lane == 0) part[(size_t)r * nchunk + chunk] = s;
+}
+
+__global__ void abd_rows_sum_kernel(const double* part, int qm, int nchunk, double* yq) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= qm) return;
+    double s = 0.0;
+    for (int k = 0; k < nchunk; ++k) s += part[(size_t)r * nchunk + k];
+    yq[r] = s;
 }
 
 // yq = A xq + E x_f[act]   (one warp per ABD row)
@@ -1114,10 +1186,19 @@ void launch_gather_x(const double* x, int n, int fo, double* xpad, cudaStream_t 
 }
 
 void launch_full_spmv(const FullSpmv& f, cudaStream_t st) {
-    HSC_COUNTED(bsr_spmv64_kernel<<<blocks((long long)f.n * 4), 256, 0, st>>>(f.rowptr, f.colidx, f.v64, f.nnz, f.n, f.xpad,
-                                                                  f.ypad));
+    if (f.bcoo_values)
+        HSC_COUNTED(bcoo_row_spmv_kernel<<<blocks((long long)f.n * 4), 256, 0, st>>>(f.rowptr, f.colidx, f.src,
+                                                                                  f.bcoo_values, f.n, f.xpad, f.ypad));
+    else
+        HSC_COUNTED(bsr_spmv64_kernel<<<blocks((long long)f.n * 4), 256, 0, st>>>(f.rowptr, f.colidx, f.v64, f.nnz, f.n,
+                                                                               f.xpad, f.ypad));
     if (f.qm && f.a) HSC_COUNTED(et_xq_kernel<<<blocks(f.a), 256, 0, st>>>(f.E, f.qm, f.a, f.act, f.xq, f.ypad));
-    if (f.qm)
+    if (f.qm && f.rowpart) {
+        const int nchunk = abd_row_chunks(f.a);
+        HSC_COUNTED(abd_rows_part_kernel<<<dim3(nchunk, (f.qm + 7) / 8), 256, 0, st>>>(f.A, f.E, f.qm, f.a, f.act, f.xq,
+                                                                                      f.xpad, nchunk, f.rowpart));
+        HSC_COUNTED(abd_rows_sum_kernel<<<blocks(f.qm), 256, 0, st>>>(f.rowpart, f.qm, nchunk, f.yq));
+    } else if (f.qm)
         HSC_COUNTED(abd_rows_kernel<<<blocks((long long)f.qm * 32), 256, 0, st>>>(f.A, f.E, f.qm, f.a, f.act, f.xq, f.xpad,
                                                                       f.yq));
 }

@@ -70,6 +70,9 @@ struct FullSpmv {
     const double* xpad;    // node-padded FEM x
     double* ypad;          // node-padded FEM y
     double* yq;            // qm
+    double* rowpart = nullptr;            // qm x abd_row_chunks(a) partials of the ABD rows (null: one warp per row)
+    const int* src = nullptr;             // set: read the blocks from the BCOO values through the plan
+    const double* bcoo_values = nullptr;  // (column-major 3x3, one triangle) instead of the BSR planes
 };
 
 void launch_pattern_hash(const int* rows, const int* cols, long long nnzb, unsigned long long* out, cudaStream_t st);
@@ -103,6 +106,8 @@ void launch_backsub(const double* P, const double* W, int qm, int kmax, const in
                     const double* t, double* xq_out, double* xq_copy, cudaStream_t st);
 void launch_scatter_x(const double* xpad, int n, int fo, double* xout, cudaStream_t st);
 void launch_gather_x(const double* x, int n, int fo, double* xpad, cudaStream_t st);
+constexpr int kRowChunk = 1024;  // coupled columns per warp in the ABD rows of the full SpMV
+inline int abd_row_chunks(int a) { return a > 0 ? (a + kRowChunk - 1) / kRowChunk : 1; }
 void launch_full_spmv(const FullSpmv& f, cudaStream_t st);
 void launch_residual(const double* bf, const double* yf, const double* xf, int n, const double* bq, const double* yq,
                      const double* xq, int qm, double* part, int np, double* out, cudaStream_t st);
