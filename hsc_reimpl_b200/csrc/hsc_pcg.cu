@@ -36,6 +36,7 @@
 // r.z partials are fetched in one pass, the SpMV issues the column indices and
 // gathers of several blocks before using them, and each CTA keeps its block of
 // Vt (the rows of its own coupled dofs) in shared memory for the whole solve.
+#include "../../include/hsc_c_api.h"
 #include <type_traits>
 
 #include "hsc_check.cuh"
@@ -1215,3 +1216,56 @@ int pcg_blocks_per_sm(int precision, int tpr, size_t smem) {
 }
 
 }  // namespace hsc
+
+// ---------------------------------------------------------------------------
+// Self-test of the PCG's grid barrier failure path (failure detection without a
+// GPU fault): one cooperative launch in which CTA `absent` never arrives, so
+// barrier 0 cannot complete.  CTA 1 waits at most `first_limit` polls, gives
+// up, raises the abort flag and sets the counter's top bit; the other CTAs,
+// with a much larger limit, must then leave at once and report failure.  Every
+// wait is bounded by its poll limit.
+// ---------------------------------------------------------------------------
+namespace hsc {
+namespace {
+__global__ void barrier_selftest_kernel(GridBar* gb, int absent, long long first_limit, long long limit, int* status) {
+    if (threadIdx.x != 0) return;
+    if ((int)blockIdx.x == absent) { status[blockIdx.x] = 2; return; }
+    const long long lim = blockIdx.x == 1 ? first_limit : limit;
+    status[blockIdx.x] = grid_arrive_wait(gb, gridDim.x, lim, 0) ? 1 : 0;
+}
+}  // namespace
+}  // namespace hsc
+
+extern "C" int hsc_debug_barrier_selftest(int32_t ctas, int32_t absent, int64_t first_limit, int64_t limit,
+                                          int32_t* statuses, int32_t* abort_flag, int32_t* where) {
+    using namespace hsc;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return HSC_ERR_CUDA;
+    if (ctas < 2 || ctas > sms || !statuses || first_limit < 1 || limit < first_limit || limit > 100000000)
+        return HSC_ERR_INVALID;
+    GridBar* gb = nullptr;
+    int* st = nullptr;
+    if (cudaMalloc(&gb, sizeof(GridBar)) != cudaSuccess) return HSC_ERR_ALLOC;
+    if (cudaMalloc(&st, sizeof(int) * ctas) != cudaSuccess) { cudaFree(gb); return HSC_ERR_ALLOC; }
+    int rc = HSC_OK;
+    GridBar h{};
+    if (cudaMemset(gb, 0, sizeof(GridBar)) != cudaSuccess || cudaMemset(st, 0xff, sizeof(int) * ctas) != cudaSuccess) {
+        rc = HSC_ERR_CUDA;
+    } else {
+        long long fl = first_limit, l = limit;
+        int ab = absent;
+        void* args[] = {&gb, &ab, &fl, &l, &st};
+        count_launch();
+        if (cudaLaunchCooperativeKernel((void*)barrier_selftest_kernel, dim3(ctas), dim3(32), args, 0, 0) != cudaSuccess ||
+            cudaDeviceSynchronize() != cudaSuccess ||
+            cudaMemcpy(statuses, st, sizeof(int) * ctas, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(&h, gb, sizeof(GridBar), cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = HSC_ERR_CUDA;
+    }
+    if (abort_flag) *abort_flag = h.abort;
+    if (where) *where = h.where;
+    cudaFree(gb);
+    cudaFree(st);
+    return rc;
+}

@@ -309,6 +309,13 @@ HSC_EXPORT long long hsc_kernel_launches(void);
 /* First failed index guard of a self-checking build (-DHSC_CHECKED) as
  * (code, value) pairs for the ACA, PCG and setup kernels; zeros otherwise. */
 HSC_EXPORT int hsc_debug_checks(long long* out6);
+/* Self-test of the PCG grid barrier's failure path, with no GPU fault: one cooperative launch of `ctas`
+ * CTAs (2..SM count) where CTA `absent` never arrives (-1: every CTA arrives); CTA 1 polls at most
+ * `first_limit` times and the others at most `limit` times.  statuses[c] = 1 barrier passed, 0 left with
+ * failure, 2 absent; *abort_flag / *where are the barrier's abort flag and the epoch that gave up.
+ * (No reference counterpart: it checks this library's bounded waits.) */
+HSC_EXPORT int hsc_debug_barrier_selftest(int32_t ctas, int32_t absent, int64_t first_limit, int64_t limit,
+                                          int32_t* statuses, int32_t* abort_flag, int32_t* where);
 
 #ifdef __cplusplus
 }
