@@ -329,6 +329,9 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
     __shared__ double s_w[kWarps][2];
     __shared__ double s_bc[4];
     __shared__ int s_ok;
+    // this CTA's share of the tt_j = (Vt^T p)_j recurrence: columns j = lcta + ncta * q, their
+    // partial-sum reads issued at the loop top by the warps idle there, their tt and d kept here
+    __shared__ double s_zsum[kMaxRank], s_ttown[kMaxRank], s_dpown[kMaxRank];
     extern __shared__ __align__(16) double smem[];
 
     const int cta = blockIdx.x;
@@ -347,6 +350,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
     const bool leader_cta = (cta == cb);
     const int n = S.n, nnz = S.nnz, a = S.a;
     const int rank = *S.rank;
+    const int tt_own = rank > lcta ? (rank - lcta + ncta - 1) / ncta : 0;  // columns this CTA reduces
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int gwarp = lcta * kWarps + warp, nwarp = ncta * kWarps;
     const double omega = prm.omega;
@@ -753,6 +757,10 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
 
     // ---------------- prologue: r = rhs, x = 0, z = M r ----------------
     {
+        for (int q = threadIdx.x; q < tt_own; q += kThreads) {
+            s_ttown[q] = 0.0;
+            s_dpown[q] = __ldg(S.dpiv + lcta + (size_t)ncta * q);
+        }
         double acc_rr = 0.0, acc_rz = 0.0;
         for (int row = rb + threadIdx.x; row < re; row += kThreads) {
             double r0, r1, r2;
@@ -790,6 +798,14 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
             double srr, srz;
             warp_sum_parts(prm.part_rr, prm.part_rz, cb, ce, srr, srz);
             if (lane == 0) { s_bc[0] = srr; s_bc[1] = srz; }
+        } else {
+            // the other warps read this CTA's columns of the per-CTA Vt^T z partials (final since the
+            // preconditioner's barrier) in the same round trip; used by phase A of a normal slot
+            for (int q = warp - 1; q < tt_own; q += kWarps - 1) {
+                double sz, unused;
+                warp_sum_parts(S.zpart + (size_t)(lcta + ncta * q) * ncta, nullptr, 0, ncta, sz, unused);
+                if (lane == 0) s_zsum[q] = sz;
+            }
         }
         mark(14);
         __syncthreads();
@@ -914,15 +930,12 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
                 }
                 __syncthreads();
                 mark(10);
-                // tt_j = (Vt^T z)_j + beta tt_j from the per-CTA partials of Vt^T z
-                for (int j = gwarp; j < rank; j += nwarp) {
-                    double sz, unused;
-                    warp_sum_parts(S.zpart + (size_t)j * ncta, nullptr, 0, ncta, sz, unused);
-                    if (lane == 0) {
-                        const double t = sz + bd * S.tt[j];
-                        S.tt[j] = t;
-                        acc -= __ldg(S.dpiv + j) * t * t;
-                    }
+                // tt_j = (Vt^T z)_j + beta tt_j for this CTA's columns (sums read at the loop top)
+                for (int q = threadIdx.x; q < tt_own; q += kThreads) {
+                    const double t = s_zsum[q] + bd * s_ttown[q];
+                    s_ttown[q] = t;
+                    S.tt[lcta + (size_t)ncta * q] = t;
+                    acc -= s_dpown[q] * t * t;
                 }
             } else if (slot == kReplace) {
                 // r = rhs - D x in FP64 (the assembled matrix, not the bulk precision)
