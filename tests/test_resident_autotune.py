@@ -98,3 +98,22 @@ def test_autotuner_picks_a_candidate_that_meets_the_target(api, torch):
     assert all(r["max_rank"] == 64 for r in ok) and len(ok) == 2, table
     fastest = min(ok, key=lambda r: r["ms"])
     assert (best.threads_per_row, best.max_rank) == (fastest["threads_per_row"], fastest["max_rank"])
+
+
+@pytest.mark.parametrize("resident", [False, True])
+def test_partition_weights_agree(api, torch, vehicle_system, monkeypatch, resident):
+    """The CTA row partition weights each coupled node by its low-rank work; the weight moves row
+    boundaries and so the reduction order only: every weight gives the same solve to its tolerance."""
+    ds = api.DeviceSystem.from_system(vehicle_system)
+    outs = {}
+    for w in ("0", "0.5", "2", "8"):
+        monkeypatch.setenv("HSC_ACTIVE_ROW_WEIGHT", w)
+        ctx = api.HSCContext(api.HSCOptions(resident=resident))
+        x, st = ctx.solve(ds)
+        assert st["status"] == 0 and st["full_relative_residual"] <= 1e-6, (w, st)
+        outs[w] = (x.cpu().numpy(), st["pcg_iterations"])
+        ctx.close()
+    x0, it0 = outs["0"]
+    for w, (x, it) in outs.items():
+        assert abs(it - it0) <= 2, (w, it, it0)
+        assert np.linalg.norm(x - x0) <= 1e-5 * np.linalg.norm(x0), w
