@@ -112,8 +112,8 @@ typedef struct hsc_options {
     int32_t trace_iterations;    /* > 0: record per-CTA SM clocks at the PCG phase boundaries of the
                                     first iterations (hsc_get_trace) */
     int32_t resident;            /* 1 (default): each PCG CTA keeps its BSR slice, vector window and own-row
-                                    vectors in shared memory when they fit (vehicle system: 6 % less time per
-                                    iteration in FP64, 15 % in FP32); 0: stream them from L2 */
+                                    vectors in shared memory when they fit (vehicle system: 10-15 % less time
+                                    per iteration in FP32, FP64 within 1 %); 0: stream them from L2 */
     int32_t fuse_update;         /* resident mode, FEM-basis polynomial of 2+ terms: 1 folds the x/r update
                                     into the first preconditioner phase (each CTA forms
                                     t0 = w Dd^-1 (r - alpha S p) over its own window), one grid barrier
