@@ -142,6 +142,8 @@ struct hsc_ctx {
     std::vector<const void*> gkey;
     DevScal* h_pinned = nullptr;
     size_t h_pinned_n = 0;
+    unsigned char* h_stage = nullptr;  // pinned staging of the per-solve reads (one synchronisation)
+    size_t h_stage_bytes = 0;
 };
 
 namespace {
@@ -999,9 +1001,12 @@ void lanczos_extremes(const double* coef, int m, double& lo, double& hi) {
         }
         return c;
     };
+    // bisection to a relative width of 1e-12 (about 40 Sturm counts from the Gershgorin bounds, not a
+    // fixed 200: this runs on the host after every solve, before the call returns)
     auto kth = [&](int k) {
         double a = gl, b = gu;
         for (int it = 0; it < 200; ++it) {
+            if (b - a <= 1e-12 * std::max(std::fabs(a), std::fabs(b)) || !(b > a)) break;
             const double mid = 0.5 * (a + b);
             if (count_below(mid) > k) b = mid; else a = mid;
         }
@@ -1091,23 +1096,51 @@ int read_scalars(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st, int
         CK(cudaMallocHost((void**)&ctx->h_pinned, sizeof(DevScal) * idx.size()));
         ctx->h_pinned_n = idx.size();
     }
+    // everything else of this read goes through one pinned staging buffer as well: copies into
+    // pageable memory would each wait for their own round trip
+    size_t need = 2 * sizeof(GridBar);
+    for (size_t s = 0; s < idx.size(); ++s) {
+        const System& S = ctx->sys[idx[s]];
+        need += sizeof(double) * 2 * kMaxCoef + ((sizeof(int) * (S.a / 3) + 7) & ~(size_t)7);
+    }
+    if (ctx->h_stage_bytes < need) {
+        if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+        ctx->h_stage = nullptr;
+        ctx->h_stage_bytes = 0;
+        CK(cudaMallocHost((void**)&ctx->h_stage, need));
+        ctx->h_stage_bytes = need;
+    }
     for (size_t s = 0; s < idx.size(); ++s)
         CK(cudaMemcpyAsync(ctx->h_pinned + s, ctx->sys[idx[s]].scal.p, sizeof(DevScal), cudaMemcpyDeviceToHost, st));
-    GridBar gb{}, ga{};
-    if (ctx->d_bar.p) CK(cudaMemcpyAsync(&gb, ctx->d_bar.p, sizeof(GridBar), cudaMemcpyDeviceToHost, st));
-    if (ctx->aca_bar.p) CK(cudaMemcpyAsync(&ga, ctx->aca_bar.p, sizeof(GridBar), cudaMemcpyDeviceToHost, st));
+    GridBar* gbs = reinterpret_cast<GridBar*>(ctx->h_stage);
+    gbs[0] = GridBar{};
+    gbs[1] = GridBar{};
+    if (ctx->d_bar.p) CK(cudaMemcpyAsync(&gbs[0], ctx->d_bar.p, sizeof(GridBar), cudaMemcpyDeviceToHost, st));
+    if (ctx->aca_bar.p) CK(cudaMemcpyAsync(&gbs[1], ctx->aca_bar.p, sizeof(GridBar), cudaMemcpyDeviceToHost, st));
+    size_t off = 2 * sizeof(GridBar);
+    std::vector<size_t> offs(idx.size());
     for (size_t s = 0; s < idx.size(); ++s) {
         System& S = ctx->sys[idx[s]];
-        S.h_node_nz.resize(S.a / 3);
-        if (S.a) CK(cudaMemcpyAsync(S.h_node_nz.data(), S.node_nz.p, sizeof(int) * (S.a / 3), cudaMemcpyDeviceToHost, st));
-        if (S.cg.p) CK(cudaMemcpyAsync(S.h_cg, S.cg.p, sizeof(double) * 2 * kMaxCoef, cudaMemcpyDeviceToHost, st));
+        offs[s] = off;
+        if (S.cg.p)
+            CK(cudaMemcpyAsync(ctx->h_stage + off, S.cg.p, sizeof(double) * 2 * kMaxCoef, cudaMemcpyDeviceToHost, st));
+        off += sizeof(double) * 2 * kMaxCoef;
+        if (S.a)
+            CK(cudaMemcpyAsync(ctx->h_stage + off, S.node_nz.p, sizeof(int) * (S.a / 3), cudaMemcpyDeviceToHost, st));
+        off += (sizeof(int) * (S.a / 3) + 7) & ~(size_t)7;
     }
     CK(cudaStreamSynchronize(st));
-    grid_abort = gb.abort | ga.abort;
+    grid_abort = gbs[0].abort | gbs[1].abort;
     for (size_t s = 0; s < idx.size(); ++s) {
-        const double d7 = ctx->sys[idx[s]].h_scal.pcg[7];
-        ctx->sys[idx[s]].h_scal = ctx->h_pinned[s];
-        ctx->sys[idx[s]].h_scal.pcg[7] = d7;
+        System& S = ctx->sys[idx[s]];
+        const double d7 = S.h_scal.pcg[7];
+        S.h_scal = ctx->h_pinned[s];
+        S.h_scal.pcg[7] = d7;
+        if (S.cg.p) std::memcpy(S.h_cg, ctx->h_stage + offs[s], sizeof(double) * 2 * kMaxCoef);
+        S.h_node_nz.resize(S.a / 3);
+        if (S.a)
+            std::memcpy(S.h_node_nz.data(), ctx->h_stage + offs[s] + sizeof(double) * 2 * kMaxCoef,
+                        sizeof(int) * (S.a / 3));
     }
     return HSC_OK;
 }
@@ -1238,6 +1271,7 @@ void hsc_destroy(hsc_ctx* ctx) {
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
     delete ctx;
 }
 
