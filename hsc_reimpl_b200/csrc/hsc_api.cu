@@ -990,30 +990,38 @@ void lanczos_extremes(const double* coef, int m, double& lo, double& hi) {
         gl = std::min(gl, d[i] - rad);
         gu = std::max(gu, d[i] + rad);
     }
-    auto count_below = [&](double x) {
-        int c = 0;
-        double q = d[0] - x;
-        if (q < 0) ++c;
-        for (int i = 1; i < n; ++i) {
-            if (q == 0) q = 1e-300;
-            q = d[i] - x - e[i - 1] * e[i - 1] / q;
-            if (q < 0) ++c;
+    // both extremes at once, each bracket quartered per pass: six independent Sturm counts share one
+    // walk down the diagonal (their divisions overlap), to a relative width of 1e-12
+    std::vector<double> e2(std::max(1, n - 1));
+    for (int i = 0; i + 1 < n; ++i) e2[i] = e[i] * e[i];
+    double a[2] = {gl, gl}, b[2] = {gu, gu};
+    const int kk[2] = {0, n - 1};
+    for (int it = 0; it < 100; ++it) {
+        bool done[2];
+        for (int t = 0; t < 2; ++t) done[t] = !(b[t] - a[t] > 1e-12 * std::max(std::fabs(a[t]), std::fabs(b[t])));
+        if (done[0] && done[1]) break;
+        double x[6], q[6];
+        int c[6];
+        for (int t = 0; t < 2; ++t)
+            for (int p = 0; p < 3; ++p) x[3 * t + p] = a[t] + (b[t] - a[t]) * 0.25 * (p + 1);
+        for (int j = 0; j < 6; ++j) { q[j] = d[0] - x[j]; c[j] = q[j] < 0; }
+        for (int i = 1; i < n; ++i)
+            for (int j = 0; j < 6; ++j) {
+                if (q[j] == 0) q[j] = 1e-300;
+                q[j] = d[i] - x[j] - e2[i - 1] / q[j];
+                c[j] += q[j] < 0;
+            }
+        for (int t = 0; t < 2; ++t) {
+            if (done[t]) continue;
+            const int k = kk[t];  // the bracket keeps the k-th eigenvalue: count(lower) <= k < count(upper)
+            if (c[3 * t] > k) b[t] = x[3 * t];
+            else if (c[3 * t + 1] > k) { a[t] = x[3 * t]; b[t] = x[3 * t + 1]; }
+            else if (c[3 * t + 2] > k) { a[t] = x[3 * t + 1]; b[t] = x[3 * t + 2]; }
+            else a[t] = x[3 * t + 2];
         }
-        return c;
-    };
-    // bisection to a relative width of 1e-12 (about 40 Sturm counts from the Gershgorin bounds, not a
-    // fixed 200: this runs on the host after every solve, before the call returns)
-    auto kth = [&](int k) {
-        double a = gl, b = gu;
-        for (int it = 0; it < 200; ++it) {
-            if (b - a <= 1e-12 * std::max(std::fabs(a), std::fabs(b)) || !(b > a)) break;
-            const double mid = 0.5 * (a + b);
-            if (count_below(mid) > k) b = mid; else a = mid;
-        }
-        return 0.5 * (a + b);
-    };
-    lo = kth(0);
-    hi = kth(n - 1);
+    }
+    lo = 0.5 * (a[0] + b[0]);
+    hi = 0.5 * (a[1] + b[1]);
 }
 
 void fill_stats(hsc_ctx* ctx, System& S, const DevScal& h, hsc_stats* out, bool residual, int refinement_steps,
