@@ -634,7 +634,11 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const PcgParams prm_ar
     // summed in the same order in every CTA
     auto sum_tparts = [&](const double* P) {
         constexpr int JW = 8;
-        for (int j0 = warp * JW; j0 < rank; j0 += kWarps * JW) {
+        // the warps take the column groups in an order rotated by the CTA, so the coupled CTAs do not
+        // all read the same partials at the same moment
+        const int ngroups = (rank + JW - 1) / JW;
+        for (int g = warp; g < ngroups; g += kWarps) {
+            const int j0 = ((g + aidx) % ngroups) * JW;
             double v[JW];
 #pragma unroll
             for (int q = 0; q < JW; ++q) v[q] = 0.0;
