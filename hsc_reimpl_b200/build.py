@@ -50,7 +50,7 @@ def build(force=False, verbose=False, checked=False):
         objs.append(str(o))
     if force or not lib.exists() or lib.stat().st_mtime < max(Path(o).stat().st_mtime for o in objs):
         _run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-cudart", "static",
-              "-o", str(lib), *objs])
+              "-o", str(lib), *objs, "-lpthread"])
     return lib
 
 

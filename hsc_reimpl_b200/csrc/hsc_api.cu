@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <unordered_set>
 #include <vector>
 
@@ -1487,6 +1488,27 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
             ctx->err = "refinement did not reach refine_target";
         }
     }
+    // Lanczos extremes of every system (host bisection, independent per system): a batch spreads
+    // them over a few host threads
+    std::vector<double> lz_lo(count, 0.0), lz_hi(count, 0.0);
+    {
+        auto lz = [&](int s0, int s1) {
+            for (int s = s0; s < s1; ++s) {
+                const System& S = ctx->sys[s];
+                const int m = std::min(kMaxCoef, std::max(0, (int)S.h_scal.pcg[0]));
+                lanczos_extremes(S.h_cg, m, lz_lo[s], lz_hi[s]);
+            }
+        };
+        const int nth = count >= 8 ? std::min(8, (int)std::max(1u, std::thread::hardware_concurrency())) : 1;
+        if (nth <= 1) {
+            lz(0, count);
+        } else {
+            std::vector<std::thread> pool;
+            for (int t = 1; t < nth; ++t) pool.emplace_back(lz, count * t / nth, count * (t + 1) / nth);
+            lz(0, count / nth);
+            for (auto& th : pool) th.join();
+        }
+    }
     for (int s = 0; s < count; ++s) {
         System& S = ctx->sys[s];
         std::string msg;
@@ -1504,8 +1526,7 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
         }
         // Lanczos extremes of this solve; they become the next solve's record
         const int m = std::min(kMaxCoef, std::max(0, (int)S.h_scal.pcg[0]));
-        double lo = 0, hi = 0;
-        lanczos_extremes(S.h_cg, m, lo, hi);
+        const double lo = lz_lo[s], hi = lz_hi[s];
         if (out) { out[s].lanczos_min = lo; out[s].lanczos_max = hi; }
         if (m > 0 && lo > 0) {
             S.h_last[0] = 1.0; S.h_last[1] = lo; S.h_last[2] = hi; S.h_last[3] = S.h_scal.pcg[0];
