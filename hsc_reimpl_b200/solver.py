@@ -57,7 +57,7 @@ class HSCOptions:
     refine_target: float = 0.0
     max_refinements: int = 20
     fallback_on_stall: bool = True
-    threads_per_row: int = 4
+    threads_per_row: int = 0               # SpMV tile width 2, 4 or 8; 0: 4 resident, 2 streaming
     spin_limit: int = 20_000_000
     check_residual: bool = True
     trace_iterations: int = 0

@@ -106,7 +106,8 @@ typedef struct hsc_options {
     int32_t fallback_on_stall;   /* polynomial / learned preconditioners: redo a single-system solve with plain
                                     Neumann (neumann_order) when PCG breaks down or hits max_iter */
     int32_t threads_per_row;     /* SpMV tile width: 2, 4 or 8 -> 1, 2 or 4 slices of 32 blocks loaded per
-                                    warp round trip (autotuned, default 4) */
+                                    warp round trip (autotuned); 0 (default): 4 on the shared-memory-resident
+                                    path, 2 when the slices stream from memory */
     int64_t spin_limit;          /* bound on every device-side barrier wait */
     int32_t check_residual;      /* 1: compute the full residual and enforce full_residual_limit */
     int32_t trace_iterations;    /* > 0: record per-CTA SM clocks at the PCG phase boundaries of the
