@@ -40,9 +40,9 @@ TARGET = 1e-6
 # DRAM bytes per PCG iteration on the vehicle workload, per mode, from ncu
 # captures of one order-2 solve on the default (shared-memory-resident) path
 # (profiles/pcg_kernel_vehicle.md): FP64 24.84 MB read + 1.11 MB written over
-# 204 iterations, FP32 32.17 MB + 0.51 MB over 245.  The learned modes run
+# 204 iterations, FP32 32.19 MB + 0.50 MB over 245.  The learned modes run
 # the same kernel with eight Schur-basis terms and have no capture of their own.
-NCU_TRAFFIC_PER_ITER = {"fp64": (24.84e6 + 1.11e6) / 204, "fp32": (32.17e6 + 0.51e6) / 245}
+NCU_TRAFFIC_PER_ITER = {"fp64": (24.84e6 + 1.11e6) / 204, "fp32": (32.19e6 + 0.50e6) / 245}
 
 
 def parse():
