@@ -38,8 +38,8 @@ METRIC = "HSC solves/s & PCG iters to rel-res 1e-6: learned/FP32 vs plain FP64, 
 UNIT = "solves/s"
 TARGET = 1e-6
 # DRAM bytes per PCG iteration on the vehicle workload, per mode, from ncu
-# captures of one order-2 solve on the default (shared-memory-resident) path
-# (profiles/pcg_kernel_vehicle.md): FP64 24.84 MB read + 1.11 MB written over
+# captures (dram__bytes_read.sum / dram__bytes_write.sum of pcg_kernel) of one
+# order-2 solve on the default (shared-memory-resident) path: FP64 24.84 MB read + 1.11 MB written over
 # 204 iterations, FP32 32.19 MB + 0.50 MB over 245.  The learned modes run
 # the same kernel with eight Schur-basis terms and have no capture of their own.
 NCU_TRAFFIC_PER_ITER = {"fp64": (24.84e6 + 1.11e6) / 204, "fp32": (32.19e6 + 0.50e6) / 245}
@@ -199,7 +199,7 @@ class ClockSampler:
 
 
 def pcg_bytes_per_iteration(ctx_stats, s, prec, order, schur=False):
-    """Algorithmic bytes one PCG iteration moves in this layout (see DESIGN.md):
+    """Algorithmic bytes one PCG iteration moves in this layout:
     `order` passes over the full BSR D (values + column indices + row pointers),
     the node-padded vector traffic of the phases and Dd^-1 planes; the low-rank
     terms (a x k FP64) are added explicitly."""
