@@ -53,23 +53,27 @@ def partition_systems(works, world_size):
 def solve_batch_distributed(systems, options=None, dist=None, use_graph=False, solve=None):
     """Solve this rank's share of `systems`; rank 0 returns every system's stats in input order
     (other ranks return None).  `solve(share) -> list of stats dicts` replaces the GPU solve
-    (tests run the host logic on CPU ranks)."""
+    (tests run the host logic on CPU ranks).  A share that raises is reported per system as
+    {"status": the HSCError code or -1, "error": ...}; a rank that leaves without joining the
+    gather makes the process group's timeout end rank 0's gather with an error."""
     ws = dist.get_world_size() if dist is not None else 1
     rank = dist.get_rank() if dist is not None else 0
     owner, _ = partition_systems([system_work(s) for s in systems], ws)
     mine = [i for i, o in enumerate(owner) if o == rank]
-    if solve is None:
-        from .solver import DeviceSystem, HSCContext
-        import torch
-        devs = [DeviceSystem.from_system(systems[i]) for i in mine]
-        ctx = HSCContext(options)
-        stream = torch.cuda.Stream()
-        with torch.cuda.stream(stream):
-            _, stats = ctx.solve_batch(devs, use_graph=use_graph, stream=stream, raise_on_error=False) if devs else (None, [])
-        stream.synchronize()
-        ctx.close()
-    else:
-        stats = solve([systems[i] for i in mine]) if mine else []
+    try:
+        if solve is None:
+            stats = _solve_share([systems[i] for i in mine], options, use_graph)
+        else:
+            stats = solve([systems[i] for i in mine]) if mine else []
+        if len(stats) != len(mine):
+            raise RuntimeError(f"{len(stats)} stats for {len(mine)} systems")
+    except Exception as e:
+        # A rank whose share failed on the host (bad input, a CUDA error raised by the runtime)
+        # still takes the gather below, so the other ranks never wait on it; its systems come
+        # back to rank 0 marked with the error.
+        code = getattr(e, "code", None)
+        stats = [{"status": code if isinstance(code, int) and code > 0 else -1,
+                  "error": f"{type(e).__name__}: {e}", "solved_on_rank": rank} for _ in mine]
     local = list(zip(mine, stats))
     if dist is None or ws == 1:
         gathered = [local]
@@ -83,6 +87,24 @@ def solve_batch_distributed(systems, options=None, dist=None, use_graph=False, s
         for i, st in part:
             out[i] = st
     return out
+
+
+def _solve_share(share, options, use_graph):
+    """One launch for this rank's systems on its own stream."""
+    if not share:
+        return []
+    from .solver import DeviceSystem, HSCContext
+    import torch
+    devs = [DeviceSystem.from_system(s) for s in share]
+    ctx = HSCContext(options)
+    try:
+        stream = torch.cuda.Stream()
+        with torch.cuda.stream(stream):
+            _, stats = ctx.solve_batch(devs, use_graph=use_graph, stream=stream, raise_on_error=False)
+        stream.synchronize()
+    finally:
+        ctx.close()
+    return stats
 
 
 def main(argv=None):
@@ -102,9 +124,11 @@ def main(argv=None):
     opts = HSCOptions(precision="fp32", residual_replacement=50, omega=0.6, max_rank=256)
     stats = solve_batch_distributed(systems, opts, dist if ws > 1 else None)
     if stats is not None:
-        print(json.dumps({"systems": len(stats), "ranks": ws,
-                          "ok": sum(s["status"] == 0 for s in stats),
-                          "max_full_relative_residual": max(s["full_relative_residual"] for s in stats)}))
+        ok = [s for s in stats if s["status"] == 0]
+        print(json.dumps({"systems": len(stats), "ranks": ws, "ok": len(ok),
+                          "errors": sorted({s["error"] for s in stats if "error" in s}),
+                          "max_full_relative_residual": max((s["full_relative_residual"] for s in ok),
+                                                            default=None)}))
     if ws > 1:
         dist.destroy_process_group()
 
