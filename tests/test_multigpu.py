@@ -147,4 +147,4 @@ def test_single_rank_batch_on_the_gpu():
     from hsc_reimpl_b200.systems import make_cube_system
     systems = [make_cube_system(seed=i, n=4 + i) for i in range(3)]
     stats = MG.solve_batch_distributed(systems, HSCOptions(omega=2 / 3))
-    assert len(stats) == 3 and all(s["status"] == 0 and s["full_relative_residual"] <= 1e-6 for s in stats)
+    assert len(stats) == 3 and all(s["status"] == 0 and s["full_relative_residual"] <= 1e-6 for s in stats), stats
