@@ -272,6 +272,37 @@ def test_nonpositive_fem_diagonal_is_reported(api, torch, cube_system):
     assert st["status"] == 2  # HSC_ERR_NONSPD
 
 
+@pytest.mark.parametrize("drop", [False, True])
+def test_uncoupled_system_solves_with_rank_zero(api, torch, cube_system, drop):
+    """No ABD-FEM coupling (linear_hsc.cu:216-247 finds no active dof: every
+    cross block is zero, or absent): rank 0, dq = A^-1 b_q, and the PCG over D
+    alone meets the residual target.  (x itself is not compared with a direct
+    solve: cond(D) of this cube is about 8e10.)"""
+    s = cube_system
+    qo, qm, fo, fn = s.layout
+    qb = (s.rows < (qo + qm) // 3) != (s.cols < (qo + qm) // 3)
+    assert qb.any()
+    rows, cols, vals = s.rows, s.cols, s.vals.copy()
+    if drop:
+        rows, cols, vals = rows[~qb], cols[~qb], vals[~qb]
+    else:
+        vals[qb] = 0.0
+    H = O.full_from_bcoo(rows, cols, vals, s.nblock)
+    assert O.extract(H, s.layout)[3].size == 0
+    cm = lambda v: torch.from_numpy(np.ascontiguousarray(np.transpose(v, (0, 2, 1)).reshape(-1, 9))).cuda()
+    ds = api.DeviceSystem(torch.from_numpy(rows.astype(np.int32)).cuda(), torch.from_numpy(cols.astype(np.int32)).cuda(),
+                          cm(vals), s.nblock, tuple(s.layout), torch.from_numpy(s.b).cuda())
+    ctx = api.HSCContext(api.HSCOptions(omega=2 / 3, abd_inverse="exact"))
+    x, st = ctx.solve(ds, raise_on_error=False)
+    assert st["status"] == 0, st
+    assert st["rank"] == 0 and st["active_fem_dofs"] == 0
+    xh = x.cpu().numpy()
+    A = H[qo:qo + qm, qo:qo + qm].toarray()
+    assert rel(xh[qo:qo + qm], np.linalg.solve(A, s.b[qo:qo + qm])) <= 1e-8
+    true_res = np.linalg.norm(H @ xh - s.b) / np.linalg.norm(s.b)
+    assert st["full_relative_residual"] <= 1e-5 and true_res <= 1e-5, (st, true_res)
+
+
 def test_iteration_cap_reports_noconv(api, torch, vehicle_system):
     ctx = api.HSCContext(api.HSCOptions(max_iter=5, tol=1e-12))
     x, st = ctx.solve(api.DeviceSystem.from_system(vehicle_system), raise_on_error=False)
