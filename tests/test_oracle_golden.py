@@ -119,3 +119,24 @@ def test_cube_matches_core(golden, cube_system):
     assert abs(st["pcg_iterations"] - int(g["exact/iterations"])) <= 1
     assert rel(core_order(x), g["exact/x"]) < 1e-5
     assert st["full_relative_residual"] < 1e-6
+
+
+@pytest.mark.parametrize("drop", [False, True])
+def test_uncoupled_cube_oracle(cube_system, drop):
+    """No active FEM dof (every coupling block zero, or none stored): ACA returns
+    rank 0 (core.py:22-50 with a zero E), dq = P b_q and the PCG runs over D alone."""
+    s = cube_system
+    qo, qm, fo, fn = s.layout
+    qb = (s.rows < (qo + qm) // 3) != (s.cols < (qo + qm) // 3)
+    rows, cols, vals = s.rows, s.cols, s.vals.copy()
+    if drop:
+        rows, cols, vals = rows[~qb], cols[~qb], vals[~qb]
+    else:
+        vals[qb] = 0.0
+    H = O.full_from_bcoo(rows, cols, vals, s.nblock)
+    x, st, orc = O.hsc_solve(H, s.layout, s.b, order=2, omega=2 / 3, tol=1e-6, max_iter=20000,
+                             abd_inverse="exact")
+    assert orc.rank == 0 and orc.active.size == 0 and orc.aca_error == 0.0
+    A = H[qo:qo + qm, qo:qo + qm].toarray()
+    assert rel(x[qo:qo + qm], np.linalg.solve(A, s.b[qo:qo + qm])) < 1e-8
+    assert st["converged"] and st["full_relative_residual"] < 1e-5
