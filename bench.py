@@ -1,11 +1,15 @@
 #!/usr/bin/env python
 """HSC solves/s on the vehicle-scale synthetic Newton system, one B200.
 
-Workload (the configuration the metric is quoted on): 7 Tet4 tire tori
-(78,120 tets, 19,530 nodes, 58,590 FEM dofs) and 12 affine bodies (144 dofs),
-E=1e10 carried / 1e6 ground tires, rim stitches and 5-15 % tread contacts,
-made by ``hsc_reimpl_b200.systems.make_vehicle_system`` from a seed.  A step
-is one full HSC solve through the public API (``HSCContext.solve`` ->
+Workload (the configuration the metric is quoted on): the vehicle scene's own
+Tet4 tire mesh placed seven times (78,197 tets, 24,836 nodes, 74,508 FEM dofs,
+149,513 stored upper FEM blocks) and 12 affine bodies (144 dofs), E=1e10
+mounted / 1e6 ground tires, each tire's 39 rim-connection nodes stitched to
+its rim body and 5-15 % tread contacts to the ground body, made by
+``hsc_reimpl_b200.systems.make_reference_vehicle_system`` from a seed.  On this
+mesh lambda_max(Dd^-1 D) = 3.89, so the Neumann step is omega = 0.5 (the
+reference's 0.7 makes the order-2 polynomial indefinite here: PCG breaks down
+at iteration 3).  A step is one full HSC solve through the public API (``HSCContext.solve`` ->
 ``hsc_solve``): BCOO->BSR fill, Dd^-1, coupling extraction, ACA, ABD inverse,
 reduced core, the persistent Schur PCG to a relative Schur residual of 1e-6,
 back-substitution and the FP64 full-system residual check, which every
@@ -15,7 +19,10 @@ Modes: ``fp64`` (plain FP64 Neumann order 2, the bar) and ``fp32`` (FP32
 bulk SpMV/Neumann with FP64 coupled-node blocks, FP64 residual replacement
 every 50 iterations, FP64-verified result).  ``value`` is the flagship mode
 (the fastest one that met the FP64-verified residual); every mode's numbers
-are in ``modes``.
+are in ``modes``.  ``other_workloads`` repeats fp64/fp32 on the structured
+annulus tires (``make_vehicle_system``).  ``e2e_repattern`` is ``e2e`` with a
+different sparsity pattern every step (two seeds alternate), so the pattern
+analysis is inside the timed region.
 
 Multi-GPU: replicas only (one independent system per rank, no data-path
 collective); value = solves of all ranks / max-over-ranks time.
@@ -55,6 +62,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-other", action="store_true", help="skip the annulus-tire workload lines")
     return ap.parse_args()
 
 
@@ -79,11 +87,20 @@ def replica_throughput(steps, ws, max_ms):
     return ws * steps / (max_ms / 1000.0)
 
 
+OMEGA = 0.5
+
+
+def make_workload(seed):
+    from hsc_reimpl_b200.systems import make_reference_vehicle_system
+    return make_reference_vehicle_system(seed=seed)
+
+
 def workload_config(s):
     m = s.meta
-    return {"workload": "vehicle_7tires_78k_tets", "tires": m["tires"], "tets": m["tets"], "nodes": m["nodes"],
+    return {"workload": "vehicle_tire_tet4_78k_tets", "mesh": "reproduction/vehicle_research/prepared/tire_tet4.npz "
+            "x 7 (scene_manifest placements)", "tires": m["tires"], "tets": m["tets"], "nodes": m["nodes"],
             "fem_dofs": s.layout[3], "abd_dofs": s.layout[1], "nnzb_one_triangle": m["nnzb"],
-            "neumann_order": 2, "omega": 0.7, "schur_tol": 1e-6, "full_residual_target": TARGET,
+            "neumann_order": 2, "omega": OMEGA, "schur_tol": 1e-6, "full_residual_target": TARGET,
             "abd_inverse": "exact FP64 Cholesky", "aca": "fixed rank cap 128, roundoff guard",
             "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas", "seed": m["seed"]}
 
@@ -93,9 +110,14 @@ def workload_config(s):
 # cpu_baseline leg are the only users of oracle/ in this file)
 # ----------------------------------------------------------------------------
 def cpu_solve_once(s):
+    """One FP64 solve with the oracle port, on one host thread: SciPy's CSR product is
+    single-threaded, and the BLAS of the small dense parts is held to one thread too, so
+    ``cores`` = 1 is the thread count that actually ran."""
+    from threadpoolctl import threadpool_limits
     from oracle import hsc_oracle as O
-    x, st, _ = O.hsc_solve(s.H, s.layout, s.b, order=2, omega=0.7, tol=1e-6, max_iter=20000,
-                           abd_inverse="exact", max_rank=128)
+    with threadpool_limits(limits=1):
+        x, st, _ = O.hsc_solve(s.H, s.layout, s.b, order=2, omega=OMEGA, tol=1e-6, max_iter=20000,
+                               abd_inverse="exact", max_rank=128)
     return x, st
 
 
@@ -109,18 +131,17 @@ def cpu_baseline(s, budget_s=12.0):
         times.append(time.perf_counter() - t)
         iters.append(st["pcg_iterations"])
     med = statistics.median(times)
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": 1.0 / med, "unit": UNIT, "cores": cores, "kind": "port",
+    return {"value": 1.0 / med, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"{len(times)} full FP64 solves of the vehicle system (median {med:.3f} s, "
-                      f"{iters[0]} PCG iterations) with the NumPy/SciPy oracle port, after 1 warm-up"}
+                      f"{iters[0]} PCG iterations) with the NumPy/SciPy oracle port on one host thread "
+                      f"({os.cpu_count()} cores on the host), after 1 warm-up"}
 
 
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    from hsc_reimpl_b200.systems import make_vehicle_system
-    s = make_vehicle_system(seed=args.seed)
+    s = make_workload(args.seed)
     for _ in range(args.warmup):
         cpu_solve_once(s)
     t = time.perf_counter()
@@ -130,14 +151,15 @@ def run_reference(args):
         full.append(st["full_relative_residual"])
     el = time.perf_counter() - t
     v = args.steps / el
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    cores = 1
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000 * el / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(s),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": f"{args.steps} full FP64 solves of the vehicle system with the "
-                                       "NumPy/SciPy restatement of the reference algorithm"},
+                                       "NumPy/SciPy restatement of the reference algorithm on one host thread "
+                                       "(SciPy's CSR product is single-threaded)"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "max_full_relative_residual": max(full)}
     print(json.dumps(line), flush=True)
@@ -198,75 +220,58 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def pcg_bytes_per_iteration(ctx_stats, s, prec, order, schur=False):
-    """Algorithmic bytes one PCG iteration moves in this layout:
-    `order` passes over the full BSR D (values + column indices + row pointers),
-    the node-padded vector traffic of the phases and Dd^-1 planes; the low-rank
-    terms (a x k FP64) are added explicitly."""
-    sv = 8 if prec == "fp64" else 4
-    sx = 8 if prec == "fp64" else 4
-    n = s.layout[3] // 3
+def survey_bytes_per_iteration(s, a, k, order, sb):
+    """Algorithmic bytes of one Schur PCG iteration at Neumann order r, the formula the
+    hot-path scope fixes: r SpMVs over the STORED (one-triangle) FEM blocks,
+    nnzb (9 s + 4) + 4 (n + 1) + 2 N s each; the low-rank apply (2 a k + k^2) s; the
+    vector passes: update 4N, Jacobi r (9n + 2N), axpby 6 (r - 1) N, three dots 2N each,
+    all times s (s = 8 FP64, 4 FP32)."""
     qo, qm, fo, fn = s.layout
+    n, N = fn // 3, fn
     fb0 = fo // 3
-    ff = (s.rows >= fb0) & (s.cols >= fb0)
-    nnz_d = 2 * int((ff & (s.rows != s.cols)).sum()) + int((ff & (s.rows == s.cols)).sum())
-    spmv = nnz_d * (9 * sv + 4) + 4 * (n + 1)
-    dinv = 9 * sv * n
-    vec = 4 * n  # node-padded entries
-    # phase A: gather z,p (2 reads of the vector per row-owner pass) + write p,y
-    a_vec = 4 * vec * sx
-    # phase B: read p,y,x(8),r(8) write x,r,t,z
-    b_vec = 2 * vec * sx + 4 * vec * 8 + 2 * vec * sx + dinv
-    # C phases: read t, z, write t, z (+ r on the last) + Dd^-1
-    c_vec = (order - 1) * (4 * vec * sx + dinv) + vec * 8
-    a = ctx_stats["active_fem_dofs"]
-    k = ctx_stats["rank"]
-    lowrank = 3 * a * k * 8
-    if schur:  # Schur-basis terms: Vt^T t partials and the low-rank correction in every C phase
-        lowrank += (order - 1) * 2 * a * k * 8
-    return order * spmv + a_vec + b_vec + c_vec + lowrank
+    nnzb = int(((s.rows >= fb0) & (s.cols >= fb0)).sum())
+    spmv = nnzb * (9 * sb + 4) + 4 * (n + 1) + 2 * N * sb
+    lowrank = (2 * a * k + k * k) * sb
+    vec = (4 * N + order * (9 * n + 2 * N) + 6 * (order - 1) * N + 3 * 2 * N) * sb
+    return order * spmv + lowrank + vec
 
 
-def run_gpu(args):
+def measure_l2_copy_gbs(dev):
+    """Copy bandwidth with both buffers L2-resident (2 x 24 MiB), read + write bytes over the
+    best of 5 bursts of 50 copies (CUDA events): the denominator of the L2 fraction."""
+    import torch
+    a = torch.empty(6 * 1024 * 1024, dtype=torch.float32, device=dev).normal_()
+    b = torch.empty_like(a)
+    for _ in range(20):
+        b.copy_(a)
+    best = 1e30
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(5):
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(50):
+            b.copy_(a)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 50)
+    return 2 * a.numel() * 4 / (best / 1000.0) / 1e9
+
+
+def time_modes(args, s, ds, ctx_holder, mode_opts, flush, dist, dev, lib, sample_clocks=True, steps=None):
     import numpy as np
     import torch
-    ws, rank, local = dist_env()
-    torch.cuda.set_device(local)
-    dist = None
-    if ws > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-    from hsc_reimpl_b200 import _lib
-    from hsc_reimpl_b200.solver import HSCContext, HSCOptions, DeviceSystem
-    from hsc_reimpl_b200.systems import make_vehicle_system
     import scipy.sparse.linalg as spla
-
-    s = make_vehicle_system(seed=args.seed + rank)
+    ws = dist.get_world_size() if dist is not None else 1
+    steps = steps or args.steps
     x_direct = spla.splu(s.H.tocsc()).solve(s.b)
-    dev = torch.device("cuda", local)
-    ds = DeviceSystem.from_system(s, device=dev)
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
-    lib = _lib.load()
-    modes = {}
-    mode_opts = {
-        "fp64": HSCOptions(neumann_order=2, omega=0.7, tol=1e-6, abd_inverse="exact", precision="fp64"),
-        "fp32": HSCOptions(neumann_order=2, omega=0.7, tol=1e-6, abd_inverse="exact", precision="fp32",
-                           residual_replacement=50),
-        "learned64": HSCOptions(learned=True, omega=0.7, tol=1e-6, abd_inverse="exact", precision="fp64"),
-        "learned32": HSCOptions(learned=True, omega=0.7, tol=1e-6, abd_inverse="exact", precision="fp32",
-                                residual_replacement=50),
-    }
-    from hsc_reimpl_b200 import learned as L
-    model = L.load_model()[0] if L.MODEL_PATH.exists() else None
-    want = [m for m in args.modes.split(",") if m in mode_opts and (model is not None or "learned" not in m)]
-    ctx = None
-    clocks = None
-    launches = None
-    for mi, mode in enumerate(want):
-        opt = mode_opts[mode]
-        ctx = HSCContext(opt) if ctx is None else ctx
-        if model is not None:
-            ctx.set_learned_model(model)
+    modes, clocks, launches = {}, None, None
+    for mi, (mode, opt) in enumerate(mode_opts.items()):
+        if ctx_holder[0] is None:
+            from hsc_reimpl_b200.solver import HSCContext
+            ctx_holder[0] = HSCContext(opt)
+        ctx = ctx_holder[0]
+        if ctx_holder[1] is not None:
+            ctx.set_learned_model(ctx_holder[1])
         ctx.set_options(opt)
         x = torch.empty_like(ds.b)
         for _ in range(args.warmup):
@@ -274,14 +279,14 @@ def run_gpu(args):
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
-        sampler = ClockSampler(local) if mi == 0 else None
+        sampler = ClockSampler(dev.index) if (mi == 0 and sample_clocks) else None
         if sampler:
             sampler.start()
         l0 = lib.hsc_kernel_launches()
         total_ms, pcg_ms, stats_all = 0.0, 0.0, []
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
-        for _ in range(args.steps):
+        for _ in range(steps):
             flush.zero_()
             torch.cuda.synchronize()
             ev0.record()
@@ -303,18 +308,18 @@ def run_gpu(args):
         xs = x.cpu().numpy()
         ok = all(t["status"] == 0 and t["full_relative_residual"] <= TARGET for t in stats_all)
         iters = last["pcg_iterations"]
-        terms = 8 if "learned" in mode else 2
-        bytes_iter = pcg_bytes_per_iteration(last, s, "fp64" if mode.endswith("64") else "fp32", terms,
-                                             schur="learned" in mode)
-        pcg_launch_ms = pcg_ms / args.steps
+        sb = 8 if mode.endswith("64") else 4
+        bytes_iter = survey_bytes_per_iteration(s, last["active_fem_dofs"], last["rank"], 2, sb)
+        pcg_launch_ms = pcg_ms / steps
         modes[mode] = {
-            "solves_per_s": replica_throughput(args.steps, ws, total_ms),
-            "ms_per_solve": total_ms / args.steps,
+            "solves_per_s": replica_throughput(steps, ws, total_ms),
+            "ms_per_solve": total_ms / steps,
             "pcg_iterations": iters,
             "full_relative_residual": max(t["full_relative_residual"] for t in stats_all),
             "schur_relative_residual": last["schur_relative_residual"],
             "error_vs_direct": float(np.linalg.norm(xs - x_direct) / np.linalg.norm(x_direct)),
             "met_target": ok, "status": last["status_name"] if "status_name" in last else last["status"],
+            "fallback": last.get("fallback", 0),
             "rank": last["rank"], "active_fem_dofs": last["active_fem_dofs"],
             "residual_replacements": last["residual_replacements"],
             "stage_ms": [round(v, 4) for v in last["stage_ms"]],
@@ -322,6 +327,106 @@ def run_gpu(args):
             "pcg_us_per_iteration": 1000.0 * pcg_launch_ms / max(1, iters),
             "pcg_bytes_per_iteration": bytes_iter,
         }
+    return modes, clocks, launches
+
+
+def timed_e2e(args, ctx, opt, systems_dev, flush, dist, dev, repattern):
+    """Solves through the public API from pinned host buffers: H2D of the matrix values and b
+    (and of rows/cols when ``repattern``: two systems of different sparsity alternate, so every
+    step pays the pattern analysis), the solve, D2H of x."""
+    import torch
+    from hsc_reimpl_b200.solver import DeviceSystem
+    ws = dist.get_world_size() if dist is not None else 1
+    ctx.set_options(opt)
+    host = []
+    for ds in systems_dev:
+        host.append(dict(rows=ds.rows.cpu().pin_memory(), cols=ds.cols.cpu().pin_memory(),
+                         vals=ds.values.cpu().pin_memory(), b=ds.b.cpu().pin_memory()))
+    nmax = max(h["rows"].numel() for h in host)
+    Nmax = max(h["b"].numel() for h in host)
+    # one index buffer pair per pattern: the solver keys its cached analysis on these pointers,
+    # so alternating patterns re-run the analysis up front every step
+    idx_d = [(torch.empty(nmax, dtype=torch.int32, device=dev), torch.empty(nmax, dtype=torch.int32, device=dev))
+             for _ in host]
+    vals_d = torch.empty((nmax, 9), dtype=torch.float64, device=dev)
+    b_d = torch.empty(Nmax, dtype=torch.float64, device=dev)
+    x_d = torch.empty(Nmax, dtype=torch.float64, device=dev)
+    x_h = torch.empty(Nmax, dtype=torch.float64).pin_memory()
+    h2d = d2h = 0
+    fails = 0
+
+    def step(i):
+        nonlocal h2d, d2h, fails
+        h = host[i % len(host)]
+        src = systems_dev[i % len(host)]
+        nz, N = h["rows"].numel(), h["b"].numel()
+        rows_d, cols_d = idx_d[i % len(host)]
+        if repattern:
+            rows_d[:nz].copy_(h["rows"], non_blocking=True)
+            cols_d[:nz].copy_(h["cols"], non_blocking=True)
+        vals_d[:nz].copy_(h["vals"], non_blocking=True)
+        b_d[:N].copy_(h["b"], non_blocking=True)
+        ds2 = DeviceSystem(rows_d[:nz] if repattern else src.rows, cols_d[:nz] if repattern else src.cols,
+                           vals_d[:nz], src.nblock, src.layout, b_d[:N])
+        _, st = ctx.solve(ds2, x=x_d[:N], raise_on_error=False)
+        fails += st["status"] != 0
+        x_h[:N].copy_(x_d[:N], non_blocking=True)
+        h2d = (2 * nz * 4 if repattern else 0) + nz * 72 + N * 8
+        d2h = N * 8
+
+    for i in range(max(args.warmup, 2)):
+        step(i)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    tot = 0.0
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    fails = 0
+    for i in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ev0.record()
+        step(i)
+        ev1.record()
+        torch.cuda.synchronize()
+        tot += ev0.elapsed_time(ev1)
+    tot = max_over_ranks(tot, dist, dev)
+    return {"value": replica_throughput(args.steps, ws, tot), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "failed_solves": int(fails)}
+
+
+def run_gpu(args):
+    import torch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    from hsc_reimpl_b200 import _lib
+    from hsc_reimpl_b200.solver import HSCOptions, DeviceSystem
+    from hsc_reimpl_b200.systems import make_vehicle_system
+
+    s = make_workload(args.seed + rank)
+    dev = torch.device("cuda", local)
+    ds = DeviceSystem.from_system(s, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
+    lib = _lib.load()
+    base = dict(neumann_order=2, omega=OMEGA, tol=1e-6, abd_inverse="exact")
+    mode_opts = {
+        "fp64": HSCOptions(precision="fp64", **base),
+        "fp32": HSCOptions(precision="fp32", residual_replacement=50, **base),
+        "learned64": HSCOptions(learned=True, omega=OMEGA, tol=1e-6, abd_inverse="exact", precision="fp64"),
+        "learned32": HSCOptions(learned=True, omega=OMEGA, tol=1e-6, abd_inverse="exact", precision="fp32",
+                                residual_replacement=50),
+    }
+    from hsc_reimpl_b200 import learned as L
+    model = L.load_model()[0] if L.MODEL_PATH.exists() else None
+    want = {m: o for m, o in mode_opts.items() if m in args.modes.split(",") and (model is not None or "learned" not in m)}
+    ctx_holder = [None, model]
+    modes, clocks, launches = time_modes(args, s, ds, ctx_holder, want, flush, dist, dev, lib)
+    ctx = ctx_holder[0]
     # flagship: fastest mode that met the FP64-verified target
     ok_modes = [m for m in modes if modes[m]["met_target"]]
     flag = max(ok_modes, key=lambda m: modes[m]["solves_per_s"]) if ok_modes else "fp64"
@@ -332,51 +437,40 @@ def run_gpu(args):
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    achieved = F["pcg_bytes_per_iteration"] * F["pcg_iterations"] / (F["pcg_ms"] / 1000.0) / 1e9
+    alg_bytes = F["pcg_bytes_per_iteration"] * F["pcg_iterations"]
+    achieved = alg_bytes / (F["pcg_ms"] / 1000.0) / 1e9
+    l2_gbs = measure_l2_copy_gbs(dev)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": (NCU_TRAFFIC_PER_ITER[flag] * F["pcg_iterations"]) if flag in NCU_TRAFFIC_PER_ITER else None,
-                "kernel": "hsc::pcg_kernel (persistent Schur PCG)",
+                "kernel": "hsc::pcg_kernel (persistent Schur PCG), one launch per solve",
+                "bytes": "per iteration: r SpMVs over the stored one-triangle FEM blocks "
+                         "nnzb (9 s + 4) + 4 (n + 1) + 2 N s, low-rank (2 a k + k^2) s, vector passes "
+                         "(4N + r (9n + 2N) + 6 (r - 1) N + 6N) s; times the launch's iterations",
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s",
-                "note": "the vehicle matrix (~20 MB FP64) stays L2-resident across iterations, so the "
-                        "achieved figure can exceed the HBM copy peak"}
-    # end-to-end through the public API with host buffers
-    e2e = None
+                "l2": {"achieved": achieved, "peak": l2_gbs, "unit": "GB/s", "frac": achieved / l2_gbs,
+                       "peak_source": "measured in this run: torch copy between two L2-resident 24 MiB buffers"},
+                "note": "the vehicle matrix stays in L2 and the CTAs' shared memory across iterations, so "
+                        "HBM is not the binding resource; the l2 entry puts the same bytes against L2"}
+    e2e = e2e_rep = None
     if not args.no_e2e:
-        opt = mode_opts[flag]
-        ctx.set_options(opt)
-        vals_h = ds.values.cpu().pin_memory()
-        b_h = ds.b.cpu().pin_memory()
-        x_h = torch.empty_like(b_h).pin_memory()
-        vals_d = torch.empty_like(ds.values)
-        b_d = torch.empty_like(ds.b)
-        x_d = torch.empty_like(ds.b)
-        ds2 = DeviceSystem(ds.rows, ds.cols, vals_d, ds.nblock, ds.layout, b_d)
-        for _ in range(args.warmup):
-            vals_d.copy_(vals_h, non_blocking=True)
-            b_d.copy_(b_h, non_blocking=True)
-            ctx.solve(ds2, x=x_d, raise_on_error=False)
-            x_h.copy_(x_d, non_blocking=True)
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-        tot = 0.0
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        for _ in range(args.steps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            ev0.record()
-            vals_d.copy_(vals_h, non_blocking=True)
-            b_d.copy_(b_h, non_blocking=True)
-            ctx.solve(ds2, x=x_d, raise_on_error=False)
-            x_h.copy_(x_d, non_blocking=True)
-            ev1.record()
-            torch.cuda.synchronize()
-            tot += ev0.elapsed_time(ev1)
-        tot = max_over_ranks(tot, dist, dev)
-        e2e = {"value": replica_throughput(args.steps, ws, tot), "unit": UNIT,
-               "h2d_bytes_per_step": int(vals_h.numel() * 8 + b_h.numel() * 8),
-               "d2h_bytes_per_step": int(x_h.numel() * 8), "mode": flag}
+        e2e = timed_e2e(args, ctx, want[flag], [ds], flush, dist, dev, repattern=False)
+        e2e["mode"] = flag
+        s_alt = make_workload(args.seed + rank + 1000)
+        ds_alt = DeviceSystem.from_system(s_alt, device=dev)
+        e2e_rep = timed_e2e(args, ctx, want[flag], [ds, ds_alt], flush, dist, dev, repattern=True)
+        e2e_rep["mode"] = flag
+        e2e_rep["note"] = "two seeds with different contact sets alternate; rows/cols copied every step"
+    other = None
+    if not args.no_other:
+        sa = make_vehicle_system(seed=args.seed + rank)
+        dsa = DeviceSystem.from_system(sa, device=dev)
+        oo = {"fp64": HSCOptions(precision="fp64", neumann_order=2, omega=0.7, tol=1e-6, abd_inverse="exact"),
+              "fp32": HSCOptions(precision="fp32", neumann_order=2, omega=0.7, tol=1e-6, abd_inverse="exact",
+                                 residual_replacement=50)}
+        om, _, _ = time_modes(args, sa, dsa, ctx_holder, oo, flush, dist, dev, lib, sample_clocks=False,
+                              steps=min(args.steps, 10))
+        other = {"vehicle_annulus_78k_tets": {"nodes": sa.meta["nodes"], "fem_dofs": sa.layout[3], "omega": 0.7,
+                                              "modes": om}}
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(s)
@@ -384,11 +478,11 @@ def run_gpu(args):
         line = {"metric": METRIC, "value": F["solves_per_s"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": F["ms_per_solve"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64" if flag == "fp64" else "f32",
-                "data": "synthetic (seeded vehicle-scale Newton system; no public dataset)",
+                "data": "synthetic (seeded Newton system on the vehicle scene's tire mesh; no public dataset)",
                 "config": workload_config(s), "mode": flag, "pcg_iterations": F["pcg_iterations"],
                 "full_relative_residual": F["full_relative_residual"], "error_vs_direct": F["error_vs_direct"],
-                "modes": modes, "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
-                "roofline": roofline, "cpu_baseline": cpu}
+                "modes": modes, "clocks": clocks, "e2e": e2e, "e2e_repattern": e2e_rep, "gpu_launches": launches,
+                "roofline": roofline, "cpu_baseline": cpu, "other_workloads": other}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -121,6 +121,8 @@ EXPORTS = {
     "hsc_debug_checks": (C.c_int, [C.POINTER(C.c_longlong)]),
     "hsc_debug_barrier_selftest": (C.c_int, [C.c_int32, C.c_int32, C.c_int64, C.c_int64, C.POINTER(C.c_int32),
                                              C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "hsc_debug_dmv_accumulate": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                           C.c_void_p]),
     "hsc_set_learned_model": (C.c_int, [C.c_void_p, C.c_void_p]),
     "hsc_get_features": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
     "hsc_get_poly_weights": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),

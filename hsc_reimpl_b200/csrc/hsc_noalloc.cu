@@ -20,8 +20,18 @@
 // the array and give wrong results: order them on one stream.  The first call
 // on a device looks up the array's device address (cudaGetSymbolAddress, with
 // that device current) and caches it; make that first call before any stream
-// capture begins.  The sums use FP64 atomics, so the last bits may differ from
-// hsc_spmv's fixed-order row sums.
+// capture begins.  Under lazy module loading (CUDA_MODULE_LOADING=LAZY, the
+// default since CUDA 12.2) the module that holds the array is loaded, and the
+// array created, by that first call too: "allocates nothing" holds from the
+// second call on a device.  The sums use FP64 atomics, so the last bits may
+// differ from hsc_spmv's fixed-order row sums.
+//
+// There is no analysis step to validate the triplets, so the product kernel
+// checks every block index against nblock itself: a triplet with a row or
+// column outside [0, nblock) is skipped (nothing is read or written for it)
+// and raises a second file-scope flag, which the call reads back after the
+// product and turns into HSC_ERR_INVALID.  Reading the flag waits for the
+// stream, so the call returns with y complete.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -34,21 +44,28 @@ constexpr long long kNoAllocMaxDofs = 1 << 20;
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) double g_noalloc_acc[kNoAllocMaxDofs];
+// triplets the last call skipped because a block index was out of range
+static __device__ int g_noalloc_bad;
 
 std::mutex g_mutex;
 double* g_acc_ptr[kMaxDevices] = {};
 
 __global__ void noalloc_zero_kernel(double* acc, long long n) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) g_noalloc_bad = 0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         acc[i] = 0.0;
 }
 
 // one thread per stored triplet: its block and, off the diagonal, its transpose
 __global__ void noalloc_spmv_kernel(const int* rows, const int* cols, const double* vals, long long nnzb,
-                                    const double* x, double* acc) {
+                                    int nblock, const double* x, double* acc) {
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= nnzb) return;
     const int r = rows[t], c = cols[t];
+    if ((unsigned)r >= (unsigned)nblock || (unsigned)c >= (unsigned)nblock) {
+        atomicAdd(&g_noalloc_bad, 1);
+        return;
+    }
     const double* B = vals + 9 * t;  // column-major: B(i, j) = B[i + 3 j]
     const double xc0 = x[3 * (long long)c], xc1 = x[3 * (long long)c + 1], xc2 = x[3 * (long long)c + 2];
     for (int i = 0; i < 3; ++i)
@@ -86,15 +103,26 @@ extern "C" int hsc_spmv_noalloc(const hsc_bcoo3* A, const double* d_x, double* d
     if ((A->nnzb > 0 && (!A->d_rows || !A->d_cols || !A->d_values))) return HSC_ERR_INVALID;
     const long long n = 3LL * A->nblock;
     if (n > kNoAllocMaxDofs) return HSC_ERR_INVALID;  // beyond the fixed scratch array
+    // an error left pending by the caller's own earlier work is not ours to
+    // report or to clear: refuse to launch behind it
+    if (cudaPeekAtLastError() != cudaSuccess) return HSC_ERR_CUDA;
     double* acc = nullptr;
     const int rc = scratch_address(&acc);
     if (rc != HSC_OK) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     const int grid_n = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
     noalloc_zero_kernel<<<grid_n, 256, 0, st>>>(acc, n);
-    if (A->nnzb > 0)
+    if (cudaGetLastError() != cudaSuccess) return HSC_ERR_CUDA;
+    if (A->nnzb > 0) {
         noalloc_spmv_kernel<<<(unsigned)((A->nnzb + 255) / 256), 256, 0, st>>>(A->d_rows, A->d_cols, A->d_values,
-                                                                              A->nnzb, d_x, acc);
+                                                                              A->nnzb, A->nblock, d_x, acc);
+        if (cudaGetLastError() != cudaSuccess) return HSC_ERR_CUDA;
+    }
     noalloc_copy_kernel<<<grid_n, 256, 0, st>>>(acc, d_y, n);
-    return cudaGetLastError() == cudaSuccess ? HSC_OK : HSC_ERR_CUDA;
+    if (cudaGetLastError() != cudaSuccess) return HSC_ERR_CUDA;
+    int bad = 0;
+    if (cudaMemcpyFromSymbolAsync(&bad, g_noalloc_bad, sizeof(int), 0, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return HSC_ERR_CUDA;
+    return bad ? HSC_ERR_INVALID : HSC_OK;
 }

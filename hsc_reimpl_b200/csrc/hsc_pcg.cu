@@ -1286,3 +1286,48 @@ extern "C" int hsc_debug_barrier_selftest(int32_t ctas, int32_t absent, int64_t 
     cudaFree(st);
     return rc;
 }
+
+// ---------------------------------------------------------------------------
+// z += omega * blockdiag(B) x at the authors' kernel shape (dmv_accumulate_kernel of
+// Guo-2026-HSC sparse_linear_solvers/conjugate_gradient_cuda.cuh, exercised by
+// reproduction/cuda_original.py with bs 3 and 12).  For bs = 3 the block product is
+// the PCG kernel's own dinv_apply over 9 planes d[e * nb + b]; bs = 12 applies the
+// same row-major arithmetic to 144 planes.  Test hook: no reference counterpart in
+// the solve itself.
+// ---------------------------------------------------------------------------
+namespace hsc {
+namespace {
+template <int BS>
+__global__ void dmv_accumulate_kernel(int nb, const double* planes, const double* x, double* z, double omega) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    if constexpr (BS == 3) {
+        double o0, o1, o2;
+        dinv_apply(planes, nb, b, omega, x[3 * b], x[3 * b + 1], x[3 * b + 2], o0, o1, o2);
+        z[3 * b] += o0;
+        z[3 * b + 1] += o1;
+        z[3 * b + 2] += o2;
+    } else {
+        for (int i = 0; i < BS; ++i) {
+            double acc = 0.0;
+            for (int j = 0; j < BS; ++j) acc += planes[(size_t)(i * BS + j) * nb + b] * x[BS * b + j];
+            z[BS * b + i] += omega * acc;
+        }
+    }
+}
+}  // namespace
+}  // namespace hsc
+
+extern "C" int hsc_debug_dmv_accumulate(int32_t bs, int32_t nblocks, const double* d_planes, const double* d_x,
+                                        double* d_z, double omega, void* stream) {
+    using namespace hsc;
+    if (nblocks < 0 || (nblocks > 0 && (!d_planes || !d_x || !d_z))) return HSC_ERR_INVALID;
+    if (nblocks == 0) return HSC_OK;
+    const int grid = (nblocks + 127) / 128;
+    cudaStream_t st = (cudaStream_t)stream;
+    count_launch();
+    if (bs == 3) dmv_accumulate_kernel<3><<<grid, 128, 0, st>>>(nblocks, d_planes, d_x, d_z, omega);
+    else if (bs == 12) dmv_accumulate_kernel<12><<<grid, 128, 0, st>>>(nblocks, d_planes, d_x, d_z, omega);
+    else return HSC_ERR_INVALID;
+    return cudaGetLastError() == cudaSuccess ? HSC_OK : HSC_ERR_CUDA;
+}

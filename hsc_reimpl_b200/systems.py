@@ -405,6 +405,83 @@ def make_vehicle_system(seed=0, nr=4, na=5, nc=93, E_carried=1e10, E_ground=1e6,
     return _finish("vehicle_7tires", asm, (0, qm, qm, fn), rng, meta)
 
 
+def tire_mesh():
+    """The vehicle scene's Tet4 tire (3,548 nodes, 11,171 tets, tire axis = local y) and
+    the placements of the seven tires the vehicle workload uses (four mounted, three
+    lying flat), as extracted by ``hsc_reimpl_b200/data/make_tire_mesh.py``."""
+    from pathlib import Path
+    return np.load(Path(__file__).resolve().parent / "data" / "tire_tet4.npz")
+
+
+def make_reference_vehicle_system(seed=0, E_carried=1e10, E_ground=1e6, nu=0.3, rho=1000.0,
+                                  E_abd=1e10, contact_frac=(0.05, 0.15), k_range=(1e6, 1e9),
+                                  k_rim=1e7, k_joint=1e9, perturb=0.02, tread_radius=0.4259):
+    """Vehicle-scale system on the vehicle scene's own tire mesh: 7 tires x 3,548 nodes =
+    24,836 nodes (74,508 FEM dofs), 78,197 Tet4, 149,513 upper blocks, 12 affine bodies.
+
+    Tires 0-3 are the mounted (carried) tires, E = ``E_carried``; 4-6 lie on the ground,
+    E = ``E_ground``; positions and orientations are the scene's.  Bodies 0-6 are the
+    rims, each stitched to its tire's 39 rim-connection nodes (``BC_CONN``); 7-10 are
+    spindles jointed to rims 0-3 and to each other; 11 is the ground body.  Each tire's
+    contact patch is the seeded share ``contact_frac`` of its tread-node count (surface
+    nodes at tire radius >= ``tread_radius``), taken as the surface nodes nearest the
+    ground plane z = 0; each patch node touches the ground body through a barrier block
+    k n n^T, k log-uniform in ``k_range``, n = +z with a 5 % seeded tilt.
+    """
+    rng = np.random.default_rng(seed)
+    m = tire_mesh()
+    xl, tl = m["vertices"], m["tetrahedra"].astype(np.int64)
+    conn = m["bc_conn"].astype(np.int64)
+    surf = np.unique(m["surface_triangles"])
+    rad = np.hypot(xl[:, 0], xl[:, 2])
+    ntread = int(np.count_nonzero(rad[surf] >= tread_radius))
+    Rs, Ts, mounted = m["placement_rotation"], m["placement_translation"], m["placement_mounted"]
+    ntire, nbody = Rs.shape[0], 12
+    nodes_per = xl.shape[0]
+    nn = ntire * nodes_per
+    qm, fn = 12 * nbody, 3 * nn
+    asm = _Assembler(qm + fn)
+    ground_center = np.array([-1.5, 0.0, -1.0])
+    ntets = active_nodes = 0
+    for t in range(ntire):
+        x = xl @ Rs[t].T + Ts[t]
+        tets = _orient(x, tl)
+        center = Ts[t]
+        base = t * nodes_per
+        E = E_carried if mounted[t] else E_ground
+        r, c, v, _ = fem_hessian(x, tets, E, nu, rho, perturb=perturb, rng=rng)
+        asm.add(qm + 3 * base + r, qm + 3 * base + c, v)
+        ntets += tets.shape[0]
+        rim_pts = x[conn] - center
+        rim_vol = np.pi * 0.25 ** 2 * 0.28 * 0.1
+        asm.add_dense(12 * t + np.arange(12), abd_block(20.0, rim_pts, E_abd, rim_vol))
+        for node in conn:
+            _stitch(asm, qm, base + node, t, x[node] - center, k_rim)
+        active_nodes += conn.size
+        frac = rng.uniform(*contact_frac)
+        count = max(1, int(round(frac * ntread)))
+        cand = surf[~np.isin(surf, conn)]
+        patch = cand[np.argsort(x[cand, 2], kind="stable")[:count]]
+        ks = np.exp(rng.uniform(np.log(k_range[0]), np.log(k_range[1]), patch.size))
+        for node, k in zip(patch, ks):
+            nrm = np.array([0.0, 0.0, 1.0]) + 0.05 * rng.standard_normal(3)
+            nrm /= np.linalg.norm(nrm)
+            _barrier_coupling(asm, qm, base + node, 11, x[node] - ground_center, nrm, k)
+        active_nodes += patch.size
+    for s in range(4):  # spindles
+        pts = rng.uniform(-0.1, 0.1, (16, 3))
+        asm.add_dense(12 * (7 + s) + np.arange(12), abd_block(10.0, pts, E_abd, 0.004))
+        for p in (np.array([0.0, 0.1, 0.0]), np.array([0.05, 0.1, 0.05]), np.array([0.0, 0.1, 0.08])):
+            _joint(asm, 7 + s, p, s, p + np.array([0.0, -0.25, 0.0]), k_joint)
+    for s in range(3):
+        _joint(asm, 7 + s, np.array([0.3, 0.0, 0.0]), 8 + s, np.array([-0.3, 0.0, 0.0]), 1e-2 * k_joint)
+    gpts = rng.uniform(-2.0, 2.0, (32, 3))
+    asm.add_dense(12 * 11 + np.arange(12), abd_block(1e4, gpts, E_abd, 10.0))
+    meta = dict(config="vehicle_tire_tet4", nodes=nn, tets=ntets, bodies=nbody, tires=ntire,
+                coupled_nodes=int(active_nodes), seed=seed, mesh="tire_tet4")
+    return _finish("vehicle_tire_tet4_78k", asm, (0, qm, qm, fn), rng, meta)
+
+
 def make_torus_system(seed=0, target_tets=10000, bodies=4, E=1e8, nu=0.3, rho=1000.0,
                       E_abd=1e10, contact_frac=0.1, k_range=(1e6, 1e9), k_rim=1e7,
                       nr=3, na=4, E_rim=None, perturb=0.02, name="torus"):

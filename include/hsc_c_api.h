@@ -194,6 +194,11 @@ HSC_EXPORT int hsc_spmv(hsc_ctx* ctx, const hsc_bcoo3* A, const hsc_dof_layout* 
  * 1,048,576 dofs (3 * nblock); larger systems get HSC_ERR_INVALID.  Calls that
  * overlap on the GPU share that array and race; the first call on a device
  * looks up the array's address and should come before any stream capture.
+ * Under lazy module loading (the CUDA 12 default) that first call also loads
+ * the module that holds the array, so nothing is allocated from the second
+ * call on.  Triplets with a block index outside [0, nblock) are skipped by the
+ * kernel and make the call return HSC_ERR_INVALID (y then holds the product of
+ * the valid triplets).  The call waits for its stream before it returns.
  * y may alias x.  This entry point has no counterpart in the reference. */
 HSC_EXPORT int hsc_spmv_noalloc(const hsc_bcoo3* A, const double* d_x, double* d_y, void* stream);
 
@@ -317,6 +322,13 @@ HSC_EXPORT int hsc_debug_checks(long long* out6);
  * (No reference counterpart: it checks this library's bounded waits.) */
 HSC_EXPORT int hsc_debug_barrier_selftest(int32_t ctas, int32_t absent, int64_t first_limit, int64_t limit,
                                           int32_t* statuses, int32_t* abort_flag, int32_t* where);
+
+/* z += omega * blockdiag(B) x over nblocks bs x bs blocks (bs 3 or 12), B given as bs*bs planes
+ * d_planes[(i * bs + j) * nblocks + b] = B_b(i, j).  The shape of the authors' dmv_accumulate_kernel
+ * (Guo-2026-HSC conjugate_gradient_cuda.cuh, run by reproduction/cuda_original.py); bs = 3 runs the PCG
+ * kernel's own block-Jacobi product.  Test hook. */
+HSC_EXPORT int hsc_debug_dmv_accumulate(int32_t bs, int32_t nblocks, const double* d_planes, const double* d_x,
+                                        double* d_z, double omega, void* stream);
 
 #ifdef __cplusplus
 }

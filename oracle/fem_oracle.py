@@ -3,10 +3,11 @@
 Only ``tests/`` may import it.  It restates in NumPy the per-tet log-Neo-Hookean
 Hessian of the reference and its assembly into a one-triangle BCOO:
 
-* ``raw_hessian``  -- ``log_neo_hookean_function.h:92-106``: H[i+3a][j+3b] =
+* ``energy``, ``first_piola`` -- ``E`` and ``dEdF``, ``log_neo_hookean_function.h:77-91``;
+* ``raw_hessian``  -- ``log_neo_hookean_function.h:93-104``: H[i+3a][j+3b] =
   mu d_ij d_ab + lambda G[i][a] G[j][b] - (lambda ln J - mu) G[i][b] G[j][a],
   G = cof(F)/J, column-major vec(F);
-* ``spd``          -- ``ddEddF_spd`` (``log_neo_hookean_function.h:108-150``):
+* ``spd``          -- ``ddEddF_spd`` (``log_neo_hookean_function.h:106-150``):
   the eigen-decomposition with negative eigenvalues clamped at 0 (here by
   LAPACK's symmetric solver instead of cyclic Jacobi);
 * ``assemble``     -- ``log_neo_hookean_3d.cu:62-135``: F = Ds Dm^-1, the
@@ -18,6 +19,8 @@ Hessian of the reference and its assembly into a one-triangle BCOO:
 from __future__ import annotations
 
 import numpy as np
+
+MIN_JACOBIAN = 1e-8
 
 
 def lame(E, nu):
@@ -31,6 +34,23 @@ def cofactor(F):
             C[..., i, j] = (F[..., (i + 1) % 3, (j + 1) % 3] * F[..., (i + 2) % 3, (j + 2) % 3]
                             - F[..., (i + 1) % 3, (j + 2) % 3] * F[..., (i + 2) % 3, (j + 1) % 3])
     return C
+
+
+def energy(F, mu, lam):
+    """log-NH energy density psi = mu/2 (|F|^2 - 3) - mu ln J + lambda/2 (ln J)^2
+    (``log_neo_hookean_function.h:77-83``); +inf unless det F > 1e-8."""
+    J = np.linalg.det(F)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        lnJ = np.log(J)
+    psi = 0.5 * mu * (np.sum(F * F, axis=(-2, -1)) - 3.0) - mu * lnJ + 0.5 * lam * lnJ * lnJ
+    return np.where(J > MIN_JACOBIAN, psi, np.inf)
+
+
+def first_piola(F, mu, lam):
+    """dpsi/dF = mu F + (lambda ln J - mu) cof(F) / J (``log_neo_hookean_function.h:85-91``)."""
+    J = np.linalg.det(F)
+    FinvT = np.swapaxes(np.linalg.inv(F), -1, -2)
+    return mu[..., None, None] * F + (lam * np.log(J) - mu)[..., None, None] * FinvT
 
 
 def raw_hessian(F, mu, lam):
@@ -83,9 +103,6 @@ def assemble(tets, rest_x, x, E, rho=1000.0, nu=0.3, dt=1.0 / 30.0, project=True
     keys = np.array(sorted(blocks))
     vals = np.array([np.asarray(blocks[k]).T.reshape(9) for k in keys])  # column-major
     return (keys // n).astype(np.int32), (keys % n).astype(np.int32), vals
-
-
-MIN_JACOBIAN = 1e-8
 
 
 def _triple(a, b, c):

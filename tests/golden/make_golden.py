@@ -3,7 +3,7 @@
 Run in a container where the reference checkout exists (it is read, never
 written):
 
-    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py /root/reference
+    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py <reference-checkout> [--only projection]
 
 It imports ``reproduction/core.py`` unmodified and records:
 
@@ -19,7 +19,10 @@ It imports ``reproduction/core.py`` unmodified and records:
   ``hsc_reimpl_b200.systems.make_cube_system(seed=0)`` at order 2, omega 2/3,
   ACA rtol 1e-4, PCG rtol 1e-6 (one solve, the exact-affine variant and
   ``core.refinement`` to a 1e-6 full residual).  Only outputs and an input
-  checksum are stored; the inputs are regenerated from the seed.
+  checksum are stored; the inputs are regenerated from the seed;
+* ``projection.npz`` -- ``core.affine_projection`` (``core.py:201-206``), the
+  3x12 affine-body Jacobian of the reference's core, at 64 seeded rest points
+  (numpy ``default_rng(206)``, standard normal, the first one the origin).
 """
 import csv
 import hashlib
@@ -42,12 +45,24 @@ def input_digest(H, b):
     return h.hexdigest()
 
 
-def main(ref_root):
+def projection(core):
+    rest = np.random.default_rng(206).standard_normal((64, 3))
+    rest[0] = 0.0
+    P = np.stack([core.affine_projection(r) for r in rest])
+    np.savez_compressed(HERE / "projection.npz", rest=rest, P=P)
+
+
+def main(ref_root, only=None):
     os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
     os.environ.setdefault("OMP_NUM_THREADS", "1")
     sys.dont_write_bytecode = True
     sys.path.insert(0, str(Path(ref_root) / "reproduction"))
     import core  # the reference's NumPy HSC core, unmodified
+
+    if only in (None, "projection"):
+        projection(core)
+    if only == "projection":
+        return
 
     out = {}
     saved_summary = {}
@@ -141,4 +156,8 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    only = sys.argv[sys.argv.index("--only") + 1] if "--only" in sys.argv else None
+    if only:
+        args = [a for a in args if a != only]
+    main(args[0] if args else "/root/reference", only)

@@ -191,6 +191,62 @@ def test_vehicle_fp64_matches_oracle(api, torch, vehicle_system, vehicle_oracle)
     assert st["full_relative_residual"] <= 1e-6
 
 
+@pytest.fixture(scope="module")
+def tire_system():
+    from hsc_reimpl_b200.systems import make_reference_vehicle_system
+    return make_reference_vehicle_system(seed=0)
+
+
+@pytest.fixture(scope="module")
+def tire_oracle(tire_system):
+    s = tire_system
+    return O.hsc_solve(s.H, s.layout, s.b, order=2, omega=0.5, tol=1e-6, max_iter=20000,
+                       abd_inverse="exact", max_rank=128)
+
+
+def test_tire_mesh_vehicle_fp64_matches_oracle(api, torch, tire_system, tire_oracle):
+    """The benchmark workload: the vehicle scene's own tire mesh (24,836 nodes, 74,508 FEM
+    dofs, 149,513 stored upper FEM blocks), plain FP64 Neumann order 2, omega 0.5."""
+    s = tire_system
+    assert s.layout[3] == 74508 and s.meta["tets"] == 78197
+    fb0 = s.layout[2] // 3
+    assert int(((s.rows >= fb0) & (s.cols >= fb0)).sum()) == 149513
+    xo, so, orc = tire_oracle
+    ctx = api.HSCContext(api.HSCOptions(neumann_order=2, omega=0.5, tol=1e-6))
+    x, st = ctx.solve(api.DeviceSystem.from_system(s))
+    assert st["status"] == 0
+    assert st["rank"] == so["rank"]
+    assert st["active_fem_dofs"] == so["active_fem_dofs"]
+    k, a, act = ctx.factors()
+    # the active FEM dofs, in the FEM block's own numbering, equal the oracle's extraction
+    np.testing.assert_array_equal(np.sort(act), np.sort(orc.active))
+    assert abs(st["pcg_iterations"] - so["pcg_iterations"]) <= 1
+    assert rel(x.cpu().numpy(), xo) < 1e-5
+    assert st["full_relative_residual"] <= 1e-6
+
+
+@pytest.mark.parametrize("prec", ("fp32", "bf16"))
+def test_tire_mesh_mixed_precision_error_against_fp64(api, torch, tire_system, prec):
+    """Reduced-precision bulk against a tight FP64 solve of the same system (Schur tol 1e-12):
+    relative error of x and of its A-norm (through H) below 1e-5, which is what a 1e-6 residual
+    allows on this system (the FP64 form at 1e-6 is checked against the same solution)."""
+    s = tire_system
+    ds = api.DeviceSystem.from_system(s)
+    ref = api.HSCContext(api.HSCOptions(neumann_order=2, omega=0.5, tol=1e-12, max_iter=20000))
+    xr, st_r = ref.solve(ds)
+    xr = xr.cpu().numpy()
+    assert st_r["status"] == 0
+    ctx = api.HSCContext(api.HSCOptions(neumann_order=2, omega=0.5, tol=1e-6, precision=prec,
+                                        residual_replacement=50, max_iter=20000))
+    x, st = ctx.solve(ds)
+    x = x.cpu().numpy()
+    assert st["status"] == 0 and st["full_relative_residual"] <= 1e-6
+    e = x - xr
+    anorm = np.sqrt(abs(e @ (s.H @ e)) / abs(xr @ (s.H @ xr)))
+    assert rel(x, xr) < 1e-5, rel(x, xr)
+    assert anorm < 1e-5, anorm
+
+
 @pytest.mark.parametrize("prec", ("fp32", "bf16"))
 def test_vehicle_mixed_precision_reaches_fp64_target(api, torch, vehicle_system, prec):
     """FP32 / BF16 bulk with FP64 residual replacement: the FP64 full residual
