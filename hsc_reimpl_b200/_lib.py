@@ -60,6 +60,7 @@ class Options(C.Structure):
         ("resident", C.c_int32),
         ("fuse_update", C.c_int32),
         ("aca_cluster", C.c_int32),
+        ("reorder", C.c_int32),
     ]
 
 
@@ -115,6 +116,9 @@ EXPORTS = {
     "hsc_get_factors": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                   C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p]),
     "hsc_get_abd_inverse": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "hsc_get_partition": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_void_p,
+                                    C.c_void_p]),
+    "hsc_partition_nodes": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "hsc_get_trace": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "hsc_version": (C.c_int, []),
     "hsc_kernel_launches": (C.c_longlong, []),

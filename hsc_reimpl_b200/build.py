@@ -15,7 +15,8 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 BUILD = CSRC / "_build"
 LIB = HERE / "libhsc_b200.so"
-SOURCES = ["hsc_api.cu", "hsc_setup.cu", "hsc_pcg.cu", "hsc_aca.cu", "hsc_learned.cu", "hsc_assemble.cu", "hsc_coupling.cu", "hsc_noalloc.cu"]
+SOURCES = ["hsc_api.cu", "hsc_setup.cu", "hsc_pcg.cu", "hsc_aca.cu", "hsc_learned.cu", "hsc_assemble.cu", "hsc_coupling.cu",
+           "hsc_noalloc.cu", "hsc_partition.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",
@@ -36,9 +37,9 @@ def build(force=False, verbose=False, checked=False):
     lib = HERE / ("libhsc_b200_checked.so" if checked else "libhsc_b200.so")
     extra = ["-DHSC_CHECKED"] if checked else []
     build_dir.mkdir(parents=True, exist_ok=True)
-    headers = list(CSRC.glob("*.cuh")) + [HERE.parent / "include" / "hsc_c_api.h"]
+    headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [HERE.parent / "include" / "hsc_c_api.h"]
     newest_header = max(h.stat().st_mtime for h in headers)
-    objs = []
+    objs, jobs = [], []
     for src in SOURCES:
         s = CSRC / src
         o = build_dir / (s.stem + ".o")
@@ -46,8 +47,13 @@ def build(force=False, verbose=False, checked=False):
             cmd = [NVCC, *FLAGS, *extra, "-c", str(s), "-o", str(o)]
             if verbose:
                 print(" ".join(cmd))
-            _run(cmd)
+            jobs.append(cmd)
         objs.append(str(o))
+    # the translation units are independent: compile them in parallel
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(_run, cmd) for cmd in jobs]:
+            f.result()
     if force or not lib.exists() or lib.stat().st_mtime < max(Path(o).stat().st_mtime for o in objs):
         _run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-cudart", "static",
               "-o", str(lib), *objs, "-lpthread"])

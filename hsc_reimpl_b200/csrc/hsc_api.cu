@@ -24,6 +24,7 @@
 
 #include "../../include/hsc_c_api.h"
 #include "hsc_learned.cuh"
+#include "hsc_partition.h"
 #include "hsc_setup.cuh"
 
 using namespace hsc;
@@ -91,12 +92,15 @@ struct System {
     // sizes
     int n = 0, nnz = 0, a = 0, nqq = 0, nqf = 0, kmax = 0, qm = 0, qo = 0, fo = 0, fn = 0;
     std::vector<int> h_rowptr, h_act, h_colidx, h_rowflag;
+    std::vector<int> h_perm, h_iperm, h_part_ptr, h_actp, h_actperm;  // node renumbering, parts, PCG-order active dofs
+    bool reordered = false;
+    std::vector<int> h_node_body;   // (active node in the caller's order, body) of every coupling block
     // plan
-    DevBuf rowptr, colidx, rowid, src, diag_pos, qq, qf, act, ident, rowflag;
+    DevBuf rowptr, colidx, rowid, src, diag_pos, qq, qf, act, ident, rowflag, perm, actp, actperm;
     // numeric
     DevBuf r2;
     DevBuf v64, vf32, vbf16, dinv, A, E, R0, R1, U, V, hist, P, Ptmp, T, term, Binv, L, W, C, Lc, dpiv, vt64, vtmt,
-        cvec, tt, ttx, bq, bf, x, r, z, p0, p1, y, t0, t1, node_nz, xq, ypad, yq, work, cg, scal, dact, pact, yact,
+        cvec, tt, ttx, bq, bf, x, r, z, p0, p1, y, t0, t1, node_nz, xq, ypad, yq, work, cg, scal, dact, pact, yact, vt64p,
         zpart, tpart, lcol, rowpart;
     DevBuf dvec[4];           // contiguous-N scratch for refinement
     double h_last[kPrev] = {};   // record of the last solve: 1, lanczos min, max, iterations, q(0)
@@ -126,6 +130,7 @@ struct hsc_ctx {
     int vt_smem = 0;           // doubles of PCG shared memory after the d.*tt slot
     size_t pcg_smem = 0;       // dynamic shared memory bytes of the PCG launch
     int part_key_gen = -1;
+    bool block_layout = false;  // CTA rows = the analysis' parts (the block preconditioner)
     // ACA
     DevBuf aca_psum, aca_pmax, aca_pidx, aca_bar;
     int aca_grid = 0;
@@ -241,16 +246,54 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
             return fail(ctx, HSC_ERR_INVALID, "triplet outside the ABD and FEM dof ranges");
         }
     }
-    // full BSR plan: rows of D, columns sorted
+    // FEM node renumbering: compact parts of balanced weight, numbered part by part, so that
+    // CTA k's contiguous row range is part k (hsc_partition.h).  perm[new] = caller's node.
+    {
+        std::vector<int> deg(S.n + 1, 0);
+        for (long long t = 0; t < T; ++t) {
+            const int r = rows[t], c = cols[t];
+            if (isF(r) && isF(c) && r != c) { deg[r - fb0]++; deg[c - fb0]++; }
+        }
+        std::vector<int> aptr(S.n + 1, 0);
+        for (int i = 0; i < S.n; ++i) aptr[i + 1] = aptr[i] + deg[i];
+        std::vector<int> adj(aptr[S.n]), fillp(aptr.begin(), aptr.end() - 1);
+        for (long long t = 0; t < T; ++t) {
+            const int r = rows[t], c = cols[t];
+            if (isF(r) && isF(c) && r != c) { adj[fillp[r - fb0]++] = c - fb0; adj[fillp[c - fb0]++] = r - fb0; }
+        }
+        const int nparts = o.reorder ? std::max(1, std::min(ctx->num_sms, S.n / 16)) : 1;
+        std::vector<int> part;
+        if (nparts > 1) {
+            std::vector<double> wgt(S.n);
+            for (int i = 0; i < S.n; ++i) wgt[i] = 1.0 + cnt[i];
+            part = partition_nodes(S.n, aptr, adj, wgt, nparts);
+        } else {
+            part.assign(S.n, 0);
+        }
+        S.h_part_ptr.assign(nparts + 1, 0);
+        for (int i = 0; i < S.n; ++i) S.h_part_ptr[part[i] + 1]++;
+        for (int p = 0; p < nparts; ++p) S.h_part_ptr[p + 1] += S.h_part_ptr[p];
+        S.h_perm.assign(S.n, 0);
+        S.h_iperm.assign(S.n, 0);
+        std::vector<int> fill(S.h_part_ptr.begin(), S.h_part_ptr.end() - 1);
+        for (int i = 0; i < S.n; ++i) {
+            const int ni = fill[part[i]]++;
+            S.h_perm[ni] = i;
+            S.h_iperm[i] = ni;
+        }
+        S.reordered = nparts > 1;
+    }
+    const std::vector<int>& iperm = S.h_iperm;
+    // full BSR plan over the renumbered nodes: rows of D, columns sorted
     S.h_rowptr.assign(S.n + 1, 0);
-    for (int i = 0; i < S.n; ++i) S.h_rowptr[i + 1] = S.h_rowptr[i] + cnt[i];
+    for (int i = 0; i < S.n; ++i) S.h_rowptr[i + 1] = S.h_rowptr[i] + cnt[S.h_perm[i]];
     S.nnz = S.h_rowptr[S.n];
     std::vector<int> fillpos(S.h_rowptr.begin(), S.h_rowptr.end() - 1);
     std::vector<long long> ent(S.nnz);  // (col << 32) | packed src
     for (long long t = 0; t < T; ++t) {
         const int r = rows[t], c = cols[t];
         if (isF(r) && isF(c)) {
-            const int i = r - fb0, j = c - fb0;
+            const int i = iperm[r - fb0], j = iperm[c - fb0];
             ent[fillpos[i]++] = ((long long)j << 32) | (unsigned)(2 * t);
             if (i != j) ent[fillpos[j]++] = ((long long)i << 32) | (unsigned)(2 * t + 1);
         }
@@ -278,19 +321,41 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
             seen[(size_t)i * nb + j] = 1;
         }
     }
-    // active FEM nodes (structural) and the coupling list
+    // active FEM nodes (structural) and the coupling list.  The active list keeps the caller's
+    // dof order (E's columns, and so the ACA's pivot order, are the reference's); its device copy
+    // holds the internal dof numbers.  The PCG sees the same nodes sorted by internal number
+    // (actp: each CTA's coupled dofs form one contiguous range), with actperm mapping back.
     std::vector<int> act_index(S.n, -1);
     int nact = 0;
     for (int i = 0; i < S.n; ++i)
         if (fnode_active[i]) act_index[i] = nact++;
     S.a = 3 * nact;
     S.h_act.resize(S.a);
+    std::vector<int> act_int(S.a);
     for (int i = 0; i < S.n; ++i)
         if (act_index[i] >= 0)
-            for (int c = 0; c < 3; ++c) S.h_act[3 * act_index[i] + c] = 3 * i + c;
+            for (int c = 0; c < 3; ++c) {
+                S.h_act[3 * act_index[i] + c] = 3 * i + c;
+                act_int[3 * act_index[i] + c] = 3 * iperm[i] + c;
+            }
+    S.h_actp.resize(S.a);
+    std::vector<int> actperm(S.a);
     std::vector<int> rowflag(S.n, -1);
-    for (int i = 0; i < S.n; ++i) rowflag[i] = act_index[i];
+    {
+        int ap = 0;
+        for (int ni = 0; ni < S.n; ++ni) {
+            const int an = act_index[S.h_perm[ni]];
+            if (an < 0) continue;
+            rowflag[ni] = ap;
+            for (int c = 0; c < 3; ++c) {
+                S.h_actp[3 * ap + c] = 3 * ni + c;
+                actperm[3 * ap + c] = 3 * an + c;
+            }
+            ++ap;
+        }
+    }
     S.h_rowflag = rowflag;
+    S.h_actperm = actperm;
     std::vector<int> qf;
     qf.reserve(qfraw.size());
     {
@@ -301,6 +366,8 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
             qf.push_back(qfraw[e]); qf.push_back(qfraw[e + 1]); qf.push_back(act_index[qfraw[e + 2]]); qf.push_back(qfraw[e + 3]);
         }
     }
+    S.h_node_body.clear();
+    for (size_t e = 0; e < qf.size(); e += 4) { S.h_node_body.push_back(qf[e + 2]); S.h_node_body.push_back(qf[e + 1] / 4); }
     S.nqq = (int)qq.size() / 3;
     S.nqf = (int)qf.size() / 4;
     S.kmax = std::min(std::min(o.max_rank, L.qm), S.a);
@@ -313,7 +380,10 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
     GROW(S.qq, sizeof(int) * std::max<size_t>(3, qq.size()));
     GROW(S.qf, sizeof(int) * std::max<size_t>(4, qf.size()));
     GROW(S.act, sizeof(int) * std::max(1, S.a));
+    GROW(S.actp, sizeof(int) * std::max(1, S.a));
+    GROW(S.actperm, sizeof(int) * std::max(1, S.a));
     GROW(S.rowflag, sizeof(int) * std::max(1, S.n));
+    GROW(S.perm, sizeof(int) * std::max(1, S.n));
     CK(cudaMemcpyAsync(S.rowptr.p, S.h_rowptr.data(), sizeof(int) * (S.n + 1), cudaMemcpyHostToDevice, st));
     {
         std::vector<int> rid(std::max(1, S.nnz));
@@ -331,7 +401,12 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
     CK(cudaMemcpyAsync(S.diag_pos.p, diag.data(), sizeof(int) * S.n, cudaMemcpyHostToDevice, st));
     if (!qq.empty()) CK(cudaMemcpyAsync(S.qq.p, qq.data(), sizeof(int) * qq.size(), cudaMemcpyHostToDevice, st));
     if (!qf.empty()) CK(cudaMemcpyAsync(S.qf.p, qf.data(), sizeof(int) * qf.size(), cudaMemcpyHostToDevice, st));
-    if (S.a) CK(cudaMemcpyAsync(S.act.p, S.h_act.data(), sizeof(int) * S.a, cudaMemcpyHostToDevice, st));
+    if (S.a) {
+        CK(cudaMemcpyAsync(S.act.p, act_int.data(), sizeof(int) * S.a, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(S.actp.p, S.h_actp.data(), sizeof(int) * S.a, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(S.actperm.p, actperm.data(), sizeof(int) * S.a, cudaMemcpyHostToDevice, st));
+    }
+    CK(cudaMemcpyAsync(S.perm.p, S.h_perm.data(), sizeof(int) * S.n, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(S.rowflag.p, rowflag.data(), sizeof(int) * S.n, cudaMemcpyHostToDevice, st));
     const size_t nz = std::max(1, S.nnz), n4 = 4 * (size_t)std::max(1, S.n), qm = std::max(1, S.qm);
     const size_t km = std::max(1, S.kmax), aa = std::max(1, S.a);
@@ -358,6 +433,7 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
     GROW(S.Lc, sizeof(double) * km * km);
     GROW(S.dpiv, sizeof(double) * km);
     GROW(S.vt64, sizeof(double) * aa * km);
+    GROW(S.vt64p, sizeof(double) * aa * km);
     GROW(S.cvec, sizeof(double) * km);
     GROW(S.tt, sizeof(double) * 256);
     GROW(S.ttx, sizeof(double) * 256);
@@ -397,7 +473,7 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
     CK(cudaMemcpyAsync(&S.hash, &S.scal.as<DevScal>()->hash, sizeof(S.hash), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     S.rows = M.d_rows; S.cols = M.d_cols; S.nnzb = M.nnzb; S.nblock = M.nblock; S.lay = L;
-    S.kmax_for = o.max_rank * 16 + o.precision;
+    S.kmax_for = (o.max_rank * 16 + o.precision) * 2 + (o.reorder ? 1 : 0);
     S.analyzed = true;
     ctx->part_key_gen = -1;  // CTA partition must be rebuilt
     if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
@@ -407,7 +483,7 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
 bool same_key(const System& S, const hsc_bcoo3& M, const hsc_dof_layout& L, const hsc_options& o) {
     return S.analyzed && S.rows == M.d_rows && S.cols == M.d_cols && S.nnzb == M.nnzb && S.nblock == M.nblock &&
            S.lay.qo == L.qo && S.lay.qm == L.qm && S.lay.fo == L.fo && S.lay.fn == L.fn &&
-           S.kmax_for == o.max_rank * 16 + o.precision;
+           S.kmax_for == (o.max_rank * 16 + o.precision) * 2 + (o.reorder ? 1 : 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -502,7 +578,7 @@ int numeric_pre(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, cudaStream_t st) {
     __nv_bfloat16* vb = P == 2 ? S.vbf16.as<__nv_bfloat16>() : nullptr;
     launch_fill_bsr(S.src.as<int>(), M.d_values, S.nnz, S.v64.as<double>(), vf, vb, st);
     launch_dinv(P, S.diag_pos.as<int>(), S.v64.as<double>(), S.nnz, S.n, S.dinv.p, &ds->bad_fem, st);
-    launch_split_active_diag(S.act.as<int>(), S.a / 3, S.diag_pos.as<int>(), S.v64.as<double>(), S.nnz, vf, vb,
+    launch_split_active_diag(S.actp.as<int>(), S.a / 3, S.diag_pos.as<int>(), S.v64.as<double>(), S.nnz, vf, vb,
                              S.dact.as<double>(), st);
     launch_extract(S.qq.as<int>(), S.nqq, S.qf.as<int>(), S.nqf, M.d_values, S.qm, S.a, S.A.as<double>(),
                    S.E.as<double>(), S.node_nz.as<int>(), st);
@@ -554,6 +630,8 @@ int numeric_post(hsc_ctx* ctx, System& S, cudaStream_t st, bool allow_sync) {
         CK(cudaMemsetAsync(S.vt64.p, 0, sizeof(double) * S.a * S.kmax, st));
         gemm(S.Lc.as<double>(), S.kmax, 1, S.V.as<double>(), S.a, 0, S.vt64.as<double>(), S.a, S.kmax, S.a, S.kmax,
              1.0, 0.0, st, dk, nullptr, dk);
+        // the PCG's copy: rows in internal node order (actp)
+        launch_gather_rows(S.vt64.as<double>(), S.a, S.kmax, S.actperm.as<int>(), S.vt64p.as<double>(), st);
     }
     stage_mark(ctx, 4, st);
     return HSC_OK;
@@ -562,7 +640,7 @@ int numeric_post(hsc_ctx* ctx, System& S, cudaStream_t st, bool allow_sync) {
 // rhs of the Schur system for right-hand side b (contiguous N)
 void schur_rhs(System& S, const double* b, cudaStream_t st) {
     DevScal* ds = S.scal.as<DevScal>();
-    launch_split_rhs(b, S.qo, S.qm, S.fo, S.n, S.bq.as<double>(), S.bf.as<double>(), st);
+    launch_split_rhs(b, S.qo, S.qm, S.fo, S.n, S.perm.as<int>(), S.bq.as<double>(), S.bf.as<double>(), st);
     if (S.kmax > 0) {
         launch_wt_vec(S.W.as<double>(), S.qm, S.kmax, &ds->rank, S.bq.as<double>(), S.cvec.as<double>(), st);
         launch_rhs_lowrank(S.V.as<double>(), S.a, &ds->rank, S.cvec.as<double>(), S.act.as<int>(), S.bf.as<double>(), st);
@@ -577,11 +655,11 @@ void back_substitute(System& S, const double* b, double* x_out, bool residual, c
         launch_vt_x(S.V.as<double>(), S.a, S.kmax, &ds->rank, S.act.as<int>(), S.x.as<double>(), S.cvec.as<double>(), st);
     else
         cudaMemsetAsync(S.cvec.p, 0, sizeof(double) * std::max(1, S.kmax), st);
-    launch_split_rhs(b, S.qo, S.qm, S.fo, S.n, S.bq.as<double>(), S.bf.as<double>(), st);
+    launch_split_rhs(b, S.qo, S.qm, S.fo, S.n, S.perm.as<int>(), S.bq.as<double>(), S.bf.as<double>(), st);
     if (S.qm)
         launch_backsub(S.P.as<double>(), S.W.as<double>(), S.qm, std::max(1, S.kmax), &ds->rank, S.bq.as<double>(),
                        S.cvec.as<double>(), x_out + S.qo, S.xq.as<double>(), st);
-    launch_scatter_x(S.x.as<double>(), S.n, S.fo, x_out, st);
+    launch_scatter_x(S.x.as<double>(), S.n, S.fo, S.perm.as<int>(), x_out, st);
     if (residual) {
         FullSpmv f{S.rowptr.as<int>(), S.colidx.as<int>(), S.v64.as<double>(), S.nnz, S.n, S.A.as<double>(),
                    S.E.as<double>(), S.qm, S.a, S.act.as<int>(), S.xq.as<double>(), S.x.as<double>(),
@@ -601,7 +679,7 @@ void residual_dots(hsc_ctx* ctx, System& S, cudaStream_t st) {
 // y = H x for contiguous N vectors
 void full_spmv_contig(System& S, const double* x, double* y, cudaStream_t st, const double* bcoo_values = nullptr) {
     double* xpad = S.dvec[3].as<double>();
-    launch_gather_x(x, S.n, S.fo, xpad, st);
+    launch_gather_x(x, S.n, S.fo, S.perm.as<int>(), xpad, st);
     if (S.qm) cudaMemcpyAsync(S.xq.p, x + S.qo, sizeof(double) * S.qm, cudaMemcpyDeviceToDevice, st);
     FullSpmv f{S.rowptr.as<int>(), S.colidx.as<int>(), S.v64.as<double>(), S.nnz, S.n, S.A.as<double>(),
                S.E.as<double>(), S.qm, S.a, S.act.as<int>(), S.xq.as<double>(), xpad, S.ypad.as<double>(),
@@ -609,7 +687,7 @@ void full_spmv_contig(System& S, const double* x, double* y, cudaStream_t st, co
     f.rowpart = S.rowpart.as<double>();
     if (bcoo_values) { f.src = S.src.as<int>(); f.bcoo_values = bcoo_values; }
     launch_full_spmv(f, st);
-    launch_scatter_y(S.ypad.as<double>(), S.n, S.fo, S.yq.as<double>(), S.qm, S.qo, y, st);
+    launch_scatter_y(S.ypad.as<double>(), S.n, S.fo, S.perm.as<int>(), S.yq.as<double>(), S.qm, S.qo, y, st);
 }
 
 // CTA partition of the persistent launch over the systems in `idx`
@@ -674,17 +752,21 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
         const auto& pre = wpre[s];
         const long long rows_w = pre[S.n];
         int row = 0;
+        // the analysis' parts, when the block preconditioner asks for one CTA per part, else a
+        // weighted split of the rows (it also weighs the coupled rows' low-rank work)
+        const bool by_part = ctx->block_layout && (int)S.h_part_ptr.size() == nc[s] + 1 && nc[s] > 1;
         for (int k = 0; k < nc[s]; ++k, ++c) {
             const long long target = rows_w * (k + 1) / nc[s];
             const int rb = row;
             if (k == nc[s] - 1) row = S.n;
+            else if (by_part) row = S.h_part_ptr[k + 1];
             else
                 while (row < S.n && pre[row] < target) ++row;
             cta_sys[c] = s;
             cta_row[2 * c] = rb;
             cta_row[2 * c + 1] = row;
-            cta_act[2 * c] = (int)(std::lower_bound(S.h_act.begin(), S.h_act.end(), 3 * rb) - S.h_act.begin());
-            cta_act[2 * c + 1] = (int)(std::lower_bound(S.h_act.begin(), S.h_act.end(), 3 * row) - S.h_act.begin());
+            cta_act[2 * c] = (int)(std::lower_bound(S.h_actp.begin(), S.h_actp.end(), 3 * rb) - S.h_actp.begin());
+            cta_act[2 * c + 1] = (int)(std::lower_bound(S.h_actp.begin(), S.h_actp.end(), 3 * row) - S.h_actp.begin());
         }
         SysDesc& d = desc[s];
         d.n = S.n; d.nnz = S.nnz; d.a = S.a; d.kmax = S.kmax; d.cta_begin = b; d.cta_end = c;
@@ -692,8 +774,8 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
         d.vals = o.precision ? S.vf32.p : S.v64.p;
         d.vals_pc = o.precision == 2 ? S.vbf16.p : d.vals;
         d.vals64 = S.v64.as<double>(); d.dinv = S.dinv.p;
-        d.act = S.act.as<int>(); d.rowflag = S.rowflag.as<int>(); d.dact = S.dact.as<double>();
-        d.vt64 = S.vt64.as<double>(); d.dpiv = S.dpiv.as<double>(); d.rank = &S.scal.as<DevScal>()->rank;
+        d.act = S.actp.as<int>(); d.rowflag = S.rowflag.as<int>(); d.dact = S.dact.as<double>();
+        d.vt64 = S.vt64p.as<double>(); d.dpiv = S.dpiv.as<double>(); d.rank = &S.scal.as<DevScal>()->rank;
         d.pact = S.pact.as<double>(); d.yact = S.yact.as<double>(); d.ttx = S.ttx.as<double>();
         GROW(S.zpart, sizeof(double) * std::max(1, S.kmax) * (size_t)(c - b));
         d.zpart = S.zpart.as<double>();
@@ -1163,7 +1245,7 @@ FeatArgs feat_args(hsc_ctx* ctx, System& S, bool with_model) {
     f.n = S.n; f.nnz = S.nnz; f.a = S.a; f.kmax = S.kmax;
     f.rowptr = S.rowptr.as<int>(); f.colidx = S.colidx.as<int>(); f.diag_pos = S.diag_pos.as<int>();
     f.rowflag = S.rowflag.as<int>(); f.v64 = S.v64.as<double>(); f.rank = &ds->rank;
-    f.vt64 = S.vt64.as<double>(); f.dpiv = S.dpiv.as<double>(); f.prev = ds->prev;
+    f.vt64 = S.vt64p.as<double>(); f.dpiv = S.dpiv.as<double>(); f.prev = ds->prev;
     f.mlp = with_model ? ctx->mlp.as<uint16_t>() : nullptr;
     f.feat = ds->feat; f.w = ds->wl;
     f.part = ctx->feat_part.as<double>();
@@ -1240,6 +1322,7 @@ int hsc_options_default(hsc_options* o) {
     o->resident = 1;
     o->fuse_update = 0;
     o->aca_cluster = 1;
+    o->reorder = 1;
     return HSC_OK;
 }
 
@@ -1655,6 +1738,33 @@ int hsc_get_lanczos(hsc_ctx* ctx, int32_t sys, double* coef, int32_t max_pairs, 
     const int k = std::min<int>(m, std::max(0, max_pairs));
     if (pairs) *pairs = k;
     if (coef) std::memcpy(coef, S.h_cg, sizeof(double) * 2 * k);
+    return HSC_OK;
+}
+
+int hsc_get_partition(hsc_ctx* ctx, int32_t sys, int32_t* n, int32_t* nparts, int32_t* perm, int32_t* part_ptr) {
+    if (!ctx || sys < 0 || sys >= (int)ctx->sys.size() || !ctx->sys[sys].analyzed) return HSC_ERR_NOTREADY;
+    const System& S = ctx->sys[sys];
+    if (n) *n = S.n;
+    if (nparts) *nparts = (int)S.h_part_ptr.size() - 1;
+    if (perm && S.n) std::memcpy(perm, S.h_perm.data(), sizeof(int) * S.n);
+    if (part_ptr) std::memcpy(part_ptr, S.h_part_ptr.data(), sizeof(int) * S.h_part_ptr.size());
+    return HSC_OK;
+}
+
+int hsc_partition_nodes(int32_t n, const int32_t* adj_ptr, const int32_t* adj, const double* weight, int32_t nparts,
+                        int32_t* part) {
+    if (n < 0 || nparts < 1 || (n > 0 && (!adj_ptr || !adj || !weight || !part))) return HSC_ERR_INVALID;
+    if (n == 0) return HSC_OK;
+    std::vector<int> ptr(adj_ptr, adj_ptr + n + 1);
+    if (ptr[0] != 0) return HSC_ERR_INVALID;
+    for (int i = 0; i < n; ++i)
+        if (ptr[i + 1] < ptr[i] || !(weight[i] > 0)) return HSC_ERR_INVALID;
+    std::vector<int> a(adj, adj + ptr[n]);
+    for (int v : a)
+        if (v < 0 || v >= n) return HSC_ERR_INVALID;
+    std::vector<double> w(weight, weight + n);
+    const std::vector<int> p = partition_nodes(n, ptr, a, w, nparts);
+    std::memcpy(part, p.data(), sizeof(int) * n);
     return HSC_OK;
 }
 

@@ -725,12 +725,14 @@ __global__ void frob_kernel(const double* X, int n, double* out) {
 // ---------------------------------------------------------------------------
 // vectors
 // ---------------------------------------------------------------------------
-// split b (contiguous N) into bq (qm) and node-padded FEM part bf
-__global__ void split_rhs_kernel(const double* b, int qo, int qm, int fo, int n, double* bq, double* bf) {
+// split b (contiguous N) into bq (qm) and node-padded FEM part bf; internal node i
+// is the caller's node perm[i] (perm null: the identity)
+__global__ void split_rhs_kernel(const double* b, int qo, int qm, int fo, int n, const int* perm, double* bq,
+                                 double* bf) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < qm) bq[i] = b[qo + i];
     if (i < n) {
-        const double* s = b + fo + 3 * (size_t)i;
+        const double* s = b + fo + 3 * (size_t)(perm ? perm[i] : i);
         bf[4 * (size_t)i] = s[0];
         bf[4 * (size_t)i + 1] = s[1];
         bf[4 * (size_t)i + 2] = s[2];
@@ -791,19 +793,19 @@ __global__ void backsub_kernel(const double* P, const double* W, int qm, int kma
     }
 }
 
-__global__ void scatter_x_kernel(const double* xpad, int n, int fo, double* xout) {
+__global__ void scatter_x_kernel(const double* xpad, int n, int fo, const int* perm, double* xout) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    double* d = xout + fo + 3 * (size_t)i;
+    double* d = xout + fo + 3 * (size_t)(perm ? perm[i] : i);
     d[0] = xpad[4 * (size_t)i];
     d[1] = xpad[4 * (size_t)i + 1];
     d[2] = xpad[4 * (size_t)i + 2];
 }
 
-__global__ void gather_x_kernel(const double* x, int n, int fo, double* xpad) {
+__global__ void gather_x_kernel(const double* x, int n, int fo, const int* perm, double* xpad) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const double* s = x + fo + 3 * (size_t)i;
+    const double* s = x + fo + 3 * (size_t)(perm ? perm[i] : i);
     xpad[4 * (size_t)i] = s[0];
     xpad[4 * (size_t)i + 1] = s[1];
     xpad[4 * (size_t)i + 2] = s[2];
@@ -970,10 +972,11 @@ __global__ void residual_final_kernel(const double* part, int np, double* out) {
 }
 
 // y (contiguous N) from node-padded y_f and yq
-__global__ void scatter_y_kernel(const double* ypad, int n, int fo, const double* yq, int qm, int qo, double* y) {
+__global__ void scatter_y_kernel(const double* ypad, int n, int fo, const int* perm, const double* yq, int qm, int qo,
+                                 double* y) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
-        double* d = y + fo + 3 * (size_t)i;
+        double* d = y + fo + 3 * (size_t)(perm ? perm[i] : i);
         d[0] = ypad[4 * (size_t)i];
         d[1] = ypad[4 * (size_t)i + 1];
         d[2] = ypad[4 * (size_t)i + 2];
@@ -1019,6 +1022,14 @@ __global__ void split_active_diag_kernel(const int* act, int nact_nodes, const i
         if (vf) vf[o] = 0.0f;
         if (vb) vb[o] = __float2bfloat16_rn(0.0f);
     }
+}
+
+// dst[j * a + i] = src[j * a + perm[i]]: rows of an a x k column-major matrix reordered
+__global__ void gather_rows_kernel(const double* src, int a, int k, const int* perm, double* dst) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= (long long)a * k) return;
+    const int j = (int)(e / a), i = (int)(e - (long long)j * a);
+    dst[e] = src[(size_t)j * a + perm[i]];
 }
 
 __global__ void f64_to_f32_kernel(const double* src, float* dst, long long n) {
@@ -1154,8 +1165,9 @@ void launch_symmetrize(double* P, int m, cudaStream_t st) { HSC_COUNTED(symmetri
 
 void launch_frob(const double* X, int n, double* out, cudaStream_t st) { HSC_COUNTED(frob_kernel<<<1, 1024, 0, st>>>(X, n, out)); }
 
-void launch_split_rhs(const double* b, int qo, int qm, int fo, int n, double* bq, double* bf, cudaStream_t st) {
-    HSC_COUNTED(split_rhs_kernel<<<blocks(std::max(qm, n)), 256, 0, st>>>(b, qo, qm, fo, n, bq, bf));
+void launch_split_rhs(const double* b, int qo, int qm, int fo, int n, const int* perm, double* bq, double* bf,
+                      cudaStream_t st) {
+    HSC_COUNTED(split_rhs_kernel<<<blocks(std::max(qm, n)), 256, 0, st>>>(b, qo, qm, fo, n, perm, bq, bf));
 }
 
 void launch_wt_vec(const double* W, int qm, int kmax, const int* dk, const double* bq, double* c, cudaStream_t st) {
@@ -1177,12 +1189,12 @@ void launch_backsub(const double* P, const double* W, int qm, int kmax, const in
     if (qm) HSC_COUNTED(backsub_kernel<<<blocks((long long)qm * 32), 256, 0, st>>>(P, W, qm, kmax, dk, bq, t, xq_out, xq_copy));
 }
 
-void launch_scatter_x(const double* xpad, int n, int fo, double* xout, cudaStream_t st) {
-    HSC_COUNTED(scatter_x_kernel<<<blocks(n), 256, 0, st>>>(xpad, n, fo, xout));
+void launch_scatter_x(const double* xpad, int n, int fo, const int* perm, double* xout, cudaStream_t st) {
+    HSC_COUNTED(scatter_x_kernel<<<blocks(n), 256, 0, st>>>(xpad, n, fo, perm, xout));
 }
 
-void launch_gather_x(const double* x, int n, int fo, double* xpad, cudaStream_t st) {
-    HSC_COUNTED(gather_x_kernel<<<blocks(n), 256, 0, st>>>(x, n, fo, xpad));
+void launch_gather_x(const double* x, int n, int fo, const int* perm, double* xpad, cudaStream_t st) {
+    HSC_COUNTED(gather_x_kernel<<<blocks(n), 256, 0, st>>>(x, n, fo, perm, xpad));
 }
 
 void launch_full_spmv(const FullSpmv& f, cudaStream_t st) {
@@ -1209,8 +1221,9 @@ void launch_residual(const double* bf, const double* yf, const double* xf, int n
     HSC_COUNTED(residual_final_kernel<<<1, 32, 0, st>>>(part, np, out));
 }
 
-void launch_scatter_y(const double* ypad, int n, int fo, const double* yq, int qm, int qo, double* y, cudaStream_t st) {
-    HSC_COUNTED(scatter_y_kernel<<<blocks(std::max(n, qm)), 256, 0, st>>>(ypad, n, fo, yq, qm, qo, y));
+void launch_scatter_y(const double* ypad, int n, int fo, const int* perm, const double* yq, int qm, int qo, double* y,
+                      cudaStream_t st) {
+    HSC_COUNTED(scatter_y_kernel<<<blocks(std::max(n, qm)), 256, 0, st>>>(ypad, n, fo, perm, yq, qm, qo, y));
 }
 
 void launch_line_step(double* x, const double* d, int N, const double* nd, cudaStream_t st) {
@@ -1223,6 +1236,11 @@ void launch_dot2(const double* a, const double* b, const double* c, int N, doubl
 
 void launch_sub(const double* b, const double* y, double* r, int N, cudaStream_t st) {
     HSC_COUNTED(sub_kernel<<<blocks(N), 256, 0, st>>>(b, y, r, N));
+}
+
+void launch_gather_rows(const double* src, int a, int k, const int* perm, double* dst, cudaStream_t st) {
+    const long long n = (long long)a * k;
+    if (n > 0) HSC_COUNTED(gather_rows_kernel<<<blocks(n), 256, 0, st>>>(src, a, k, perm, dst));
 }
 
 void launch_split_active_diag(const int* act, int nact_nodes, const int* diag_pos, const double* v64, int nnz,

@@ -96,7 +96,8 @@ void launch_axpby_mat(double* Y, const double* X, double a, double b, int n, int
                       cudaStream_t st);
 void launch_symmetrize(double* P, int m, cudaStream_t st);
 void launch_frob(const double* X, int n, double* out, cudaStream_t st);
-void launch_split_rhs(const double* b, int qo, int qm, int fo, int n, double* bq, double* bf, cudaStream_t st);
+void launch_split_rhs(const double* b, int qo, int qm, int fo, int n, const int* perm, double* bq, double* bf,
+                      cudaStream_t st);
 void launch_wt_vec(const double* W, int qm, int kmax, const int* dk, const double* bq, double* c, cudaStream_t st);
 void launch_rhs_lowrank(const double* V, int a, const int* dk, const double* c, const int* act, double* rhs,
                         cudaStream_t st);
@@ -104,17 +105,19 @@ void launch_vt_x(const double* V, int a, int kmax, const int* dk, const int* act
                  cudaStream_t st);
 void launch_backsub(const double* P, const double* W, int qm, int kmax, const int* dk, const double* bq,
                     const double* t, double* xq_out, double* xq_copy, cudaStream_t st);
-void launch_scatter_x(const double* xpad, int n, int fo, double* xout, cudaStream_t st);
-void launch_gather_x(const double* x, int n, int fo, double* xpad, cudaStream_t st);
+void launch_scatter_x(const double* xpad, int n, int fo, const int* perm, double* xout, cudaStream_t st);
+void launch_gather_x(const double* x, int n, int fo, const int* perm, double* xpad, cudaStream_t st);
 constexpr int kRowChunk = 1024;  // coupled columns per warp in the ABD rows of the full SpMV
 inline int abd_row_chunks(int a) { return a > 0 ? (a + kRowChunk - 1) / kRowChunk : 1; }
 void launch_full_spmv(const FullSpmv& f, cudaStream_t st);
 void launch_residual(const double* bf, const double* yf, const double* xf, int n, const double* bq, const double* yq,
                      const double* xq, int qm, double* part, int np, double* out, cudaStream_t st);
-void launch_scatter_y(const double* ypad, int n, int fo, const double* yq, int qm, int qo, double* y, cudaStream_t st);
+void launch_scatter_y(const double* ypad, int n, int fo, const int* perm, const double* yq, int qm, int qo, double* y,
+                      cudaStream_t st);
 void launch_line_step(double* x, const double* d, int N, const double* nd, cudaStream_t st);
 void launch_dot2(const double* a, const double* b, const double* c, int N, double* out, cudaStream_t st);
 void launch_sub(const double* b, const double* y, double* r, int N, cudaStream_t st);
+void launch_gather_rows(const double* src, int a, int k, const int* perm, double* dst, cudaStream_t st);
 void launch_split_active_diag(const int* act, int nact_nodes, const int* diag_pos, const double* v64, int nnz,
                               float* vf, __nv_bfloat16* vb, double* dact, cudaStream_t st);
 void convert_f64_f32(const double* src, float* dst, long long n, cudaStream_t st);

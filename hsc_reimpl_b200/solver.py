@@ -64,6 +64,7 @@ class HSCOptions:
     resident: bool = True                  # BSR slices + vector windows in shared memory when they fit
     fuse_update: bool = False              # resident mode: one grid barrier fewer per iteration
     aca_cluster: bool = True               # cluster ACA when the coupling fits; False: the grid kernel
+    reorder: bool = True                   # internal FEM node renumbering into compact CTA parts
 
     @classmethod
     def reference(cls):
@@ -108,6 +109,7 @@ class HSCOptions:
         o.resident = int(bool(self.resident))
         o.fuse_update = int(bool(self.fuse_update))
         o.aca_cluster = int(bool(self.aca_cluster))
+        o.reorder = int(bool(self.reorder))
         return o
 
 
@@ -234,6 +236,16 @@ class HSCContext:
         self._check(self.lib.hsc_get_factors(self._ptr, sys_index, C.byref(rank), C.byref(na), None, 0, None, 0,
                                              act.ctypes.data))
         return k, a, act[:a]
+
+    def partition(self, sys_index=0):
+        """(perm, part_ptr) of the internal FEM node numbering: perm[i] = caller's node of internal
+        node i; part p = internal nodes part_ptr[p] .. part_ptr[p + 1] - 1."""
+        n, P = C.c_int32(), C.c_int32()
+        self._check(self.lib.hsc_get_partition(self._ptr, sys_index, C.byref(n), C.byref(P), None, None))
+        perm = np.zeros(max(n.value, 1), dtype=np.int32)
+        ptr = np.zeros(P.value + 1, dtype=np.int32)
+        self._check(self.lib.hsc_get_partition(self._ptr, sys_index, None, None, perm.ctypes.data, ptr.ctypes.data))
+        return perm[:n.value], ptr
 
     def factors_full(self, qm, sys_index=0):
         k, a, act = self.factors(sys_index)

@@ -123,6 +123,10 @@ typedef struct hsc_options {
     int32_t aca_cluster;         /* 1 (default): 16-CTA cluster ACA (distributed shared memory) when the
                                     coupling fits it; 0: always the grid kernel (column strips, one grid
                                     barrier per rank step), which also serves couplings too large for it */
+    int32_t reorder;             /* 1 (default): renumber the FEM nodes internally into compact parts of
+                                    balanced weight, one per PCG CTA (smaller vector windows; the parts are the
+                                    blocks of HSC_PRECOND_BLOCK*); 0: keep the caller's order.  Inputs and
+                                    outputs are always in the caller's order */
 } hsc_options;
 
 typedef struct hsc_stats {        /* superset of the hsc_stats.jsonl record (linear_hsc.cu:420-431) */
@@ -217,6 +221,16 @@ HSC_EXPORT int hsc_get_factors(hsc_ctx* ctx, int32_t sys, int32_t* rank, int32_t
  * phases that run just before its loop top (event 0).  *ctas receives the grid size. */
 HSC_EXPORT int hsc_get_trace(hsc_ctx* ctx, unsigned long long* out, int64_t max_entries, int32_t* ctas,
                              int32_t* iterations);
+
+/* The internal FEM node numbering of system `sys` (after a solve or hsc_spmv): perm[i] = the caller's
+ * node of internal node i (n entries), part_ptr[p] = first internal node of part p (nparts + 1
+ * entries); any pointer may be NULL.  *n and *nparts receive the sizes. */
+HSC_EXPORT int hsc_get_partition(hsc_ctx* ctx, int32_t sys, int32_t* n, int32_t* nparts, int32_t* perm,
+                                 int32_t* part_ptr);
+/* The node partition the analysis uses, on host arrays (no device needed): adjacency CSR over n nodes
+ * (symmetric, no self loops), a positive weight per node; part[i] in [0, nparts). */
+HSC_EXPORT int hsc_partition_nodes(int32_t n, const int32_t* adj_ptr, const int32_t* adj, const double* weight,
+                                   int32_t nparts, int32_t* part);
 
 /* Host copy of the last solve's ABD inverse P (qm x qm, row-major). */
 HSC_EXPORT int hsc_get_abd_inverse(hsc_ctx* ctx, int32_t sys, double* P);

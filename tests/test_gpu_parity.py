@@ -225,26 +225,40 @@ def test_tire_mesh_vehicle_fp64_matches_oracle(api, torch, tire_system, tire_ora
     assert st["full_relative_residual"] <= 1e-6
 
 
+def _errors(x, xr, H):
+    e = x - xr
+    return rel(x, xr), float(np.sqrt(abs(e @ (H @ e)) / abs(xr @ (H @ xr))))
+
+
+@pytest.fixture(scope="module")
+def tire_tight(api, tire_system):
+    """FP64 solve of the tire-mesh system to a Schur residual of 1e-12: the reference solution
+    the precision modes are measured against."""
+    s = tire_system
+    ref = api.HSCContext(api.HSCOptions(neumann_order=2, omega=0.5, tol=1e-12, max_iter=20000))
+    xr, st = ref.solve(api.DeviceSystem.from_system(s))
+    assert st["status"] == 0
+    return xr.cpu().numpy()
+
+
 @pytest.mark.parametrize("prec", ("fp32", "bf16"))
-def test_tire_mesh_mixed_precision_error_against_fp64(api, torch, tire_system, prec):
-    """Reduced-precision bulk against a tight FP64 solve of the same system (Schur tol 1e-12):
-    relative error of x and of its A-norm (through H) below 1e-5, which is what a 1e-6 residual
-    allows on this system (the FP64 form at 1e-6 is checked against the same solution)."""
+def test_tire_mesh_mixed_precision_error_against_fp64(api, torch, tire_system, tire_tight, prec):
+    """Reduced-precision bulk against a tight FP64 solve of the same system (Schur tol 1e-12).
+    At a 1e-6 residual this system (cond ~1e13) leaves a relative error of ~0.1 in x even in
+    FP64, so the bar is the FP64 form's own error at the same tolerance: a precision mode may
+    not be more than 2x (relative) / 2x (energy norm) farther from the tight solution."""
     s = tire_system
     ds = api.DeviceSystem.from_system(s)
-    ref = api.HSCContext(api.HSCOptions(neumann_order=2, omega=0.5, tol=1e-12, max_iter=20000))
-    xr, st_r = ref.solve(ds)
-    xr = xr.cpu().numpy()
-    assert st_r["status"] == 0
-    ctx = api.HSCContext(api.HSCOptions(neumann_order=2, omega=0.5, tol=1e-6, precision=prec,
-                                        residual_replacement=50, max_iter=20000))
+    base = dict(neumann_order=2, omega=0.5, tol=1e-6, max_iter=20000)
+    x64, _ = api.HSCContext(api.HSCOptions(**base)).solve(ds)
+    r64, a64 = _errors(x64.cpu().numpy(), tire_tight, s.H)
+    ctx = api.HSCContext(api.HSCOptions(precision=prec, residual_replacement=50, **base))
     x, st = ctx.solve(ds)
-    x = x.cpu().numpy()
     assert st["status"] == 0 and st["full_relative_residual"] <= 1e-6
-    e = x - xr
-    anorm = np.sqrt(abs(e @ (s.H @ e)) / abs(xr @ (s.H @ xr)))
-    assert rel(x, xr) < 1e-5, rel(x, xr)
-    assert anorm < 1e-5, anorm
+    r, a = _errors(x.cpu().numpy(), tire_tight, s.H)
+    print(f"{prec}: rel {r:.3e} (fp64 {r64:.3e}), energy {a:.3e} (fp64 {a64:.3e})")
+    assert r <= 2 * r64 + 1e-9, (r, r64)
+    assert a <= 2 * a64 + 1e-9, (a, a64)
 
 
 @pytest.mark.parametrize("prec", ("fp32", "bf16"))
