@@ -30,6 +30,7 @@ STATUS_NAMES = {0: "ok", 1: "invalid", 2: "nonspd", 3: "breakdown", 4: "noconv",
 HSC_FP64, HSC_FP32, HSC_BF16 = 0, 1, 2
 HSC_ABD_NEUMANN, HSC_ABD_ADAPTIVE, HSC_ABD_EXACT = 0, 1, 2
 HSC_PRECOND_NEUMANN, HSC_PRECOND_POLY, HSC_PRECOND_SCHUR_POLY, HSC_PRECOND_LEARNED = 0, 1, 2, 3
+HSC_PRECOND_BLOCK, HSC_PRECOND_BLOCK_LEARNED = 4, 5
 HSC_MAX_POLY = 16
 HSC_FEATURES, HSC_MLP_HIDDEN, HSC_MLP_OUT, HSC_MLP_PARAMS = 16, 64, 8, 5768
 

@@ -18,11 +18,13 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <functional>
 #include <thread>
 #include <unordered_set>
 #include <vector>
 
 #include "../../include/hsc_c_api.h"
+#include "hsc_block.cuh"
 #include "hsc_learned.cuh"
 #include "hsc_partition.h"
 #include "hsc_setup.cuh"
@@ -95,6 +97,12 @@ struct System {
     std::vector<int> h_perm, h_iperm, h_part_ptr, h_actp, h_actperm;  // node renumbering, parts, PCG-order active dofs
     bool reordered = false;
     std::vector<int> h_node_body;   // (active node in the caller's order, body) of every coupling block
+    // block-local Woodbury preconditioner (hsc_block.cu)
+    DevBuf blk_Y, blk_Yact, blk_Vc, blk_pG, blk_G, blk_K, blk_Ka, blk_Kb, blk_pY, blk_pV, blk_pX, blk_pdot, blk_mpub,
+        blk_xpub, blk_colof, blk_colptr, blk_cols, blk_bad, blk_C, blk_cta_comp_ptr, blk_cta_comp, blk_cta_comp_slot,
+        blk_comp_slot_ptr, blk_comp_of_body, blk_ident;
+    BlockPlan blk{};
+    int blk_nact_cta = 0;
     // plan
     DevBuf rowptr, colidx, rowid, src, diag_pos, qq, qf, act, ident, rowflag, perm, actp, actperm;
     // numeric
@@ -142,6 +150,7 @@ struct hsc_ctx {
     DevBuf mlp, feat_part;     // learned model (BF16 parameters), feature partials
     bool has_model = false;
     cudaEvent_t ev[9] = {};
+    cudaEvent_t ev_blk = nullptr;  // end of the block preconditioner's setup (Y, K) inside the PCG stage
     bool stage_events = false;  // record the per-stage events (single system, no graph)
     // graph cache (batch)
     cudaGraphExec_t gexec = nullptr;
@@ -186,12 +195,16 @@ int validate_options(const hsc_options* o, std::string& why) {
     if (!(o->tol >= 0)) { why = "tol must be >= 0"; return 0; }
     if (o->precision < 0 || o->precision > 2) { why = "unknown precision"; return 0; }
     if (o->abd_inverse < 0 || o->abd_inverse > 2) { why = "unknown abd_inverse"; return 0; }
-    if (o->preconditioner < HSC_PRECOND_NEUMANN || o->preconditioner > HSC_PRECOND_LEARNED) {
+    if (o->preconditioner < HSC_PRECOND_NEUMANN || o->preconditioner > HSC_PRECOND_BLOCK_LEARNED) {
         why = "unknown preconditioner";
         return 0;
     }
     if ((o->preconditioner == HSC_PRECOND_POLY || o->preconditioner == HSC_PRECOND_SCHUR_POLY) &&
         (o->poly_degree < 1 || o->poly_degree > HSC_MAX_POLY)) {
+        why = "poly_degree must be in [1, 16]";
+        return 0;
+    }
+    if (o->preconditioner == HSC_PRECOND_BLOCK && (o->poly_degree < 0 || o->poly_degree > HSC_MAX_POLY)) {
         why = "poly_degree must be in [1, 16]";
         return 0;
     }
@@ -625,6 +638,8 @@ int numeric_post(hsc_ctx* ctx, System& S, cudaStream_t st, bool allow_sync) {
         // C = U^T W (k x k, ld kmax)
         gemm(S.U.as<double>(), S.qm, 0, S.W.as<double>(), S.kmax, 0, S.C.as<double>(), S.kmax, S.kmax, S.kmax, S.qm,
              1.0, 0.0, st, dk, dk, nullptr);
+        if (ctx->block_layout && S.blk_C.p)  // the block preconditioner's operator needs C itself
+            CK(cudaMemcpyAsync(S.blk_C.p, S.C.p, sizeof(double) * S.kmax * S.kmax, cudaMemcpyDeviceToDevice, st));
         launch_ldlt(S.C.as<double>(), S.kmax, dk, S.Lc.as<double>(), S.dpiv.as<double>(), &ds->bad_ldlt, st);
         // Vt^T (k x a row-major == Vt column-major a x k) = Lc^T V^T
         CK(cudaMemsetAsync(S.vt64.p, 0, sizeof(double) * S.a * S.kmax, st));
@@ -1051,6 +1066,211 @@ int launch_pcg_all(hsc_ctx* ctx, int nsys, cudaStream_t st) {
     return HSC_OK;
 }
 
+// ---------------------------------------------------------------------------
+// block-local Woodbury preconditioner: the static plan (coupling components,
+// their contributor CTAs, shared-memory layout) after build_partition laid the
+// CTAs on the analysis' parts, and the per-solve launches
+// ---------------------------------------------------------------------------
+int build_block_plan(hsc_ctx* ctx, System& S, cudaStream_t st) {
+    const hsc_options& o = ctx->opt;
+    if (!ctx->resident || ctx->grid < 1) return fail(ctx, HSC_ERR_INVALID, "the block preconditioner needs the resident CTA windows");
+    const int G = ctx->grid;
+    // cta rows / coupled ranges as build_partition placed them
+    std::vector<int> cta_row(2 * G), cta_act(2 * G), cta_aidx(G), win_off(G + 1);
+    CK(cudaMemcpyAsync(cta_row.data(), ctx->d_cta_row.p, sizeof(int) * 2 * G, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(cta_act.data(), ctx->d_cta_act.p, sizeof(int) * 2 * G, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(cta_aidx.data(), ctx->d_cta_aidx.p, sizeof(int) * G, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(win_off.data(), ctx->d_win_off.p, sizeof(int) * (G + 1), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // coupling components: bodies joined through the FEM nodes they share (union-find)
+    const int nbody = S.qm / 12;
+    std::vector<int> root(std::max(1, nbody));
+    for (int b = 0; b < nbody; ++b) root[b] = b;
+    std::function<int(int)> find = [&](int b) { while (root[b] != b) { root[b] = root[root[b]]; b = root[b]; } return b; };
+    const int nact_nodes = S.a / 3;
+    std::vector<int> node_first_body(std::max(1, nact_nodes), -1);
+    for (size_t e = 0; e < S.h_node_body.size(); e += 2) {
+        const int an = S.h_node_body[e], b = S.h_node_body[e + 1];
+        if (node_first_body[an] < 0) node_first_body[an] = b;
+        else {
+            const int ra = find(node_first_body[an]), rb = find(b);
+            if (ra != rb) root[std::max(ra, rb)] = std::min(ra, rb);
+        }
+    }
+    std::vector<int> comp_of_body(std::max(1, nbody), 0);
+    std::vector<int> comp_id(std::max(1, nbody), -1);
+    int ncomp = 0;
+    for (int b = 0; b < nbody; ++b) {
+        const int r = find(b);
+        if (comp_id[r] < 0) comp_id[r] = ncomp++;
+        comp_of_body[b] = comp_id[r];
+    }
+    if (ncomp > 256) return fail(ctx, HSC_ERR_INVALID, "the block preconditioner supports at most 256 coupling components");
+    // per CTA: the components of its coupled nodes (actp order), and each component's contributor CTAs
+    std::vector<std::vector<int>> comps(G);
+    for (int c = 0; c < G; ++c) {
+        std::vector<int> cs;
+        for (int i = cta_act[2 * c]; i < cta_act[2 * c + 1]; i += 3) {
+            const int b = node_first_body[S.h_actperm[i] / 3];
+            if (b >= 0) cs.push_back(comp_of_body[b]);
+        }
+        std::sort(cs.begin(), cs.end());
+        cs.erase(std::unique(cs.begin(), cs.end()), cs.end());
+        comps[c] = cs;
+    }
+    std::vector<int> comp_slot_ptr(ncomp + 1, 0);
+    for (int c = 0; c < G; ++c)
+        for (int g : comps[c]) comp_slot_ptr[g + 1]++;
+    for (int g = 0; g < ncomp; ++g) comp_slot_ptr[g + 1] += comp_slot_ptr[g];
+    std::vector<int> fill(comp_slot_ptr.begin(), comp_slot_ptr.end() - 1);
+    std::vector<int> cta_comp_ptr(G + 1, 0), cta_comp, cta_comp_slot;
+    for (int c = 0; c < G; ++c) {
+        for (int g : comps[c]) { cta_comp.push_back(g); cta_comp_slot.push_back(fill[g]++); }
+        cta_comp_ptr[c + 1] = (int)cta_comp.size();
+    }
+    const int nslot = comp_slot_ptr[ncomp];
+    // columns a component can hold: 12 per body, 3 per coupled node, the rank cap
+    std::vector<int> comp_bodies(ncomp, 0), comp_nodes(ncomp, 0), comp_cap(ncomp, 0);
+    for (int b = 0; b < nbody; ++b) comp_bodies[comp_of_body[b]]++;
+    for (int an = 0; an < nact_nodes; ++an)
+        if (node_first_body[an] >= 0) comp_nodes[comp_of_body[node_first_body[an]]]++;
+    for (int g = 0; g < ncomp; ++g) comp_cap[g] = std::min(std::min(12 * comp_bodies[g], 3 * comp_nodes[g]), S.kmax);
+    int NCOL = 1;
+    for (int c = 0; c < G; ++c) {
+        int nc = 0;
+        for (int g : comps[c]) nc += comp_cap[g];
+        NCOL = std::max(NCOL, std::min(nc, std::max(1, S.kmax)));
+    }
+    int nact_cta = 0;
+    for (int c = 0; c < G; ++c) nact_cta += cta_aidx[c] >= 0;
+    // maxima for the shared-memory layout
+    int R = 1, BLK = 1, W = 1, NA = 1;
+    for (int c = 0; c < G; ++c) {
+        const int rb = cta_row[2 * c], re = cta_row[2 * c + 1];
+        R = std::max(R, re - rb);
+        BLK = std::max(BLK, S.h_rowptr[re] - S.h_rowptr[rb]);
+        W = std::max(W, win_off[c + 1] - win_off[c]);
+        NA = std::max(NA, cta_act[2 * c + 1] - cta_act[2 * c]);
+    }
+    const int km = std::max(1, S.kmax);
+    const size_t n4 = 4 * (size_t)std::max(1, S.n);
+    GROW(S.blk_Y, sizeof(float) * km * n4);
+    GROW(S.blk_Yact, sizeof(double) * std::max(1, S.a) * km);
+    GROW(S.blk_Vc, sizeof(double) * std::max(1, S.a) * km);
+    GROW(S.blk_pG, sizeof(double) * std::max(1, nact_cta) * km * km);
+    GROW(S.blk_G, sizeof(double) * km * km);
+    GROW(S.blk_K, sizeof(double) * km * km);
+    GROW(S.blk_Ka, sizeof(double) * km * km);
+    GROW(S.blk_Kb, sizeof(double) * km * km);
+    GROW(S.blk_C, sizeof(double) * km * km);
+    GROW(S.blk_pY, sizeof(double) * std::max(1, nslot) * km);
+    GROW(S.blk_pV, sizeof(double) * std::max(1, nslot) * km);
+    GROW(S.blk_pX, sizeof(double) * std::max(1, nslot) * km);
+    GROW(S.blk_pdot, sizeof(double) * 4 * G);
+    GROW(S.blk_mpub, sizeof(double) * n4);
+    GROW(S.blk_xpub, sizeof(double) * n4);
+    GROW(S.blk_colof, sizeof(int) * km);
+    GROW(S.blk_colptr, sizeof(int) * (ncomp + 1));
+    GROW(S.blk_cols, sizeof(int) * km);
+    GROW(S.blk_bad, sizeof(int) * 4);
+    GROW(S.blk_cta_comp_ptr, sizeof(int) * (G + 1));
+    GROW(S.blk_cta_comp, sizeof(int) * std::max<size_t>(1, cta_comp.size()));
+    GROW(S.blk_cta_comp_slot, sizeof(int) * std::max<size_t>(1, cta_comp_slot.size()));
+    GROW(S.blk_comp_slot_ptr, sizeof(int) * (ncomp + 1));
+    GROW(S.blk_comp_of_body, sizeof(int) * std::max(1, nbody));
+    if (S.blk_ident.cap < sizeof(double) * km * km) {
+        GROW(S.blk_ident, sizeof(double) * km * km);
+        std::vector<double> I((size_t)km * km, 0.0);
+        for (int i = 0; i < km; ++i) I[(size_t)i * km + i] = 1.0;
+        CK(cudaMemcpyAsync(S.blk_ident.p, I.data(), sizeof(double) * I.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    CK(cudaMemcpyAsync(S.blk_cta_comp_ptr.p, cta_comp_ptr.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice, st));
+    if (!cta_comp.empty()) {
+        CK(cudaMemcpyAsync(S.blk_cta_comp.p, cta_comp.data(), sizeof(int) * cta_comp.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(S.blk_cta_comp_slot.p, cta_comp_slot.data(), sizeof(int) * cta_comp_slot.size(),
+                           cudaMemcpyHostToDevice, st));
+    }
+    CK(cudaMemcpyAsync(S.blk_comp_slot_ptr.p, comp_slot_ptr.data(), sizeof(int) * (ncomp + 1), cudaMemcpyHostToDevice, st));
+    if (nbody)
+        CK(cudaMemcpyAsync(S.blk_comp_of_body.p, comp_of_body.data(), sizeof(int) * nbody, cudaMemcpyHostToDevice, st));
+    BlockPlan& b = S.blk;
+    b = BlockPlan{};
+    b.n = S.n; b.nnz = S.nnz; b.a = S.a; b.kmax = km; b.qm = S.qm;
+    b.rank = &S.scal.as<DevScal>()->rank;
+    b.rowptr = S.rowptr.as<int>(); b.colidx = S.colidx.as<int>();
+    b.vals = o.precision ? S.vf32.p : S.v64.p;
+    b.dinv = S.dinv.p;
+    b.dact = o.precision ? S.dact.as<double>() : nullptr;
+    b.rowflag = S.rowflag.as<int>(); b.actp = S.actp.as<int>(); b.actperm = S.actperm.as<int>();
+    b.V = S.V.as<double>(); b.C = S.blk_C.as<double>(); b.Lc = S.Lc.as<double>(); b.dpiv = S.dpiv.as<double>();
+    b.U = S.U.as<double>();
+    b.K = S.blk_K.as<double>(); b.Ka = S.blk_Ka.as<double>(); b.Kb = S.blk_Kb.as<double>();
+    b.Y = S.blk_Y.as<float>(); b.Yact = S.blk_Yact.as<double>(); b.Vc = S.blk_Vc.as<double>();
+    b.pG = S.blk_pG.as<double>(); b.G = S.blk_G.as<double>();
+    b.bad = S.blk_bad.as<int>();
+    b.ident = S.blk_ident.as<double>();
+    b.G_ctas = G;
+    b.cta_row = ctx->d_cta_row.as<int>(); b.cta_act = ctx->d_cta_act.as<int>(); b.cta_aidx = ctx->d_cta_aidx.as<int>();
+    b.win_off = ctx->d_win_off.as<int>(); b.win_nodes = ctx->d_win_nodes.as<int>(); b.win_own = ctx->d_win_own.as<int>();
+    b.lcol = S.lcol.as<unsigned short>();
+    b.ncomp = ncomp;
+    b.comp_of_body = S.blk_comp_of_body.as<int>();
+    b.cta_comp_ptr = S.blk_cta_comp_ptr.as<int>(); b.cta_comp = S.blk_cta_comp.as<int>();
+    b.cta_comp_slot = S.blk_cta_comp_slot.as<int>(); b.comp_slot_ptr = S.blk_comp_slot_ptr.as<int>();
+    b.nslot = nslot;
+    b.comp_of_col = S.blk_colof.as<int>(); b.comp_col_ptr = S.blk_colptr.as<int>(); b.comp_cols = S.blk_cols.as<int>();
+    b.x = S.x.as<double>(); b.rhs = S.bf.as<double>(); b.mpub = S.blk_mpub.as<double>(); b.xpub = S.blk_xpub.as<double>();
+    b.pY = S.blk_pY.as<double>(); b.pV = S.blk_pV.as<double>(); b.pX = S.blk_pX.as<double>(); b.pdot = S.blk_pdot.as<double>();
+    b.bar = ctx->d_bar.as<GridBar>();
+    b.out = S.scal.as<DevScal>()->pcg;
+    b.cg_coef = S.cg.as<double>(); b.max_coef = kMaxCoef;
+    b.R = R; b.BLK = BLK; b.W = W; b.NA = NA; b.NCOL = NCOL;
+    // stage the value planes and the Y columns when they fit, the planes first
+    const size_t cap = (size_t)block_max_smem();
+    if (block_smem_bytes(o.precision, b, true, true) > cap && block_smem_bytes(o.precision, b, true, false) > cap)
+        block_smem_bytes(o.precision, b, false, false);
+    if (std::max(b.smem, b.smem_y) > cap)
+        return fail(ctx, HSC_ERR_INVALID, "a part of the block preconditioner does not fit one CTA's shared memory");
+    S.blk_nact_cta = nact_cta;
+    return HSC_OK;
+}
+
+// numeric part of the block form: component columns, Y = L V, the Woodbury core K, the PCG
+int launch_block_solve(hsc_ctx* ctx, System& S, cudaStream_t st) {
+    const hsc_options& o = ctx->opt;
+    BlockPlan& b = S.blk;
+    const bool learned = o.preconditioner == HSC_PRECOND_BLOCK_LEARNED;
+    if (learned) {
+        b.nterms = kPolyOut;
+        b.wdev = S.scal.as<DevScal>()->wl;
+        for (int k = 0; k < kPolyOut; ++k) b.w[k] = 1.0;
+    } else {
+        b.wdev = nullptr;
+        b.nterms = o.poly_degree > 0 ? o.poly_degree : o.neumann_order;
+        for (int k = 0; k < b.nterms; ++k) b.w[k] = o.poly_degree > 0 ? o.poly_weights[k] : 1.0;
+    }
+    b.omega = o.omega;
+    b.tol = o.tol;
+    b.max_iter = o.max_iter;
+    b.rr_every = o.residual_replacement;
+    b.spin_limit = o.spin_limit;
+    // grid barriers: two per iteration, two more per true-residual check
+    if ((double)(o.max_iter + 4) * 4 * b.G_ctas >= (double)kBarAbortBit)
+        return fail(ctx, HSC_ERR_INVALID, "max_iter too large for the grid barrier counter");
+    if (S.kmax > 0) {
+        launch_block_columns(b, st);
+        CK(launch_block_y(o.precision, b, st));
+        launch_block_k(b, S.blk_nact_cta, st);
+    } else {
+        CK(cudaMemsetAsync(S.blk_colptr.p, 0, sizeof(int) * (b.ncomp + 1), st));
+    }
+    if (ctx->stage_events) CK(cudaEventRecord(ctx->ev_blk, st));
+    CK(cudaMemsetAsync(ctx->d_bar.p, 0, sizeof(GridBar), st));
+    CK(launch_block_pcg(o.precision, b, st));
+    return HSC_OK;
+}
+
 // extreme Ritz values of the CG Lanczos tridiagonal (bisection on Sturm counts)
 void lanczos_extremes(const double* coef, int m, double& lo, double& hi) {
     lo = hi = 0.0;
@@ -1179,6 +1399,7 @@ int ensure_common(hsc_ctx* ctx, cudaStream_t st) {
     if (!ctx->aca_grid) ctx->aca_grid = std::min(4096, std::max(1, aca_blocks_per_sm()) * ctx->num_sms);
     if (!ctx->ev[0])
         for (auto& e : ctx->ev) CK(cudaEventCreate(&e));
+        CK(cudaEventCreate(&ctx->ev_blk));
     (void)st;
     return HSC_OK;
 }
@@ -1256,9 +1477,10 @@ FeatArgs feat_args(hsc_ctx* ctx, System& S, bool with_model) {
 // sum of the polynomial weights the current options use for system S (q(0))
 double weight_sum(const hsc_options& o, const System& S) {
     double w = 0.0;
-    if (o.preconditioner == HSC_PRECOND_LEARNED)
+    if (o.preconditioner == HSC_PRECOND_LEARNED || o.preconditioner == HSC_PRECOND_BLOCK_LEARNED)
         for (int k = 0; k < kPolyOut; ++k) w += S.h_scal.wl[k];
-    else if (o.preconditioner == HSC_PRECOND_POLY || o.preconditioner == HSC_PRECOND_SCHUR_POLY)
+    else if (o.preconditioner == HSC_PRECOND_POLY || o.preconditioner == HSC_PRECOND_SCHUR_POLY ||
+             (o.preconditioner == HSC_PRECOND_BLOCK && o.poly_degree > 0))
         for (int k = 0; k < o.poly_degree; ++k) w += o.poly_weights[k];
     else
         w = o.neumann_order;
@@ -1403,16 +1625,23 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
         any_new |= re;
         idx[s] = s;
     }
-    if (any_new || ctx->part_key_gen != count) {
+    const bool block = o.preconditioner == HSC_PRECOND_BLOCK || o.preconditioner == HSC_PRECOND_BLOCK_LEARNED;
+    if (block && count != 1) return fail(ctx, HSC_ERR_INVALID, "the block preconditioner solves one system per call");
+    if (any_new || ctx->part_key_gen != 2 * count + (block ? 1 : 0)) {
+        ctx->block_layout = block;
         rc = build_partition(ctx, idx, st);
         if (rc) return rc;
-        ctx->part_key_gen = count;
+        ctx->part_key_gen = 2 * count + (block ? 1 : 0);
         if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+        if (block) {
+            rc = build_block_plan(ctx, ctx->sys[0], st);
+            if (rc) return rc;
+        }
     }
     const bool refine = o.refine_target > 0 && count == 1;
     const bool residual = o.check_residual || refine;
-    const bool learned = o.preconditioner == HSC_PRECOND_LEARNED;
-    if (learned && !ctx->has_model) return fail(ctx, HSC_ERR_INVALID, "HSC_PRECOND_LEARNED without a model (hsc_set_learned_model)");
+    const bool learned = o.preconditioner == HSC_PRECOND_LEARNED || o.preconditioner == HSC_PRECOND_BLOCK_LEARNED;
+    if (learned && !ctx->has_model) return fail(ctx, HSC_ERR_INVALID, "a learned preconditioner without a model (hsc_set_learned_model)");
     // the features of this solve see the record of the previous solve of the same system
     for (int s = 0; s < count; ++s) {
         System& S = ctx->sys[s];
@@ -1447,7 +1676,7 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
         if (learned)
             for (int s = 0; s < count; ++s) CK(launch_features(feat_args(ctx, ctx->sys[s], true), st));
         CK(cudaEventRecord(ctx->ev[5], st));
-        int r3 = launch_pcg_all(ctx, count, st);
+        int r3 = block ? launch_block_solve(ctx, ctx->sys[0], st) : launch_pcg_all(ctx, count, st);
         if (r3) return r3;
         CK(cudaEventRecord(ctx->ev[6], st));
         for (int s = 0; s < count; ++s) {
@@ -1497,6 +1726,10 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
         if (ctx->stage_events)
             for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms_stage[i], ctx->ev[i], ctx->ev[i + 1]);
         ms_stage[5] = ms_pcg;
+        if (block && ctx->stage_events) {  // the block form's Y / K setup, apart from the PCG proper
+            cudaEventElapsedTime(&ms_stage[7], ctx->ev[5], ctx->ev_blk);
+            ms_stage[5] = ms_pcg - ms_stage[7];
+        }
     }
     cudaEventElapsedTime(&ms_total, ctx->ev[0], ctx->ev[8]);
     int total_iters = -1, steps = 1;
@@ -1548,7 +1781,7 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
             if (full <= o.refine_target || steps >= o.max_refinements) break;
             // next direction
             schur_rhs(S, res, st);
-            int r4 = launch_pcg_all(ctx, 1, st);
+            int r4 = block ? launch_block_solve(ctx, S, st) : launch_pcg_all(ctx, 1, st);
             if (r4) return r4;
             back_substitute(S, res, d_x[0], false, st);
             int ga = 0;

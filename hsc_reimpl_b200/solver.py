@@ -53,6 +53,7 @@ class HSCOptions:
     poly_weights: tuple | None = None      # set -> polynomial preconditioner with these weights
     poly_basis: str = "fem"                # "fem": terms on D (HSC_PRECOND_POLY); "schur": on S
     learned: bool = False                  # HSC_PRECOND_LEARNED (needs HSCContext.set_learned_model)
+    block: bool = False                    # HSC_PRECOND_BLOCK (/ _BLOCK_LEARNED with learned=True)
     residual_replacement: int = 0
     refine_target: float = 0.0
     max_refinements: int = 20
@@ -84,7 +85,19 @@ class HSCOptions:
         o.abd_inverse_tol = float(self.abd_inverse_tol)
         o.full_residual_limit = float(self.full_residual_limit)
         o.precision = PRECISIONS[self.precision]
-        if self.learned:
+        if self.block:
+            # block-local polynomial with the exact coupling correction (pipelined PCG)
+            if self.learned:
+                o.preconditioner = _lib.HSC_PRECOND_BLOCK_LEARNED
+            else:
+                o.preconditioner = _lib.HSC_PRECOND_BLOCK
+                w = [] if self.poly_weights is None else [float(v) for v in self.poly_weights]
+                if len(w) > _lib.HSC_MAX_POLY:
+                    raise ValueError("at most 16 polynomial weights")
+                o.poly_degree = len(w)
+                for i, v in enumerate(w):
+                    o.poly_weights[i] = v
+        elif self.learned:
             o.preconditioner = _lib.HSC_PRECOND_LEARNED
         elif self.poly_weights is not None:
             w = [float(v) for v in self.poly_weights]

@@ -75,6 +75,14 @@ extern "C" {
 #define HSC_PRECOND_LEARNED 3    /* 8 weights per system from the context's learned model
                                     (hsc_set_learned_model), computed on the device from the
                                     system's features; falls back to plain Neumann on a stall */
+/* Block-local Woodbury preconditioner (no reference counterpart): z = L r + Y K Y^T r with
+   L = sum_k w_k (I - w Dd^-1 D_loc)^k w Dd^-1, D_loc the blocks of D whose two nodes lie in the same
+   part (one part per PCG CTA, from the analysis' renumbering), Y = L V and K = (C^-1 - V^T Y)^-1, so
+   that M = L^-1 - V C V^T (Woodbury): the coupling's soft modes are handled exactly and the PCG
+   iterates only against the local polynomial's error.  A term needs no grid barrier.  Runs in a
+   pipelined PCG (two grid barriers per iteration); one system per call. */
+#define HSC_PRECOND_BLOCK 4          /* poly_degree caller weights (0: neumann_order unit weights) */
+#define HSC_PRECOND_BLOCK_LEARNED 5  /* 8 weights per system from the learned model (as _LEARNED) */
 
 /* learned model: 16 features -> 64 -> 64 -> 8 positive weights (ReLU, softplus), BF16 parameters,
    flat row-major (out x in): W1[64][16], b1[64], W2[64][64], b2[64], W3[8][64], b3[8] */
@@ -143,7 +151,8 @@ typedef struct hsc_stats {        /* superset of the hsc_stats.jsonl record (lin
     double descent;                   /* b^T x */
     double setup_ms, pcg_ms, total_ms;/* device time between stream events */
     double lanczos_min, lanczos_max;  /* extreme Ritz values of the preconditioned Schur operator */
-    double stage_ms[8];               /* fill+extract, ACA, ABD inverse, reduced core, rhs, PCG, back-sub+residual, unused */
+    double stage_ms[8];               /* fill+extract, ACA, ABD inverse, reduced core, rhs, PCG, back-sub+residual,
+                                         block preconditioner setup (Y = L V, K; the PCG stage excludes it) */
     int64_t nnzb;
 } hsc_stats;
 

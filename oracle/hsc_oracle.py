@@ -21,7 +21,11 @@ It restates, in NumPy/SciPy, the reference's algorithm for the path:
                        true residual each iteration instead);
 * ``hsc_solve``     -- ``linear_hsc.cu:344-406`` / ``core.py:141-168`` plus the
                        quadratic refinement of ``core.py:171-198``;
-* ``direct_solve``  -- the FP64 direct-solve oracle (``scipy.sparse.linalg.splu``).
+* ``direct_solve``  -- the FP64 direct-solve oracle (``scipy.sparse.linalg.splu``);
+* ``hsc_solve_block`` -- this build's fast form (no reference counterpart): the
+                       block-local polynomial preconditioner with the exact Woodbury
+                       correction for the coupling, in a pipelined PCG; its setup is
+                       the reference's (``core.py:141-168``).
 
 Parity pins: ``tests/golden`` holds outputs of the reference's own
 ``core.py`` (generated by ``tests/golden/make_golden.py``); the CPU tests
@@ -411,3 +415,184 @@ def direct_solve(H, b):
     """FP64 direct solve of the full system (splu)."""
     lu = spla.splu(sp.csc_matrix(H))
     return lu.solve(np.asarray(b, dtype=np.float64))
+
+
+# ----------------------------------------------------------------------------
+# Block-local preconditioner with the exact coupling correction, pipelined PCG
+# (this build's fast form; no reference counterpart -- the reference's
+# preconditioner is the global Neumann series above)
+# ----------------------------------------------------------------------------
+def part_of_nodes(perm, part_ptr):
+    """part id of every caller node from the solver's internal numbering (hsc_get_partition)."""
+    perm = np.asarray(perm)
+    out = np.empty(perm.size, dtype=np.int64)
+    for p in range(len(part_ptr) - 1):
+        out[perm[part_ptr[p]:part_ptr[p + 1]]] = p
+    return out
+
+
+def local_block(D, part):
+    """D with only the 3x3 blocks whose row and column nodes share a part."""
+    Db = sp.csr_matrix(D).tobsr(blocksize=(3, 3))
+    Db.sort_indices()
+    n = Db.shape[0] // 3
+    rows = np.repeat(np.arange(n), np.diff(Db.indptr))
+    keep = part[rows] == part[Db.indices]
+    Dl = sp.bsr_matrix((Db.data * keep[:, None, None], Db.indices, Db.indptr), shape=D.shape).tocsr()
+    Dl.eliminate_zeros()
+    return Dl
+
+
+def block_poly_apply(Dl, Dinv, r, weights, omega):
+    """L r = sum_k w_k t_k, t_0 = w Dd^-1 r, t_k = t_{k-1} - w Dd^-1 D_loc t_{k-1}; r may hold columns."""
+    def bd(v):
+        if v.ndim == 1:
+            return block_diag_apply(Dinv, v)
+        n = Dinv.shape[0]
+        return np.einsum("kij,kjc->kic", Dinv, v.reshape(n, 3, -1)).reshape(v.shape)
+    term = omega * bd(r)
+    z = weights[0] * term
+    for k in range(1, len(weights)):
+        term = term - omega * bd(Dl @ term)
+        z = z + weights[k] * term
+    return z
+
+
+def ldlt(C):
+    """C = L diag(d) L^T, L unit lower triangular (no pivoting)."""
+    k = C.shape[0]
+    L = np.eye(k)
+    d = np.zeros(k)
+    A = np.array(C, dtype=np.float64)
+    for j in range(k):
+        d[j] = A[j, j] - (L[j, :j] ** 2) @ d[:j]
+        for i in range(j + 1, k):
+            L[i, j] = (A[i, j] - (L[i, :j] * L[j, :j]) @ d[:j]) / d[j]
+    return L, d
+
+
+class BlockWoodbury:
+    """z = L r + Y K Y^T r with L the block-local polynomial, Y = L V (V embedded at the
+    active FEM dofs) and K = (C^-1 - V^T Y)^-1, formed as L_c (diag(1/d) - L_c^T G L_c)^-1 L_c^T
+    from C = L_c diag(d) L_c^T, G = V^T Y.  With L = D^-1 this is S^-1 exactly (Woodbury), so
+    the PCG iterates only against the error of the local polynomial.  Y is rounded to FP32, as
+    the device applies it.  A failed Cholesky of K^-1 leaves z = L r."""
+
+    def __init__(self, orc, part, weights, omega):
+        self.Dl = local_block(orc.D, part)
+        self.Dinv = orc.Dinv
+        self.w = np.asarray(weights, dtype=np.float64)
+        self.omega = omega
+        N = orc.D.shape[0]
+        k = orc.rank
+        self.K = np.zeros((k, k))
+        self.Y = np.zeros((N, k))
+        self.spd = True
+        if k:
+            Vf = np.zeros((N, k))
+            Vf[orc.active] = orc.V
+            self.Y = block_poly_apply(self.Dl, self.Dinv, Vf, self.w, omega).astype(np.float32).astype(np.float64)
+            G = Vf.T @ self.Y
+            G = 0.5 * (G + G.T)
+            Lc, d = ldlt(orc.C)
+            Ki = np.diag(1.0 / d) - Lc.T @ G @ Lc
+            Ki = 0.5 * (Ki + Ki.T)
+            try:
+                Lk = np.linalg.cholesky(Ki)
+                Kt = np.linalg.solve(Lk.T, np.linalg.solve(Lk, np.eye(k)))
+                self.K = Lc @ Kt @ Lc.T
+                self.K = 0.5 * (self.K + self.K.T)
+            except np.linalg.LinAlgError:
+                self.spd = False
+
+    def __call__(self, r):
+        z = block_poly_apply(self.Dl, self.Dinv, r, self.w, self.omega)
+        if self.K.size:
+            z = z + self.Y @ (self.K @ (self.Y.T @ r))
+        return z
+
+
+def pcg_pipelined(matvec, rhs, precond, tol, max_iter, rr_every=0):
+    """Pipelined PCG (Ghysels & Vanroose 2014): one reduction phase per iteration overlaps the
+    preconditioner and the operator product of the next.  Recursive-residual stop test, then one
+    true-residual check; a failed check (or every ``rr_every`` iterations) restarts from the true
+    residual.  Returns (x, stats)."""
+    x = np.zeros_like(rhs)
+    normb = float(np.linalg.norm(rhs))
+    if normb == 0:
+        return x, dict(iterations=0, relative=0.0, converged=True, restarts=0)
+    r = rhs.copy()
+    u = precond(r)
+    w = matvec(u)
+    z = q = s = p = np.zeros_like(rhs)
+    it = restarts = 0
+    alpha_prev = gamma_prev = None
+    rel = 1.0
+    while True:
+        gamma, delta, rr = float(r @ u), float(w @ u), float(r @ r)
+        rel = np.sqrt(rr) / normb
+        replace = rr_every > 0 and it > 0 and it % rr_every == 0 and alpha_prev is not None
+        if rel <= tol or replace or it >= max_iter:
+            rt = rhs - matvec(x)
+            rel = float(np.linalg.norm(rt)) / normb
+            restarts += 1
+            if rel <= tol or it >= max_iter:
+                break
+            r = rt
+            u = precond(r)
+            w = matvec(u)
+            alpha_prev = None
+            continue
+        m = precond(w)
+        nv = matvec(m)
+        if alpha_prev is None:
+            beta = 0.0
+            den = delta
+        else:
+            beta = gamma / gamma_prev
+            den = delta - beta * gamma / alpha_prev
+        if not (np.isfinite(den) and den > 0 and np.isfinite(gamma) and gamma > 0):
+            raise BreakdownError(f"pipelined PCG breakdown at iteration {it}: den={den}, gamma={gamma}")
+        alpha = gamma / den
+        z = nv + beta * z
+        q = m + beta * q
+        s = w + beta * s
+        p = u + beta * p
+        x = x + alpha * p
+        r = r - alpha * s
+        u = u - alpha * q
+        w = w - alpha * z
+        alpha_prev, gamma_prev = alpha, gamma
+        it += 1
+    return x, dict(iterations=it, relative=rel, converged=rel <= tol, restarts=restarts)
+
+
+def hsc_solve_block(H, layout, b, perm, part_ptr, weights, omega, tol=1e-6, max_iter=20000, rr_every=0,
+                    max_rank=128):
+    """The fast form end to end: the reference's setup (ACA, exact ABD inverse, C = U^T P U,
+    Schur rhs), the block-local Woodbury preconditioner over the solver's parts, pipelined PCG,
+    back-substitution.  Returns (x, stats, oracle, preconditioner)."""
+    orc = HSCOracle(H, layout, order=2, omega=omega, tol=tol, max_iter=max_iter, abd_inverse="exact",
+                    max_rank=max_rank)
+    qo, qm, fo, fn = layout
+    part = part_of_nodes(perm, part_ptr)
+    M = BlockWoodbury(orc, part, weights, omega)
+    b = np.asarray(b, dtype=np.float64)
+    bq, bx = b[qo:qo + qm], b[fo:fo + fn]
+    rhs = bx.copy()
+    if orc.rank:
+        c = orc.U.T @ (orc.P @ bq)
+        rhs[orc.active] -= orc.V @ c
+    dx, st = pcg_pipelined(orc.schur, rhs, M, tol, max_iter, rr_every)
+    if orc.rank:
+        dq = orc.P @ (bq - orc.U @ (orc.V.T @ dx[orc.active]))
+    else:
+        dq = orc.P @ bq
+    x = np.zeros_like(b)
+    x[fo:fo + fn] = dx
+    x[qo:qo + qm] = dq
+    bn = float(np.linalg.norm(b))
+    st = dict(st, pcg_iterations=st["iterations"], rank=orc.rank, active_fem_dofs=int(orc.active.size),
+              full_relative_residual=float(np.linalg.norm(b - orc.H @ x) / bn) if bn else 0.0,
+              woodbury_spd=M.spd)
+    return x, st, orc, M
