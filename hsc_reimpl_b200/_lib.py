@@ -62,6 +62,7 @@ class Options(C.Structure):
         ("fuse_update", C.c_int32),
         ("aca_cluster", C.c_int32),
         ("reorder", C.c_int32),
+        ("aca_components", C.c_int32),
     ]
 
 

@@ -16,7 +16,8 @@ CSRC = HERE / "csrc"
 BUILD = CSRC / "_build"
 LIB = HERE / "libhsc_b200.so"
 SOURCES = ["hsc_api.cu", "hsc_setup.cu", "hsc_pcg.cu", "hsc_aca.cu", "hsc_learned.cu", "hsc_assemble.cu", "hsc_coupling.cu",
-           "hsc_noalloc.cu", "hsc_partition.cpp", "hsc_block.cu"]
+           "hsc_noalloc.cu", "hsc_partition.cpp", "hsc_block.cu",
+           "hsc_aca_comp.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",

@@ -97,6 +97,11 @@ struct System {
     std::vector<int> h_perm, h_iperm, h_part_ptr, h_actp, h_actperm;  // node renumbering, parts, PCG-order active dofs
     bool reordered = false;
     std::vector<int> h_node_body;   // (active node in the caller's order, body) of every coupling block
+    bool aca_comp_ok = false;       // the component ACA applies (components of at most 256 rows)
+    int ncomp_coupled = 0;
+    AcaComp acomp{};
+    DevBuf ac_row_ptr, ac_rows, ac_col_ptr, ac_cols, ac_r_off, ac_s_off, ac_u_off, ac_v_off, ac_R, ac_Ug, ac_Vg,
+        ac_piv_abs, ac_piv_idx, ac_sums, ac_nsteps, ac_cur, ac_order, ac_esum;
     // block-local Woodbury preconditioner (hsc_block.cu)
     DevBuf blk_Y, blk_Yact, blk_Vc, blk_pG, blk_G, blk_K, blk_Ka, blk_Kb, blk_pY, blk_pV, blk_pX, blk_pdot, blk_mpub,
         blk_xpub, blk_colof, blk_colptr, blk_cols, blk_bad, blk_C, blk_cta_comp_ptr, blk_cta_comp, blk_cta_comp_slot,
@@ -381,9 +386,89 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
     }
     S.h_node_body.clear();
     for (size_t e = 0; e < qf.size(); e += 4) { S.h_node_body.push_back(qf[e + 2]); S.h_node_body.push_back(qf[e + 1] / 4); }
+    // coupling components for the ACA: bodies joined through the coupled FEM nodes they share
+    // (union-find); E is block diagonal over them (rows of their bodies x columns of their nodes)
+    std::vector<std::vector<int>> comp_rows, comp_cols;
+    {
+        const int nbody = S.qm / 12;
+        std::vector<int> root(std::max(1, nbody));
+        for (int b = 0; b < nbody; ++b) root[b] = b;
+        auto find = [&](int b) { while (root[b] != b) { root[b] = root[root[b]]; b = root[b]; } return b; };
+        std::vector<int> node_body(std::max(1, nact), -1);
+        for (size_t e = 0; e < S.h_node_body.size(); e += 2) {
+            const int an = S.h_node_body[e], b = S.h_node_body[e + 1];
+            if (node_body[an] < 0) node_body[an] = b;
+            else {
+                const int ra = find(node_body[an]), rb = find(b);
+                if (ra != rb) root[std::max(ra, rb)] = std::min(ra, rb);
+            }
+        }
+        std::vector<int> id(std::max(1, nbody), -1);
+        int nc = 0;
+        for (int an = 0; an < nact; ++an)   // in order of each component's first coupled node
+            if (node_body[an] >= 0 && id[find(node_body[an])] < 0) id[find(node_body[an])] = nc++;
+        S.ncomp_coupled = nc;
+        comp_rows.assign(nc, {});
+        comp_cols.assign(nc, {});
+        for (int b = 0; b < nbody; ++b)
+            if (id[find(b)] >= 0)
+                for (int d = 0; d < 12; ++d) comp_rows[id[find(b)]].push_back(12 * b + d);
+        for (int an = 0; an < nact; ++an)
+            if (node_body[an] >= 0)
+                for (int d = 0; d < 3; ++d) comp_cols[id[find(node_body[an])]].push_back(3 * an + d);
+    }
     S.nqq = (int)qq.size() / 3;
     S.nqf = (int)qf.size() / 4;
     S.kmax = std::min(std::min(o.max_rank, L.qm), S.a);
+    // the component ACA's plan
+    S.aca_comp_ok = S.kmax > 0 && S.ncomp_coupled > 0;
+    for (const auto& r : comp_rows) S.aca_comp_ok = S.aca_comp_ok && r.size() <= 256;
+    if (S.aca_comp_ok) {
+        const int ncg = S.ncomp_coupled;
+        std::vector<int> row_ptr(ncg + 1, 0), col_ptr(ncg + 1, 0), rows_all, cols_all, s_off(ncg);
+        std::vector<long long> r_off(ncg), u_off(ncg), v_off(ncg);
+        long long rtot = 0, utot = 0, vtot = 0;
+        int stot = 0;
+        for (int g = 0; g < ncg; ++g) {
+            const int mr = (int)comp_rows[g].size(), ncl = (int)comp_cols[g].size();
+            const int steps = std::min(std::min(mr, ncl), S.kmax);
+            rows_all.insert(rows_all.end(), comp_rows[g].begin(), comp_rows[g].end());
+            cols_all.insert(cols_all.end(), comp_cols[g].begin(), comp_cols[g].end());
+            row_ptr[g + 1] = (int)rows_all.size();
+            col_ptr[g + 1] = (int)cols_all.size();
+            r_off[g] = rtot; rtot += (long long)mr * ncl;
+            u_off[g] = utot; utot += (long long)mr * steps;
+            v_off[g] = vtot; vtot += (long long)ncl * steps;
+            s_off[g] = stot; stot += steps;
+        }
+        GROW(S.ac_row_ptr, sizeof(int) * (ncg + 1));
+        GROW(S.ac_col_ptr, sizeof(int) * (ncg + 1));
+        GROW(S.ac_rows, sizeof(int) * rows_all.size());
+        GROW(S.ac_cols, sizeof(int) * cols_all.size());
+        GROW(S.ac_r_off, sizeof(long long) * ncg);
+        GROW(S.ac_u_off, sizeof(long long) * ncg);
+        GROW(S.ac_v_off, sizeof(long long) * ncg);
+        GROW(S.ac_s_off, sizeof(int) * ncg);
+        GROW(S.ac_R, sizeof(double) * std::max<long long>(1, rtot));
+        GROW(S.ac_Ug, sizeof(double) * std::max<long long>(1, utot));
+        GROW(S.ac_Vg, sizeof(double) * std::max<long long>(1, vtot));
+        GROW(S.ac_piv_abs, sizeof(double) * std::max(1, stot));
+        GROW(S.ac_piv_idx, sizeof(long long) * std::max(1, stot));
+        GROW(S.ac_sums, sizeof(double) * (stot + ncg));
+        GROW(S.ac_nsteps, sizeof(int) * ncg);
+        GROW(S.ac_cur, sizeof(int) * ncg);
+        GROW(S.ac_order, sizeof(int) * 2 * S.kmax);
+        GROW(S.ac_esum, sizeof(double));
+        CK(cudaMemcpyAsync(S.ac_row_ptr.p, row_ptr.data(), sizeof(int) * (ncg + 1), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(S.ac_col_ptr.p, col_ptr.data(), sizeof(int) * (ncg + 1), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(S.ac_rows.p, rows_all.data(), sizeof(int) * rows_all.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(S.ac_cols.p, cols_all.data(), sizeof(int) * cols_all.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(S.ac_r_off.p, r_off.data(), sizeof(long long) * ncg, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(S.ac_u_off.p, u_off.data(), sizeof(long long) * ncg, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(S.ac_v_off.p, v_off.data(), sizeof(long long) * ncg, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(S.ac_s_off.p, s_off.data(), sizeof(int) * ncg, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    }
     // ---- device plans and buffers ----
     const int P = o.precision;
     GROW(S.rowptr, sizeof(int) * (S.n + 1));
@@ -609,6 +694,25 @@ int aca_all(hsc_ctx* ctx, int count, cudaStream_t st) {
         System& S = ctx->sys[s];
         if (S.kmax <= 0 || S.aca_on_cluster) continue;
         DevScal* ds = S.scal.as<DevScal>();
+        if (o.aca_components && S.aca_comp_ok) {
+            AcaComp& c = S.acomp;
+            c.E = S.E.as<double>(); c.qm = S.qm; c.a = S.a; c.kmax = S.kmax;
+            c.rtol = o.aca_rtol > 0 ? o.aca_rtol : 0.0;
+            c.ncomp = S.ncomp_coupled;
+            c.row_ptr = S.ac_row_ptr.as<int>(); c.rows = S.ac_rows.as<int>();
+            c.col_ptr = S.ac_col_ptr.as<int>(); c.cols = S.ac_cols.as<int>();
+            c.r_off = S.ac_r_off.as<long long>(); c.s_off = S.ac_s_off.as<int>();
+            c.u_off = S.ac_u_off.as<long long>(); c.v_off = S.ac_v_off.as<long long>();
+            c.Rscratch = S.ac_R.as<double>(); c.Ug = S.ac_Ug.as<double>(); c.Vg = S.ac_Vg.as<double>();
+            c.piv_abs = S.ac_piv_abs.as<double>(); c.piv_idx = S.ac_piv_idx.as<long long>();
+            c.sums = S.ac_sums.as<double>(); c.nsteps = S.ac_nsteps.as<int>(); c.cur = S.ac_cur.as<int>();
+            c.order = S.ac_order.as<int>(); c.esumsq = S.ac_esum.as<double>();
+            c.smem_doubles = (int)aca_comp_smem_doubles();
+            c.U = S.U.as<double>(); c.V = S.V.as<double>(); c.hist = S.hist.as<double>();
+            c.rank = &ds->rank; c.err = &ds->aca_err;
+            CK(launch_aca_comp(c, st));
+            continue;
+        }
         CK(cudaMemcpyAsync(S.R0.p, S.E.p, sizeof(double) * S.qm * S.a, cudaMemcpyDeviceToDevice, st));
         AcaParams ap{};
         ap.R0 = S.R0.as<double>(); ap.R1 = S.R1.as<double>();
@@ -978,6 +1082,7 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
         System& S = ctx->sys[idx[s2]];
         S.aca_on_cluster = false;
         if (S.kmax <= 0 || !o.aca_cluster || !aca_cluster_fits(S.qm, S.a)) continue;
+        if (o.aca_components && S.aca_comp_ok) continue;  // the component ACA serves it
         const size_t need = aca_cluster_smem_doubles(S.qm, S.a);
         if (ctx->aca_cluster_ok < 0) ctx->aca_cluster_ok = aca_cluster_supported(25600) > 0 ? 1 : 0;
         if (!ctx->aca_cluster_ok) continue;
@@ -1545,6 +1650,7 @@ int hsc_options_default(hsc_options* o) {
     o->fuse_update = 0;
     o->aca_cluster = 1;
     o->reorder = 1;
+    o->aca_components = 1;
     return HSC_OK;
 }
 

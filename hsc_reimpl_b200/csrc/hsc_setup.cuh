@@ -35,6 +35,40 @@ struct AcaSys {
     int* rank;
     double* err;
 };
+// full-pivot ACA by coupling component, merged into the global pivot order (hsc_aca_comp.cu)
+struct AcaComp {
+    const double* E;       // coupling, row-major qm x a
+    int qm, a, kmax;
+    double rtol;
+    int ncomp;             // components with at least one coupled column
+    const int* row_ptr;    // ncomp + 1
+    const int* rows;       // rows of E (12 per body of the component), ascending
+    const int* col_ptr;    // ncomp + 1
+    const int* cols;       // columns of E (the component's coupled dofs), ascending
+    const long long* r_off;// per component: offset of its residual block in Rscratch (when it misses shared memory)
+    const int* s_off;      // per component: offset of its step arrays (piv_abs, piv_idx; sums add g)
+    const long long* u_off;// per component: offset of its u columns in Ug
+    const long long* v_off;// per component: offset of its v columns in Vg
+    double* Rscratch;
+    double* Ug;
+    double* Vg;
+    double* piv_abs;
+    long long* piv_idx;
+    double* sums;          // sum of squares of each component's residual before each step (and after the last)
+    int* nsteps;
+    int* cur;              // merge cursor per component
+    int* order;            // 2 x kmax: (component, step) of each global column
+    double* esumsq;        // |E|_F^2
+    int smem_doubles;
+    double* U;             // qm x kmax column-major
+    double* V;             // a x kmax column-major
+    double* hist;
+    int* rank;
+    double* err;
+};
+size_t aca_comp_smem_doubles();
+cudaError_t launch_aca_comp(const AcaComp& p, cudaStream_t st);
+
 size_t aca_cluster_smem_doubles(int m, int nc);
 bool aca_cluster_fits(int m, int nc);
 cudaError_t launch_aca_cluster(const AcaSys* d_sys, int nsys, size_t smem_doubles, cudaStream_t st);

@@ -66,6 +66,7 @@ class HSCOptions:
     fuse_update: bool = False              # resident mode: one grid barrier fewer per iteration
     aca_cluster: bool = True               # cluster ACA when the coupling fits; False: the grid kernel
     reorder: bool = True                   # internal FEM node renumbering into compact CTA parts
+    aca_components: bool = True            # ACA per coupling component, merged (same factors as global)
 
     @classmethod
     def reference(cls):
@@ -123,6 +124,7 @@ class HSCOptions:
         o.fuse_update = int(bool(self.fuse_update))
         o.aca_cluster = int(bool(self.aca_cluster))
         o.reorder = int(bool(self.reorder))
+        o.aca_components = int(bool(self.aca_components))
         return o
 
 

@@ -135,6 +135,10 @@ typedef struct hsc_options {
                                     balanced weight, one per PCG CTA (smaller vector windows; the parts are the
                                     blocks of HSC_PRECOND_BLOCK*); 0: keep the caller's order.  Inputs and
                                     outputs are always in the caller's order */
+    int32_t aca_components;      /* 1 (default): run the ACA per coupling component (bodies joined through
+                                    shared FEM nodes, on which E is block diagonal), one CTA each, and merge
+                                    the pivot sequences by magnitude: the same pivots, columns and column
+                                    order as the global full-pivot ACA; 0: the global cluster / grid ACA */
 } hsc_options;
 
 typedef struct hsc_stats {        /* superset of the hsc_stats.jsonl record (linear_hsc.cu:420-431) */

@@ -78,13 +78,15 @@ def test_aca_factors_match_reference_core(api, torch, golden, tag):
     assert np.all(Vg[mask] == 0)
 
 
-@pytest.mark.parametrize("cluster", (True, False))
-def test_aca_cluster_and_grid_kernels_match_oracle(api, torch, vehicle_system, cluster):
-    """Both ACA kernels (16-CTA cluster in distributed shared memory, and the
-    grid kernel with column strips) reproduce the oracle's full-pivot ACA on
-    the vehicle coupling (144 x 1749): same rank, same pivots, same factors."""
+@pytest.mark.parametrize("mode", ("components", "cluster", "grid"))
+def test_aca_cluster_and_grid_kernels_match_oracle(api, torch, vehicle_system, mode):
+    """The three ACA paths (per coupling component with the merged pivot order,
+    16-CTA cluster in distributed shared memory, grid kernel with column strips)
+    reproduce the oracle's full-pivot ACA on the vehicle coupling (144 x 1749):
+    same rank, same pivots, same factors."""
     s = vehicle_system
-    ctx = api.HSCContext(api.HSCOptions(aca_cluster=cluster, max_rank=128))
+    ctx = api.HSCContext(api.HSCOptions(aca_cluster=mode == "cluster", aca_components=mode == "components",
+                                        max_rank=128))
     ds = api.DeviceSystem.from_system(s)
     ctx.solve(ds)
     U, V, act = ctx.factors_full(s.layout[1])
@@ -94,6 +96,24 @@ def test_aca_cluster_and_grid_kernels_match_oracle(api, torch, vehicle_system, c
     assert U.shape == Uo.shape
     assert np.max(np.abs(U - Uo)) <= 1e-11 * np.max(np.abs(Uo))
     assert np.max(np.abs(V - Vo)) <= 1e-11 * np.max(np.abs(Vo))
+
+
+def test_component_aca_is_bitwise_the_global_aca(api, torch, tire_system):
+    """On the tire-mesh vehicle (8 coupling components: 7 rims and the ground) the component
+    ACA's merged factors equal the global cluster ACA's bit for bit, in the same column order."""
+    s = tire_system
+    ds = api.DeviceSystem.from_system(s)
+    out = {}
+    for comp in (True, False):
+        ctx = api.HSCContext(api.HSCOptions(aca_components=comp, aca_cluster=True, omega=0.5, max_rank=128))
+        _, st = ctx.solve(ds)
+        out[comp] = (ctx.factors_full(s.layout[1]), st["rank"])
+    (U1, V1, a1), k1 = out[True]
+    (U0, V0, a0), k0 = out[False]
+    assert k1 == k0 == 96
+    np.testing.assert_array_equal(a1, a0)
+    np.testing.assert_array_equal(U1, U0)
+    np.testing.assert_array_equal(V1, V0)
 
 
 @pytest.mark.parametrize("tag", STIFF)
