@@ -33,41 +33,39 @@ namespace {
 constexpr int kCompThreads = 512;
 constexpr int kCompWarps = kCompThreads / 32;
 
-__device__ __forceinline__ void better(double& v, long long& i, double qv, long long qi) {
-    if (qv > v || (qv == v && qi < i)) { v = qv; i = qi; }
-}
-
-// CTA-wide (max |.|, first global index, sum of squares) of the residual block
-__device__ void block_stats(const double* R, int mr, int nc, const int* rows, const int* cols, int a, double& vmax,
-                            long long& imax, double& sum) {
+// CTA-wide (max |.|, first local row-major index, sum of squares) of the residual
+// block.  Rows and columns of a component ascend, so the local row-major order is
+// the global one restricted to the block: the first local maximum is the global
+// argmax's choice among the block's entries.
+__device__ void block_stats(const double* R, int n, double& vmax, int& imax, double& sum) {
     __shared__ double s_v[kCompWarps], s_s[kCompWarps];
-    __shared__ long long s_i[kCompWarps];
+    __shared__ int s_i[kCompWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double lv = -1.0, ls = 0.0;
-    long long li = LLONG_MAX;
-    for (int e = threadIdx.x; e < mr * nc; e += kCompThreads) {
+    int li = INT_MAX;
+    for (int e = threadIdx.x; e < n; e += kCompThreads) {
         const double x = R[e];
         ls += x * x;
-        const int r = e / nc, c = e - r * nc;
-        better(lv, li, fabs(x), (long long)rows[r] * a + cols[c]);
+        const double ax = fabs(x);
+        if (ax > lv) { lv = ax; li = e; }     // a thread's entries ascend: ties keep the first
     }
     for (int o = 16; o > 0; o >>= 1) {
         const double qv = __shfl_xor_sync(0xffffffffu, lv, o);
-        const long long qi = __shfl_xor_sync(0xffffffffu, li, o);
+        const int qi = __shfl_xor_sync(0xffffffffu, li, o);
         ls += __shfl_xor_sync(0xffffffffu, ls, o);
-        better(lv, li, qv, qi);
+        if (qv > lv || (qv == lv && qi < li)) { lv = qv; li = qi; }
     }
     if (lane == 0) { s_v[warp] = lv; s_i[warp] = li; s_s[warp] = ls; }
     __syncthreads();
     if (warp == 0) {
         lv = lane < kCompWarps ? s_v[lane] : -1.0;
-        li = lane < kCompWarps ? s_i[lane] : LLONG_MAX;
+        li = lane < kCompWarps ? s_i[lane] : INT_MAX;
         ls = lane < kCompWarps ? s_s[lane] : 0.0;
         for (int o = 16; o > 0; o >>= 1) {
             const double qv = __shfl_xor_sync(0xffffffffu, lv, o);
-            const long long qi = __shfl_xor_sync(0xffffffffu, li, o);
+            const int qi = __shfl_xor_sync(0xffffffffu, li, o);
             ls += __shfl_xor_sync(0xffffffffu, ls, o);
-            better(lv, li, qv, qi);
+            if (qv > lv || (qv == lv && qi < li)) { lv = qv; li = qi; }
         }
         if (lane == 0) { s_v[0] = lv; s_i[0] = li; s_s[0] = ls; }
     }
@@ -113,8 +111,8 @@ __global__ void __launch_bounds__(kCompThreads) aca_comp_kernel(AcaComp p) {
     __syncthreads();
     const double scale = sqrt(*p.esumsq);
     double vmax, sum;
-    long long imax;
-    block_stats(R, mr, nc, rows, cols, p.a, vmax, imax, sum);
+    int imax;
+    block_stats(R, mr * nc, vmax, imax, sum);
     double* piv_abs = p.piv_abs + p.s_off[g];
     long long* piv_idx = p.piv_idx + p.s_off[g];
     double* sums = p.sums + p.s_off[g] + g;   // steps_max + 1 entries per component
@@ -123,15 +121,11 @@ __global__ void __launch_bounds__(kCompThreads) aca_comp_kernel(AcaComp p) {
     int s = 0;
     for (; s < steps_max; ++s) {
         if (threadIdx.x == 0) sums[s] = sum;
-        if (!(vmax > DBL_EPSILON * fmax(scale, DBL_MIN)) || imax == LLONG_MAX) break;  // zero-pivot guard
+        if (!(vmax > DBL_EPSILON * fmax(scale, DBL_MIN)) || imax == INT_MAX) break;  // zero-pivot guard
         if (threadIdx.x == 0) {
+            const int li = imax / nc, lj = imax - li * nc;
             piv_abs[s] = vmax;
-            piv_idx[s] = imax;
-            // the pivot's local row and column
-            const int gr = (int)(imax / p.a), gc = (int)(imax - (long long)gr * p.a);
-            int li = 0, lj = 0;
-            while (li < mr - 1 && rows[li] != gr) ++li;
-            while (lj < nc - 1 && cols[lj] != gc) ++lj;
+            piv_idx[s] = (long long)rows[li] * p.a + cols[lj];  // the global row-major index, for the merge
             s_i = li;
             s_j = lj;
         }
@@ -150,7 +144,7 @@ __global__ void __launch_bounds__(kCompThreads) aca_comp_kernel(AcaComp p) {
             R[e] = __dsub_rn(R[e], __dmul_rn(s_u[r], Vg[(size_t)s * nc + c]));
         }
         __syncthreads();
-        block_stats(R, mr, nc, rows, cols, p.a, vmax, imax, sum);
+        block_stats(R, mr * nc, vmax, imax, sum);
     }
     if (threadIdx.x == 0) {
         p.nsteps[g] = s;

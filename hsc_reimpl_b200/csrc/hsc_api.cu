@@ -293,11 +293,16 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
         for (int p = 0; p < nparts; ++p) S.h_part_ptr[p + 1] += S.h_part_ptr[p];
         S.h_perm.assign(S.n, 0);
         S.h_iperm.assign(S.n, 0);
-        std::vector<int> fill(S.h_part_ptr.begin(), S.h_part_ptr.end() - 1);
-        for (int i = 0; i < S.n; ++i) {
-            const int ni = fill[part[i]]++;
-            S.h_perm[ni] = i;
-            S.h_iperm[i] = ni;
+        // inside a part, nodes by decreasing block count (ties by index): rows of similar length sit
+        // together, so the 32-row slices of the block preconditioner's layout carry little padding
+        std::vector<int> order(S.n);
+        for (int i = 0; i < S.n; ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            return part[x] != part[y] ? part[x] < part[y] : cnt[x] > cnt[y];
+        });
+        for (int ni = 0; ni < S.n; ++ni) {
+            S.h_perm[ni] = order[ni];
+            S.h_iperm[order[ni]] = ni;
         }
         S.reordered = nparts > 1;
     }
@@ -972,7 +977,9 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
     // and of the column indices is dropped (in that order) when the budget does
     // not hold them
     const int budget = (int)(smem_cap / sizeof(double));
-    const int res_budget = (int)((227 * 1024 - 1024) / sizeof(double));
+    // the kernel's static shared memory (parameter block, system descriptor, three k-vectors of
+    // kMaxRank doubles, warp scratch: about 7.5 KB) comes out of the same 227 KB
+    const int res_budget = (int)((227 * 1024 - 8 * 1024) / sizeof(double));
     const int base = kMaxRank + Zmax + 3 * Rmax + 2;
     if (base > budget) return fail(ctx, HSC_ERR_INVALID, "too many rows or coupled dofs in one CTA");
     const size_t vtb = vt_bytes(o.precision), mtb = o.precision == 0 ? 8 : 4;
@@ -1371,6 +1378,15 @@ int launch_block_solve(hsc_ctx* ctx, System& S, cudaStream_t st) {
         CK(cudaMemsetAsync(S.blk_colptr.p, 0, sizeof(int) * (b.ncomp + 1), st));
     }
     if (ctx->stage_events) CK(cudaEventRecord(ctx->ev_blk, st));
+    b.trace = nullptr;
+    b.trace_iters = 0;
+    if (o.trace_iterations > 0) {
+        const size_t nt = (size_t)b.G_ctas * o.trace_iterations * kTraceEvents;
+        GROW(ctx->d_trace, sizeof(unsigned long long) * nt);
+        CK(cudaMemsetAsync(ctx->d_trace.p, 0, sizeof(unsigned long long) * nt, st));
+        b.trace = ctx->d_trace.as<unsigned long long>();
+        b.trace_iters = o.trace_iterations;
+    }
     CK(cudaMemsetAsync(ctx->d_bar.p, 0, sizeof(GridBar), st));
     CK(launch_block_pcg(o.precision, b, st));
     return HSC_OK;

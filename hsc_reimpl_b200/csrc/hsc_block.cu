@@ -374,20 +374,37 @@ __global__ void __launch_bounds__(kThreads, 1) block_y_kernel(const BlockPlan p_
             Vc[e] = p.V[(size_t)s_cols[q] * p.a + p.actperm[s.ab + il]];
         }
     }
-    // partial G_c[j][l] = sum_{own coupled dofs} V[., j] Yact[., l]  (dense kmax^2, zero outside)
+    // partial G_c[j][l] = sum_{own coupled dofs} V[., j] Yact[., l]  (dense kmax^2, zero outside).
+    // The CTA's rows of V ([q][dof]) and of Y ([dof][q]) are staged in the (now free) vector region
+    // when they fit: a warp takes a row q_a, its lanes the columns q_b, and walks the dofs.
     const int aidx = p.cta_aidx[cta];
-    if (aidx >= 0) {
+    if (aidx >= 0) {  // uniform in the CTA
+        __syncthreads();  // the compact rows of V above are read back below
         double* Gc = p.pG + (size_t)aidx * p.kmax * p.kmax;
         for (int e = threadIdx.x; e < p.kmax * p.kmax; e += blockDim.x) Gc[e] = 0.0;
+        const bool staged = 2 * (size_t)s.na * ncols <= (size_t)16 * R3;
+        double* Vs = vec;
+        double* Ys = vec + (size_t)s.na * ncols;
+        if (staged)
+            for (int e = threadIdx.x; e < ncols * s.na; e += blockDim.x) {
+                const int q = e / s.na, il = e - q * s.na;
+                Vs[e] = p.Vc[(size_t)p.kmax * s.ab + e];
+                Ys[(size_t)il * ncols + q] = p.Yact[(size_t)s_cols[q] * p.a + s.ab + il];
+            }
         __syncthreads();
-        for (int e = threadIdx.x; e < ncols * ncols; e += blockDim.x) {
-            const int qa = e / ncols, qb = e - qa * ncols;
-            const int j = s_cols[qa], l = s_cols[qb];
-            double acc = 0.0;
-            for (int il = 0; il < s.na; ++il)
-                acc += p.V[(size_t)j * p.a + p.actperm[s.ab + il]] * p.Yact[(size_t)l * p.a + s.ab + il];
-            if (j < k && l < k) Gc[(size_t)j * p.kmax + l] = acc;
-        }
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int qa = warp; qa < ncols; qa += kWarps)
+            for (int qb = lane; qb < ncols; qb += 32) {
+                const int j = s_cols[qa], l = s_cols[qb];
+                double acc = 0.0;
+                if (staged) {
+                    for (int il = 0; il < s.na; ++il) acc += Vs[(size_t)qa * s.na + il] * Ys[(size_t)il * ncols + qb];
+                } else {
+                    for (int il = 0; il < s.na; ++il)
+                        acc += p.Vc[(size_t)p.kmax * s.ab + (size_t)qa * s.na + il] * p.Yact[(size_t)l * p.a + s.ab + il];
+                }
+                if (j < k && l < k) Gc[(size_t)j * p.kmax + l] = acc;
+            }
     }
 }
 
@@ -646,13 +663,22 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
     }
     __syncthreads();
 
-    int pass = kPassStart, it = 0, status = -1, restarts = 0;
+    int pass = kPassStart, it = 0, status = -1, restarts = 0, npass = 0;
+    // phase clocks (trace mode): 0 pass top, 1 polynomial done, 2 partials written, 3 after barrier A,
+    // 4 sums read, 5 K s done, 6 m formed, 7 V^T m partials / decisions, 8 after barrier B, 9 window
+    // staged, 10 V^T m summed, 11 D m done, 12 low-rank done, 13 updates done
+    auto mark = [&](int ev) {
+        if (p.trace && threadIdx.x == 0 && npass < p.trace_iters)
+            p.trace[((size_t)cta * p.trace_iters + npass) * 16 + ev] = (unsigned long long)clock64();
+    };
     double normb = -1.0, rel = 1.0, alpha = 0.0, beta = 0.0, alpha_prev = 0.0, gamma_prev = 0.0;
     bool fresh = true;  // next normal pass is the first after a (re)start: beta = 0
     for (;;) {
         // ---------------- phase 1 ----------------
+        mark(0);
         const double* v = pass == kPassStart ? Rr : Ww;
         local_poly<MT>(p, sl, split, v, Mt, T0, T1);
+        mark(1);
         y_partials(v, p.pY);
         {
             double g = 0, d = 0, rr = 0;
@@ -663,11 +689,14 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
             }
             cta_partials(g, d, rr, 0.0, p.pdot, 0, 3);
         }
+        mark(2);
         if (!barrier()) return;
+        mark(3);
         // ---------------- phase 2 ----------------
         sum_slots(p.pY, s_sv);
         sum_dots();
         __syncthreads();
+        mark(4);
         for (int q = warp; q < ncols; q += kWarps) {
             const int j = s_cols[q];
             double a = 0.0;
@@ -676,6 +705,7 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
             if (lane == 0) s_c[q] = a;
         }
         __syncthreads();
+        mark(5);
         for (int e = threadIdx.x; e < R; e += blockDim.x) {
             double m0 = Mt[3 * e], m1 = Mt[3 * e + 1], m2 = Mt[3 * e + 2];
             for (int q = 0; q < ncols; ++q) {
@@ -686,6 +716,7 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
             Vec4<double>::store(p.mpub, sl.rb + e, m0, m1, m2);
         }
         __syncthreads();
+        mark(6);
         v_partials(Mm, p.pV);
         // decisions (identical in every CTA)
         bool check = false;
@@ -718,16 +749,23 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
             }
         }
         if (status >= 0) break;
+        mark(7);
         if (!barrier()) return;
+        mark(8);
         // ---------------- phase 3 ----------------
         if (!check) {
             stage(p.mpub, Mm);
+            __syncthreads();
+            mark(9);
             sum_slots(p.pV, s_vt);
             __syncthreads();
+            mark(10);
             op_spmv(Mm, Nn);
             __syncthreads();
+            mark(11);
             lowrank_sub(Nn);
             __syncthreads();
+            mark(12);
             if (pass == kPassStart) {
                 for (int e = threadIdx.x; e < R3; e += blockDim.x) { Uu[e] = Mm[e]; Ww[e] = Nn[e]; }
                 pass = kPassNormal;
@@ -746,6 +784,8 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
                 fresh = false;
             }
             __syncthreads();
+            mark(13);
+            ++npass;
             continue;
         }
         // ---------------- true residual: r = rhs - (D x - V C V^T x) ----------------

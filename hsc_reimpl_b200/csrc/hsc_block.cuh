@@ -105,6 +105,8 @@ struct BlockPlan {
     double* out;                 // iterations, relative residual, status, |rhs|, restarts
     double* cg_coef;             // alpha_i, beta_{i+1} pairs (Lanczos of the preconditioned operator)
     int max_coef;
+    unsigned long long* trace;   // optional: per CTA x trace_iters x 16 SM clocks at the phase boundaries
+    int trace_iters;
     // shared-memory layout (bytes from the dynamic base, the same in every CTA)
     int R, BLK, W, NA, NCOL;     // maxima over CTAs: rows, blocks, window nodes, coupled dofs, Y columns
     int stage_vals, stage_yc;
