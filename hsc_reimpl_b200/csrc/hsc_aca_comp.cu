@@ -12,10 +12,12 @@
 // row-major index, as argmax takes them).
 //
 // Here every component runs its own ACA in one CTA (its residual block in
-// shared memory when it fits), all components at once; one thread then merges
-// the sequences, applying the global stop rules (rank cap, relative Frobenius
-// residual from the components' sums of squares, zero-pivot guard), and the
-// columns are scattered into U and V in merged order.  The result is the
+// shared memory when it fits), all components at once, until its residual
+// vanishes; one warp then merges the sequences, applying the global stop rules
+// (rank cap, relative Frobenius residual from the components' sums of squares,
+// zero-pivot guard against |E|_F, which is the root of the sum of the
+// components' initial sums since E vanishes outside them), and the columns are
+// scattered into U and V in merged order.  The result is the
 // global ACA's factorization: the same pivots, the same columns in the same
 // order, each entry computed with the same operations (R - u v rounded as
 // numpy rounds it).  A coupling of vehicle size (144 x 2,976, rank 96) takes
@@ -76,21 +78,6 @@ __device__ void block_stats(const double* R, int n, double& vmax, int& imax, dou
     __syncthreads();
 }
 
-// sum of squares of E (the scale of the zero-pivot guard and of the residuals)
-__global__ void e_sumsq_kernel(const double* E, long long n, double* out) {
-    __shared__ double s[32];
-    double a = 0.0;
-    for (long long e = threadIdx.x; e < n; e += blockDim.x) a += E[e] * E[e];
-    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = a;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s[w];
-        *out = t;
-    }
-}
-
 __global__ void __launch_bounds__(kCompThreads) aca_comp_kernel(AcaComp p) {
     const int g = blockIdx.x;
     const int r0 = p.row_ptr[g], mr = p.row_ptr[g + 1] - r0;
@@ -104,12 +91,11 @@ __global__ void __launch_bounds__(kCompThreads) aca_comp_kernel(AcaComp p) {
     __shared__ double s_u[256];          // u = R[:, j]; the host admits components of at most 256 rows
     __shared__ double s_piv;
     __shared__ int s_i, s_j;
-    for (int e = threadIdx.x; e < mr * nc; e += kCompThreads) {
-        const int r = e / nc, c = e - r * nc;
-        R[e] = p.E[(size_t)rows[r] * p.a + cols[c]];
+    for (int r = 0; r < mr; ++r) {
+        const double* Er = p.E + (size_t)rows[r] * p.a;
+        for (int c = threadIdx.x; c < nc; c += kCompThreads) R[(size_t)r * nc + c] = Er[cols[c]];
     }
     __syncthreads();
-    const double scale = sqrt(*p.esumsq);
     double vmax, sum;
     int imax;
     block_stats(R, mr * nc, vmax, imax, sum);
@@ -121,7 +107,7 @@ __global__ void __launch_bounds__(kCompThreads) aca_comp_kernel(AcaComp p) {
     int s = 0;
     for (; s < steps_max; ++s) {
         if (threadIdx.x == 0) sums[s] = sum;
-        if (!(vmax > DBL_EPSILON * fmax(scale, DBL_MIN)) || imax == INT_MAX) break;  // zero-pivot guard
+        if (!(vmax > 0.0) || imax == INT_MAX) break;  // the residual vanished (the merge applies the guard)
         if (threadIdx.x == 0) {
             const int li = imax / nc, lj = imax - li * nc;
             piv_abs[s] = vmax;
@@ -136,12 +122,13 @@ __global__ void __launch_bounds__(kCompThreads) aca_comp_kernel(AcaComp p) {
         __syncthreads();
         const double pivot = s_piv;
         for (int r = threadIdx.x; r < mr; r += kCompThreads) Ug[(size_t)s * mr + r] = s_u[r];
-        // v = R[i, :] / pivot, then R -= u v^T (the product rounded, then the difference: numpy's order)
-        for (int c = threadIdx.x; c < nc; c += kCompThreads) Vg[(size_t)s * nc + c] = R[(size_t)i * nc + c] / pivot;
-        __syncthreads();
-        for (int e = threadIdx.x; e < mr * nc; e += kCompThreads) {
-            const int r = e / nc, c = e - r * nc;
-            R[e] = __dsub_rn(R[e], __dmul_rn(s_u[r], Vg[(size_t)s * nc + c]));
+        // v = R[i, :] / pivot, then R -= u v^T (the product rounded, then the difference: numpy's
+        // order); each thread updates the columns whose v it computed, so no barrier between
+        double* Vs = Vg + (size_t)s * nc;
+        for (int c = threadIdx.x; c < nc; c += kCompThreads) {
+            const double vc = R[(size_t)i * nc + c] / pivot;
+            Vs[c] = vc;
+            for (int r = 0; r < mr; ++r) R[(size_t)r * nc + c] = __dsub_rn(R[(size_t)r * nc + c], __dmul_rn(s_u[r], vc));
         }
         __syncthreads();
         block_stats(R, mr * nc, vmax, imax, sum);
@@ -152,35 +139,75 @@ __global__ void __launch_bounds__(kCompThreads) aca_comp_kernel(AcaComp p) {
     }
 }
 
-// one thread: merge the components' pivot sequences into the global order and
-// apply the global stop rules; order[t] = (component, its step)
-__global__ void aca_merge_kernel(AcaComp p) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const double scale = sqrt(*p.esumsq);
+constexpr int kMergePer = 8;  // components per lane in the warp merge (256 / 32)
+
+// one warp: merge the components' pivot sequences into the global order and apply the global
+// stop rules; order[t] = (component, its step).  The step records are staged in shared memory
+// first (all 256 threads), then lane l follows the cursors of components l, l + 32, ...
+__global__ void __launch_bounds__(256) aca_merge_kernel(AcaComp p) {
+    extern __shared__ double msm[];
+    const int G = p.ncomp, ns = p.stot;
+    double* pa = msm;                                            // ns
+    double* su = pa + ns;                                        // ns + G
+    long long* pi = reinterpret_cast<long long*>(su + ns + G);   // ns
+    int* so = reinterpret_cast<int*>(pi + ns);                   // G
+    int* nst = so + G;                                           // G
+    for (int e = threadIdx.x; e < ns; e += blockDim.x) { pa[e] = p.piv_abs[e]; pi[e] = p.piv_idx[e]; }
+    for (int e = threadIdx.x; e < ns + G; e += blockDim.x) su[e] = p.sums[e];
+    for (int e = threadIdx.x; e < G; e += blockDim.x) { so[e] = p.s_off[e]; nst[e] = p.nsteps[e]; }
+    __syncthreads();
+    if (threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
+    double e2 = 0.0;
+    for (int c = lane; c < G; c += 32) e2 += su[so[c] + c];
+    for (int o = 16; o > 0; o >>= 1) e2 += __shfl_xor_sync(0xffffffffu, e2, o);
+    const double scale = sqrt(e2);
+    int cur[kMergePer];
+#pragma unroll
+    for (int i = 0; i < kMergePer; ++i) cur[i] = 0;
     int t = 0;
-    for (int g = 0; g < p.ncomp; ++g) p.cur[g] = 0;
     for (;; ++t) {
         double rs = 0.0;
-        for (int g = 0; g < p.ncomp; ++g) rs += p.sums[p.s_off[g] + g + p.cur[g]];
-        const double residual = t == 0 ? (scale > 0 ? 1.0 : 0.0) : sqrt(rs) / scale;
-        p.hist[t] = residual;
-        if (!(residual > p.rtol) || t >= p.kmax) break;
-        int best = -1;
-        for (int g = 0; g < p.ncomp; ++g) {
-            if (p.cur[g] >= p.nsteps[g]) continue;
-            if (best < 0) { best = g; continue; }
-            const double v = p.piv_abs[p.s_off[g] + p.cur[g]];
-            const long long i = p.piv_idx[p.s_off[g] + p.cur[g]];
-            const double bv = p.piv_abs[p.s_off[best] + p.cur[best]];
-            const long long bi = p.piv_idx[p.s_off[best] + p.cur[best]];
-            if (v > bv || (v == bv && i < bi)) best = g;
+#pragma unroll
+        for (int i = 0; i < kMergePer; ++i) {
+            const int c = lane + 32 * i;
+            if (c < G) rs += su[so[c] + c + cur[i]];
         }
-        if (best < 0) break;  // every component is exhausted: the guard stops the global ACA too
-        p.order[2 * t] = best;
-        p.order[2 * t + 1] = p.cur[best]++;
+        for (int o = 16; o > 0; o >>= 1) rs += __shfl_xor_sync(0xffffffffu, rs, o);
+        const double residual = t == 0 ? (scale > 0 ? 1.0 : 0.0) : sqrt(rs) / scale;
+        if (lane == 0) p.hist[t] = residual;
+        if (!(residual > p.rtol) || t >= p.kmax) break;
+        double bv = -1.0;
+        long long bi = LLONG_MAX;
+        int bc = -1, bs = 0;
+#pragma unroll
+        for (int i = 0; i < kMergePer; ++i) {
+            const int c = lane + 32 * i;
+            if (c < G && cur[i] < nst[c]) {
+                const double v = pa[so[c] + cur[i]];
+                const long long ix = pi[so[c] + cur[i]];
+                if (v > bv || (v == bv && ix < bi)) { bv = v; bi = ix; bc = c; bs = cur[i]; }
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double qv = __shfl_xor_sync(0xffffffffu, bv, o);
+            const long long qi = __shfl_xor_sync(0xffffffffu, bi, o);
+            const int qc = __shfl_xor_sync(0xffffffffu, bc, o), qs = __shfl_xor_sync(0xffffffffu, bs, o);
+            if (qv > bv || (qv == bv && qi < bi)) { bv = qv; bi = qi; bc = qc; bs = qs; }
+        }
+        if (bc < 0) break;  // every component is exhausted: the global residual vanished too
+        if (!(bv > DBL_EPSILON * fmax(scale, DBL_MIN))) break;  // zero-pivot guard (the global argmax)
+        if (lane == 0) { p.order[2 * t] = bc; p.order[2 * t + 1] = bs; }
+        if ((bc & 31) == lane) {
+#pragma unroll
+            for (int i = 0; i < kMergePer; ++i)
+                if (i == (bc >> 5)) ++cur[i];
+        }
     }
-    *p.rank = t;
-    *p.err = p.hist[t];
+    if (lane == 0) {
+        *p.rank = t;
+        *p.err = p.hist[t];
+    }
 }
 
 // U[:, t] and V[:, t] from the components' columns (zero elsewhere), t < kmax
@@ -206,9 +233,15 @@ __global__ void aca_scatter_kernel(AcaComp p) {
 
 size_t aca_comp_smem_doubles() { return (220 * 1024) / sizeof(double); }
 
+size_t aca_merge_smem_bytes(int ncomp, int stot) {
+    return sizeof(double) * (3 * (size_t)stot + ncomp) + sizeof(int) * 2 * (size_t)ncomp;
+}
+
+bool aca_merge_fits(int ncomp, int stot) {
+    return ncomp <= 32 * kMergePer && aca_merge_smem_bytes(ncomp, stot) <= 200 * 1024;
+}
+
 cudaError_t launch_aca_comp(const AcaComp& p, cudaStream_t st) {
-    count_launch();
-    e_sumsq_kernel<<<1, 1024, 0, st>>>(p.E, (long long)p.qm * p.a, p.esumsq);
     if (p.ncomp > 0) {
         const size_t smem = sizeof(double) * (size_t)p.smem_doubles;
         cudaError_t e = cudaFuncSetAttribute(aca_comp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -216,11 +249,14 @@ cudaError_t launch_aca_comp(const AcaComp& p, cudaStream_t st) {
         count_launch();
         aca_comp_kernel<<<p.ncomp, kCompThreads, smem, st>>>(p);
     }
+    const size_t msmem = aca_merge_smem_bytes(p.ncomp, p.stot);
+    cudaError_t e = cudaFuncSetAttribute(aca_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem);
+    if (e != cudaSuccess) return e;
     count_launch();
-    aca_merge_kernel<<<1, 32, 0, st>>>(p);
+    aca_merge_kernel<<<1, 256, msmem, st>>>(p);
     count_launch();
     aca_scatter_kernel<<<p.kmax, 256, 0, st>>>(p);
-    return cudaGetLastError();
+    return cudaPeekAtLastError();
 }
 
 }  // namespace hsc

@@ -101,11 +101,15 @@ struct System {
     int ncomp_coupled = 0;
     AcaComp acomp{};
     DevBuf ac_row_ptr, ac_rows, ac_col_ptr, ac_cols, ac_r_off, ac_s_off, ac_u_off, ac_v_off, ac_R, ac_Ug, ac_Vg,
-        ac_piv_abs, ac_piv_idx, ac_sums, ac_nsteps, ac_cur, ac_order, ac_esum;
+        ac_piv_abs, ac_piv_idx, ac_sums, ac_nsteps, ac_order;
+    int ac_stot = 0;
+    DevBuf abd_bptr, abd_bidx;  // A's diagonal blocks over coupled bodies (the exact ABD inverse by block)
+    int abd_nblk = 0, abd_maxblk = 0;
     // block-local Woodbury preconditioner (hsc_block.cu)
     DevBuf blk_Y, blk_Yact, blk_Vc, blk_pG, blk_G, blk_K, blk_Ka, blk_Kb, blk_pY, blk_pV, blk_pX, blk_pdot, blk_mpub,
         blk_xpub, blk_colof, blk_colptr, blk_cols, blk_bad, blk_C, blk_cta_comp_ptr, blk_cta_comp, blk_cta_comp_slot,
-        blk_comp_slot_ptr, blk_comp_of_body, blk_ident;
+        blk_comp_slot_ptr, blk_comp_of_body, blk_ident, blk_sslice, blk_cslice, blk_cchunk, blk_nloc, blk_slc,
+        blk_ssrc, blk_svals;
     BlockPlan blk{};
     int blk_nact_cta = 0;
     // plan
@@ -156,6 +160,8 @@ struct hsc_ctx {
     bool has_model = false;
     cudaEvent_t ev[9] = {};
     cudaEvent_t ev_blk = nullptr;  // end of the block preconditioner's setup (Y, K) inside the PCG stage
+    cudaStream_t side = nullptr;   // the ABD inverses run here, beside the ACA
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool stage_events = false;  // record the per-stage events (single system, no graph)
     // graph cache (batch)
     cudaGraphExec_t gexec = nullptr;
@@ -424,10 +430,49 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
     }
     S.nqq = (int)qq.size() / 3;
     S.nqf = (int)qf.size() / 4;
+    // A's blocks: bodies joined by a nonzero body-body block of A (union-find), each block's dofs ascending
+    {
+        const int nb = S.qm / 12;
+        std::vector<int> root(std::max(1, nb));
+        for (int b = 0; b < nb; ++b) root[b] = b;
+        auto findb = [&](int b) { while (root[b] != b) { root[b] = root[root[b]]; b = root[b]; } return b; };
+        for (size_t e = 0; e + 2 < qq.size(); e += 3) {
+            const int ra = findb(qq[e + 1] / 4), rb = findb(qq[e + 2] / 4);
+            if (ra != rb) root[std::max(ra, rb)] = std::min(ra, rb);
+        }
+        std::vector<int> gid(std::max(1, nb), -1), bptr(1, 0), bidx;
+        std::vector<std::vector<int>> members;
+        for (int b = 0; b < nb; ++b) {
+            const int r = findb(b);
+            if (gid[r] < 0) { gid[r] = (int)members.size(); members.emplace_back(); }
+            members[gid[r]].push_back(b);
+        }
+        S.abd_maxblk = 0;
+        for (const auto& mb : members) {
+            for (int b : mb)
+                for (int d = 0; d < 12; ++d) bidx.push_back(12 * b + d);
+            bptr.push_back((int)bidx.size());
+            S.abd_maxblk = std::max(S.abd_maxblk, 12 * (int)mb.size());
+        }
+        S.abd_nblk = (int)members.size();
+        if (S.abd_nblk > 0) {
+            GROW(S.abd_bptr, sizeof(int) * bptr.size());
+            GROW(S.abd_bidx, sizeof(int) * bidx.size());
+            CK(cudaMemcpyAsync(S.abd_bptr.p, bptr.data(), sizeof(int) * bptr.size(), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(S.abd_bidx.p, bidx.data(), sizeof(int) * bidx.size(), cudaMemcpyHostToDevice, st));
+            CK(cudaStreamSynchronize(st));
+        }
+    }
     S.kmax = std::min(std::min(o.max_rank, L.qm), S.a);
     // the component ACA's plan
     S.aca_comp_ok = S.kmax > 0 && S.ncomp_coupled > 0;
     for (const auto& r : comp_rows) S.aca_comp_ok = S.aca_comp_ok && r.size() <= 256;
+    if (S.aca_comp_ok) {
+        int stot = 0;
+        for (int g = 0; g < S.ncomp_coupled; ++g)
+            stot += std::min(std::min((int)comp_rows[g].size(), (int)comp_cols[g].size()), S.kmax);
+        S.aca_comp_ok = aca_merge_fits(S.ncomp_coupled, stot);
+    }
     if (S.aca_comp_ok) {
         const int ncg = S.ncomp_coupled;
         std::vector<int> row_ptr(ncg + 1, 0), col_ptr(ncg + 1, 0), rows_all, cols_all, s_off(ncg);
@@ -461,9 +506,8 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
         GROW(S.ac_piv_idx, sizeof(long long) * std::max(1, stot));
         GROW(S.ac_sums, sizeof(double) * (stot + ncg));
         GROW(S.ac_nsteps, sizeof(int) * ncg);
-        GROW(S.ac_cur, sizeof(int) * ncg);
         GROW(S.ac_order, sizeof(int) * 2 * S.kmax);
-        GROW(S.ac_esum, sizeof(double));
+        S.ac_stot = stot;
         CK(cudaMemcpyAsync(S.ac_row_ptr.p, row_ptr.data(), sizeof(int) * (ncg + 1), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(S.ac_col_ptr.p, col_ptr.data(), sizeof(int) * (ncg + 1), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(S.ac_rows.p, rows_all.data(), sizeof(int) * rows_all.size(), cudaMemcpyHostToDevice, st));
@@ -606,7 +650,10 @@ int abd_inverse(hsc_ctx* ctx, System& S, cudaStream_t st, bool allow_sync) {
     double* P = S.P.as<double>();
     if (m == 0) return HSC_OK;
     if (o.abd_inverse == HSC_ABD_EXACT) {
-        if (!launch_chol_inverse(S.A.as<double>(), m, P, &ds->bad_abd, st)) {
+        const bool by_block = S.abd_nblk > 1 &&
+                              launch_inverse_blocks(S.A.as<double>(), m, S.abd_nblk, S.abd_maxblk, S.abd_bptr.as<int>(),
+                                                    S.abd_bidx.as<int>(), P, &ds->bad_abd, st);
+        if (!by_block && !launch_chol_inverse(S.A.as<double>(), m, P, &ds->bad_abd, st)) {
             launch_cholesky(S.A.as<double>(), m, S.L.as<double>(), &ds->bad_abd, st);
             launch_chol_solve(S.L.as<double>(), m, S.ident.as<double>(), m, P, m, m, nullptr, S.work.as<double>(), st);
         }
@@ -710,8 +757,8 @@ int aca_all(hsc_ctx* ctx, int count, cudaStream_t st) {
             c.u_off = S.ac_u_off.as<long long>(); c.v_off = S.ac_v_off.as<long long>();
             c.Rscratch = S.ac_R.as<double>(); c.Ug = S.ac_Ug.as<double>(); c.Vg = S.ac_Vg.as<double>();
             c.piv_abs = S.ac_piv_abs.as<double>(); c.piv_idx = S.ac_piv_idx.as<long long>();
-            c.sums = S.ac_sums.as<double>(); c.nsteps = S.ac_nsteps.as<int>(); c.cur = S.ac_cur.as<int>();
-            c.order = S.ac_order.as<int>(); c.esumsq = S.ac_esum.as<double>();
+            c.sums = S.ac_sums.as<double>(); c.nsteps = S.ac_nsteps.as<int>();
+            c.order = S.ac_order.as<int>(); c.stot = S.ac_stot;
             c.smem_doubles = (int)aca_comp_smem_doubles();
             c.U = S.U.as<double>(); c.V = S.V.as<double>(); c.hist = S.hist.as<double>();
             c.rank = &ds->rank; c.err = &ds->aca_err;
@@ -734,11 +781,10 @@ int aca_all(hsc_ctx* ctx, int count, cudaStream_t st) {
 }
 
 // numeric setup, part 2: ABD inverse P, W = P U, C = U^T W = L D L^T, Vt = V L
-int numeric_post(hsc_ctx* ctx, System& S, cudaStream_t st, bool allow_sync) {
+// numeric setup, part 2 (after the ACA and the ABD inverse): the reduced core C = U^T P U and its
+// LDL^T factors, and (classic PCG) the scaled copy V L_c of V
+int numeric_post(hsc_ctx* ctx, System& S, cudaStream_t st) {
     DevScal* ds = S.scal.as<DevScal>();
-    int rc = abd_inverse(ctx, S, st, allow_sync);
-    if (rc) return rc;
-    stage_mark(ctx, 3, st);
     if (S.kmax > 0) {
         const int* dk = &ds->rank;
         // W = P U  (qm x k, ld kmax); U column-major (qm x cap) == row-major U^T
@@ -750,12 +796,14 @@ int numeric_post(hsc_ctx* ctx, System& S, cudaStream_t st, bool allow_sync) {
         if (ctx->block_layout && S.blk_C.p)  // the block preconditioner's operator needs C itself
             CK(cudaMemcpyAsync(S.blk_C.p, S.C.p, sizeof(double) * S.kmax * S.kmax, cudaMemcpyDeviceToDevice, st));
         launch_ldlt(S.C.as<double>(), S.kmax, dk, S.Lc.as<double>(), S.dpiv.as<double>(), &ds->bad_ldlt, st);
-        // Vt^T (k x a row-major == Vt column-major a x k) = Lc^T V^T
-        CK(cudaMemsetAsync(S.vt64.p, 0, sizeof(double) * S.a * S.kmax, st));
-        gemm(S.Lc.as<double>(), S.kmax, 1, S.V.as<double>(), S.a, 0, S.vt64.as<double>(), S.a, S.kmax, S.a, S.kmax,
-             1.0, 0.0, st, dk, nullptr, dk);
-        // the PCG's copy: rows in internal node order (actp)
-        launch_gather_rows(S.vt64.as<double>(), S.a, S.kmax, S.actperm.as<int>(), S.vt64p.as<double>(), st);
+        if (!ctx->block_layout) {  // the block form applies V C V^T from V and C
+            // Vt^T (k x a row-major == Vt column-major a x k) = Lc^T V^T
+            CK(cudaMemsetAsync(S.vt64.p, 0, sizeof(double) * S.a * S.kmax, st));
+            gemm(S.Lc.as<double>(), S.kmax, 1, S.V.as<double>(), S.a, 0, S.vt64.as<double>(), S.a, S.kmax, S.a,
+                 S.kmax, 1.0, 0.0, st, dk, nullptr, dk);
+            // the PCG's copy: rows in internal node order (actp)
+            launch_gather_rows(S.vt64.as<double>(), S.a, S.kmax, S.actperm.as<int>(), S.vt64p.as<double>(), st);
+        }
     }
     stage_mark(ctx, 4, st);
     return HSC_OK;
@@ -1188,7 +1236,8 @@ int build_block_plan(hsc_ctx* ctx, System& S, cudaStream_t st) {
     if (!ctx->resident || ctx->grid < 1) return fail(ctx, HSC_ERR_INVALID, "the block preconditioner needs the resident CTA windows");
     const int G = ctx->grid;
     // cta rows / coupled ranges as build_partition placed them
-    std::vector<int> cta_row(2 * G), cta_act(2 * G), cta_aidx(G), win_off(G + 1);
+    std::vector<int> cta_row(2 * G), cta_act(2 * G), cta_aidx(G), win_off(G + 1), win_own(G);
+    CK(cudaMemcpyAsync(win_own.data(), ctx->d_win_own.p, sizeof(int) * G, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(cta_row.data(), ctx->d_cta_row.p, sizeof(int) * 2 * G, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(cta_act.data(), ctx->d_cta_act.p, sizeof(int) * 2 * G, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(cta_aidx.data(), ctx->d_cta_aidx.p, sizeof(int) * G, cudaMemcpyDeviceToHost, st));
@@ -1256,14 +1305,76 @@ int build_block_plan(hsc_ctx* ctx, System& S, cudaStream_t st) {
     int nact_cta = 0;
     for (int c = 0; c < G; ++c) nact_cta += cta_aidx[c] >= 0;
     // maxima for the shared-memory layout
-    int R = 1, BLK = 1, W = 1, NA = 1;
+    int R = 1, W = 1, NA = 1;
     for (int c = 0; c < G; ++c) {
         const int rb = cta_row[2 * c], re = cta_row[2 * c + 1];
         R = std::max(R, re - rb);
-        BLK = std::max(BLK, S.h_rowptr[re] - S.h_rowptr[rb]);
         W = std::max(W, win_off[c + 1] - win_off[c]);
         NA = std::max(NA, cta_act[2 * c + 1] - cta_act[2 * c]);
     }
+    if (R > kBlockMaxRows)
+        return fail(ctx, HSC_ERR_INVALID, "a part of the block preconditioner has more rows than one CTA holds");
+    if (S.h_lcol.size() != (size_t)S.nnz)
+        return fail(ctx, HSC_ERR_INVALID, "the block preconditioner needs the CTA windows of the BSR entries");
+    // sliced ELL of each CTA's rows: slices of kSliceRows rows; a row's slots are its diagonal block,
+    // its blocks whose column lies in the part (ascending), the others (ascending), then padding to
+    // the slice's even width; lane 2 r + h of chunk c holds slot 2 c + h of the slice's row r
+    std::vector<int4> sslice;
+    std::vector<int> cslice(G + 1, 0), cchunk(G + 1, 0), ssrc;
+    std::vector<unsigned short> nloc(std::max(1, S.n), 0), slc;
+    int NS = 1, NCH = 1;
+    {
+        std::vector<int> order;
+        std::vector<std::vector<int>> rowslots(kSliceRows);
+        for (int c = 0; c < G; ++c) {
+            const int rb = cta_row[2 * c], re = cta_row[2 * c + 1];
+            int ch_rel = 0;
+            for (int r0 = rb; r0 < re; r0 += kSliceRows) {
+                const int r1 = std::min(re, r0 + kSliceRows);
+                int width = 0, lwidth = 0;
+                for (int r = r0; r < r1; ++r) {
+                    std::vector<int>& sl = rowslots[r - r0];
+                    sl.clear();
+                    int diag = -1;
+                    for (int e = S.h_rowptr[r]; e < S.h_rowptr[r + 1]; ++e)
+                        if (S.h_colidx[e] == r) diag = e;
+                    sl.push_back(diag);
+                    for (int e = S.h_rowptr[r]; e < S.h_rowptr[r + 1]; ++e) {
+                        const int col = S.h_colidx[e];
+                        if (col >= rb && col < re && S.h_lcol[e] != win_own[c] + (col - rb))
+                            return fail(ctx, HSC_ERR_INVALID, "a part's rows are not contiguous in its window");
+                        if (col != r && col >= rb && col < re) sl.push_back(e);
+                    }
+                    nloc[r] = (unsigned short)sl.size();
+                    for (int e = S.h_rowptr[r]; e < S.h_rowptr[r + 1]; ++e) {
+                        const int col = S.h_colidx[e];
+                        if (col < rb || col >= re) sl.push_back(e);
+                    }
+                    width = std::max(width, (int)sl.size());
+                    lwidth = std::max(lwidth, (int)nloc[r]);
+                }
+                const int nch = (width + 1) / 2;
+                sslice.push_back(make_int4(ch_rel, nch, (lwidth + 1) / 2, 0));
+                const size_t base = ssrc.size();
+                ssrc.resize(base + (size_t)32 * nch, -1);
+                slc.resize(base + (size_t)32 * nch, (unsigned short)win_own[c]);
+                for (int r = r0; r < r1; ++r) {
+                    const std::vector<int>& sl = rowslots[r - r0];
+                    for (int j = 0; j < (int)sl.size(); ++j) {
+                        const size_t at = base + (size_t)32 * (j / 2) + 2 * (r - r0) + (j & 1);
+                        ssrc[at] = sl[j];
+                        slc[at] = sl[j] >= 0 ? S.h_lcol[sl[j]] : (unsigned short)win_own[c];
+                    }
+                }
+                ch_rel += nch;
+            }
+            cslice[c + 1] = (int)sslice.size();
+            cchunk[c + 1] = cchunk[c] + ch_rel;
+            NS = std::max(NS, cslice[c + 1] - cslice[c]);
+            NCH = std::max(NCH, ch_rel);
+        }
+    }
+    const long long nchunk = cchunk[G];
     const int km = std::max(1, S.kmax);
     const size_t n4 = 4 * (size_t)std::max(1, S.n);
     GROW(S.blk_Y, sizeof(float) * km * n4);
@@ -1290,6 +1401,22 @@ int build_block_plan(hsc_ctx* ctx, System& S, cudaStream_t st) {
     GROW(S.blk_cta_comp_slot, sizeof(int) * std::max<size_t>(1, cta_comp_slot.size()));
     GROW(S.blk_comp_slot_ptr, sizeof(int) * (ncomp + 1));
     GROW(S.blk_comp_of_body, sizeof(int) * std::max(1, nbody));
+    GROW(S.blk_sslice, sizeof(int4) * std::max<size_t>(1, sslice.size()));
+    GROW(S.blk_cslice, sizeof(int) * (G + 1));
+    GROW(S.blk_cchunk, sizeof(int) * (G + 1));
+    GROW(S.blk_nloc, sizeof(unsigned short) * nloc.size());
+    GROW(S.blk_slc, sizeof(unsigned short) * std::max<size_t>(1, slc.size()));
+    GROW(S.blk_ssrc, sizeof(int) * std::max<size_t>(1, ssrc.size()));
+    GROW(S.blk_svals, (o.precision ? sizeof(float) : sizeof(double)) * kChunkVals * std::max<long long>(1, nchunk));
+    if (!sslice.empty())
+        CK(cudaMemcpyAsync(S.blk_sslice.p, sslice.data(), sizeof(int4) * sslice.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(S.blk_cslice.p, cslice.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(S.blk_cchunk.p, cchunk.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(S.blk_nloc.p, nloc.data(), sizeof(unsigned short) * nloc.size(), cudaMemcpyHostToDevice, st));
+    if (!slc.empty()) {
+        CK(cudaMemcpyAsync(S.blk_slc.p, slc.data(), sizeof(unsigned short) * slc.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(S.blk_ssrc.p, ssrc.data(), sizeof(int) * ssrc.size(), cudaMemcpyHostToDevice, st));
+    }
     if (S.blk_ident.cap < sizeof(double) * km * km) {
         GROW(S.blk_ident, sizeof(double) * km * km);
         std::vector<double> I((size_t)km * km, 0.0);
@@ -1310,7 +1437,6 @@ int build_block_plan(hsc_ctx* ctx, System& S, cudaStream_t st) {
     b = BlockPlan{};
     b.n = S.n; b.nnz = S.nnz; b.a = S.a; b.kmax = km; b.qm = S.qm;
     b.rank = &S.scal.as<DevScal>()->rank;
-    b.rowptr = S.rowptr.as<int>(); b.colidx = S.colidx.as<int>();
     b.vals = o.precision ? S.vf32.p : S.v64.p;
     b.dinv = S.dinv.p;
     b.dact = o.precision ? S.dact.as<double>() : nullptr;
@@ -1325,7 +1451,9 @@ int build_block_plan(hsc_ctx* ctx, System& S, cudaStream_t st) {
     b.G_ctas = G;
     b.cta_row = ctx->d_cta_row.as<int>(); b.cta_act = ctx->d_cta_act.as<int>(); b.cta_aidx = ctx->d_cta_aidx.as<int>();
     b.win_off = ctx->d_win_off.as<int>(); b.win_nodes = ctx->d_win_nodes.as<int>(); b.win_own = ctx->d_win_own.as<int>();
-    b.lcol = S.lcol.as<unsigned short>();
+    b.sell_slice = S.blk_sslice.as<int4>(); b.cta_slice = S.blk_cslice.as<int>(); b.cta_chunk = S.blk_cchunk.as<int>();
+    b.sell_nloc = S.blk_nloc.as<unsigned short>(); b.sell_lc = S.blk_slc.as<unsigned short>();
+    b.sell_src = S.blk_ssrc.as<int>(); b.sell_vals = S.blk_svals.p; b.nchunk = nchunk;
     b.ncomp = ncomp;
     b.comp_of_body = S.blk_comp_of_body.as<int>();
     b.cta_comp_ptr = S.blk_cta_comp_ptr.as<int>(); b.cta_comp = S.blk_cta_comp.as<int>();
@@ -1337,7 +1465,7 @@ int build_block_plan(hsc_ctx* ctx, System& S, cudaStream_t st) {
     b.bar = ctx->d_bar.as<GridBar>();
     b.out = S.scal.as<DevScal>()->pcg;
     b.cg_coef = S.cg.as<double>(); b.max_coef = kMaxCoef;
-    b.R = R; b.BLK = BLK; b.W = W; b.NA = NA; b.NCOL = NCOL;
+    b.R = R; b.NS = NS; b.NCH = NCH; b.W = W; b.NA = NA; b.NCOL = NCOL;
     // stage the value planes and the Y columns when they fit, the planes first
     const size_t cap = (size_t)block_max_smem();
     if (block_smem_bytes(o.precision, b, true, true) > cap && block_smem_bytes(o.precision, b, true, false) > cap)
@@ -1370,6 +1498,7 @@ int launch_block_solve(hsc_ctx* ctx, System& S, cudaStream_t st) {
     // grid barriers: two per iteration, two more per true-residual check
     if ((double)(o.max_iter + 4) * 4 * b.G_ctas >= (double)kBarAbortBit)
         return fail(ctx, HSC_ERR_INVALID, "max_iter too large for the grid barrier counter");
+    launch_block_fill(o.precision, b, st);
     if (S.kmax > 0) {
         launch_block_columns(b, st);
         CK(launch_block_y(o.precision, b, st));
@@ -1518,9 +1647,13 @@ int ensure_common(hsc_ctx* ctx, cudaStream_t st) {
     GROW(ctx->res_part, sizeof(double) * 3 * kResParts);
     GROW(ctx->feat_part, sizeof(double) * kFeatParts * 2 * std::max(1, ctx->num_sms));
     if (!ctx->aca_grid) ctx->aca_grid = std::min(4096, std::max(1, aca_blocks_per_sm()) * ctx->num_sms);
-    if (!ctx->ev[0])
+    if (!ctx->ev[0]) {
         for (auto& e : ctx->ev) CK(cudaEventCreate(&e));
         CK(cudaEventCreate(&ctx->ev_blk));
+        CK(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+        CK(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+    }
     (void)st;
     return HSC_OK;
 }
@@ -1709,6 +1842,10 @@ void hsc_destroy(hsc_ctx* ctx) {
     if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
+    if (ctx->ev_blk) cudaEventDestroy(ctx->ev_blk);
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
     if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
     delete ctx;
@@ -1787,11 +1924,21 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
             if (r2) return r2;
         }
         stage_mark(ctx, 1, st);
+        // the ABD inverses (A only) run on the side stream beside the ACA (E only)
+        CK(cudaEventRecord(ctx->ev_fork, st));
+        CK(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
+        for (int s = 0; s < count; ++s) {
+            int r2 = abd_inverse(ctx, ctx->sys[s], ctx->side, allow_sync);
+            if (r2) return r2;
+        }
+        CK(cudaEventRecord(ctx->ev_join, ctx->side));
         int r1 = aca_all(ctx, count, st);
         if (r1) return r1;
         stage_mark(ctx, 2, st);
+        CK(cudaStreamWaitEvent(st, ctx->ev_join, 0));
+        stage_mark(ctx, 3, st);
         for (int s = 0; s < count; ++s) {
-            int r2 = numeric_post(ctx, ctx->sys[s], st, allow_sync);
+            int r2 = numeric_post(ctx, ctx->sys[s], st);
             if (r2) return r2;
             schur_rhs(ctx->sys[s], d_b[s], st);
         }

@@ -11,6 +11,9 @@ namespace hsc {
 
 namespace {
 
+// the storage type of Dd^-1: float beside the FP32 planes, double beside FP64 ones.  The
+// arithmetic is FP64 throughout: the Woodbury core amplifies any difference between the L that
+// built Y and the L the PCG applies, so L must be the same linear map to FP64 rounding.
 template <class MT> struct BlkDinv { using T = float; };
 template <> struct BlkDinv<double> { using T = double; };
 
@@ -30,22 +33,82 @@ __device__ __forceinline__ void blk_dinv(const DT* sd, int stride, int lr, doubl
     o2 = s * ((double)d[6 * stride] * r0 + (double)d[7 * stride] * r1 + (double)d[8 * stride] * r2);
 }
 
+// the 3x3 block (row-major: y_r = sum_c b[3 r + c] x_c) of lane `lane` in a chunk of kChunkVals
+// values: planes 0-3 as [lane][4], planes 4-7 as [lane][4], plane 8 as [lane]
+template <class MT>
+__device__ __forceinline__ void ld_blk(const MT* chunk, int lane, bool global, MT b[9]) {
+    if constexpr (std::is_same<MT, float>::value) {
+        const float4* c0 = reinterpret_cast<const float4*>(chunk) + lane;
+        const float4* c1 = reinterpret_cast<const float4*>(chunk + 128) + lane;
+        const float4 q0 = global ? __ldg(c0) : *c0;
+        const float4 q1 = global ? __ldg(c1) : *c1;
+        b[0] = q0.x; b[1] = q0.y; b[2] = q0.z; b[3] = q0.w;
+        b[4] = q1.x; b[5] = q1.y; b[6] = q1.z; b[7] = q1.w;
+        b[8] = global ? __ldg(chunk + 256 + lane) : chunk[256 + lane];
+    } else {
+        const double2* c0 = reinterpret_cast<const double2*>(chunk) + 2 * lane;
+        const double2* c1 = reinterpret_cast<const double2*>(chunk + 128) + 2 * lane;
+        const double2 q0 = global ? __ldg(c0) : c0[0], q1 = global ? __ldg(c0 + 1) : c0[1];
+        const double2 q2 = global ? __ldg(c1) : c1[0], q3 = global ? __ldg(c1 + 1) : c1[1];
+        b[0] = q0.x; b[1] = q0.y; b[2] = q1.x; b[3] = q1.y;
+        b[4] = q2.x; b[5] = q2.y; b[6] = q3.x; b[7] = q3.y;
+        b[8] = global ? __ldg(chunk + 256 + lane) : chunk[256 + lane];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// sliced-ELL values from the BSR planes: one thread per slot (padding slots get zeros)
+// ---------------------------------------------------------------------------
+template <class MT>
+__global__ void block_fill_kernel(const BlockPlan p) {
+    const long long nslot = p.nchunk * 32;
+    const MT* vals = reinterpret_cast<const MT*>(p.vals);
+    MT* out = reinterpret_cast<MT*>(p.sell_vals);
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nslot; e += (long long)gridDim.x * blockDim.x) {
+        const int src = p.sell_src[e];
+        const int lane = (int)(e & 31);
+        MT b[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) b[q] = src >= 0 ? vals[(size_t)q * p.nnz + src] : MT(0);
+        MT* c = out + (e >> 5) * kChunkVals;
+        if constexpr (std::is_same<MT, float>::value) {
+            reinterpret_cast<float4*>(c)[lane] = make_float4(b[0], b[1], b[2], b[3]);
+            reinterpret_cast<float4*>(c + 128)[lane] = make_float4(b[4], b[5], b[6], b[7]);
+        } else {
+            reinterpret_cast<double2*>(c)[2 * lane] = make_double2(b[0], b[1]);
+            reinterpret_cast<double2*>(c)[2 * lane + 1] = make_double2(b[2], b[3]);
+            reinterpret_cast<double2*>(c + 128)[2 * lane] = make_double2(b[4], b[5]);
+            reinterpret_cast<double2*>(c + 128)[2 * lane + 1] = make_double2(b[6], b[7]);
+        }
+        c[256 + lane] = b[8];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // columns of each coupling component: the body of U[:, j]'s first nonzero row
-// gives its component; counting sort into comp_col_ptr / comp_cols (one CTA)
+// gives its component (a warp per column, its lanes over 32 rows at a time);
+// counting sort into comp_col_ptr / comp_cols (one CTA, kmax <= kMaxRank)
 // ---------------------------------------------------------------------------
-__global__ void block_columns_kernel(BlockPlan p) {
+__global__ void __launch_bounds__(256) block_columns_kernel(BlockPlan p) {
     __shared__ int s_cnt[257];
+    __shared__ int s_comp[kMaxRank];
     const int k = *p.rank;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     for (int g = threadIdx.x; g <= p.ncomp; g += blockDim.x) s_cnt[g] = 0;
     __syncthreads();
-    for (int j = threadIdx.x; j < p.kmax; j += blockDim.x) {
+    for (int j = warp; j < p.kmax; j += nwarps) {
         int comp = -1;
         if (j < k)
-            for (int i = 0; i < p.qm; ++i)
-                if (p.U[(size_t)j * p.qm + i] != 0.0) { comp = p.comp_of_body[i / 12]; break; }
-        p.comp_of_col[j] = comp;
-        if (comp >= 0) atomicAdd(&s_cnt[comp + 1], 1);
+            for (int i0 = 0; i0 < p.qm; i0 += 32) {
+                const int i = i0 + lane;
+                const unsigned nz = __ballot_sync(0xffffffffu, i < p.qm && p.U[(size_t)j * p.qm + i] != 0.0);
+                if (nz) { comp = p.comp_of_body[(i0 + __ffs(nz) - 1) / 12]; break; }
+            }
+        if (lane == 0) {
+            s_comp[j] = comp;
+            p.comp_of_col[j] = comp;
+            if (comp >= 0) atomicAdd(&s_cnt[comp + 1], 1);
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -53,7 +116,7 @@ __global__ void block_columns_kernel(BlockPlan p) {
         for (int g = 0; g <= p.ncomp; ++g) p.comp_col_ptr[g] = s_cnt[g];
         // columns in increasing order inside each component (deterministic)
         for (int j = 0; j < k; ++j) {
-            const int comp = p.comp_of_col[j];
+            const int comp = s_comp[j];
             if (comp >= 0) p.comp_cols[s_cnt[comp]++] = j;
         }
     }
@@ -82,225 +145,169 @@ __device__ int build_cols(const BlockPlan& p, int cta, int* s_cols, int* s_slot)
 }
 
 // ---------------------------------------------------------------------------
-// shared-memory staging of a CTA's rows: local row pointers, window positions of
-// the blocks' columns, value planes (when staged), Dd^-1 planes, window node ids
+// shared-memory staging of a CTA's part: its slices, the rows' local slot
+// counts, the slots' window positions, the value chunks (when staged), the
+// Dd^-1 planes, the coupled rows' FP64 diagonal blocks (mixed modes) and (for
+// the operator) the window node ids
 // ---------------------------------------------------------------------------
 template <class MT>
-struct Slice {
-    int rb, re, R, kb0, nblk, wn0, nwin, wown, ab, ae, na;
-    int* rp;
-    unsigned short* lc;
-    const MT* val;        // planes, stride pstride (shared or global)
-    size_t pstride;
+struct Part {
+    int rb, re, R, ns, nch, wn0, nwin, wown, ab, ae, na;
+    const int4* meta;                  // per slice: first chunk (from the CTA's first), chunks, local chunks
+    const unsigned short* nloc;        // per row: slots holding its diagonal and local blocks
+    const unsigned short* lc;          // per slot: window position
+    const MT* val;                     // chunks (shared or global)
     const typename BlkDinv<MT>::T* dinv;  // planes, stride R
+    const int* aflag;                  // per row: its coupled node among the CTA's, or -1
+    const double* dact;                // 9 per coupled node of the CTA (mixed modes), else null
     int* wn;
 };
 
 template <class MT>
-__device__ Slice<MT> stage_slice(const BlockPlan& p, int cta, unsigned char* sm) {
+__device__ Part<MT> stage_part(const BlockPlan& p, int cta, unsigned char* sm, bool window) {
     using DT = typename BlkDinv<MT>::T;
-    Slice<MT> s;
+    Part<MT> s;
     s.rb = p.cta_row[2 * cta];
     s.re = p.cta_row[2 * cta + 1];
     s.R = s.re - s.rb;
-    s.kb0 = __ldg(p.rowptr + s.rb);
-    s.nblk = __ldg(p.rowptr + s.re) - s.kb0;
+    const int sl0 = p.cta_slice[cta];
+    s.ns = p.cta_slice[cta + 1] - sl0;
+    const long long ch0 = p.cta_chunk[cta];
+    s.nch = p.cta_chunk[cta + 1] - (int)ch0;
     s.wn0 = p.win_off[cta];
     s.nwin = p.win_off[cta + 1] - s.wn0;
     s.wown = p.win_own[cta];
     s.ab = p.cta_act[2 * cta];
     s.ae = p.cta_act[2 * cta + 1];
     s.na = s.ae - s.ab;
-    s.rp = reinterpret_cast<int*>(sm + p.off_rp);
-    s.lc = reinterpret_cast<unsigned short*>(sm + p.off_lc);
-    s.wn = reinterpret_cast<int*>(sm + p.off_wn);
+    int4* meta = reinterpret_cast<int4*>(sm + p.off_meta);
+    unsigned short* nloc = reinterpret_cast<unsigned short*>(sm + p.off_nloc);
+    unsigned short* lc = reinterpret_cast<unsigned short*>(sm + p.off_lc);
     DT* sd = reinterpret_cast<DT*>(sm + p.off_dinv);
-    const MT* vals = reinterpret_cast<const MT*>(p.vals);
+    s.wn = reinterpret_cast<int*>(sm + p.off_wn);
     const DT* dinv = reinterpret_cast<const DT*>(p.dinv);
-    for (int e = threadIdx.x; e <= s.R; e += blockDim.x) s.rp[e] = __ldg(p.rowptr + s.rb + e) - s.kb0;
-    for (int e = threadIdx.x; e < s.nblk; e += blockDim.x) s.lc[e] = p.lcol[s.kb0 + e];
-    for (int e = threadIdx.x; e < s.nwin; e += blockDim.x) s.wn[e] = p.win_nodes[s.wn0 + e];
+    const MT* vals = reinterpret_cast<const MT*>(p.sell_vals) + ch0 * kChunkVals;
+    for (int e = threadIdx.x; e < s.ns; e += blockDim.x) meta[e] = p.sell_slice[sl0 + e];
+    for (int e = threadIdx.x; e < s.R; e += blockDim.x) nloc[e] = p.sell_nloc[s.rb + e];
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(p.sell_lc + ch0 * 32);  // 64 B per chunk
+        uint4* dst = reinterpret_cast<uint4*>(lc);
+        for (int e = threadIdx.x; e < 4 * s.nch; e += blockDim.x) dst[e] = __ldg(src + e);
+    }
+    if (window)
+        for (int e = threadIdx.x; e < s.nwin; e += blockDim.x) s.wn[e] = p.win_nodes[s.wn0 + e];
     for (int e = threadIdx.x; e < 9 * s.R; e += blockDim.x) {
         const int pl = e / s.R, lr = e - pl * s.R;
         sd[e] = dinv[(size_t)pl * p.n + s.rb + lr];
     }
-    if (p.stage_vals) {
-        MT* sv = reinterpret_cast<MT*>(sm + p.off_val);
-        for (int e = threadIdx.x; e < 9 * s.nblk; e += blockDim.x) {
-            const int pl = e / s.nblk, kl = e - pl * s.nblk;
-            sv[e] = vals[(size_t)pl * p.nnz + s.kb0 + kl];
-        }
-        s.val = sv;
-        s.pstride = (size_t)s.nblk;
-    } else {
-        s.val = vals + s.kb0;
-        s.pstride = (size_t)p.nnz;
+    int* aflag = reinterpret_cast<int*>(sm + p.off_aflag);
+    for (int e = threadIdx.x; e < s.R; e += blockDim.x) {
+        const int an = p.rowflag[s.rb + e];
+        aflag[e] = an >= 0 ? an - s.ab / 3 : -1;
     }
+    double* sdact = reinterpret_cast<double*>(sm + p.off_dact);
+    if (p.dact)
+        for (int e = threadIdx.x; e < 3 * s.na; e += blockDim.x) sdact[e] = p.dact[(size_t)3 * s.ab + e];
+    s.aflag = aflag;
+    s.dact = p.dact ? sdact : nullptr;
+    if (p.stage_vals) {
+        const int4* src = reinterpret_cast<const int4*>(vals);
+        int4* dst = reinterpret_cast<int4*>(sm + p.off_val);
+        const int n16 = (int)(s.nch * kChunkVals * sizeof(MT) / 16);
+        for (int e = threadIdx.x; e < n16; e += blockDim.x) dst[e] = __ldg(src + e);
+        s.val = reinterpret_cast<const MT*>(sm + p.off_val);
+    } else {
+        s.val = vals;
+    }
+    s.meta = meta;
+    s.nloc = nloc;
+    s.lc = lc;
     s.dinv = sd;
     __syncthreads();
     return s;
 }
 
-template <class MT>
-__device__ __forceinline__ double ldv(const Slice<MT>& s, size_t off, bool global) {
-    return global ? (double)__ldg(s.val + off) : (double)s.val[off];
-}
-
-// y_row = sum over the row's blocks B x[col], four threads per row, for the
-// CTA's own rows.  `local` restricts to the blocks whose column is an own row
-// (D_loc) and then reads x from the own-row vector xo (3 per row); otherwise x
-// comes from the staged window xw (4 per window node).  Fixed summation order.
-template <class MT, class Epi>
-__device__ __forceinline__ void slice_spmv(const Slice<MT>& s, bool gvals, bool local, const double* xo,
-                                           const double* xw, Epi& epi) {
-    const int sub = threadIdx.x & 3;
-    for (int lr0 = 0; lr0 < s.R; lr0 += blockDim.x / 4) {
-        const int lr = lr0 + (threadIdx.x >> 2);
-        double a0 = 0, a1 = 0, a2 = 0;
-        if (lr < s.R) {
-            const int k1 = s.rp[lr + 1];
-            for (int kk = s.rp[lr] + sub; kk < k1; kk += 4) {
-                const int w = s.lc[kk];
-                double x0, x1, x2;
-                if (local) {
-                    const int ol = w - s.wown;
-                    if (ol < 0 || ol >= s.R) continue;
-                    x0 = xo[3 * ol]; x1 = xo[3 * ol + 1]; x2 = xo[3 * ol + 2];
-                } else {
-                    x0 = xw[4 * w]; x1 = xw[4 * w + 1]; x2 = xw[4 * w + 2];
-                }
-                const size_t o = kk, ps = s.pstride;
-                a0 += ldv(s, o, gvals) * x0 + ldv(s, o + ps, gvals) * x1 + ldv(s, o + 2 * ps, gvals) * x2;
-                a1 += ldv(s, o + 3 * ps, gvals) * x0 + ldv(s, o + 4 * ps, gvals) * x1 + ldv(s, o + 5 * ps, gvals) * x2;
-                a2 += ldv(s, o + 6 * ps, gvals) * x0 + ldv(s, o + 7 * ps, gvals) * x1 + ldv(s, o + 8 * ps, gvals) * x2;
-            }
-        }
-        a0 += __shfl_xor_sync(0xffffffffu, a0, 1);
-        a1 += __shfl_xor_sync(0xffffffffu, a1, 1);
-        a2 += __shfl_xor_sync(0xffffffffu, a2, 1);
-        a0 += __shfl_xor_sync(0xffffffffu, a0, 2);
-        a1 += __shfl_xor_sync(0xffffffffu, a1, 2);
-        a2 += __shfl_xor_sync(0xffffffffu, a2, 2);
-        if (lr < s.R && sub == 0) epi(lr, a0, a1, a2);
-    }
-}
-
-// the FP64 diagonal block of a coupled node (mixed modes keep it out of the planes)
-__device__ __forceinline__ void add_dact(const BlockPlan& p, int node, double x0, double x1, double x2, double& y0,
-                                         double& y1, double& y2) {
-    const int an = p.rowflag[node];
-    if (an < 0) return;
-    const double* d = p.dact + 9 * (size_t)an;
-    y0 += d[0] * x0 + d[1] * x1 + d[2] * x2;
-    y1 += d[3] * x0 + d[4] * x1 + d[5] * x2;
-    y2 += d[6] * x0 + d[7] * x1 + d[8] * x2;
-}
-
 __device__ __forceinline__ double poly_weight(const BlockPlan& p, int k) { return p.wdev ? p.wdev[k] : p.w[k]; }
 
-// z = L v over the CTA's rows (v, z, t, u: 3 R doubles in shared memory; t and u
-// are scratch).  Each term is one local SpMV; no grid barrier.
-template <class MT>
-__device__ void local_poly(const BlockPlan& p, const Slice<MT>& s, bool split, const double* v, double* z, double* t,
-                           double* u) {
-    using DT = typename BlkDinv<MT>::T;
-    const bool gv = !p.stage_vals;
-    const double w0 = poly_weight(p, 0);
-    for (int e = threadIdx.x; e < s.R; e += blockDim.x) {
-        double o0, o1, o2;
-        blk_dinv<DT>(s.dinv, s.R, e, p.omega, v[3 * e], v[3 * e + 1], v[3 * e + 2], o0, o1, o2);
-        t[3 * e] = o0; t[3 * e + 1] = o1; t[3 * e + 2] = o2;
-        z[3 * e] = w0 * o0; z[3 * e + 1] = w0 * o1; z[3 * e + 2] = w0 * o2;
-    }
-    __syncthreads();
-    double* tc = t;
-    double* tn = u;
-    for (int k = 1; k < p.nterms; ++k) {
-        const double wk = poly_weight(p, k);
-        auto epi = [&](int lr, double y0, double y1, double y2) {
-            const double c0 = tc[3 * lr], c1 = tc[3 * lr + 1], c2 = tc[3 * lr + 2];
-            if (split) add_dact(p, s.rb + lr, c0, c1, c2, y0, y1, y2);
-            double e0, e1, e2;
-            blk_dinv<DT>(s.dinv, s.R, lr, p.omega, y0, y1, y2, e0, e1, e2);
-            const double n0 = c0 - e0, n1 = c1 - e1, n2 = c2 - e2;
-            tn[3 * lr] = n0; tn[3 * lr + 1] = n1; tn[3 * lr + 2] = n2;
-            z[3 * lr] += wk * n0; z[3 * lr + 1] += wk * n1; z[3 * lr + 2] += wk * n2;
-        };
-        slice_spmv<MT>(s, gv, true, tc, nullptr, epi);
-        __syncthreads();
-        double* tmp = tc; tc = tn; tn = tmp;
-    }
-}
-
-// the same polynomial on NB vectors at once (column c of an NB-batch at offset
-// c * 3 p.R): one pass over the blocks per term serves all NB
+// z_c = L v_c for the NB vectors c of a batch, over the CTA's rows:
+//   t_0 = w Dd^-1 v,  t_k = (1 - w) t_{k-1} - w Dd^-1 (O t_{k-1}),  z = sum_k w_k t_k,
+// O the blocks between two different rows of the part (Dd^-1 D_loc = I + Dd^-1 O), so each
+// term is one pass over the rows' local slots and no grid barrier.  In the mixed modes a
+// coupled row keeps t_k = t_{k-1} - w Dd^-1 (Dc t_{k-1} + O t_{k-1}) with its FP64 diagonal block
+// Dc: D - V C V^T cancels most of Dc there, and a Dd^-1 rounded to FP32 is not Dc's inverse
+// closely enough to drop the product (about a third more PCG iterations on a vehicle).
+// v, z, t, u: NB x 3R doubles (3 per row; stride ld).  Rows are 24 bytes apart, so the gathers
+// of a warp spread over the banks.  The slot loop has no branch (a slot that is not a local
+// block reads row 0 and adds zero), so consecutive slots' loads overlap.  Ends synchronised;
+// z holds the result.
 template <class MT, int NB>
-__device__ void local_poly_multi(const BlockPlan& p, const Slice<MT>& s, bool split, const double* v, double* z,
-                                 double* t, double* u) {
+__device__ void part_poly(const BlockPlan& p, const Part<MT>& s, const double* v, double* z, double* t, double* u,
+                          int ld) {
     using DT = typename BlkDinv<MT>::T;
     const bool gv = !p.stage_vals;
-    const int ld = 3 * p.R;
+    const double om = p.omega, om1 = 1.0 - p.omega;
     const double w0 = poly_weight(p, 0);
     for (int e = threadIdx.x; e < NB * s.R; e += blockDim.x) {
         const int c = e / s.R, lr = e - c * s.R;
-        const double* vc = v + (size_t)c * ld;
+        const size_t o = (size_t)c * ld + 3 * lr;
         double o0, o1, o2;
-        blk_dinv<DT>(s.dinv, s.R, lr, p.omega, vc[3 * lr], vc[3 * lr + 1], vc[3 * lr + 2], o0, o1, o2);
-        double* tc = t + (size_t)c * ld;
-        double* zc = z + (size_t)c * ld;
-        tc[3 * lr] = o0; tc[3 * lr + 1] = o1; tc[3 * lr + 2] = o2;
-        zc[3 * lr] = w0 * o0; zc[3 * lr + 1] = w0 * o1; zc[3 * lr + 2] = w0 * o2;
+        blk_dinv<DT>(s.dinv, s.R, lr, om, v[o], v[o + 1], v[o + 2], o0, o1, o2);
+        t[o] = o0; t[o + 1] = o1; t[o + 2] = o2;
+        z[o] = w0 * o0; z[o + 1] = w0 * o1; z[o + 2] = w0 * o2;
     }
     __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, h = lane & 1;
     double* tc = t;
     double* tn = u;
-    const int sub = threadIdx.x & 3;
     for (int k = 1; k < p.nterms; ++k) {
         const double wk = poly_weight(p, k);
-        for (int lr0 = 0; lr0 < s.R; lr0 += blockDim.x / 4) {
-            const int lr = lr0 + (threadIdx.x >> 2);
+        for (int sl = warp; sl < s.ns; sl += kWarps) {
+            const int4 m = s.meta[sl];
+            const int lr = kSliceRows * sl + (lane >> 1);
+            const bool ok = lr < s.R;
+            const int nl = ok ? (int)s.nloc[lr] : 0;
             double a[NB][3];
 #pragma unroll
             for (int c = 0; c < NB; ++c) a[c][0] = a[c][1] = a[c][2] = 0.0;
-            if (lr < s.R) {
-                const int k1 = s.rp[lr + 1];
-                for (int kk = s.rp[lr] + sub; kk < k1; kk += 4) {
-                    const int ol = (int)s.lc[kk] - s.wown;
-                    if (ol < 0 || ol >= s.R) continue;
-                    const size_t o = kk, ps = s.pstride;
-                    double b[9];
+#pragma unroll 2
+            for (int cc = 0; cc < m.z; ++cc) {
+                const int j = 2 * cc + h;
+                const bool use = j >= 1 && j < nl;  // slot 0 is the diagonal block
+                const int ch = m.x + cc;
+                const int ol = use ? (int)s.lc[ch * 32 + lane] - s.wown : 0;
+                MT b[9];
+                ld_blk<MT>(s.val + (size_t)ch * kChunkVals, lane, gv, b);
 #pragma unroll
-                    for (int e = 0; e < 9; ++e) b[e] = ldv(s, o + e * ps, gv);
-#pragma unroll
-                    for (int c = 0; c < NB; ++c) {
-                        const double* xc = tc + (size_t)c * ld + 3 * ol;
-                        const double x0 = xc[0], x1 = xc[1], x2 = xc[2];
-                        a[c][0] += b[0] * x0 + b[1] * x1 + b[2] * x2;
-                        a[c][1] += b[3] * x0 + b[4] * x1 + b[5] * x2;
-                        a[c][2] += b[6] * x0 + b[7] * x1 + b[8] * x2;
-                    }
+                for (int c = 0; c < NB; ++c) {
+                    const double* xc = tc + (size_t)c * ld + 3 * ol;
+                    const double x0 = use ? xc[0] : 0.0, x1 = use ? xc[1] : 0.0, x2 = use ? xc[2] : 0.0;
+                    a[c][0] += (double)b[0] * x0 + (double)b[1] * x1 + (double)b[2] * x2;
+                    a[c][1] += (double)b[3] * x0 + (double)b[4] * x1 + (double)b[5] * x2;
+                    a[c][2] += (double)b[6] * x0 + (double)b[7] * x1 + (double)b[8] * x2;
                 }
             }
 #pragma unroll
             for (int c = 0; c < NB; ++c)
 #pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    a[c][d] += __shfl_xor_sync(0xffffffffu, a[c][d], 1);
-                    a[c][d] += __shfl_xor_sync(0xffffffffu, a[c][d], 2);
-                }
-            if (lr < s.R && sub == 0) {
+                for (int d = 0; d < 3; ++d) a[c][d] += __shfl_xor_sync(0xffffffffu, a[c][d], 1);
+            if (ok && h == 0) {
+                const int an = s.dact ? s.aflag[lr] : -1;
 #pragma unroll
                 for (int c = 0; c < NB; ++c) {
-                    const double* cc = tc + (size_t)c * ld + 3 * lr;
-                    double y0 = a[c][0], y1 = a[c][1], y2 = a[c][2];
-                    const double c0 = cc[0], c1 = cc[1], c2 = cc[2];
-                    if (split) add_dact(p, s.rb + lr, c0, c1, c2, y0, y1, y2);
-                    double e0, e1, e2;
-                    blk_dinv<DT>(s.dinv, s.R, lr, p.omega, y0, y1, y2, e0, e1, e2);
-                    double* nn = tn + (size_t)c * ld + 3 * lr;
-                    double* zz = z + (size_t)c * ld + 3 * lr;
-                    nn[0] = c0 - e0; nn[1] = c1 - e1; nn[2] = c2 - e2;
-                    zz[0] += wk * nn[0]; zz[1] += wk * nn[1]; zz[2] += wk * nn[2];
+                    const size_t o = (size_t)c * ld + 3 * lr;
+                    const double c0 = tc[o], c1 = tc[o + 1], c2 = tc[o + 2];
+                    double f = om1, e0, e1, e2;
+                    if (an >= 0) {
+                        const double* d = s.dact + 9 * an;
+                        a[c][0] += d[0] * c0 + d[1] * c1 + d[2] * c2;
+                        a[c][1] += d[3] * c0 + d[4] * c1 + d[5] * c2;
+                        a[c][2] += d[6] * c0 + d[7] * c1 + d[8] * c2;
+                        f = 1.0;
+                    }
+                    blk_dinv<DT>(s.dinv, s.R, lr, om, a[c][0], a[c][1], a[c][2], e0, e1, e2);
+                    const double n0 = f * c0 - e0, n1 = f * c1 - e1, n2 = f * c2 - e2;
+                    tn[o] = n0; tn[o + 1] = n1; tn[o + 2] = n2;
+                    z[o] += wk * n0; z[o + 1] += wk * n1; z[o + 2] += wk * n2;
                 }
             }
         }
@@ -308,6 +315,54 @@ __device__ void local_poly_multi(const BlockPlan& p, const Slice<MT>& s, bool sp
         double* tmp = tc; tc = tn; tn = tmp;
     }
 }
+
+// out = D m over the CTA's rows: every slot of every row (padding slots, and the slots of the
+// rows past R, hold zeros and a valid window position), m from the staged window (3 doubles per
+// window node), FP64; in the mixed modes the coupled rows' diagonal blocks come from the staged
+// FP64 copies and `own`.
+template <class MT>
+__device__ void part_op(const Part<MT>& s, bool gv, const double* win, const double* own, double* out) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int sl = warp; sl < s.ns; sl += kWarps) {
+        const int4 m = s.meta[sl];
+        const int lr = kSliceRows * sl + (lane >> 1);
+        const bool ok = lr < s.R;
+        double a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll 2
+        for (int cc = 0; cc < m.y; ++cc) {
+            const int ch = m.x + cc;
+            const int w = s.lc[ch * 32 + lane];
+            MT b[9];
+            ld_blk<MT>(s.val + (size_t)ch * kChunkVals, lane, gv, b);
+            const double x0 = win[3 * w], x1 = win[3 * w + 1], x2 = win[3 * w + 2];
+            a0 += (double)b[0] * x0 + (double)b[1] * x1 + (double)b[2] * x2;
+            a1 += (double)b[3] * x0 + (double)b[4] * x1 + (double)b[5] * x2;
+            a2 += (double)b[6] * x0 + (double)b[7] * x1 + (double)b[8] * x2;
+        }
+        a0 += __shfl_xor_sync(0xffffffffu, a0, 1);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, 1);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, 1);
+        if (ok && (lane & 1) == 0) {
+            if (s.dact) {
+                const int an = s.aflag[lr];
+                if (an >= 0) {
+                    const double* d = s.dact + 9 * an;
+                    const double x0 = own[3 * lr], x1 = own[3 * lr + 1], x2 = own[3 * lr + 2];
+                    a0 += d[0] * x0 + d[1] * x1 + d[2] * x2;
+                    a1 += d[3] * x0 + d[4] * x1 + d[5] * x2;
+                    a2 += d[6] * x0 + d[7] * x1 + d[8] * x2;
+                }
+            }
+            out[3 * lr] = a0; out[3 * lr + 1] = a1; out[3 * lr + 2] = a2;
+        }
+    }
+}
+
+constexpr int kYBatch = 4;  // columns per pass of the Y kernel
+
+// doubles of the Y kernel's vector region: the batch's inputs and the polynomial's three
+// vectors, 3R per column each
+__host__ __device__ inline size_t y_region_doubles(int R) { return (size_t)4 * kYBatch * 3 * R; }
 
 // ---------------------------------------------------------------------------
 // Y = L V on each part (columns of the part's components), Y at the coupled
@@ -315,33 +370,33 @@ __device__ void local_poly_multi(const BlockPlan& p, const Slice<MT>& s, bool sp
 // ---------------------------------------------------------------------------
 template <class MT>
 __global__ void __launch_bounds__(kThreads, 1) block_y_kernel(const BlockPlan p_arg) {
+    using AT = double;
     __shared__ __align__(16) unsigned char s_p_raw[sizeof(BlockPlan)];
     BlockPlan& p = *reinterpret_cast<BlockPlan*>(s_p_raw);
     if (threadIdx.x == 0) p = p_arg;
     __syncthreads();
     extern __shared__ __align__(16) unsigned char sm[];
     const int cta = blockIdx.x;
-    const Slice<MT> s = stage_slice<MT>(p, cta, sm);
+    const Part<MT> s = stage_part<MT>(p, cta, sm, false);
     int* s_cols = reinterpret_cast<int*>(sm + p.off_cols);
     int* s_slot = s_cols + p.kmax;
     double* vec = reinterpret_cast<double*>(sm + p.off_vec);
     const int R3 = 3 * p.R;
-    double* v = vec;                 // four regions of 4 columns x 3 R doubles
-    double* z = vec + 4 * R3;
-    double* t = vec + 8 * R3;
-    double* u = vec + 12 * R3;
+    constexpr int NB = kYBatch;
+    double* v = vec;                                   // NB x 3R
+    AT* z = reinterpret_cast<AT*>(vec + NB * R3);      // NB x 4R each
+    AT* t = z + NB * R3;
+    AT* u = t + NB * R3;
     int* s_act = reinterpret_cast<int*>(sm + p.off_act);
     for (int e = threadIdx.x; e < s.na; e += blockDim.x) s_act[e] = p.actp[s.ab + e] - 3 * s.rb;
     const int ncols = build_cols(p, cta, s_cols, s_slot);
     const int k = *p.rank;
-    const bool split = p.dact != nullptr;
     // Y at the coupled dofs: zero the CTA's rows first (columns of other components stay zero)
     for (int e = threadIdx.x; e < s.na * p.kmax; e += blockDim.x) {
         const int j = e / s.na, il = e - j * s.na;
         p.Yact[(size_t)j * p.a + s.ab + il] = 0.0;
     }
     __syncthreads();
-    constexpr int NB = 4;  // columns per pass over the blocks
     for (int q0 = 0; q0 < ncols; q0 += NB) {
         for (int e = threadIdx.x; e < NB * R3; e += blockDim.x) v[e] = 0.0;
         __syncthreads();
@@ -350,19 +405,23 @@ __global__ void __launch_bounds__(kThreads, 1) block_y_kernel(const BlockPlan p_
             if (q0 + c < ncols) v[(size_t)c * R3 + s_act[il]] = p.V[(size_t)s_cols[q0 + c] * p.a + p.actperm[s.ab + il]];
         }
         __syncthreads();
-        local_poly_multi<MT, NB>(p, s, split, v, z, t, u);
+        part_poly<MT, NB>(p, s, v, z, t, u, R3);
+        // the PCG applies the FP32 copy of Y; the Woodbury core is built from the same rounded values
         for (int e = threadIdx.x; e < NB * s.R; e += blockDim.x) {
             const int c = e / s.R, lr = e - c * s.R;
             if (q0 + c >= ncols) continue;
-            const double* zc = z + (size_t)c * R3 + 3 * lr;
+            const AT* zr = z + (size_t)c * R3 + 3 * lr;
+            const AT z0 = zr[0], z1 = zr[1], z2 = zr[2];
             float* Yj = p.Y + (size_t)s_cols[q0 + c] * 4 * p.n;
-            reinterpret_cast<float4*>(Yj)[s.rb + lr] = make_float4((float)zc[0], (float)zc[1], (float)zc[2], 0.f);
+            reinterpret_cast<float4*>(Yj)[s.rb + lr] = make_float4((float)z0, (float)z1, (float)z2, 0.f);
         }
-        // the PCG applies the FP32 copy of Y; the Woodbury core is built from the same rounded values
         for (int e = threadIdx.x; e < NB * s.na; e += blockDim.x) {
             const int c = e / s.na, il = e - c * s.na;
-            if (q0 + c < ncols)
-                p.Yact[(size_t)s_cols[q0 + c] * p.a + s.ab + il] = (double)(float)z[(size_t)c * R3 + s_act[il]];
+            if (q0 + c < ncols) {
+                const int dof = s_act[il];
+                const AT zv = z[(size_t)c * R3 + dof];
+                p.Yact[(size_t)s_cols[q0 + c] * p.a + s.ab + il] = (double)(float)zv;
+            }
         }
         __syncthreads();
     }
@@ -382,7 +441,7 @@ __global__ void __launch_bounds__(kThreads, 1) block_y_kernel(const BlockPlan p_
         __syncthreads();  // the compact rows of V above are read back below
         double* Gc = p.pG + (size_t)aidx * p.kmax * p.kmax;
         for (int e = threadIdx.x; e < p.kmax * p.kmax; e += blockDim.x) Gc[e] = 0.0;
-        const bool staged = 2 * (size_t)s.na * ncols <= (size_t)16 * R3;
+        const bool staged = 2 * (size_t)s.na * ncols <= y_region_doubles(p.R);
         double* Vs = vec;
         double* Ys = vec + (size_t)s.na * ncols;
         if (staged)
@@ -445,7 +504,8 @@ __global__ void block_k_finish_kernel(double* K, int kmax, const int* dk, const 
 // ---------------------------------------------------------------------------
 // the pipelined PCG.  Per pass, with v the vector the preconditioner takes
 // (r on a (re)start, w otherwise):
-//   phase 1: mt = L v (local), partials of Y^T v and of the dots (r,u) (w,u) (r,r)
+//   phase 1: partials of Y^T v and of the dots (r,u) (w,u) (r,r), then
+//            mt = L v (local)
 //   -- grid barrier --
 //   phase 2: s = Y^T v, c = K s on the CTA's columns, m = mt + Y c (published),
 //            partials of V^T m; dots summed -> stop test, alpha, beta
@@ -458,11 +518,20 @@ __global__ void block_k_finish_kernel(double* K, int kmax, const int* dk, const 
 // recursive residual reaches tol, at max_iter, and every rr_every iterations;
 // if it fails the PCG restarts from the true residual.  Every CTA sums the same
 // partials in the same order, so all CTAs take the same decisions.
+//
+// Each thread owns dofs e = tid + kThreads i (i < kDofs) of the CTA's rows and
+// keeps x, r, u, p, s, q, z of them in registers; w, m and n, which other
+// threads read, live in shared memory.  The rows of K and C for the CTA's
+// columns (at most 32 columns of a rank of at most 128) live in registers too.
 // ---------------------------------------------------------------------------
 enum { kPassStart = 0, kPassNormal = 1 };
+constexpr int kDofs = 2;      // 3 R <= kDofs * kThreads  (R <= kBlockMaxRows)
+constexpr int kRegCols = 2;   // K and C rows held per warp
+constexpr int kRegK = 4;      // 32-wide strips of a K / C row per lane
 
 template <class MT>
 __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan p_arg) {
+    using AT = double;
     __shared__ __align__(16) unsigned char s_p_raw[sizeof(BlockPlan)];
     BlockPlan& p = *reinterpret_cast<BlockPlan*>(s_p_raw);
     if (threadIdx.x == 0) p = p_arg;
@@ -471,28 +540,21 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
     const int cta = blockIdx.x;
     const unsigned int G = gridDim.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const Slice<MT> sl = stage_slice<MT>(p, cta, sm);
+    const Part<MT> sl = stage_part<MT>(p, cta, sm, true);
     const bool gv = !p.stage_vals;
-    const bool split = p.dact != nullptr;
     const int R = sl.R, R3 = 3 * R, ld = 3 * p.R;
-    double* vec = reinterpret_cast<double*>(sm + p.off_vec);
-    double* X = vec;             // own-row vectors, 3 per row
-    double* Rr = vec + ld;
-    double* Uu = vec + 2 * ld;
-    double* Ww = vec + 3 * ld;
-    double* Pp = vec + 4 * ld;
-    double* Ss = vec + 5 * ld;
-    double* Qq = vec + 6 * ld;
-    double* Zz = vec + 7 * ld;
-    double* Mm = vec + 8 * ld;
-    double* Mt = vec + 9 * ld;
-    double* T0 = vec + 10 * ld;
-    double* T1 = vec + 11 * ld;
-    double* Nn = T0;             // n = S m (phase 3) reuses the polynomial's scratch (phase 1)
-    double* win = reinterpret_cast<double*>(sm + p.off_win);   // 4 per window node
+    AT* Pz = reinterpret_cast<AT*>(sm + p.off_vec);  // L v, then the polynomial's scratch
+    AT* Pt = Pz + ld;
+    AT* Pu = Pt + ld;
+    double* vec = Pu + ld;
+    double* Wb = vec;            // w (r on a (re)start): the preconditioner's input
+    double* Mm = vec + ld;       // m (x during a true-residual check)
+    double* Nn = vec + 2 * ld;   // n = S m
+    double* win = reinterpret_cast<double*>(sm + p.off_win);   // 3 per window node
     int* s_act = reinterpret_cast<int*>(sm + p.off_act);       // own coupled dofs, local (3 lr + d)
     int* s_cols = reinterpret_cast<int*>(sm + p.off_cols);
     int* s_slot = s_cols + p.kmax;
+    int* s_srng = reinterpret_cast<int*>(sm + p.off_srng);     // per column j < k: its component's slots
     double* s_sv = reinterpret_cast<double*>(sm + p.off_kv);  // Y^T v sums (kmax)
     double* s_vt = s_sv + p.kmax;                             // V^T m sums (kmax)
     double* s_c = s_vt + p.kmax;                              // K s on the CTA's columns (by list position)
@@ -501,8 +563,13 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
     __shared__ double s_dot[4];
     __shared__ int s_ok;
     for (int e = threadIdx.x; e < sl.na; e += blockDim.x) s_act[e] = p.actp[sl.ab + e] - 3 * sl.rb;
-    const int ncols = build_cols(p, cta, s_cols, s_slot);
+    const int ncols = build_cols(p, cta, s_cols, s_slot);  // synchronises: s_act is complete
     const int k = *p.rank;
+    for (int j = threadIdx.x; j < k; j += blockDim.x) {
+        const int g = p.comp_of_col[j];
+        s_srng[2 * j] = g >= 0 ? p.comp_slot_ptr[g] : 0;
+        s_srng[2 * j + 1] = g >= 0 ? p.comp_slot_ptr[g + 1] : 0;
+    }
     int epoch = 0;
     const bool yc_on = p.stage_yc && ncols <= p.NCOL;
     if (yc_on) {
@@ -513,8 +580,20 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
             float* o = yc + (size_t)q * ld + 3 * lr;
             o[0] = y.x; o[1] = y.y; o[2] = y.z;
         }
-        __syncthreads();
     }
+    // the rows of K and C for the CTA's columns: column q = warp + kWarps c, entries l = lane + 32 i
+    const bool kreg = ncols <= kRegCols * kWarps && k <= 32 * kRegK;
+    double kr[kRegCols][kRegK], cr[kRegCols][kRegK];
+#pragma unroll
+    for (int c = 0; c < kRegCols; ++c)
+#pragma unroll
+        for (int i = 0; i < kRegK; ++i) {
+            const int q = warp + kWarps * c, l = lane + 32 * i;
+            const bool in = kreg && q < ncols && l < k;
+            kr[c][i] = in ? p.K[(size_t)s_cols[q] * p.kmax + l] : 0.0;
+            cr[c][i] = in ? p.C[(size_t)s_cols[q] * p.kmax + l] : 0.0;
+        }
+    __syncthreads();
 
     // grid barrier: the CTA's partials are already in global memory
     auto barrier = [&]() -> bool {
@@ -527,66 +606,116 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
     // CTA sums of per-thread values -> pdot[cta * 4 + i] for i in [i0, i1).  The pass's dots use
     // slots 0-2 and the true-residual check slot 3: a check's slot is still being read when a fast
     // CTA already writes the next pass's dots (no barrier between the two)
-    auto cta_partials = [&](double a0, double a1, double a2, double a3, double* out, int i0, int i1) {
+    auto cta_partials = [&](double a0, double a1, double a2, double a3, int i0, int i1) {
         a0 = bwarp_sum(a0); a1 = bwarp_sum(a1); a2 = bwarp_sum(a2); a3 = bwarp_sum(a3);
         if (lane == 0) { s_red[4 * warp] = a0; s_red[4 * warp + 1] = a1; s_red[4 * warp + 2] = a2; s_red[4 * warp + 3] = a3; }
         __syncthreads();
         if ((int)threadIdx.x >= i0 && (int)threadIdx.x < i1) {
             double t = 0.0;
             for (int w = 0; w < kWarps; ++w) t += s_red[4 * w + threadIdx.x];
-            out[4 * cta + threadIdx.x] = t;
+            p.pdot[4 * cta + threadIdx.x] = t;
         }
     };
-    // the dots of all CTAs, summed in CTA order by warp 0 (same bits everywhere)
+    // the dots of all CTAs, summed in CTA order (same bits everywhere): the last warp sums slots
+    // 0-1, the one before it slots 2-3; every load is issued before the first add waits
     auto sum_dots = [&]() {
-        if (warp == 0) {
-            double a[4] = {0, 0, 0, 0};
-            for (unsigned c = lane; c < G; c += 32)
+        if (warp < kWarps - 2) return;
+        const int half = warp == kWarps - 1 ? 0 : 1;
+        const double2* pd = reinterpret_cast<const double2*>(p.pdot) + half;
+        constexpr int kB = 5;
+        double2 v[kB];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) a[i] += p.pdot[4 * c + i];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = bwarp_sum(a[i]);
-            if (lane == 0)
-#pragma unroll
-                for (int i = 0; i < 4; ++i) s_dot[i] = a[i];
+        for (int i = 0; i < kB; ++i) {
+            const unsigned c = lane + 32 * i;
+            v[i] = c < G ? __ldcg(pd + 2 * c) : make_double2(0.0, 0.0);
         }
-    };
-    // out[j] = sum of the contributor slots of column j's component, for every j < k; each warp
-    // issues the loads of four columns before it reduces them (one round trip serves four)
-    auto sum_slots = [&](const double* part, double* out) {
-        for (int j0 = 4 * warp; j0 < k; j0 += 4 * kWarps) {
-            double a[4];
+        double a0 = 0.0, a1 = 0.0;
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                a[u] = 0.0;
-                const int j = j0 + u;
+        for (int i = 0; i < kB; ++i) { a0 += v[i].x; a1 += v[i].y; }
+        for (unsigned c = lane + 32 * kB; c < G; c += 32) {
+            const double2 w = __ldcg(pd + 2 * c);
+            a0 += w.x; a1 += w.y;
+        }
+        a0 = bwarp_sum(a0);
+        a1 = bwarp_sum(a1);
+        if (lane == 0) { s_dot[2 * half] = a0; s_dot[2 * half + 1] = a1; }
+    };
+    // out[j] = sum of the contributor slots of column j's component, for every j < k: a warp per
+    // column, its lanes over the slots (each lane adds its slots in order, then a fixed butterfly),
+    // the loads of seven columns' first 64 slots in flight per warp before any add waits.  With
+    // `dots` the last two warps sum the dots instead.
+    auto sum_cols = [&](const double* part, double* out, bool dots) {
+        const int nw = dots ? kWarps - 2 : kWarps;
+        if (dots) sum_dots();
+        if (warp >= nw) return;
+        constexpr int kC = 7;
+        for (int j0 = 0; j0 < k; j0 += kC * nw) {
+            double a[kC], b2[kC];
+#pragma unroll
+            for (int i = 0; i < kC; ++i) {
+                const int j = j0 + warp + nw * i;
+                a[i] = 0.0;
+                b2[i] = 0.0;
                 if (j < k) {
-                    const int g = p.comp_of_col[j];
-                    if (g >= 0)
-                        for (int q = p.comp_slot_ptr[g] + lane; q < p.comp_slot_ptr[g + 1]; q += 32)
-                            a[u] += part[(size_t)q * p.kmax + j];
+                    const int q = s_srng[2 * j] + lane, q1 = s_srng[2 * j + 1];
+                    if (q < q1) a[i] = __ldcg(part + (size_t)q * p.kmax + j);
+                    if (q + 32 < q1) b2[i] = __ldcg(part + (size_t)(q + 32) * p.kmax + j);
                 }
             }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const double t = bwarp_sum(a[u]);
-                if (lane == 0 && j0 + u < k) out[j0 + u] = t;
+            for (int i = 0; i < kC; ++i) {
+                const int j = j0 + warp + nw * i;
+                a[i] += b2[i];
+                if (j < k)
+                    for (int q = s_srng[2 * j] + 64 + lane; q < s_srng[2 * j + 1]; q += 32)
+                        a[i] += __ldcg(part + (size_t)q * p.kmax + j);
+            }
+#pragma unroll
+            for (int i = 0; i < kC; ++i) {
+                const double t = bwarp_sum(a[i]);
+                const int j = j0 + warp + nw * i;
+                if (lane == 0 && j < k) out[j] = t;
             }
         }
     };
-    // the CTA's Y columns at its own rows: shared memory (FP32) when staged
-    const float* Yc = yc_on ? reinterpret_cast<const float*>(sm + p.off_yc) : nullptr;
-    auto yval = [&](int q, int lr, int d) -> double {
-        if (Yc) return (double)Yc[(size_t)q * ld + 3 * lr + d];
-        const float* yj = p.Y + (size_t)s_cols[q] * 4 * p.n + 4 * (size_t)(sl.rb + lr);
-        return (double)__ldg(yj + d);
+    // out[q] = (M vin)_{s_cols[q]} for the CTA's columns, M = K or C (rows in registers when kreg)
+    auto rows_times = [&](const double (&rg)[kRegCols][kRegK], const double* Mg, const double* vin, double* out) {
+        if (kreg) {
+#pragma unroll
+            for (int c = 0; c < kRegCols; ++c) {
+                const int q = warp + kWarps * c;
+                if (q < ncols) {  // warp-uniform
+                    double a = 0.0;
+#pragma unroll
+                    for (int i = 0; i < kRegK; ++i) {
+                        const int l = lane + 32 * i;
+                        a += rg[c][i] * (l < k ? vin[l] : 0.0);
+                    }
+                    a = bwarp_sum(a);
+                    if (lane == 0) out[q] = a;
+                }
+            }
+        } else {
+            for (int q = warp; q < ncols; q += kWarps) {
+                const int j = s_cols[q];
+                double a = 0.0;
+                for (int l = lane; l < k; l += 32) a += Mg[(size_t)j * p.kmax + l] * vin[l];
+                a = bwarp_sum(a);
+                if (lane == 0) out[q] = a;
+            }
+        }
     };
-    // partials of Y^T v over the own rows -> part[slot][j] for the CTA's columns
+    // the CTA's Y columns at its own dofs: shared memory (FP32) when staged
+    const float* Yc = yc_on ? reinterpret_cast<const float*>(sm + p.off_yc) : nullptr;
+    auto yval = [&](int q, int e) -> double {
+        if (Yc) return (double)Yc[(size_t)q * ld + e];
+        return (double)__ldg(p.Y + (size_t)s_cols[q] * 4 * p.n + 4 * (size_t)(sl.rb + e / 3) + e % 3);
+    };
+    // partials of Y^T v over the own dofs -> part[slot][j] for the CTA's columns
     auto y_partials = [&](const double* v, double* part) {
         for (int q = warp; q < ncols; q += kWarps) {
             double a = 0.0;
-            for (int lr = lane; lr < R; lr += 32)
-                a += yval(q, lr, 0) * v[3 * lr] + yval(q, lr, 1) * v[3 * lr + 1] + yval(q, lr, 2) * v[3 * lr + 2];
+            for (int e = lane; e < R3; e += 32) a += yval(q, e) * v[e];
             a = bwarp_sum(a);
             if (lane == 0) part[(size_t)s_slot[q] * p.kmax + s_cols[q]] = a;
         }
@@ -599,74 +728,95 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
         for (int q = warp; q < ncols; q += kWarps) {
             const double* vq = Vc + (size_t)q * sl.na;
             double a = 0.0;
-            for (int il = lane; il < sl.na; il += 32) a += vq[il] * v[s_act[il]];
+            for (int il = lane; il < sl.na; il += 32) a += __ldg(vq + il) * v[s_act[il]];
             a = bwarp_sum(a);
             if (lane == 0) part[(size_t)s_slot[q] * p.kmax + s_cols[q]] = a;
         }
     };
-    // s_t[q] = (C vt)_j for the CTA's columns, then out[own coupled dof] -= (V C vt)
+    // out[own coupled dof] -= (V s_t) (s_t = C vt on the CTA's columns)
     auto lowrank_sub = [&](double* out) {
-        if (sl.na == 0) return;
-        for (int q = warp; q < ncols; q += kWarps) {
-            const int j = s_cols[q];
-            double a = 0.0;
-            for (int l = lane; l < k; l += 32) a += p.C[(size_t)j * p.kmax + l] * s_vt[l];
-            a = bwarp_sum(a);
-            if (lane == 0) s_t[q] = a;
-        }
-        __syncthreads();
         for (int il = threadIdx.x; il < sl.na; il += blockDim.x) {
             double a = 0.0;
             int q = 0;
             for (; q + 8 <= ncols; q += 8) {
                 double vv[8];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) vv[u] = Vc[(size_t)(q + u) * sl.na + il];
+                for (int u = 0; u < 8; ++u) vv[u] = __ldg(Vc + (size_t)(q + u) * sl.na + il);
 #pragma unroll
                 for (int u = 0; u < 8; ++u) a += vv[u] * s_t[q + u];
             }
-            for (; q < ncols; ++q) a += Vc[(size_t)q * sl.na + il] * s_t[q];
+            for (; q < ncols; ++q) a += __ldg(Vc + (size_t)q * sl.na + il) * s_t[q];
             out[s_act[il]] -= a;
         }
     };
     // stage the window of a published vector (own rows from shared memory)
-    auto stage = [&](const double* pub, const double* own) {
-        for (int e = threadIdx.x; e < sl.nwin; e += blockDim.x) {
+    // stage the window of a published vector (own rows from shared memory) and sum the V^T v
+    // partials into s_vt: the window loads (two per thread in registers) are issued first, so
+    // they are in flight while the column sums wait on theirs
+    auto stage_and_sum = [&](const double* pub, const double* own, const double* part) {
+        double wv[2][3];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int e = threadIdx.x + kThreads * i;
+            wv[i][0] = wv[i][1] = wv[i][2] = 0.0;
+            if (e < sl.nwin) {
+                const int node = sl.wn[e];
+                if (node >= sl.rb && node < sl.re) {
+                    const double* o = own + 3 * (node - sl.rb);
+                    wv[i][0] = o[0]; wv[i][1] = o[1]; wv[i][2] = o[2];
+                } else {
+                    const double2 lo = __ldcg(reinterpret_cast<const double2*>(pub) + 2 * (size_t)node);
+                    wv[i][0] = lo.x; wv[i][1] = lo.y; wv[i][2] = __ldcg(pub + 4 * (size_t)node + 2);
+                }
+            }
+        }
+        sum_cols(part, s_vt, false);
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int e = threadIdx.x + kThreads * i;
+            if (e < sl.nwin) { win[3 * e] = wv[i][0]; win[3 * e + 1] = wv[i][1]; win[3 * e + 2] = wv[i][2]; }
+        }
+        for (int e = threadIdx.x + 2 * kThreads; e < sl.nwin; e += blockDim.x) {
             const int node = sl.wn[e];
             double a0, a1, a2;
             if (node >= sl.rb && node < sl.re) {
                 const double* o = own + 3 * (node - sl.rb);
                 a0 = o[0]; a1 = o[1]; a2 = o[2];
             } else {
-                Vec4<double>::load(pub, node, a0, a1, a2);
+                const double2 lo = __ldcg(reinterpret_cast<const double2*>(pub) + 2 * (size_t)node);
+                a0 = lo.x; a1 = lo.y; a2 = __ldcg(pub + 4 * (size_t)node + 2);
             }
-            win[4 * e] = a0; win[4 * e + 1] = a1; win[4 * e + 2] = a2;
+            win[3 * e] = a0; win[3 * e + 1] = a1; win[3 * e + 2] = a2;
         }
     };
-    // out = D v over the own rows (window staged), FP64 coupled diagonal blocks in the mixed modes
-    auto op_spmv = [&](const double* vown, double* out) {
-        auto epi = [&](int lr, double y0, double y1, double y2) {
-            if (split) add_dact(p, sl.rb + lr, vown[3 * lr], vown[3 * lr + 1], vown[3 * lr + 2], y0, y1, y2);
-            out[3 * lr] = y0; out[3 * lr + 1] = y1; out[3 * lr + 2] = y2;
-        };
-        slice_spmv<MT>(sl, gv, false, nullptr, win, epi);
+    // n = S v over the own rows: D v (window staged) - V (C vt), vt = V^T v summed from `part`
+    auto schur_apply = [&](const double* pub, const double* vown, const double* part) {
+        stage_and_sum(pub, vown, part);
+        __syncthreads();
+        part_op<MT>(sl, gv, win, vown, Nn);
+        rows_times(cr, p.C, s_vt, s_t);
+        __syncthreads();
+        lowrank_sub(Nn);
+        __syncthreads();
     };
 
-    // ---- prologue: x = 0, r = rhs ----
-    for (int e = threadIdx.x; e < R; e += blockDim.x) {
-        double r0, r1, r2;
-        Vec4<double>::load(p.rhs, sl.rb + e, r0, r1, r2);
-        Rr[3 * e] = r0; Rr[3 * e + 1] = r1; Rr[3 * e + 2] = r2;
-        for (int d = 0; d < 3; ++d) {
-            X[3 * e + d] = 0.0; Pp[3 * e + d] = 0.0; Ss[3 * e + d] = 0.0; Qq[3 * e + d] = 0.0; Zz[3 * e + d] = 0.0;
+    // ---- prologue: x = 0, r = rhs, the first pass preconditions r ----
+    double xr[kDofs], rr_[kDofs], ur[kDofs], pr[kDofs], sr[kDofs], qr[kDofs], zr[kDofs];
+#pragma unroll
+    for (int i = 0; i < kDofs; ++i) {
+        const int e = threadIdx.x + kThreads * i;
+        xr[i] = pr[i] = sr[i] = qr[i] = zr[i] = ur[i] = rr_[i] = 0.0;
+        if (e < R3) {
+            rr_[i] = p.rhs[4 * (size_t)(sl.rb + e / 3) + e % 3];
+            Wb[e] = rr_[i];
         }
     }
     __syncthreads();
 
     int pass = kPassStart, it = 0, status = -1, restarts = 0, npass = 0;
-    // phase clocks (trace mode): 0 pass top, 1 polynomial done, 2 partials written, 3 after barrier A,
-    // 4 sums read, 5 K s done, 6 m formed, 7 V^T m partials / decisions, 8 after barrier B, 9 window
-    // staged, 10 V^T m summed, 11 D m done, 12 low-rank done, 13 updates done
+    // phase clocks (trace mode): 0 pass top, 1 Y^T v and dot partials written, 2 polynomial done,
+    // 3 after barrier A, 4 sums read, 5 K s done, 6 m formed, 7 V^T m partials / decisions, 8 after
+    // barrier B, 9 window staged and V^T m summed, 10 D m and C vt done, 11 low-rank done, 12 updates done
     auto mark = [&](int ev) {
         if (p.trace && threadIdx.x == 0 && npass < p.trace_iters)
             p.trace[((size_t)cta * p.trace_iters + npass) * 16 + ev] = (unsigned long long)clock64();
@@ -676,44 +826,41 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
     for (;;) {
         // ---------------- phase 1 ----------------
         mark(0);
-        const double* v = pass == kPassStart ? Rr : Ww;
-        local_poly<MT>(p, sl, split, v, Mt, T0, T1);
-        mark(1);
-        y_partials(v, p.pY);
+        y_partials(Wb, p.pY);
         {
             double g = 0, d = 0, rr = 0;
-            for (int e = threadIdx.x; e < R3; e += blockDim.x) {
-                const double r = Rr[e];
-                rr += r * r;
-                if (pass == kPassNormal) { g += r * Uu[e]; d += Ww[e] * Uu[e]; }
+#pragma unroll
+            for (int i = 0; i < kDofs; ++i) {
+                const int e = threadIdx.x + kThreads * i;
+                if (e < R3) {
+                    rr += rr_[i] * rr_[i];
+                    if (pass == kPassNormal) { g += rr_[i] * ur[i]; d += Wb[e] * ur[i]; }
+                }
             }
-            cta_partials(g, d, rr, 0.0, p.pdot, 0, 3);
+            cta_partials(g, d, rr, 0.0, 0, 3);
         }
+        mark(1);
+        part_poly<MT, 1>(p, sl, Wb, Pz, Pt, Pu, ld);
         mark(2);
         if (!barrier()) return;
         mark(3);
         // ---------------- phase 2 ----------------
-        sum_slots(p.pY, s_sv);
-        sum_dots();
+        sum_cols(p.pY, s_sv, true);
         __syncthreads();
         mark(4);
-        for (int q = warp; q < ncols; q += kWarps) {
-            const int j = s_cols[q];
-            double a = 0.0;
-            for (int l = lane; l < k; l += 32) a += p.K[(size_t)j * p.kmax + l] * s_sv[l];
-            a = bwarp_sum(a);
-            if (lane == 0) s_c[q] = a;
-        }
+        rows_times(kr, p.K, s_sv, s_c);
         __syncthreads();
         mark(5);
-        for (int e = threadIdx.x; e < R; e += blockDim.x) {
-            double m0 = Mt[3 * e], m1 = Mt[3 * e + 1], m2 = Mt[3 * e + 2];
-            for (int q = 0; q < ncols; ++q) {
-                const double c = s_c[q];
-                m0 += yval(q, e, 0) * c; m1 += yval(q, e, 1) * c; m2 += yval(q, e, 2) * c;
+#pragma unroll
+        for (int i = 0; i < kDofs; ++i) {
+            const int e = threadIdx.x + kThreads * i;
+            if (e < R3) {
+                const int lr = e / 3, d = e - 3 * lr;
+                double m = Pz[e];
+                for (int q = 0; q < ncols; ++q) m += yval(q, e) * s_c[q];
+                Mm[e] = m;
+                p.mpub[4 * (size_t)(sl.rb + lr) + d] = m;
             }
-            Mm[3 * e] = m0; Mm[3 * e + 1] = m1; Mm[3 * e + 2] = m2;
-            Vec4<double>::store(p.mpub, sl.rb + e, m0, m1, m2);
         }
         __syncthreads();
         mark(6);
@@ -754,63 +901,72 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
         mark(8);
         // ---------------- phase 3 ----------------
         if (!check) {
-            stage(p.mpub, Mm);
+            stage_and_sum(p.mpub, Mm, p.pV);
             __syncthreads();
             mark(9);
-            sum_slots(p.pV, s_vt);
+            part_op<MT>(sl, gv, win, Mm, Nn);
+            rows_times(cr, p.C, s_vt, s_t);
             __syncthreads();
             mark(10);
-            op_spmv(Mm, Nn);
-            __syncthreads();
-            mark(11);
             lowrank_sub(Nn);
             __syncthreads();
-            mark(12);
+            mark(11);
             if (pass == kPassStart) {
-                for (int e = threadIdx.x; e < R3; e += blockDim.x) { Uu[e] = Mm[e]; Ww[e] = Nn[e]; }
+#pragma unroll
+                for (int i = 0; i < kDofs; ++i) {
+                    const int e = threadIdx.x + kThreads * i;
+                    if (e < R3) { ur[i] = Mm[e]; Wb[e] = Nn[e]; }
+                }
                 pass = kPassNormal;
                 fresh = true;
             } else {
-                for (int e = threadIdx.x; e < R3; e += blockDim.x) {
-                    const double z = Nn[e] + beta * Zz[e], q = Mm[e] + beta * Qq[e];
-                    const double sv = Ww[e] + beta * Ss[e], pv = Uu[e] + beta * Pp[e];
-                    Zz[e] = z; Qq[e] = q; Ss[e] = sv; Pp[e] = pv;
-                    X[e] += alpha * pv;
-                    Rr[e] -= alpha * sv;
-                    Uu[e] -= alpha * q;
-                    Ww[e] -= alpha * z;
+#pragma unroll
+                for (int i = 0; i < kDofs; ++i) {
+                    const int e = threadIdx.x + kThreads * i;
+                    if (e < R3) {
+                        const double w = Wb[e];
+                        zr[i] = Nn[e] + beta * zr[i];
+                        qr[i] = Mm[e] + beta * qr[i];
+                        sr[i] = w + beta * sr[i];
+                        pr[i] = ur[i] + beta * pr[i];
+                        xr[i] += alpha * pr[i];
+                        rr_[i] -= alpha * sr[i];
+                        ur[i] -= alpha * qr[i];
+                        Wb[e] = w - alpha * zr[i];
+                    }
                 }
                 ++it;
                 fresh = false;
             }
             __syncthreads();
-            mark(13);
+            mark(12);
             ++npass;
             continue;
         }
         // ---------------- true residual: r = rhs - (D x - V C V^T x) ----------------
-        for (int e = threadIdx.x; e < R; e += blockDim.x)
-            Vec4<double>::store(p.xpub, sl.rb + e, X[3 * e], X[3 * e + 1], X[3 * e + 2]);
+#pragma unroll
+        for (int i = 0; i < kDofs; ++i) {
+            const int e = threadIdx.x + kThreads * i;
+            if (e < R3) {
+                Mm[e] = xr[i];
+                p.xpub[4 * (size_t)(sl.rb + e / 3) + e % 3] = xr[i];
+            }
+        }
         __syncthreads();
-        v_partials(X, p.pX);
+        v_partials(Mm, p.pX);
         if (!barrier()) return;
-        stage(p.xpub, X);
-        sum_slots(p.pX, s_vt);
-        __syncthreads();
-        op_spmv(X, Nn);
-        __syncthreads();
-        lowrank_sub(Nn);
-        __syncthreads();
+        schur_apply(p.xpub, Mm, p.pX);
         {
             double rr = 0.0;
-            for (int e = threadIdx.x; e < R; e += blockDim.x) {
-                double b0, b1, b2;
-                Vec4<double>::load(p.rhs, sl.rb + e, b0, b1, b2);
-                const double r0 = b0 - Nn[3 * e], r1 = b1 - Nn[3 * e + 1], r2 = b2 - Nn[3 * e + 2];
-                Rr[3 * e] = r0; Rr[3 * e + 1] = r1; Rr[3 * e + 2] = r2;
-                rr += r0 * r0 + r1 * r1 + r2 * r2;
+#pragma unroll
+            for (int i = 0; i < kDofs; ++i) {
+                const int e = threadIdx.x + kThreads * i;
+                if (e < R3) {
+                    rr_[i] = p.rhs[4 * (size_t)(sl.rb + e / 3) + e % 3] - Nn[e];
+                    rr += rr_[i] * rr_[i];
+                }
             }
-            cta_partials(0.0, 0.0, 0.0, rr, p.pdot, 3, 4);
+            cta_partials(0.0, 0.0, 0.0, rr, 3, 4);
         }
         if (!barrier()) return;
         sum_dots();
@@ -821,9 +977,23 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
         if (it >= p.max_iter) { status = 4; break; }
         if (!isfinite(rel)) { status = 3; break; }
         pass = kPassStart;  // restart from the true residual
+#pragma unroll
+        for (int i = 0; i < kDofs; ++i) {
+            const int e = threadIdx.x + kThreads * i;
+            if (e < R3) Wb[e] = rr_[i];
+        }
+        __syncthreads();
     }
     // ---- x out (own rows) and the scalars ----
-    for (int e = threadIdx.x; e < R; e += blockDim.x) Vec4<double>::store(p.x, sl.rb + e, X[3 * e], X[3 * e + 1], X[3 * e + 2]);
+#pragma unroll
+    for (int i = 0; i < kDofs; ++i) {
+        const int e = threadIdx.x + kThreads * i;
+        if (e < R3) {
+            const size_t o = 4 * (size_t)(sl.rb + e / 3) + e % 3;
+            p.x[o] = xr[i];
+            if (e % 3 == 2) p.x[o + 1] = 0.0;  // the node's pad
+        }
+    }
     if (cta == 0 && threadIdx.x == 0) {
         p.out[0] = it; p.out[1] = rel; p.out[2] = status; p.out[3] = normb; p.out[4] = restarts;
     }
@@ -834,6 +1004,15 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+void launch_block_fill(int precision, const BlockPlan& p, cudaStream_t st) {
+    const long long nslot = p.nchunk * 32;
+    if (nslot <= 0) return;
+    const int grid = (int)std::min<long long>((nslot + 255) / 256, 148LL * 8);
+    count_launch();
+    if (precision == 0) block_fill_kernel<double><<<grid, 256, 0, st>>>(p);
+    else block_fill_kernel<float><<<grid, 256, 0, st>>>(p);
+}
+
 void launch_block_columns(const BlockPlan& p, cudaStream_t st) {
     count_launch();
     block_columns_kernel<<<1, 256, 0, st>>>(p);
@@ -846,7 +1025,7 @@ static cudaError_t launch_y_t(const BlockPlan& p, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     count_launch();
     fn<<<p.G_ctas, kThreads, p.smem_y, st>>>(p);
-    return cudaGetLastError();
+    return cudaPeekAtLastError();
 }
 
 cudaError_t launch_block_y(int precision, const BlockPlan& p, cudaStream_t st) {
@@ -902,31 +1081,37 @@ cudaError_t launch_block_pcg(int precision, const BlockPlan& p, cudaStream_t st)
     return precision == 0 ? launch_pcg_t<double>(p, st) : launch_pcg_t<float>(p, st);
 }
 
-int block_max_smem() { return 227 * 1024 - 4096; }
+// the kernels' own static shared memory (the plan copy, reductions) is kept out of the budget
+int block_max_smem() { return 227 * 1024 - 8 * 1024; }
 
-// shared-memory layouts for the maxima in p (R, BLK, W, NA, NCOL, kmax): a common prefix (row
-// pointers, window positions, Dd^-1, window, coupled dofs, column lists, k-vectors, the value planes),
-// then the vectors: 16 x 3R doubles in the Y kernel (four regions of four), 12 x 3R in the PCG followed
-// by the CTA's Y columns (FP32)
+// shared-memory layouts for the maxima in p (R, NS, NCH, W, NA, NCOL, kmax): a common prefix
+// (slices, local slot counts, window positions, Dd^-1, window, coupled dofs and their diagonal
+// blocks, column lists and slot ranges, k-vectors, reduction scratch, the value chunks), then the
+// vectors: the Y kernel's batch region, or the PCG's six FP64 vectors (3 per row) followed by
+// the CTA's Y columns (FP32)
 size_t block_smem_bytes(int precision, BlockPlan& p, bool stage_vals, bool stage_yc) {
-    const size_t mt = precision == 0 ? 8 : 4, dt = precision == 0 ? 8 : 4;
+    const size_t mt = precision == 0 ? 8 : 4, dt = mt;
     auto al = [](size_t b) { return (b + 15) / 16 * 16; };
     size_t off = 0;
-    p.off_rp = (int)off; off += al(sizeof(int) * (p.R + 1));
-    p.off_lc = (int)off; off += al(sizeof(unsigned short) * p.BLK);
+    p.off_meta = (int)off; off += al(sizeof(int4) * p.NS);
+    p.off_nloc = (int)off; off += al(sizeof(unsigned short) * p.R);
+    p.off_lc = (int)off; off += al(sizeof(unsigned short) * 32 * (size_t)p.NCH);
     p.off_dinv = (int)off; off += al(dt * 9 * p.R);
     p.off_wn = (int)off; off += al(sizeof(int) * p.W);
-    p.off_win = (int)off; off += al(sizeof(double) * 4 * p.W);
+    p.off_win = (int)off; off += al(sizeof(double) * 3 * p.W);
     p.off_act = (int)off; off += al(sizeof(int) * p.NA);
+    p.off_aflag = (int)off; off += al(sizeof(int) * p.R);
+    p.off_dact = (int)off; off += al(sizeof(double) * 3 * p.NA);
     p.off_cols = (int)off; off += al(sizeof(int) * 2 * p.kmax);
+    p.off_srng = (int)off; off += al(sizeof(int) * 2 * p.kmax);
     p.off_kv = (int)off; off += al(sizeof(double) * 4 * p.kmax);
     p.off_red = (int)off; off += al(sizeof(double) * 4 * kWarps);
     p.off_val = (int)off;
     p.stage_vals = stage_vals ? 1 : 0;
-    if (stage_vals) off += al(mt * 9 * p.BLK);
+    if (stage_vals) off += al(mt * kChunkVals * (size_t)p.NCH);
     p.off_vec = (int)off;
-    p.smem_y = off + al(sizeof(double) * 16 * 3 * (size_t)p.R);
-    off += al(sizeof(double) * 12 * 3 * (size_t)p.R);
+    p.smem_y = off + al(sizeof(double) * y_region_doubles(p.R));
+    off += al(sizeof(double) * 6 * 3 * (size_t)p.R);
     p.off_yc = (int)off;
     p.stage_yc = stage_yc ? 1 : 0;
     if (stage_yc) off += al(sizeof(float) * 3 * (size_t)p.R * p.NCOL);

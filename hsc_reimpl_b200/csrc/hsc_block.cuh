@@ -37,9 +37,7 @@ struct BlockPlan {
     // system (internal FEM node numbering)
     int n, nnz, a, kmax;
     const int* rank;             // device rank k
-    const int* rowptr;
-    const int* colidx;
-    const void* vals;            // operator planes 9 x nnz (MT); mixed modes: coupled diagonal blocks zeroed
+    const void* vals;            // BSR operator planes 9 x nnz (MT); mixed modes: coupled diagonal blocks zeroed
     const void* dinv;            // Dd^-1 planes over nodes (DT)
     const double* dact;          // FP64 diagonal blocks of the coupled nodes, actp node order (mixed modes)
     const int* rowflag;          // node -> coupled-node index in actp order, or -1
@@ -69,7 +67,17 @@ struct BlockPlan {
     const int* win_off;
     const int* win_nodes;
     const int* win_own;
-    const unsigned short* lcol;  // per BSR entry: window position of its column
+    // sliced ELL of the CTAs' rows: slices of 16 rows, two slots of each row per 32-lane chunk
+    // (lane 2 r + h holds slot 2 c + h of row r in chunk c); a row's slots are its diagonal block,
+    // then the blocks whose column is a row of the same part, then the rest, then zero padding
+    const int4* sell_slice;      // per slice: first chunk, chunks, chunks holding local blocks, 0
+    const int* cta_slice;        // G + 1: each CTA's slices
+    const int* cta_chunk;        // G + 1: each CTA's chunks
+    const unsigned short* sell_nloc;  // per row: its diagonal block + local blocks (leading slots)
+    const unsigned short* sell_lc;    // per slot: window position of the block's column
+    const int* sell_src;         // per slot: BSR entry, or -1 for padding
+    void* sell_vals;             // per chunk kChunkVals MT: planes 0-3 as [lane][4], 4-7 as [lane][4], 8 as [lane]
+    long long nchunk;            // chunks over all CTAs
     // coupling components
     int ncomp;
     const int* comp_of_body;     // body -> component
@@ -108,13 +116,20 @@ struct BlockPlan {
     unsigned long long* trace;   // optional: per CTA x trace_iters x 16 SM clocks at the phase boundaries
     int trace_iters;
     // shared-memory layout (bytes from the dynamic base, the same in every CTA)
-    int R, BLK, W, NA, NCOL;     // maxima over CTAs: rows, blocks, window nodes, coupled dofs, Y columns
+    int R, NS, NCH, W, NA, NCOL; // maxima over CTAs: rows, slices, chunks, window nodes, coupled dofs, Y columns
     int stage_vals, stage_yc;
-    int off_rp, off_lc, off_val, off_dinv, off_wn, off_win, off_vec, off_act, off_cols, off_kv, off_red, off_yc;
-    size_t smem;                 // the PCG kernel (12 vectors + the staged Y columns)
-    size_t smem_y;               // the Y kernel (4 batches of 4 vectors)
+    int off_meta, off_nloc, off_lc, off_val, off_dinv, off_wn, off_win, off_act, off_aflag, off_dact;
+    int off_cols, off_srng, off_kv, off_red, off_vec, off_yc;
+    size_t smem;                 // the PCG kernel
+    size_t smem_y;               // the Y kernel
 };
 
+constexpr int kSliceRows = 16;
+constexpr int kChunkVals = 9 * 32;
+constexpr int kBlockMaxRows = 341;  // the PCG keeps a CTA's dofs in registers, two per thread
+
+// sliced-ELL values from the BSR planes (every solve)
+void launch_block_fill(int precision, const BlockPlan& p, cudaStream_t st);
 // columns of every coupling component, from U's nonzero rows (after the ACA)
 void launch_block_columns(const BlockPlan& p, cudaStream_t st);
 // Y = L V over every part, Y at the coupled dofs, and the per-CTA partials of V^T Y

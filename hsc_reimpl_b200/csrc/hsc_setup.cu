@@ -548,6 +548,100 @@ __global__ void __launch_bounds__(512) gj_inverse_reg_kernel(const double* A, in
         }
 }
 
+// The same elimination for blocks of at most 96 rows, one 1024-thread CTA per block: thread
+// (ty, tx) of a 32 x 32 grid owns rows ty + 32 r and columns tx + 32 c (r, c < 3), nine entries,
+// so every thread issues few FMAs per step and the step is short.  A block is the set of rows
+// and columns idx[ptr[g] .. ptr[g + 1]) of the m x m matrix (idx null: the whole matrix, one
+// block).  Gauss-Jordan without pivoting never mixes two blocks of a block-diagonal matrix (the
+// products across them are exact zeros), so inverting the blocks apart gives the whole inverse
+// bit for bit; entries of P outside the blocks are left to the caller.
+constexpr int kGbR = 3, kGbMax = 32 * kGbR;
+__global__ void __launch_bounds__(1024) gj_inverse_blocks_kernel(const double* A, int m, const int* ptr, const int* idx,
+                                                                 double* P, int* bad) {
+    __shared__ double s_row[2][kGbMax], s_col[2][kGbMax], s_rp[2];
+    __shared__ int s_bad;
+    const int g = blockIdx.x;
+    const int b0 = ptr ? ptr[g] : 0;
+    const int mb = ptr ? ptr[g + 1] - b0 : m;
+    const int* ix = idx ? idx + b0 : nullptr;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    int gi[kGbR], gj[kGbR];
+#pragma unroll
+    for (int r = 0; r < kGbR; ++r) {
+        const int i = ty + 32 * r, j = tx + 32 * r;
+        gi[r] = i < mb ? (ix ? ix[i] : i) : 0;
+        gj[r] = j < mb ? (ix ? ix[j] : j) : 0;
+    }
+    double w[kGbR][kGbR];
+#pragma unroll
+    for (int r = 0; r < kGbR; ++r)
+#pragma unroll
+        for (int c = 0; c < kGbR; ++c) {
+            const int i = ty + 32 * r, j = tx + 32 * c;
+            w[r][c] = (i < mb && j < mb) ? A[(size_t)gi[r] * m + gj[c]] : 0.0;
+        }
+    if (threadIdx.x == 0) s_bad = 0;
+    for (int k = 0; k < mb; ++k) {
+        const int b = k & 1, kk = k >> 5;
+        if (ty == (k & 31)) {
+#pragma unroll
+            for (int r = 0; r < kGbR; ++r)
+                if (r == kk)
+#pragma unroll
+                    for (int c = 0; c < kGbR; ++c) s_row[b][tx + 32 * c] = w[r][c];
+        }
+        if (tx == (k & 31)) {
+#pragma unroll
+            for (int c = 0; c < kGbR; ++c)
+                if (c == kk)
+#pragma unroll
+                    for (int r = 0; r < kGbR; ++r) {
+                        const int i = ty + 32 * r;
+                        s_col[b][i] = w[r][c];
+                        if (i == k) {
+                            double pv = w[r][c];
+                            if (!(pv > 0.0) || !isfinite(pv)) { s_bad = 1; pv = 1.0; }
+                            s_rp[b] = 1.0 / pv;
+                        }
+                    }
+        }
+        __syncthreads();
+        const double rp = s_rp[b];
+        double rs[kGbR];
+#pragma unroll
+        for (int c = 0; c < kGbR; ++c) rs[c] = s_row[b][tx + 32 * c] * rp;  // pivot row / pivot
+#pragma unroll
+        for (int r = 0; r < kGbR; ++r) {
+            const double ci = s_col[b][ty + 32 * r];
+#pragma unroll
+            for (int c = 0; c < kGbR; ++c) w[r][c] = fma(-ci, rs[c], w[r][c]);
+        }
+        if (tx == (k & 31)) {
+#pragma unroll
+            for (int c = 0; c < kGbR; ++c)
+                if (c == kk)
+#pragma unroll
+                    for (int r = 0; r < kGbR; ++r) w[r][c] = -s_col[b][ty + 32 * r] * rp;
+        }
+        if (ty == (k & 31)) {
+#pragma unroll
+            for (int r = 0; r < kGbR; ++r)
+                if (r == kk)
+#pragma unroll
+                    for (int c = 0; c < kGbR; ++c) w[r][c] = (tx + 32 * c == k) ? rp : rs[c];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && s_bad) atomicAdd(bad, 1);
+#pragma unroll
+    for (int r = 0; r < kGbR; ++r)
+#pragma unroll
+        for (int c = 0; c < kGbR; ++c) {
+            const int i = ty + 32 * r, j = tx + 32 * c;
+            if (i < mb && j < mb) P[(size_t)gi[r] * m + gj[c]] = w[r][c];
+        }
+}
+
 // P = A^-1 for an SPD A (m <= 160) in one 1024-thread CTA: Cholesky in
 // shared memory (2-D trailing update, two barriers per column), then each warp
 // solves L L^T x = e_c for its columns with the vector held in registers
@@ -1127,6 +1221,10 @@ void launch_cholesky(const double* A, int m, double* L, int* bad, cudaStream_t s
 }
 
 bool launch_chol_inverse(const double* A, int m, double* P, int* bad, cudaStream_t st) {
+    if (m <= kGbMax) {
+        HSC_COUNTED(gj_inverse_blocks_kernel<<<1, 1024, 0, st>>>(A, m, nullptr, nullptr, P, bad));
+        return true;
+    }
     if (m <= kGjMax) {
         HSC_COUNTED(gj_inverse_reg_kernel<<<1, 512, 0, st>>>(A, m, P, bad));
         return true;
@@ -1135,6 +1233,14 @@ bool launch_chol_inverse(const double* A, int m, double* P, int* bad, cudaStream
     if (bytes > 200 * 1024) return false;
     cudaFuncSetAttribute(gj_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     HSC_COUNTED(gj_inverse_kernel<<<1, 1024, bytes, st>>>(A, m, P, bad));
+    return true;
+}
+
+bool launch_inverse_blocks(const double* A, int m, int nblk, int max_blk, const int* ptr, const int* idx, double* P,
+                           int* bad, cudaStream_t st) {
+    if (max_blk > kGbMax || nblk < 1) return false;
+    cudaMemsetAsync(P, 0, sizeof(double) * (size_t)m * m, st);
+    HSC_COUNTED(gj_inverse_blocks_kernel<<<nblk, 1024, 0, st>>>(A, m, ptr, idx, P, bad));
     return true;
 }
 

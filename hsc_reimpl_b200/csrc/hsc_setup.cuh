@@ -56,9 +56,8 @@ struct AcaComp {
     long long* piv_idx;
     double* sums;          // sum of squares of each component's residual before each step (and after the last)
     int* nsteps;
-    int* cur;              // merge cursor per component
     int* order;            // 2 x kmax: (component, step) of each global column
-    double* esumsq;        // |E|_F^2
+    int stot;              // step slots over all components (s_off's total)
     int smem_doubles;
     double* U;             // qm x kmax column-major
     double* V;             // a x kmax column-major
@@ -67,6 +66,8 @@ struct AcaComp {
     double* err;
 };
 size_t aca_comp_smem_doubles();
+// the warp merge stages every component's step records in shared memory
+bool aca_merge_fits(int ncomp, int stot);
 cudaError_t launch_aca_comp(const AcaComp& p, cudaStream_t st);
 
 size_t aca_cluster_smem_doubles(int m, int nc);
@@ -122,6 +123,10 @@ void launch_gemm(const GemmArgs& g, int M, int N, cudaStream_t st);
 void launch_cholesky(const double* A, int m, double* L, int* bad, cudaStream_t st);
 // P = A^-1 by Cholesky in one CTA; false (nothing launched) when m is too large
 bool launch_chol_inverse(const double* A, int m, double* P, int* bad, cudaStream_t st);
+// P = A^-1 for an SPD A that is block diagonal over index sets (rows and columns idx[ptr[g] ..
+// ptr[g + 1]), every set at most 96): one CTA per set, zeros elsewhere; false if a set is larger
+bool launch_inverse_blocks(const double* A, int m, int nblk, int max_blk, const int* ptr, const int* idx, double* P,
+                           int* bad, cudaStream_t st);
 void launch_chol_solve(const double* L, int m, const double* B, int ldb, double* X, int ldx, int ncol,
                        const int* dncol, double* work, cudaStream_t st);
 void launch_ldlt(double* C, int kmax, const int* dk, double* L, double* d, int* bad, cudaStream_t st);

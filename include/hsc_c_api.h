@@ -155,8 +155,9 @@ typedef struct hsc_stats {        /* superset of the hsc_stats.jsonl record (lin
     double descent;                   /* b^T x */
     double setup_ms, pcg_ms, total_ms;/* device time between stream events */
     double lanczos_min, lanczos_max;  /* extreme Ritz values of the preconditioned Schur operator */
-    double stage_ms[8];               /* fill+extract, ACA, ABD inverse, reduced core, rhs, PCG, back-sub+residual,
-                                         block preconditioner setup (Y = L V, K; the PCG stage excludes it) */
+    double stage_ms[8];               /* fill+extract, ACA, the ABD inverse's time beyond the ACA (the two run
+                                         concurrently), reduced core, rhs, PCG, back-sub+residual, block
+                                         preconditioner setup (Y = L V, K; the PCG stage excludes it) */
     int64_t nnzb;
 } hsc_stats;
 

@@ -431,20 +431,25 @@ def part_of_nodes(perm, part_ptr):
     return out
 
 
-def local_block(D, part):
-    """D with only the 3x3 blocks whose row and column nodes share a part."""
+def local_block(D, part, offdiag=False):
+    """D with only the 3x3 blocks whose row and column nodes share a part (without the
+    diagonal blocks when ``offdiag``)."""
     Db = sp.csr_matrix(D).tobsr(blocksize=(3, 3))
     Db.sort_indices()
     n = Db.shape[0] // 3
     rows = np.repeat(np.arange(n), np.diff(Db.indptr))
     keep = part[rows] == part[Db.indices]
+    if offdiag:
+        keep &= rows != Db.indices
     Dl = sp.bsr_matrix((Db.data * keep[:, None, None], Db.indices, Db.indptr), shape=D.shape).tocsr()
     Dl.eliminate_zeros()
     return Dl
 
 
-def block_poly_apply(Dl, Dinv, r, weights, omega):
-    """L r = sum_k w_k t_k, t_0 = w Dd^-1 r, t_k = t_{k-1} - w Dd^-1 D_loc t_{k-1}; r may hold columns."""
+def block_poly_apply(Ol, Dinv, r, weights, omega):
+    """L r = sum_k w_k t_k, t_0 = w Dd^-1 r, t_k = t_{k-1} - w Dd^-1 D_loc t_{k-1}, evaluated as
+    t_k = (1 - w) t_{k-1} - w Dd^-1 O_loc t_{k-1} with O_loc = D_loc minus its diagonal blocks
+    (Dd^-1 D_loc = I + Dd^-1 O_loc), the order the CUDA kernel takes; r may hold columns."""
     def bd(v):
         if v.ndim == 1:
             return block_diag_apply(Dinv, v)
@@ -453,7 +458,7 @@ def block_poly_apply(Dl, Dinv, r, weights, omega):
     term = omega * bd(r)
     z = weights[0] * term
     for k in range(1, len(weights)):
-        term = term - omega * bd(Dl @ term)
+        term = (1.0 - omega) * term - omega * bd(Ol @ term)
         z = z + weights[k] * term
     return z
 
@@ -479,7 +484,7 @@ class BlockWoodbury:
     the device applies it.  A failed Cholesky of K^-1 leaves z = L r."""
 
     def __init__(self, orc, part, weights, omega):
-        self.Dl = local_block(orc.D, part)
+        self.Ol = local_block(orc.D, part, offdiag=True)
         self.Dinv = orc.Dinv
         self.w = np.asarray(weights, dtype=np.float64)
         self.omega = omega
@@ -491,7 +496,7 @@ class BlockWoodbury:
         if k:
             Vf = np.zeros((N, k))
             Vf[orc.active] = orc.V
-            self.Y = block_poly_apply(self.Dl, self.Dinv, Vf, self.w, omega).astype(np.float32).astype(np.float64)
+            self.Y = block_poly_apply(self.Ol, self.Dinv, Vf, self.w, omega).astype(np.float32).astype(np.float64)
             G = Vf.T @ self.Y
             G = 0.5 * (G + G.T)
             Lc, d = ldlt(orc.C)
@@ -506,7 +511,7 @@ class BlockWoodbury:
                 self.spd = False
 
     def __call__(self, r):
-        z = block_poly_apply(self.Dl, self.Dinv, r, self.w, self.omega)
+        z = block_poly_apply(self.Ol, self.Dinv, r, self.w, self.omega)
         if self.K.size:
             z = z + self.Y @ (self.K @ (self.Y.T @ r))
         return z

@@ -94,8 +94,12 @@ def test_block_mixed_precision_error_against_fp64(api, torch, tire, prec):
 def test_block_on_cube_and_fixture_systems(api, torch, golden, cube_system):
     """Small systems: the cube (1 body, 1,331 nodes, cond(H) ~ 2e13) and the reference's
     manufactured fixture, to a Schur residual of 1e-6.  The pipelined recurrences round
-    differently on the GPU and in NumPy, so the counts agree within 3 % (at least 2), and on
-    systems this ill-conditioned x agrees to 1e-4."""
+    differently on the GPU and in NumPy, so the counts agree within 3 % (at least 2).  On
+    systems this ill-conditioned two solves stopped at the same residual differ in x by far more
+    than rounding, so x is held to the restatement's own accuracy: its error against a direct
+    solve of H x = b, in the 2-norm and in the H-norm, is at most twice the restatement's."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
     from hsc_reimpl_b200 import systems as S
     g = golden["manufactured"]
     fx = S.from_dense_fixture(g["1e+06/D"], g["1e+06/A"], g["1e+06/E"], g["1e+06/b"])
@@ -107,7 +111,15 @@ def test_block_on_cube_and_fixture_systems(api, torch, golden, cube_system):
         xo, so, _, _ = O.hsc_solve_block(s.H, s.layout, s.b, perm, ptr, [1.0] * 4, om, tol=1e-6)
         it, ito = st["pcg_iterations"], so["pcg_iterations"]
         assert abs(it - ito) <= max(2, 0.03 * ito), (it, ito)
-        assert rel(x.cpu().numpy(), xo) < 1e-4
+        H = sp.csc_matrix(s.H)
+        xd = spla.spsolve(H, np.asarray(s.b, dtype=np.float64))
+
+        def errs(v):
+            e = v - xd
+            return rel(v, xd), float(np.sqrt(abs(e @ (H @ e)) / abs(xd @ (H @ xd))))
+        r, a = errs(x.cpu().numpy())
+        ro, ao = errs(xo)
+        assert r <= 2 * ro + 1e-12 and a <= 2 * ao + 1e-12, (r, ro, a, ao)
 
 
 def test_block_solve_is_bitwise_deterministic(api, torch, tire):
