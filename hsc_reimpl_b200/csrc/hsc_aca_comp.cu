@@ -32,25 +32,18 @@ namespace hsc {
 
 namespace {
 
-constexpr int kCompThreads = 512;
+constexpr int kCompThreads = 1024;
 constexpr int kCompWarps = kCompThreads / 32;
 
-// CTA-wide (max |.|, first local row-major index, sum of squares) of the residual
-// block.  Rows and columns of a component ascend, so the local row-major order is
-// the global one restricted to the block: the first local maximum is the global
-// argmax's choice among the block's entries.
-__device__ void block_stats(const double* R, int n, double& vmax, int& imax, double& sum) {
+// CTA-wide (max |.|, first local row-major index, sum of squares) from each thread's partial
+// (lv, li, ls).  Rows and columns of a component ascend, so the local row-major order is the
+// global one restricted to the block: the first local maximum is the global argmax's choice
+// among the block's entries (the maximum and its first index do not depend on the order the
+// entries were visited in).
+__device__ void block_reduce(double lv, int li, double ls, double& vmax, int& imax, double& sum) {
     __shared__ double s_v[kCompWarps], s_s[kCompWarps];
     __shared__ int s_i[kCompWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double lv = -1.0, ls = 0.0;
-    int li = INT_MAX;
-    for (int e = threadIdx.x; e < n; e += kCompThreads) {
-        const double x = R[e];
-        ls += x * x;
-        const double ax = fabs(x);
-        if (ax > lv) { lv = ax; li = e; }     // a thread's entries ascend: ties keep the first
-    }
     for (int o = 16; o > 0; o >>= 1) {
         const double qv = __shfl_xor_sync(0xffffffffu, lv, o);
         const int qi = __shfl_xor_sync(0xffffffffu, li, o);
@@ -78,6 +71,15 @@ __device__ void block_stats(const double* R, int n, double& vmax, int& imax, dou
     __syncthreads();
 }
 
+__device__ __forceinline__ void stat_add(double x, int e, double& lv, int& li, double& ls) {
+    ls += x * x;
+    const double ax = fabs(x);
+    if (ax > lv || (ax == lv && e < li)) { lv = ax; li = e; }
+}
+
+// one CTA per coupling component: the full-pivot ACA of its block of E.  Thread t owns the
+// columns t, t + kCompThreads, ... of the block (all rows), so a step is one pass: v = R[i, :] /
+// pivot and R -= u v^T on its columns, folding the next step's statistics in.
 __global__ void __launch_bounds__(kCompThreads) aca_comp_kernel(AcaComp p) {
     const int g = blockIdx.x;
     const int r0 = p.row_ptr[g], mr = p.row_ptr[g + 1] - r0;
@@ -91,14 +93,19 @@ __global__ void __launch_bounds__(kCompThreads) aca_comp_kernel(AcaComp p) {
     __shared__ double s_u[256];          // u = R[:, j]; the host admits components of at most 256 rows
     __shared__ double s_piv;
     __shared__ int s_i, s_j;
-    for (int r = 0; r < mr; ++r) {
-        const double* Er = p.E + (size_t)rows[r] * p.a;
-        for (int c = threadIdx.x; c < nc; c += kCompThreads) R[(size_t)r * nc + c] = Er[cols[c]];
+    double lv = -1.0, ls = 0.0;
+    int li = INT_MAX;
+    for (int c = threadIdx.x; c < nc; c += kCompThreads) {
+        const int gc = cols[c];
+        for (int r = 0; r < mr; ++r) {
+            const double x = p.E[(size_t)rows[r] * p.a + gc];
+            R[(size_t)r * nc + c] = x;
+            stat_add(x, r * nc + c, lv, li, ls);
+        }
     }
-    __syncthreads();
     double vmax, sum;
     int imax;
-    block_stats(R, mr * nc, vmax, imax, sum);
+    block_reduce(lv, li, ls, vmax, imax, sum);  // synchronises: R is complete
     double* piv_abs = p.piv_abs + p.s_off[g];
     long long* piv_idx = p.piv_idx + p.s_off[g];
     double* sums = p.sums + p.s_off[g] + g;   // steps_max + 1 entries per component
@@ -108,30 +115,32 @@ __global__ void __launch_bounds__(kCompThreads) aca_comp_kernel(AcaComp p) {
     for (; s < steps_max; ++s) {
         if (threadIdx.x == 0) sums[s] = sum;
         if (!(vmax > 0.0) || imax == INT_MAX) break;  // the residual vanished (the merge applies the guard)
+        const int i = imax / nc, j = imax - i * nc;
         if (threadIdx.x == 0) {
-            const int li = imax / nc, lj = imax - li * nc;
             piv_abs[s] = vmax;
-            piv_idx[s] = (long long)rows[li] * p.a + cols[lj];  // the global row-major index, for the merge
-            s_i = li;
-            s_j = lj;
+            piv_idx[s] = (long long)rows[i] * p.a + cols[j];  // the global row-major index, for the merge
+            s_piv = R[(size_t)i * nc + j];
+        }
+        for (int r = threadIdx.x; r < mr; r += kCompThreads) {
+            const double u = R[(size_t)r * nc + j];
+            s_u[r] = u;
+            Ug[(size_t)s * mr + r] = u;
         }
         __syncthreads();
-        const int i = s_i, j = s_j;
-        for (int r = threadIdx.x; r < mr; r += kCompThreads) s_u[r] = R[(size_t)r * nc + j];
-        if (threadIdx.x == 0) s_piv = R[(size_t)i * nc + j];
-        __syncthreads();
         const double pivot = s_piv;
-        for (int r = threadIdx.x; r < mr; r += kCompThreads) Ug[(size_t)s * mr + r] = s_u[r];
-        // v = R[i, :] / pivot, then R -= u v^T (the product rounded, then the difference: numpy's
-        // order); each thread updates the columns whose v it computed, so no barrier between
+        // v = R[i, :] / pivot, then R -= u v^T (the product rounded, then the difference: numpy's order)
         double* Vs = Vg + (size_t)s * nc;
+        lv = -1.0; ls = 0.0; li = INT_MAX;
         for (int c = threadIdx.x; c < nc; c += kCompThreads) {
             const double vc = R[(size_t)i * nc + c] / pivot;
             Vs[c] = vc;
-            for (int r = 0; r < mr; ++r) R[(size_t)r * nc + c] = __dsub_rn(R[(size_t)r * nc + c], __dmul_rn(s_u[r], vc));
+            for (int r = 0; r < mr; ++r) {
+                const double x = __dsub_rn(R[(size_t)r * nc + c], __dmul_rn(s_u[r], vc));
+                R[(size_t)r * nc + c] = x;
+                stat_add(x, r * nc + c, lv, li, ls);
+            }
         }
-        __syncthreads();
-        block_stats(R, mr * nc, vmax, imax, sum);
+        block_reduce(lv, li, ls, vmax, imax, sum);
     }
     if (threadIdx.x == 0) {
         p.nsteps[g] = s;
@@ -141,73 +150,118 @@ __global__ void __launch_bounds__(kCompThreads) aca_comp_kernel(AcaComp p) {
 
 constexpr int kMergePer = 8;  // components per lane in the warp merge (256 / 32)
 
-// one warp: merge the components' pivot sequences into the global order and apply the global
-// stop rules; order[t] = (component, its step).  The step records are staged in shared memory
-// first (all 256 threads), then lane l follows the cursors of components l, l + 32, ...
-__global__ void __launch_bounds__(256) aca_merge_kernel(AcaComp p) {
-    extern __shared__ double msm[];
-    const int G = p.ncomp, ns = p.stot;
-    double* pa = msm;                                            // ns
-    double* su = pa + ns;                                        // ns + G
-    long long* pi = reinterpret_cast<long long*>(su + ns + G);   // ns
-    int* so = reinterpret_cast<int*>(pi + ns);                   // G
-    int* nst = so + G;                                           // G
-    for (int e = threadIdx.x; e < ns; e += blockDim.x) { pa[e] = p.piv_abs[e]; pi[e] = p.piv_idx[e]; }
-    for (int e = threadIdx.x; e < ns + G; e += blockDim.x) su[e] = p.sums[e];
-    for (int e = threadIdx.x; e < G; e += blockDim.x) { so[e] = p.s_off[e]; nst[e] = p.nsteps[e]; }
-    __syncthreads();
-    if (threadIdx.x >= 32) return;
-    const int lane = threadIdx.x;
-    double e2 = 0.0;
-    for (int c = lane; c < G; c += 32) e2 += su[so[c] + c];
-    for (int o = 16; o > 0; o >>= 1) e2 += __shfl_xor_sync(0xffffffffu, e2, o);
-    const double scale = sqrt(e2);
-    int cur[kMergePer];
+// The greedy picks of the merge, by one warp: lane l follows the cursors of components l + 32 i
+// (i < PER); each pick is the largest current pivot (ties to the first row-major index), until the
+// rank cap, exhaustion or the zero-pivot guard.  Returns the number of picks.
+template <int PER>
+__device__ int merge_picks(const AcaComp& p, int G, const double* pa, const long long* pi, const int* so,
+                           const int* nst, int* comp, double guard) {
+    const int lane = threadIdx.x & 31;
+    int span = 1;                                                // butterfly rounds cover min(G, 32) lanes
+    while (span < min(G, 32)) span <<= 1;
+    int cur[PER], off[PER], lim[PER];
 #pragma unroll
-    for (int i = 0; i < kMergePer; ++i) cur[i] = 0;
+    for (int i = 0; i < PER; ++i) {
+        const int c = lane + 32 * i;
+        cur[i] = 0;
+        off[i] = c < G ? so[c] : 0;
+        lim[i] = c < G ? nst[c] : 0;
+    }
     int t = 0;
-    for (;; ++t) {
-        double rs = 0.0;
-#pragma unroll
-        for (int i = 0; i < kMergePer; ++i) {
-            const int c = lane + 32 * i;
-            if (c < G) rs += su[so[c] + c + cur[i]];
-        }
-        for (int o = 16; o > 0; o >>= 1) rs += __shfl_xor_sync(0xffffffffu, rs, o);
-        const double residual = t == 0 ? (scale > 0 ? 1.0 : 0.0) : sqrt(rs) / scale;
-        if (lane == 0) p.hist[t] = residual;
-        if (!(residual > p.rtol) || t >= p.kmax) break;
+    for (; t < p.kmax; ++t) {
         double bv = -1.0;
         long long bi = LLONG_MAX;
         int bc = -1, bs = 0;
 #pragma unroll
-        for (int i = 0; i < kMergePer; ++i) {
-            const int c = lane + 32 * i;
-            if (c < G && cur[i] < nst[c]) {
-                const double v = pa[so[c] + cur[i]];
-                const long long ix = pi[so[c] + cur[i]];
-                if (v > bv || (v == bv && ix < bi)) { bv = v; bi = ix; bc = c; bs = cur[i]; }
+        for (int i = 0; i < PER; ++i) {
+            if (cur[i] < lim[i]) {
+                const double v = pa[off[i] + cur[i]];
+                const long long ix = pi[off[i] + cur[i]];
+                if (v > bv || (v == bv && ix < bi)) { bv = v; bi = ix; bc = lane + 32 * i; bs = cur[i]; }
             }
         }
-        for (int o = 16; o > 0; o >>= 1) {
+        for (int o = span >> 1; o > 0; o >>= 1) {
             const double qv = __shfl_xor_sync(0xffffffffu, bv, o);
             const long long qi = __shfl_xor_sync(0xffffffffu, bi, o);
             const int qc = __shfl_xor_sync(0xffffffffu, bc, o), qs = __shfl_xor_sync(0xffffffffu, bs, o);
             if (qv > bv || (qv == bv && qi < bi)) { bv = qv; bi = qi; bc = qc; bs = qs; }
         }
-        if (bc < 0) break;  // every component is exhausted: the global residual vanished too
-        if (!(bv > DBL_EPSILON * fmax(scale, DBL_MIN))) break;  // zero-pivot guard (the global argmax)
-        if (lane == 0) { p.order[2 * t] = bc; p.order[2 * t + 1] = bs; }
+        bv = __shfl_sync(0xffffffffu, bv, 0);
+        bc = __shfl_sync(0xffffffffu, bc, 0);
+        bs = __shfl_sync(0xffffffffu, bs, 0);
+        if (bc < 0 || !(bv > guard)) break;  // exhausted, or the zero-pivot guard on the global argmax
+        if (lane == 0) { p.order[2 * t] = bc; p.order[2 * t + 1] = bs; comp[t] = bc; }
         if ((bc & 31) == lane) {
 #pragma unroll
-            for (int i = 0; i < kMergePer; ++i)
+            for (int i = 0; i < PER; ++i)
                 if (i == (bc >> 5)) ++cur[i];
         }
     }
-    if (lane == 0) {
-        *p.rank = t;
-        *p.err = p.hist[t];
+    return t;
+}
+
+// Merge the components' pivot sequences into the global order and apply the global stop rules;
+// order[t] = (component, its step).  The order depends on the pivots alone, so one warp first
+// picks greedily (the largest current pivot, ties to the first row-major index) until the rank
+// cap, exhaustion or the zero-pivot guard stops it (T picks); then every thread takes one t <= T
+// and forms the relative residual before pick t from the components' sums of squares (summed in
+// component order), and the rank is the first t whose residual reaches rtol, else T.  The step
+// records are staged in shared memory first.
+__global__ void __launch_bounds__(256) aca_merge_kernel(AcaComp p) {
+    extern __shared__ double msm[];
+    const int G = p.ncomp, ns = p.stot, K1 = p.kmax + 1;
+    double* pa = msm;                                            // ns
+    double* su = pa + ns;                                        // ns + G
+    double* tab = su + ns + G;                                   // K1 x G: sums before each pick
+    double* res = tab + (size_t)K1 * G;                          // K1
+    long long* pi = reinterpret_cast<long long*>(res + K1);      // ns
+    int* so = reinterpret_cast<int*>(pi + ns);                   // G
+    int* nst = so + G;                                           // G
+    int* comp = nst + G;                                         // K1: component of each pick
+    __shared__ int s_T, s_rank;
+    __shared__ double s_scale;
+    for (int e = threadIdx.x; e < ns; e += blockDim.x) { pa[e] = p.piv_abs[e]; pi[e] = p.piv_idx[e]; }
+    for (int e = threadIdx.x; e < ns + G; e += blockDim.x) su[e] = p.sums[e];
+    for (int e = threadIdx.x; e < G; e += blockDim.x) { so[e] = p.s_off[e]; nst[e] = p.nsteps[e]; }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        double e2 = 0.0;
+        for (int c = lane; c < G; c += 32) e2 += su[so[c] + c];
+        for (int o = 16; o > 0; o >>= 1) e2 += __shfl_xor_sync(0xffffffffu, e2, o);
+        const double scale = sqrt(e2);
+        const double guard = DBL_EPSILON * fmax(scale, DBL_MIN);
+        const int T = G <= 32 ? merge_picks<1>(p, G, pa, pi, so, nst, comp, guard)
+                              : merge_picks<kMergePer>(p, G, pa, pi, so, nst, comp, guard);
+        if (lane == 0) { s_T = T; s_scale = scale; }
     }
+    __syncthreads();
+    const int T = s_T;
+    const double scale = s_scale;
+    // tab[t][c] = component c's residual sum of squares before pick t
+    for (int c = threadIdx.x; c < G; c += blockDim.x) {
+        int n = 0;
+        for (int t = 0; t <= T; ++t) {
+            tab[(size_t)t * G + c] = su[so[c] + c + n];
+            if (t < T && comp[t] == c) ++n;
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t <= T; t += blockDim.x) {
+        double rs = 0.0;
+        for (int c = 0; c < G; ++c) rs += tab[(size_t)t * G + c];
+        res[t] = t == 0 ? (scale > 0 ? 1.0 : 0.0) : sqrt(rs) / scale;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int r = 0;
+        while (r < T && res[r] > p.rtol) ++r;
+        s_rank = r;
+        *p.rank = r;
+        *p.err = res[r];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t <= s_rank; t += blockDim.x) p.hist[t] = res[t];
 }
 
 // U[:, t] and V[:, t] from the components' columns (zero elsewhere), t < kmax
@@ -233,12 +287,13 @@ __global__ void aca_scatter_kernel(AcaComp p) {
 
 size_t aca_comp_smem_doubles() { return (220 * 1024) / sizeof(double); }
 
-size_t aca_merge_smem_bytes(int ncomp, int stot) {
-    return sizeof(double) * (3 * (size_t)stot + ncomp) + sizeof(int) * 2 * (size_t)ncomp;
+size_t aca_merge_smem_bytes(int ncomp, int stot, int kmax) {
+    const size_t k1 = (size_t)kmax + 1;
+    return sizeof(double) * (3 * (size_t)stot + ncomp + k1 * ncomp + k1) + sizeof(int) * (2 * (size_t)ncomp + k1);
 }
 
-bool aca_merge_fits(int ncomp, int stot) {
-    return ncomp <= 32 * kMergePer && aca_merge_smem_bytes(ncomp, stot) <= 200 * 1024;
+bool aca_merge_fits(int ncomp, int stot, int kmax) {
+    return ncomp <= 32 * kMergePer && aca_merge_smem_bytes(ncomp, stot, kmax) <= 200 * 1024;
 }
 
 cudaError_t launch_aca_comp(const AcaComp& p, cudaStream_t st) {
@@ -249,7 +304,7 @@ cudaError_t launch_aca_comp(const AcaComp& p, cudaStream_t st) {
         count_launch();
         aca_comp_kernel<<<p.ncomp, kCompThreads, smem, st>>>(p);
     }
-    const size_t msmem = aca_merge_smem_bytes(p.ncomp, p.stot);
+    const size_t msmem = aca_merge_smem_bytes(p.ncomp, p.stot, p.kmax);
     cudaError_t e = cudaFuncSetAttribute(aca_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem);
     if (e != cudaSuccess) return e;
     count_launch();

@@ -471,7 +471,7 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
         int stot = 0;
         for (int g = 0; g < S.ncomp_coupled; ++g)
             stot += std::min(std::min((int)comp_rows[g].size(), (int)comp_cols[g].size()), S.kmax);
-        S.aca_comp_ok = aca_merge_fits(S.ncomp_coupled, stot);
+        S.aca_comp_ok = aca_merge_fits(S.ncomp_coupled, stot, S.kmax);
     }
     if (S.aca_comp_ok) {
         const int ncg = S.ncomp_coupled;

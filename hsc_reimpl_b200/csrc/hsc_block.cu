@@ -89,7 +89,7 @@ __global__ void block_fill_kernel(const BlockPlan p) {
 // gives its component (a warp per column, its lanes over 32 rows at a time);
 // counting sort into comp_col_ptr / comp_cols (one CTA, kmax <= kMaxRank)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) block_columns_kernel(BlockPlan p) {
+__global__ void __launch_bounds__(1024) block_columns_kernel(BlockPlan p) {
     __shared__ int s_cnt[257];
     __shared__ int s_comp[kMaxRank];
     const int k = *p.rank;
@@ -98,12 +98,25 @@ __global__ void __launch_bounds__(256) block_columns_kernel(BlockPlan p) {
     __syncthreads();
     for (int j = warp; j < p.kmax; j += nwarps) {
         int comp = -1;
-        if (j < k)
-            for (int i0 = 0; i0 < p.qm; i0 += 32) {
+        if (j < k) {
+            constexpr int kPre = 8;  // the first 256 rows' loads in flight at once
+            bool nzr[kPre];
+#pragma unroll
+            for (int c = 0; c < kPre; ++c) {
+                const int i = 32 * c + lane;
+                nzr[c] = i < p.qm && p.U[(size_t)j * p.qm + i] != 0.0;
+            }
+#pragma unroll
+            for (int c = 0; c < kPre; ++c) {
+                const unsigned nz = __ballot_sync(0xffffffffu, nzr[c]);
+                if (comp < 0 && nz) comp = p.comp_of_body[(32 * c + __ffs(nz) - 1) / 12];
+            }
+            for (int i0 = 32 * kPre; i0 < p.qm && comp < 0; i0 += 32) {
                 const int i = i0 + lane;
                 const unsigned nz = __ballot_sync(0xffffffffu, i < p.qm && p.U[(size_t)j * p.qm + i] != 0.0);
-                if (nz) { comp = p.comp_of_body[(i0 + __ffs(nz) - 1) / 12]; break; }
+                if (nz) comp = p.comp_of_body[(i0 + __ffs(nz) - 1) / 12];
             }
+        }
         if (lane == 0) {
             s_comp[j] = comp;
             p.comp_of_col[j] = comp;
@@ -365,8 +378,11 @@ constexpr int kYBatch = 4;  // columns per pass of the Y kernel
 __host__ __device__ inline size_t y_region_doubles(int R) { return (size_t)4 * kYBatch * 3 * R; }
 
 // ---------------------------------------------------------------------------
-// Y = L V on each part (columns of the part's components), Y at the coupled
-// dofs, the CTA's compact rows of V, and its partial of G = V^T Y (dense kmax^2)
+// Y = L V on each part: CTA (part, b) takes columns [4 b, 4 b + 4) of the part's
+// column list (the columns of the components in the part), so the batches of a
+// part run side by side; it writes Y (FP32, node-padded), Y at the coupled dofs
+// (FP32-rounded; the rest of Yact is zeroed before the launch) and the part's
+// compact rows of V for its columns
 // ---------------------------------------------------------------------------
 template <class MT>
 __global__ void __launch_bounds__(kThreads, 1) block_y_kernel(const BlockPlan p_arg) {
@@ -377,94 +393,91 @@ __global__ void __launch_bounds__(kThreads, 1) block_y_kernel(const BlockPlan p_
     __syncthreads();
     extern __shared__ __align__(16) unsigned char sm[];
     const int cta = blockIdx.x;
-    const Part<MT> s = stage_part<MT>(p, cta, sm, false);
+    constexpr int NB = kYBatch;
+    const int q0 = NB * blockIdx.y;
     int* s_cols = reinterpret_cast<int*>(sm + p.off_cols);
     int* s_slot = s_cols + p.kmax;
+    const int ncols = build_cols(p, cta, s_cols, s_slot);
+    if (q0 >= ncols) return;  // uniform in the CTA
+    const Part<MT> s = stage_part<MT>(p, cta, sm, false);
     double* vec = reinterpret_cast<double*>(sm + p.off_vec);
     const int R3 = 3 * p.R;
-    constexpr int NB = kYBatch;
     double* v = vec;                                   // NB x 3R
-    AT* z = reinterpret_cast<AT*>(vec + NB * R3);      // NB x 4R each
+    AT* z = reinterpret_cast<AT*>(vec + NB * R3);      // NB x 3R each
     AT* t = z + NB * R3;
     AT* u = t + NB * R3;
     int* s_act = reinterpret_cast<int*>(sm + p.off_act);
     for (int e = threadIdx.x; e < s.na; e += blockDim.x) s_act[e] = p.actp[s.ab + e] - 3 * s.rb;
-    const int ncols = build_cols(p, cta, s_cols, s_slot);
-    const int k = *p.rank;
-    // Y at the coupled dofs: zero the CTA's rows first (columns of other components stay zero)
-    for (int e = threadIdx.x; e < s.na * p.kmax; e += blockDim.x) {
-        const int j = e / s.na, il = e - j * s.na;
-        p.Yact[(size_t)j * p.a + s.ab + il] = 0.0;
+    for (int e = threadIdx.x; e < NB * R3; e += blockDim.x) v[e] = 0.0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < NB * s.na; e += blockDim.x) {
+        const int c = e / s.na, il = e - c * s.na;
+        if (q0 + c < ncols) v[(size_t)c * R3 + s_act[il]] = p.V[(size_t)s_cols[q0 + c] * p.a + p.actperm[s.ab + il]];
     }
     __syncthreads();
-    for (int q0 = 0; q0 < ncols; q0 += NB) {
-        for (int e = threadIdx.x; e < NB * R3; e += blockDim.x) v[e] = 0.0;
-        __syncthreads();
-        for (int e = threadIdx.x; e < NB * s.na; e += blockDim.x) {
-            const int c = e / s.na, il = e - c * s.na;
-            if (q0 + c < ncols) v[(size_t)c * R3 + s_act[il]] = p.V[(size_t)s_cols[q0 + c] * p.a + p.actperm[s.ab + il]];
-        }
-        __syncthreads();
-        part_poly<MT, NB>(p, s, v, z, t, u, R3);
-        // the PCG applies the FP32 copy of Y; the Woodbury core is built from the same rounded values
-        for (int e = threadIdx.x; e < NB * s.R; e += blockDim.x) {
-            const int c = e / s.R, lr = e - c * s.R;
-            if (q0 + c >= ncols) continue;
-            const AT* zr = z + (size_t)c * R3 + 3 * lr;
-            const AT z0 = zr[0], z1 = zr[1], z2 = zr[2];
-            float* Yj = p.Y + (size_t)s_cols[q0 + c] * 4 * p.n;
-            reinterpret_cast<float4*>(Yj)[s.rb + lr] = make_float4((float)z0, (float)z1, (float)z2, 0.f);
-        }
-        for (int e = threadIdx.x; e < NB * s.na; e += blockDim.x) {
-            const int c = e / s.na, il = e - c * s.na;
-            if (q0 + c < ncols) {
-                const int dof = s_act[il];
-                const AT zv = z[(size_t)c * R3 + dof];
-                p.Yact[(size_t)s_cols[q0 + c] * p.a + s.ab + il] = (double)(float)zv;
-            }
-        }
-        __syncthreads();
+    part_poly<MT, NB>(p, s, v, z, t, u, R3);
+    // the PCG applies the FP32 copy of Y; the Woodbury core is built from the same rounded values
+    for (int e = threadIdx.x; e < NB * s.R; e += blockDim.x) {
+        const int c = e / s.R, lr = e - c * s.R;
+        if (q0 + c >= ncols) continue;
+        const AT* zr = z + (size_t)c * R3 + 3 * lr;
+        float* Yj = p.Y + (size_t)s_cols[q0 + c] * 4 * p.n;
+        reinterpret_cast<float4*>(Yj)[s.rb + lr] = make_float4((float)zr[0], (float)zr[1], (float)zr[2], 0.f);
     }
-    // the CTA's coupled rows of V, compact: [list position q][own coupled dof]
-    {
-        double* Vc = p.Vc + (size_t)p.kmax * s.ab;
-        for (int e = threadIdx.x; e < ncols * s.na; e += blockDim.x) {
-            const int q = e / s.na, il = e - q * s.na;
-            Vc[e] = p.V[(size_t)s_cols[q] * p.a + p.actperm[s.ab + il]];
+    double* Vc = p.Vc + (size_t)p.kmax * s.ab;  // the part's coupled rows of V, compact: [list position q][dof]
+    for (int e = threadIdx.x; e < NB * s.na; e += blockDim.x) {
+        const int c = e / s.na, il = e - c * s.na;
+        if (q0 + c < ncols) {
+            const int j = s_cols[q0 + c];
+            p.Yact[(size_t)j * p.a + s.ab + il] = (double)(float)z[(size_t)c * R3 + s_act[il]];
+            Vc[(size_t)(q0 + c) * s.na + il] = p.V[(size_t)j * p.a + p.actperm[s.ab + il]];
         }
     }
-    // partial G_c[j][l] = sum_{own coupled dofs} V[., j] Yact[., l]  (dense kmax^2, zero outside).
-    // The CTA's rows of V ([q][dof]) and of Y ([dof][q]) are staged in the (now free) vector region
-    // when they fit: a warp takes a row q_a, its lanes the columns q_b, and walks the dofs.
+}
+
+// the partial G_c[j][l] = sum over a coupled part's own coupled dofs of V[., j] Yact[., l] (dense
+// kmax^2, zero outside its columns).  The part's rows of V ([q][dof]) and of Y ([dof][q]) are staged
+// in shared memory when they fit: a warp takes a row q_a, its lanes the columns q_b, and walks the dofs.
+__global__ void __launch_bounds__(kThreads, 1) block_gpart_kernel(const BlockPlan p_arg) {
+    __shared__ __align__(16) unsigned char s_p_raw[sizeof(BlockPlan)];
+    BlockPlan& p = *reinterpret_cast<BlockPlan*>(s_p_raw);
+    if (threadIdx.x == 0) p = p_arg;
+    __syncthreads();
+    const int cta = blockIdx.x;
     const int aidx = p.cta_aidx[cta];
-    if (aidx >= 0) {  // uniform in the CTA
-        __syncthreads();  // the compact rows of V above are read back below
-        double* Gc = p.pG + (size_t)aidx * p.kmax * p.kmax;
-        for (int e = threadIdx.x; e < p.kmax * p.kmax; e += blockDim.x) Gc[e] = 0.0;
-        const bool staged = 2 * (size_t)s.na * ncols <= y_region_doubles(p.R);
-        double* Vs = vec;
-        double* Ys = vec + (size_t)s.na * ncols;
-        if (staged)
-            for (int e = threadIdx.x; e < ncols * s.na; e += blockDim.x) {
-                const int q = e / s.na, il = e - q * s.na;
-                Vs[e] = p.Vc[(size_t)p.kmax * s.ab + e];
-                Ys[(size_t)il * ncols + q] = p.Yact[(size_t)s_cols[q] * p.a + s.ab + il];
+    if (aidx < 0) return;  // uniform in the CTA
+    extern __shared__ __align__(16) unsigned char sm[];
+    int* s_cols = reinterpret_cast<int*>(sm + p.off_cols);
+    int* s_slot = s_cols + p.kmax;
+    const int ncols = build_cols(p, cta, s_cols, s_slot);
+    const int k = *p.rank;
+    const int ab = p.cta_act[2 * cta], na = p.cta_act[2 * cta + 1] - ab;
+    const double* Vc = p.Vc + (size_t)p.kmax * ab;
+    double* Gc = p.pG + (size_t)aidx * p.kmax * p.kmax;
+    for (int e = threadIdx.x; e < p.kmax * p.kmax; e += blockDim.x) Gc[e] = 0.0;
+    double* vec = reinterpret_cast<double*>(sm + p.off_vec);
+    const bool staged = 2 * (size_t)na * ncols <= y_region_doubles(p.R);
+    double* Vs = vec;
+    double* Ys = vec + (size_t)na * ncols;
+    if (staged)
+        for (int e = threadIdx.x; e < ncols * na; e += blockDim.x) {
+            const int q = e / na, il = e - q * na;
+            Vs[e] = Vc[e];
+            Ys[(size_t)il * ncols + q] = p.Yact[(size_t)s_cols[q] * p.a + ab + il];
+        }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int qa = warp; qa < ncols; qa += kWarps)
+        for (int qb = lane; qb < ncols; qb += 32) {
+            const int j = s_cols[qa], l = s_cols[qb];
+            double acc = 0.0;
+            if (staged) {
+                for (int il = 0; il < na; ++il) acc += Vs[(size_t)qa * na + il] * Ys[(size_t)il * ncols + qb];
+            } else {
+                for (int il = 0; il < na; ++il) acc += Vc[(size_t)qa * na + il] * p.Yact[(size_t)l * p.a + ab + il];
             }
-        __syncthreads();
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        for (int qa = warp; qa < ncols; qa += kWarps)
-            for (int qb = lane; qb < ncols; qb += 32) {
-                const int j = s_cols[qa], l = s_cols[qb];
-                double acc = 0.0;
-                if (staged) {
-                    for (int il = 0; il < s.na; ++il) acc += Vs[(size_t)qa * s.na + il] * Ys[(size_t)il * ncols + qb];
-                } else {
-                    for (int il = 0; il < s.na; ++il)
-                        acc += p.Vc[(size_t)p.kmax * s.ab + (size_t)qa * s.na + il] * p.Yact[(size_t)l * p.a + s.ab + il];
-                }
-                if (j < k && l < k) Gc[(size_t)j * p.kmax + l] = acc;
-            }
-    }
+            if (j < k && l < k) Gc[(size_t)j * p.kmax + l] = acc;
+        }
 }
 
 // G[e] = sum over the coupled CTAs of their partials (fixed order), symmetrised later
@@ -1015,7 +1028,7 @@ void launch_block_fill(int precision, const BlockPlan& p, cudaStream_t st) {
 
 void launch_block_columns(const BlockPlan& p, cudaStream_t st) {
     count_launch();
-    block_columns_kernel<<<1, 256, 0, st>>>(p);
+    block_columns_kernel<<<1, 1024, 0, st>>>(p);
 }
 
 template <class MT>
@@ -1023,8 +1036,14 @@ static cudaError_t launch_y_t(const BlockPlan& p, cudaStream_t st) {
     auto fn = block_y_kernel<MT>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_y);
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(block_gpart_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_y);
+    if (e != cudaSuccess) return e;
+    cudaMemsetAsync(p.Yact, 0, sizeof(double) * (size_t)p.a * p.kmax, st);
+    const int batches = std::max(1, (p.NCOL + kYBatch - 1) / kYBatch);
     count_launch();
-    fn<<<p.G_ctas, kThreads, p.smem_y, st>>>(p);
+    fn<<<dim3(p.G_ctas, batches), kThreads, p.smem_y, st>>>(p);
+    count_launch();
+    block_gpart_kernel<<<p.G_ctas, kThreads, p.smem_y, st>>>(p);
     return cudaPeekAtLastError();
 }
 
@@ -1046,7 +1065,7 @@ void launch_block_k(const BlockPlan& p, int nact_cta, cudaStream_t st) {
     block_kinv_kernel<<<(kk + 255) / 256, 256, 0, st>>>(p.Kb, p.dpiv, dk, p.kmax, p.Ka);
     // K~ = (K^-1)^-1 into Kb (Cholesky: flags a matrix that is not SPD)
     cudaMemsetAsync(p.bad, 0, sizeof(int), st);
-    if (!launch_chol_inverse(p.Ka, p.kmax, p.Kb, p.bad, st)) {
+    if (!launch_chol_inverse(p.Ka, p.kmax, p.Kb, p.bad, st, dk)) {
         launch_cholesky(p.Ka, p.kmax, p.G, p.bad, st);
         launch_chol_solve(p.G, p.kmax, p.ident, p.kmax, p.Kb, p.kmax, p.kmax, nullptr, p.pG, st);
     }

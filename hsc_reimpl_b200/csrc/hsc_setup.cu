@@ -462,9 +462,16 @@ __global__ void __launch_bounds__(1024) gj_inverse_kernel(const double* A, int m
 // this step's readers.  Per step a thread reads 14 shared values instead of
 // streaming the whole matrix through shared memory.
 constexpr int kGjR = 9, kGjC = 5, kGjMax = 16 * kGjR;
-__global__ void __launch_bounds__(512) gj_inverse_reg_kernel(const double* A, int m, double* P, int* bad) {
+constexpr int kGbR = 3, kGbMax = 32 * kGbR;  // the 1024-thread kernel below
+__global__ void __launch_bounds__(512) gj_inverse_reg_kernel(const double* A, int ld, const int* dk, double* P, int* bad) {
     __shared__ double s_row[2][32 * kGjC], s_col[2][kGjMax], s_rp[2];
     __shared__ int s_bad;
+    int m = ld;
+    if (dk) {  // the leading *dk x *dk block of an ld x ld matrix; ranks the 1024-thread kernel took are skipped
+        const int kd = *dk;
+        if (kd <= kGbMax) return;
+        m = min(ld, kd);
+    }
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     double w[kGjR][kGjC];
 #pragma unroll
@@ -472,7 +479,7 @@ __global__ void __launch_bounds__(512) gj_inverse_reg_kernel(const double* A, in
 #pragma unroll
         for (int c = 0; c < kGjC; ++c) {
             const int i = ty + 16 * r, j = tx + 32 * c;
-            w[r][c] = (i < m && j < m) ? A[(size_t)i * m + j] : 0.0;
+            w[r][c] = (i < m && j < m) ? A[(size_t)i * ld + j] : 0.0;
         }
     if (threadIdx.x == 0) s_bad = 0;
     for (int k = 0; k < m; ++k) {
@@ -544,25 +551,33 @@ __global__ void __launch_bounds__(512) gj_inverse_reg_kernel(const double* A, in
 #pragma unroll
         for (int c = 0; c < kGjC; ++c) {
             const int i = ty + 16 * r, j = tx + 32 * c;
-            if (i < m && j < m) P[(size_t)i * m + j] = w[r][c];
+            if (i < m && j < m) P[(size_t)i * ld + j] = w[r][c];
         }
 }
 
 // The same elimination for blocks of at most 96 rows, one 1024-thread CTA per block: thread
-// (ty, tx) of a 32 x 32 grid owns rows ty + 32 r and columns tx + 32 c (r, c < 3), nine entries,
-// so every thread issues few FMAs per step and the step is short.  A block is the set of rows
-// and columns idx[ptr[g] .. ptr[g + 1]) of the m x m matrix (idx null: the whole matrix, one
-// block).  Gauss-Jordan without pivoting never mixes two blocks of a block-diagonal matrix (the
-// products across them are exact zeros), so inverting the blocks apart gives the whole inverse
-// bit for bit; entries of P outside the blocks are left to the caller.
-constexpr int kGbR = 3, kGbMax = 32 * kGbR;
+// (ty, tx) of a 32 x 32 grid owns rows ty + 32 r and columns tx + 32 c (r, c < 3), nine entries.
+// A warp holds whole rows, so the pivot column's entries of its rows come by shuffle from lane
+// k mod 32; only the pivot row (one warp) and the reciprocal pivot (one lane) go through shared
+// memory, double-buffered, one barrier per step.  A block is the set of rows and columns
+// idx[ptr[g] .. ptr[g + 1]) of the m x m matrix (idx null: the whole matrix, one block; dk
+// non-null: the leading *dk x *dk block).  Gauss-Jordan without pivoting never mixes two blocks
+// of a block-diagonal matrix (the products across them are exact zeros), so inverting the blocks
+// apart gives the whole inverse bit for bit; entries of P outside the blocks are left to the caller.
+__device__ __forceinline__ double sel3(const double (&v)[3], int i) { return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]); }
+
 __global__ void __launch_bounds__(1024) gj_inverse_blocks_kernel(const double* A, int m, const int* ptr, const int* idx,
-                                                                 double* P, int* bad) {
-    __shared__ double s_row[2][kGbMax], s_col[2][kGbMax], s_rp[2];
+                                                                 const int* dk, double* P, int* bad) {
+    __shared__ double s_row[2][kGbMax], s_rp[2];
     __shared__ int s_bad;
     const int g = blockIdx.x;
     const int b0 = ptr ? ptr[g] : 0;
-    const int mb = ptr ? ptr[g + 1] - b0 : m;
+    int mb = ptr ? ptr[g + 1] - b0 : m;
+    if (dk) {  // the leading *dk x *dk block (no ptr); larger ranks go to the 512-thread kernel
+        const int kd = *dk;
+        if (kd > kGbMax) return;
+        mb = min(mb, kd);
+    }
     const int* ix = idx ? idx + b0 : nullptr;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     int gi[kGbR], gj[kGbR];
@@ -582,28 +597,18 @@ __global__ void __launch_bounds__(1024) gj_inverse_blocks_kernel(const double* A
         }
     if (threadIdx.x == 0) s_bad = 0;
     for (int k = 0; k < mb; ++k) {
-        const int b = k & 1, kk = k >> 5;
-        if (ty == (k & 31)) {
+        const int b = k & 1, kk = k >> 5, ko = k & 31;
+        double ci[kGbR];
 #pragma unroll
-            for (int r = 0; r < kGbR; ++r)
-                if (r == kk)
+        for (int r = 0; r < kGbR; ++r) ci[r] = __shfl_sync(0xffffffffu, sel3(w[r], kk), ko);  // column k
+        if (ty == ko) {  // the pivot row's warp publishes it, its pivot lane the reciprocal
 #pragma unroll
-                    for (int c = 0; c < kGbR; ++c) s_row[b][tx + 32 * c] = w[r][c];
-        }
-        if (tx == (k & 31)) {
-#pragma unroll
-            for (int c = 0; c < kGbR; ++c)
-                if (c == kk)
-#pragma unroll
-                    for (int r = 0; r < kGbR; ++r) {
-                        const int i = ty + 32 * r;
-                        s_col[b][i] = w[r][c];
-                        if (i == k) {
-                            double pv = w[r][c];
-                            if (!(pv > 0.0) || !isfinite(pv)) { s_bad = 1; pv = 1.0; }
-                            s_rp[b] = 1.0 / pv;
-                        }
-                    }
+            for (int c = 0; c < kGbR; ++c) s_row[b][tx + 32 * c] = kk == 0 ? w[0][c] : (kk == 1 ? w[1][c] : w[2][c]);
+            if (tx == ko) {
+                double pv = sel3(ci, kk);
+                if (!(pv > 0.0) || !isfinite(pv)) { s_bad = 1; pv = 1.0; }
+                s_rp[b] = 1.0 / pv;
+            }
         }
         __syncthreads();
         const double rp = s_rp[b];
@@ -611,24 +616,23 @@ __global__ void __launch_bounds__(1024) gj_inverse_blocks_kernel(const double* A
 #pragma unroll
         for (int c = 0; c < kGbR; ++c) rs[c] = s_row[b][tx + 32 * c] * rp;  // pivot row / pivot
 #pragma unroll
-        for (int r = 0; r < kGbR; ++r) {
-            const double ci = s_col[b][ty + 32 * r];
+        for (int r = 0; r < kGbR; ++r)
 #pragma unroll
-            for (int c = 0; c < kGbR; ++c) w[r][c] = fma(-ci, rs[c], w[r][c]);
+            for (int c = 0; c < kGbR; ++c) w[r][c] = fma(-ci[r], rs[c], w[r][c]);
+        // the owners of column k and row k overwrite theirs: -c_i / p, row_j / p, 1 / p
+        if (tx == ko) {
+#pragma unroll
+            for (int r = 0; r < kGbR; ++r) {
+                const double v = -ci[r] * rp;
+                if (kk == 0) w[r][0] = v; else if (kk == 1) w[r][1] = v; else w[r][2] = v;
+            }
         }
-        if (tx == (k & 31)) {
+        if (ty == ko) {
 #pragma unroll
-            for (int c = 0; c < kGbR; ++c)
-                if (c == kk)
-#pragma unroll
-                    for (int r = 0; r < kGbR; ++r) w[r][c] = -s_col[b][ty + 32 * r] * rp;
-        }
-        if (ty == (k & 31)) {
-#pragma unroll
-            for (int r = 0; r < kGbR; ++r)
-                if (r == kk)
-#pragma unroll
-                    for (int c = 0; c < kGbR; ++c) w[r][c] = (tx + 32 * c == k) ? rp : rs[c];
+            for (int c = 0; c < kGbR; ++c) {
+                const double v = (tx + 32 * c == k) ? rp : rs[c];
+                if (kk == 0) w[0][c] = v; else if (kk == 1) w[1][c] = v; else w[2][c] = v;
+            }
         }
     }
     __syncthreads();
@@ -640,6 +644,80 @@ __global__ void __launch_bounds__(1024) gj_inverse_blocks_kernel(const double* A
             const int i = ty + 32 * r, j = tx + 32 * c;
             if (i < mb && j < mb) P[(size_t)gi[r] * m + gj[c]] = w[r][c];
         }
+}
+
+// C (k x k, row-major, k from device, k <= 96) = L diag(d) L^T in one 1024-thread CTA, the
+// matrix in registers as in the kernel above (thread (ty, tx): rows ty + 32 r, columns tx + 32 c).
+// Step j: a warp takes column j of its rows by shuffle and publishes it, one barrier, then every
+// entry below and right of (j, j) takes W_il -= (W_ij / d_j) W_lj, the operations and order of
+// the shared-memory kernel below; only the lower triangle is read.  Returns at once when k > 96.
+__global__ void __launch_bounds__(1024) ldlt_reg_kernel(const double* C, int kmax, const int* dk, double* L, double* d,
+                                                        int* bad) {
+    __shared__ double s_col[2][kGbMax], s_rd[2];
+    __shared__ int s_bad;
+    const int k = *dk;
+    if (k > kGbMax) return;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    double w[kGbR][kGbR];
+#pragma unroll
+    for (int r = 0; r < kGbR; ++r)
+#pragma unroll
+        for (int c = 0; c < kGbR; ++c) {
+            const int i = ty + 32 * r, l = tx + 32 * c;
+            w[r][c] = (i < k && l < k && l <= i) ? 0.5 * (C[(size_t)i * kmax + l] + C[(size_t)l * kmax + i]) : 0.0;
+        }
+    if (threadIdx.x == 0) s_bad = 0;
+    for (int j = 0; j < k; ++j) {
+        const int b = j & 1, jj = j >> 5, jo = j & 31;
+        double ci[kGbR];
+#pragma unroll
+        for (int r = 0; r < kGbR; ++r) ci[r] = __shfl_sync(0xffffffffu, sel3(w[r], jj), jo);  // W[i][j]
+        if (tx < kGbR) s_col[b][ty + 32 * tx] = sel3(ci, tx);
+        if (ty == jo && tx == jo) {
+            const double dj = sel3(ci, jj);
+            const bool okj = isfinite(dj) && dj != 0.0;
+            if (!okj) s_bad = 1;
+            s_rd[b] = 1.0 / (okj ? dj : 1.0);
+        }
+        __syncthreads();
+        const double rd = s_rd[b];
+        double cl[kGbR];
+#pragma unroll
+        for (int c = 0; c < kGbR; ++c) cl[c] = (tx + 32 * c > j) ? s_col[b][tx + 32 * c] : 0.0;
+#pragma unroll
+        for (int r = 0; r < kGbR; ++r) {
+            const double wij = (ty + 32 * r > j) ? ci[r] * rd : 0.0;
+#pragma unroll
+            for (int c = 0; c < kGbR; ++c) w[r][c] = fma(-wij, cl[c], w[r][c]);
+        }
+        if (tx == jo) {  // column j becomes L[:, j] below the diagonal
+#pragma unroll
+            for (int r = 0; r < kGbR; ++r)
+                if (ty + 32 * r > j) {
+                    const double v = ci[r] * rd;
+                    if (jj == 0) w[r][0] = v; else if (jj == 1) w[r][1] = v; else w[r][2] = v;
+                }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kGbR; ++r)
+#pragma unroll
+        for (int c = 0; c < kGbR; ++c) {
+            const int i = ty + 32 * r, l = tx + 32 * c;
+            if (i < kmax && l < kmax) {
+                double v = 0.0;
+                if (i < k && l < k) v = (l < i) ? w[r][c] : (l == i ? 1.0 : 0.0);
+                L[(size_t)i * kmax + l] = v;
+                if (i == l) d[i] = i < k ? w[r][c] : 0.0;
+            }
+        }
+    for (int e = threadIdx.x; e < kmax * kmax; e += blockDim.x) {  // beyond the register tiles (kmax > 96)
+        const int i = e / kmax, l = e - i * kmax;
+        if (i >= kGbMax || l >= kGbMax) L[e] = 0.0;
+    }
+    for (int i = kGbMax + threadIdx.x; i < kmax; i += blockDim.x) d[i] = 0.0;
+    if (threadIdx.x == 0 && s_bad) atomicAdd(bad, 1);
 }
 
 // P = A^-1 for an SPD A (m <= 160) in one 1024-thread CTA: Cholesky in
@@ -714,6 +792,7 @@ __global__ void __launch_bounds__(1024) ldlt_kernel(double* C, int kmax, const i
                                                     int use_smem, int* bad) {
     extern __shared__ double sm[];
     const int k = *dk;
+    if (k <= kGbMax) return;  // the register kernel took it
     double* W = use_smem ? sm : C;
     const int ldw = use_smem ? k + 1 : kmax;  // odd stride in shared memory
     for (int e = threadIdx.x; e < k * k; e += blockDim.x) {  // lower triangle only (in place when W == C)
@@ -1220,13 +1299,14 @@ void launch_cholesky(const double* A, int m, double* L, int* bad, cudaStream_t s
     HSC_COUNTED(cholesky_kernel<<<1, 1024, use ? bytes : 0, st>>>(A, m, L, use, bad));
 }
 
-bool launch_chol_inverse(const double* A, int m, double* P, int* bad, cudaStream_t st) {
+bool launch_chol_inverse(const double* A, int m, double* P, int* bad, cudaStream_t st, const int* dk) {
     if (m <= kGbMax) {
-        HSC_COUNTED(gj_inverse_blocks_kernel<<<1, 1024, 0, st>>>(A, m, nullptr, nullptr, P, bad));
+        HSC_COUNTED(gj_inverse_blocks_kernel<<<1, 1024, 0, st>>>(A, m, nullptr, nullptr, dk, P, bad));
         return true;
     }
     if (m <= kGjMax) {
-        HSC_COUNTED(gj_inverse_reg_kernel<<<1, 512, 0, st>>>(A, m, P, bad));
+        if (dk) HSC_COUNTED(gj_inverse_blocks_kernel<<<1, 1024, 0, st>>>(A, m, nullptr, nullptr, dk, P, bad));
+        HSC_COUNTED(gj_inverse_reg_kernel<<<1, 512, 0, st>>>(A, m, dk, P, bad));
         return true;
     }
     const size_t bytes = sizeof(double) * ((size_t)m * (m + 1) + 2 * (size_t)m);
@@ -1240,7 +1320,7 @@ bool launch_inverse_blocks(const double* A, int m, int nblk, int max_blk, const 
                            int* bad, cudaStream_t st) {
     if (max_blk > kGbMax || nblk < 1) return false;
     cudaMemsetAsync(P, 0, sizeof(double) * (size_t)m * m, st);
-    HSC_COUNTED(gj_inverse_blocks_kernel<<<nblk, 1024, 0, st>>>(A, m, ptr, idx, P, bad));
+    HSC_COUNTED(gj_inverse_blocks_kernel<<<nblk, 1024, 0, st>>>(A, m, ptr, idx, nullptr, P, bad));
     return true;
 }
 
@@ -1254,7 +1334,9 @@ void launch_ldlt(double* C, int kmax, const int* dk, double* L, double* d, int* 
     const size_t bytes = sizeof(double) * (size_t)kmax * (kmax + 1);
     const int use = bytes <= 200 * 1024;
     if (use) cudaFuncSetAttribute(ldlt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    HSC_COUNTED(ldlt_kernel<<<1, 1024, use ? bytes : 0, st>>>(C, kmax, dk, L, d, use, bad));
+    // the register kernel for ranks up to 96, the shared-memory one beyond (each returns for the other's ranks)
+    HSC_COUNTED(ldlt_reg_kernel<<<1, 1024, 0, st>>>(C, kmax, dk, L, d, bad));
+    if (kmax > kGbMax) HSC_COUNTED(ldlt_kernel<<<1, 1024, use ? bytes : 0, st>>>(C, kmax, dk, L, d, use, bad));
 }
 
 void launch_block12_inverse(const double* A, int qm, double* Binv, int* bad, cudaStream_t st) {

@@ -67,7 +67,7 @@ struct AcaComp {
 };
 size_t aca_comp_smem_doubles();
 // the warp merge stages every component's step records in shared memory
-bool aca_merge_fits(int ncomp, int stot);
+bool aca_merge_fits(int ncomp, int stot, int kmax);
 cudaError_t launch_aca_comp(const AcaComp& p, cudaStream_t st);
 
 size_t aca_cluster_smem_doubles(int m, int nc);
@@ -122,7 +122,9 @@ int aca_blocks_per_sm();
 void launch_gemm(const GemmArgs& g, int M, int N, cudaStream_t st);
 void launch_cholesky(const double* A, int m, double* L, int* bad, cudaStream_t st);
 // P = A^-1 by Cholesky in one CTA; false (nothing launched) when m is too large
-bool launch_chol_inverse(const double* A, int m, double* P, int* bad, cudaStream_t st);
+// P = A^-1 for an SPD m x m A (dk non-null: only the leading *dk x *dk block, *dk <= m, is
+// inverted and written); false when m is too large for the one-CTA kernels
+bool launch_chol_inverse(const double* A, int m, double* P, int* bad, cudaStream_t st, const int* dk = nullptr);
 // P = A^-1 for an SPD A that is block diagonal over index sets (rows and columns idx[ptr[g] ..
 // ptr[g + 1]), every set at most 96): one CTA per set, zeros elsewhere; false if a set is larger
 bool launch_inverse_blocks(const double* A, int m, int nblk, int max_blk, const int* ptr, const int* idx, double* P,
