@@ -109,7 +109,7 @@ struct System {
     DevBuf blk_Y, blk_Yact, blk_Vc, blk_pG, blk_G, blk_K, blk_Ka, blk_Kb, blk_pY, blk_pV, blk_pX, blk_pdot, blk_mpub,
         blk_xpub, blk_colof, blk_colptr, blk_cols, blk_bad, blk_C, blk_cta_comp_ptr, blk_cta_comp, blk_cta_comp_slot,
         blk_comp_slot_ptr, blk_comp_of_body, blk_ident, blk_sslice, blk_cslice, blk_cchunk, blk_nloc, blk_slc,
-        blk_ssrc, blk_svals;
+        blk_ssrc, blk_svals, blk_coloff;
     BlockPlan blk{};
     int blk_nact_cta = 0;
     // plan
@@ -1395,6 +1395,7 @@ int build_block_plan(hsc_ctx* ctx, System& S, cudaStream_t st) {
     GROW(S.blk_colof, sizeof(int) * km);
     GROW(S.blk_colptr, sizeof(int) * (ncomp + 1));
     GROW(S.blk_cols, sizeof(int) * km);
+    GROW(S.blk_coloff, sizeof(int) * (km + 1));
     GROW(S.blk_bad, sizeof(int) * 4);
     GROW(S.blk_cta_comp_ptr, sizeof(int) * (G + 1));
     GROW(S.blk_cta_comp, sizeof(int) * std::max<size_t>(1, cta_comp.size()));
@@ -1460,6 +1461,7 @@ int build_block_plan(hsc_ctx* ctx, System& S, cudaStream_t st) {
     b.cta_comp_slot = S.blk_cta_comp_slot.as<int>(); b.comp_slot_ptr = S.blk_comp_slot_ptr.as<int>();
     b.nslot = nslot;
     b.comp_of_col = S.blk_colof.as<int>(); b.comp_col_ptr = S.blk_colptr.as<int>(); b.comp_cols = S.blk_cols.as<int>();
+    b.col_off = S.blk_coloff.as<int>();
     b.x = S.x.as<double>(); b.rhs = S.bf.as<double>(); b.mpub = S.blk_mpub.as<double>(); b.xpub = S.blk_xpub.as<double>();
     b.pY = S.blk_pY.as<double>(); b.pV = S.blk_pV.as<double>(); b.pX = S.blk_pX.as<double>(); b.pdot = S.blk_pdot.as<double>();
     b.bar = ctx->d_bar.as<GridBar>();

@@ -123,6 +123,8 @@ __global__ void __launch_bounds__(1024) block_columns_kernel(BlockPlan p) {
             if (comp >= 0) atomicAdd(&s_cnt[comp + 1], 1);
         }
     }
+    __shared__ int s_sptr[257];
+    for (int g = threadIdx.x; g <= p.ncomp; g += blockDim.x) s_sptr[g] = p.comp_slot_ptr[g];
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int g = 0; g < p.ncomp; ++g) s_cnt[g + 1] += s_cnt[g];
@@ -132,6 +134,15 @@ __global__ void __launch_bounds__(1024) block_columns_kernel(BlockPlan p) {
             const int comp = s_comp[j];
             if (comp >= 0) p.comp_cols[s_cnt[comp]++] = j;
         }
+    } else if (threadIdx.x == 32) {
+        // packed partials: column j's contributor slots at col_off[j] ..
+        int off = 0;
+        for (int j = 0; j < p.kmax; ++j) {
+            p.col_off[j] = off;
+            const int comp = j < k ? s_comp[j] : -1;
+            if (comp >= 0) off += s_sptr[comp + 1] - s_sptr[comp];
+        }
+        p.col_off[p.kmax] = off;
     }
 }
 
@@ -373,6 +384,12 @@ __device__ void part_op(const Part<MT>& s, bool gv, const double* win, const dou
 
 constexpr int kYBatch = 4;  // columns per pass of the Y kernel
 
+// the V^T Y partial kernel's shared memory: the column list and slots, then V's and Y's rows
+__host__ __device__ inline size_t gpart_stage_offset(int kmax) { return ((size_t)8 * kmax + 15) / 16 * 16; }
+__host__ __device__ inline size_t gpart_smem_bytes(int kmax, int NA, int NCOL) {
+    return gpart_stage_offset(kmax) + sizeof(double) * 2 * (size_t)NA * NCOL;
+}
+
 // doubles of the Y kernel's vector region: the batch's inputs and the polynomial's three
 // vectors, 3R per column each
 __host__ __device__ inline size_t y_region_doubles(int R) { return (size_t)4 * kYBatch * 3 * R; }
@@ -447,7 +464,7 @@ __global__ void __launch_bounds__(kThreads, 1) block_gpart_kernel(const BlockPla
     const int aidx = p.cta_aidx[cta];
     if (aidx < 0) return;  // uniform in the CTA
     extern __shared__ __align__(16) unsigned char sm[];
-    int* s_cols = reinterpret_cast<int*>(sm + p.off_cols);
+    int* s_cols = reinterpret_cast<int*>(sm);  // layout: column list and slots (2 kmax ints), then the staging
     int* s_slot = s_cols + p.kmax;
     const int ncols = build_cols(p, cta, s_cols, s_slot);
     const int k = *p.rank;
@@ -455,8 +472,8 @@ __global__ void __launch_bounds__(kThreads, 1) block_gpart_kernel(const BlockPla
     const double* Vc = p.Vc + (size_t)p.kmax * ab;
     double* Gc = p.pG + (size_t)aidx * p.kmax * p.kmax;
     for (int e = threadIdx.x; e < p.kmax * p.kmax; e += blockDim.x) Gc[e] = 0.0;
-    double* vec = reinterpret_cast<double*>(sm + p.off_vec);
-    const bool staged = 2 * (size_t)na * ncols <= y_region_doubles(p.R);
+    double* vec = reinterpret_cast<double*>(sm + gpart_stage_offset(p.kmax));
+    const bool staged = p.gpart_staged && ncols <= p.NCOL;
     double* Vs = vec;
     double* Ys = vec + (size_t)na * ncols;
     if (staged)
@@ -567,7 +584,7 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
     int* s_act = reinterpret_cast<int*>(sm + p.off_act);       // own coupled dofs, local (3 lr + d)
     int* s_cols = reinterpret_cast<int*>(sm + p.off_cols);
     int* s_slot = s_cols + p.kmax;
-    int* s_srng = reinterpret_cast<int*>(sm + p.off_srng);     // per column j < k: its component's slots
+    int* s_srng = reinterpret_cast<int*>(sm + p.off_srng);     // per column j < k: its packed partials
     double* s_sv = reinterpret_cast<double*>(sm + p.off_kv);  // Y^T v sums (kmax)
     double* s_vt = s_sv + p.kmax;                             // V^T m sums (kmax)
     double* s_c = s_vt + p.kmax;                              // K s on the CTA's columns (by list position)
@@ -578,10 +595,15 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
     for (int e = threadIdx.x; e < sl.na; e += blockDim.x) s_act[e] = p.actp[sl.ab + e] - 3 * sl.rb;
     const int ncols = build_cols(p, cta, s_cols, s_slot);  // synchronises: s_act is complete
     const int k = *p.rank;
+    // s_slot[q] becomes the position of the CTA's partial for column s_cols[q] in the packed arrays
+    for (int q = threadIdx.x; q < ncols; q += blockDim.x) {
+        const int j = s_cols[q], g = p.comp_of_col[j];
+        s_slot[q] = p.col_off[j] + s_slot[q] - p.comp_slot_ptr[g];
+    }
     for (int j = threadIdx.x; j < k; j += blockDim.x) {
         const int g = p.comp_of_col[j];
-        s_srng[2 * j] = g >= 0 ? p.comp_slot_ptr[g] : 0;
-        s_srng[2 * j + 1] = g >= 0 ? p.comp_slot_ptr[g + 1] : 0;
+        s_srng[2 * j] = p.col_off[j];
+        s_srng[2 * j + 1] = g >= 0 ? p.col_off[j + 1] : p.col_off[j];
     }
     int epoch = 0;
     const bool yc_on = p.stage_yc && ncols <= p.NCOL;
@@ -653,8 +675,8 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
         a1 = bwarp_sum(a1);
         if (lane == 0) { s_dot[2 * half] = a0; s_dot[2 * half + 1] = a1; }
     };
-    // out[j] = sum of the contributor slots of column j's component, for every j < k: a warp per
-    // column, its lanes over the slots (each lane adds its slots in order, then a fixed butterfly),
+    // out[j] = sum of column j's packed contributor partials, for every j < k: a warp per column,
+    // its lanes over the partials (each lane adds its partials in order, then a fixed butterfly),
     // the loads of seven columns' first 64 slots in flight per warp before any add waits.  With
     // `dots` the last two warps sum the dots instead.
     auto sum_cols = [&](const double* part, double* out, bool dots) {
@@ -671,8 +693,8 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
                 b2[i] = 0.0;
                 if (j < k) {
                     const int q = s_srng[2 * j] + lane, q1 = s_srng[2 * j + 1];
-                    if (q < q1) a[i] = __ldcg(part + (size_t)q * p.kmax + j);
-                    if (q + 32 < q1) b2[i] = __ldcg(part + (size_t)(q + 32) * p.kmax + j);
+                    if (q < q1) a[i] = __ldcg(part + q);
+                    if (q + 32 < q1) b2[i] = __ldcg(part + q + 32);
                 }
             }
 #pragma unroll
@@ -681,7 +703,7 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
                 a[i] += b2[i];
                 if (j < k)
                     for (int q = s_srng[2 * j] + 64 + lane; q < s_srng[2 * j + 1]; q += 32)
-                        a[i] += __ldcg(part + (size_t)q * p.kmax + j);
+                        a[i] += __ldcg(part + q);
             }
 #pragma unroll
             for (int i = 0; i < kC; ++i) {
@@ -730,7 +752,7 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
             double a = 0.0;
             for (int e = lane; e < R3; e += 32) a += yval(q, e) * v[e];
             a = bwarp_sum(a);
-            if (lane == 0) part[(size_t)s_slot[q] * p.kmax + s_cols[q]] = a;
+            if (lane == 0) part[s_slot[q]] = a;
         }
     };
     // the CTA's coupled rows of V, compact ([list position][own coupled dof], written by the Y kernel)
@@ -743,7 +765,7 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
             double a = 0.0;
             for (int il = lane; il < sl.na; il += 32) a += __ldg(vq + il) * v[s_act[il]];
             a = bwarp_sum(a);
-            if (lane == 0) part[(size_t)s_slot[q] * p.kmax + s_cols[q]] = a;
+            if (lane == 0) part[s_slot[q]] = a;
         }
     };
     // out[own coupled dof] -= (V s_t) (s_t = C vt on the CTA's columns)
@@ -1036,14 +1058,15 @@ static cudaError_t launch_y_t(const BlockPlan& p, cudaStream_t st) {
     auto fn = block_y_kernel<MT>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_y);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(block_gpart_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_y);
+    const size_t gsm = p.gpart_staged ? gpart_smem_bytes(p.kmax, p.NA, p.NCOL) : gpart_stage_offset(p.kmax);
+    e = cudaFuncSetAttribute(block_gpart_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm);
     if (e != cudaSuccess) return e;
     cudaMemsetAsync(p.Yact, 0, sizeof(double) * (size_t)p.a * p.kmax, st);
     const int batches = std::max(1, (p.NCOL + kYBatch - 1) / kYBatch);
     count_launch();
     fn<<<dim3(p.G_ctas, batches), kThreads, p.smem_y, st>>>(p);
     count_launch();
-    block_gpart_kernel<<<p.G_ctas, kThreads, p.smem_y, st>>>(p);
+    block_gpart_kernel<<<p.G_ctas, kThreads, gsm, st>>>(p);
     return cudaPeekAtLastError();
 }
 
@@ -1135,6 +1158,7 @@ size_t block_smem_bytes(int precision, BlockPlan& p, bool stage_vals, bool stage
     p.stage_yc = stage_yc ? 1 : 0;
     if (stage_yc) off += al(sizeof(float) * 3 * (size_t)p.R * p.NCOL);
     p.smem = off;
+    p.gpart_staged = gpart_smem_bytes(p.kmax, p.NA, p.NCOL) <= (size_t)block_max_smem() ? 1 : 0;
     return std::max(p.smem, p.smem_y);
 }
 

@@ -89,15 +89,16 @@ struct BlockPlan {
     int* comp_of_col;            // kmax (set after the ACA), -1 for unused columns
     int* comp_col_ptr;           // ncomp + 1
     int* comp_cols;              // kmax
+    int* col_off;                // kmax + 1: column j's contributor partials are pY[col_off[j] .. col_off[j + 1])
     // vectors (node-padded FP64)
     double* x;                   // solution (written)
     const double* rhs;           // Schur right-hand side
     double* mpub;                // m published for the neighbours' windows
     double* xpub;                // x published for the true-residual check
-    // partials
-    double* pY;                  // nslot x kmax
-    double* pV;                  // nslot x kmax
-    double* pX;                  // nslot x kmax (true-residual check)
+    // partials, packed by column (col_off), each column's in its component's slot order
+    double* pY;                  // Y^T v
+    double* pV;                  // V^T m
+    double* pX;                  // V^T x (true-residual check)
     double* pdot;                // G x 4
     // polynomial
     int nterms;
@@ -117,7 +118,7 @@ struct BlockPlan {
     int trace_iters;
     // shared-memory layout (bytes from the dynamic base, the same in every CTA)
     int R, NS, NCH, W, NA, NCOL; // maxima over CTAs: rows, slices, chunks, window nodes, coupled dofs, Y columns
-    int stage_vals, stage_yc;
+    int stage_vals, stage_yc, gpart_staged;
     int off_meta, off_nloc, off_lc, off_val, off_dinv, off_wn, off_win, off_act, off_aflag, off_dact;
     int off_cols, off_srng, off_kv, off_red, off_vec, off_yc;
     size_t smem;                 // the PCG kernel
