@@ -17,7 +17,11 @@ timed solve must pass at |b - H x| / |b| <= 1e-6.
 
 Modes: ``fp64`` (plain FP64 Neumann order 2, the bar) and ``fp32`` (FP32
 bulk SpMV/Neumann with FP64 coupled-node blocks, FP64 residual replacement
-every 50 iterations, FP64-verified result).  ``value`` is the flagship mode
+every 50 iterations, FP64-verified result); ``block64`` / ``block32`` (the
+block-local Woodbury preconditioner: a 4-term polynomial in w Dd^-1 D over each
+CTA's part of the mesh plus the exact low-rank correction Y K Y^T, pipelined
+PCG with two grid barriers per iteration; FP64 or FP32 matrix values, FP64
+vectors and arithmetic).  ``value`` is the flagship mode
 (the fastest one that met the FP64-verified residual); every mode's numbers
 are in ``modes``.  ``other_workloads`` repeats fp64/fp32 on the structured
 annulus tires (``make_vehicle_system``).  ``e2e_repattern`` is ``e2e`` with a
@@ -49,7 +53,10 @@ TARGET = 1e-6
 # order-2 solve on the default (shared-memory-resident) path: FP64 24.84 MB read + 1.11 MB written over
 # 204 iterations, FP32 32.19 MB + 0.50 MB over 245.  The learned modes run
 # the same kernel with eight Schur-basis terms and have no capture of their own.
-NCU_TRAFFIC_PER_ITER = {"fp64": (24.84e6 + 1.11e6) / 204, "fp32": (32.19e6 + 0.50e6) / 245}
+NCU_TRAFFIC_PER_ITER = {"fp64": (24.84e6 + 1.11e6) / 204, "fp32": (32.19e6 + 0.50e6) / 245,
+                        # block_pcg_kernel<float>, one solve: 20.21 MB read + 0.22 MB written over 91 iterations
+                        "block32": (20.21e6 + 0.22e6) / 91}
+BLOCK_TERMS = 4  # polynomial terms of the block modes: one operator SpMV and three local ones per iteration
 
 
 def parse():
@@ -58,7 +65,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--modes", default="fp64,fp32,learned64,learned32")
+    ap.add_argument("--modes", default="fp64,fp32,block64,block32,learned64,learned32")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -309,7 +316,10 @@ def time_modes(args, s, ds, ctx_holder, mode_opts, flush, dist, dev, lib, sample
         ok = all(t["status"] == 0 and t["full_relative_residual"] <= TARGET for t in stats_all)
         iters = last["pcg_iterations"]
         sb = 8 if mode.endswith("64") else 4
-        bytes_iter = survey_bytes_per_iteration(s, last["active_fem_dofs"], last["rank"], 2, sb)
+        # the block modes apply the FEM blocks BLOCK_TERMS times per iteration (the operator and the
+        # polynomial's local terms), counted as full SpMVs over the stored blocks
+        bytes_iter = survey_bytes_per_iteration(s, last["active_fem_dofs"], last["rank"],
+                                                BLOCK_TERMS if mode.startswith("block") else 2, sb)
         pcg_launch_ms = pcg_ms / steps
         modes[mode] = {
             "solves_per_s": replica_throughput(steps, ws, total_ms),
@@ -417,6 +427,10 @@ def run_gpu(args):
     mode_opts = {
         "fp64": HSCOptions(precision="fp64", **base),
         "fp32": HSCOptions(precision="fp32", residual_replacement=50, **base),
+        "block64": HSCOptions(block=True, poly_weights=(1.0,) * BLOCK_TERMS, omega=OMEGA, tol=1e-6,
+                              abd_inverse="exact", precision="fp64"),
+        "block32": HSCOptions(block=True, poly_weights=(1.0,) * BLOCK_TERMS, omega=OMEGA, tol=1e-6,
+                              abd_inverse="exact", precision="fp32"),
         "learned64": HSCOptions(learned=True, omega=OMEGA, tol=1e-6, abd_inverse="exact", precision="fp64"),
         "learned32": HSCOptions(learned=True, omega=OMEGA, tol=1e-6, abd_inverse="exact", precision="fp32",
                                 residual_replacement=50),
@@ -442,10 +456,13 @@ def run_gpu(args):
     l2_gbs = measure_l2_copy_gbs(dev)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": (NCU_TRAFFIC_PER_ITER[flag] * F["pcg_iterations"]) if flag in NCU_TRAFFIC_PER_ITER else None,
-                "kernel": "hsc::pcg_kernel (persistent Schur PCG), one launch per solve",
+                "kernel": ("hsc::block_pcg_kernel (persistent pipelined Schur PCG, one CTA per mesh part)"
+                           if flag.startswith("block") else "hsc::pcg_kernel (persistent Schur PCG)")
+                          + ", one launch per solve",
                 "bytes": "per iteration: r SpMVs over the stored one-triangle FEM blocks "
                          "nnzb (9 s + 4) + 4 (n + 1) + 2 N s, low-rank (2 a k + k^2) s, vector passes "
-                         "(4N + r (9n + 2N) + 6 (r - 1) N + 6N) s; times the launch's iterations",
+                         "(4N + r (9n + 2N) + 6 (r - 1) N + 6N) s; times the launch's iterations; r = 2 for the "
+                         "Neumann modes, r = 4 for the block modes (operator + three local terms)",
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s",
                 "l2": {"achieved": achieved, "peak": l2_gbs, "unit": "GB/s", "frac": achieved / l2_gbs,
                        "peak_source": "measured in this run: torch copy between two L2-resident 24 MiB buffers"},
@@ -477,7 +494,10 @@ def run_gpu(args):
     if rank == 0:
         line = {"metric": METRIC, "value": F["solves_per_s"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": F["ms_per_solve"], "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if flag == "fp64" else "f32",
+                "scaling": "weak", "vs_baseline": None,
+                # arithmetic type: the block modes compute in FP64 over FP32 or FP64 matrix planes
+                "dtype": "f64" if flag in ("fp64", "block64", "block32") else "f32",
+                "matrix_storage": "f32" if flag.endswith("32") else "f64",
                 "data": "synthetic (seeded Newton system on the vehicle scene's tire mesh; no public dataset)",
                 "config": workload_config(s), "mode": flag, "pcg_iterations": F["pcg_iterations"],
                 "full_relative_residual": F["full_relative_residual"], "error_vs_direct": F["error_vs_direct"],

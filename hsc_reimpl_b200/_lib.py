@@ -63,6 +63,7 @@ class Options(C.Structure):
         ("aca_cluster", C.c_int32),
         ("reorder", C.c_int32),
         ("aca_components", C.c_int32),
+        ("lanczos_stats", C.c_int32),
     ]
 
 
@@ -118,6 +119,7 @@ EXPORTS = {
     "hsc_get_factors": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                   C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p]),
     "hsc_get_abd_inverse": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "hsc_debug_block_plan": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
     "hsc_get_partition": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_void_p,
                                     C.c_void_p]),
     "hsc_partition_nodes": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),

@@ -1468,10 +1468,14 @@ int build_block_plan(hsc_ctx* ctx, System& S, cudaStream_t st) {
     b.out = S.scal.as<DevScal>()->pcg;
     b.cg_coef = S.cg.as<double>(); b.max_coef = kMaxCoef;
     b.R = R; b.NS = NS; b.NCH = NCH; b.W = W; b.NA = NA; b.NCOL = NCOL;
-    // stage the value planes and the Y columns when they fit, the planes first
+    // stage the value planes when they fit, then as many of a CTA's Y columns as the rest holds
     const size_t cap = (size_t)block_max_smem();
-    if (block_smem_bytes(o.precision, b, true, true) > cap && block_smem_bytes(o.precision, b, true, false) > cap)
-        block_smem_bytes(o.precision, b, false, false);
+    bool vals_in = true;
+    if (block_smem_bytes(o.precision, b, true, 0) > cap) vals_in = false;
+    int nyc = 0;
+    for (int t = NCOL; t > 0; --t)
+        if (block_smem_bytes(o.precision, b, vals_in, t) <= cap) { nyc = t; break; }
+    block_smem_bytes(o.precision, b, vals_in, nyc);
     if (std::max(b.smem, b.smem_y) > cap)
         return fail(ctx, HSC_ERR_INVALID, "a part of the block preconditioner does not fit one CTA's shared memory");
     S.blk_nact_cta = nact_cta;
@@ -1802,6 +1806,7 @@ int hsc_options_default(hsc_options* o) {
     o->aca_cluster = 1;
     o->reorder = 1;
     o->aca_components = 1;
+    o->lanczos_stats = 0;
     return HSC_OK;
 }
 
@@ -2081,7 +2086,7 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
     // Lanczos extremes of every system (host bisection, independent per system): a batch spreads
     // them over a few host threads
     std::vector<double> lz_lo(count, 0.0), lz_hi(count, 0.0);
-    {
+    if (learned || o.lanczos_stats) {
         auto lz = [&](int s0, int s1) {
             for (int s = s0; s < s1; ++s) {
                 const System& S = ctx->sys[s];
@@ -2252,6 +2257,16 @@ int hsc_get_partition(hsc_ctx* ctx, int32_t sys, int32_t* n, int32_t* nparts, in
     if (nparts) *nparts = (int)S.h_part_ptr.size() - 1;
     if (perm && S.n) std::memcpy(perm, S.h_perm.data(), sizeof(int) * S.n);
     if (part_ptr) std::memcpy(part_ptr, S.h_part_ptr.data(), sizeof(int) * S.h_part_ptr.size());
+    return HSC_OK;
+}
+
+int hsc_debug_block_plan(hsc_ctx* ctx, int64_t* out, int32_t n) {
+    if (!ctx || !out || n < 1) return HSC_ERR_INVALID;
+    if (ctx->sys.empty() || !ctx->block_layout) return HSC_ERR_NOTREADY;
+    const BlockPlan& b = ctx->sys[0].blk;
+    const int64_t v[] = {b.G_ctas, b.R, b.NS, b.NCH, b.W, b.NA, b.NCOL, b.stage_vals, b.NYC,
+                         (int64_t)b.smem, (int64_t)b.smem_y, b.ncomp, b.nslot, b.kmax};
+    for (int i = 0; i < n && i < (int)(sizeof v / sizeof v[0]); ++i) out[i] = v[i];
     return HSC_OK;
 }
 

@@ -382,6 +382,185 @@ __device__ void part_op(const Part<MT>& s, bool gv, const double* win, const dou
     }
 }
 
+// ---------------------------------------------------------------------------
+// Warp-balanced passes over a CTA's chunks (the PCG kernel).  The chunks of the
+// CTA's slices form one sequence (the polynomial takes each slice's leading
+// local chunks, the operator all of them); warp w takes the positions
+// [T w / W, T (w + 1) / W) of the T in the sequence, so no warp waits on the
+// widest slice.  A warp's run through one slice is a segment: it leaves the 16
+// rows' partial sums in shared memory, and a second pass (a thread per row) adds
+// the segments of the row's slice in sequence order, so sums are deterministic.
+// ---------------------------------------------------------------------------
+constexpr int kMaxSlices = (kBlockMaxRows + kSliceRows - 1) / kSliceRows;
+constexpr int kMaxSegs = kWarps + kMaxSlices;
+
+struct WarpPlan {
+    short fs[kWarps];            // first slice of the warp's run
+    short fc[kWarps];            // its first chunk inside that slice
+    short nc[kWarps];            // chunks in the run
+    short seg0[kWarps];          // the run's first segment
+    short sg[kMaxSlices + 1];    // segments of slice s: sg[s] .. sg[s + 1]
+};
+
+// thread 0: the plan for the slice lengths meta[s].z (local) or meta[s].y (all)
+__device__ void make_warp_plan(const int4* meta, int ns, bool all, WarpPlan& P) {
+    int tot = 0;
+    for (int s = 0; s < ns; ++s) tot += all ? meta[s].y : meta[s].z;
+    int s = 0, off = 0, seg = 0;
+    for (int sl = 0; sl <= ns; ++sl) P.sg[sl] = -1;
+    for (int w = 0; w < kWarps; ++w) {
+        const int p0 = (int)((long long)tot * w / kWarps), p1 = (int)((long long)tot * (w + 1) / kWarps);
+        while (s < ns && off + (all ? meta[s].y : meta[s].z) <= p0) { off += all ? meta[s].y : meta[s].z; ++s; }
+        P.fs[w] = (short)s;
+        P.fc[w] = (short)(p0 - off);
+        P.nc[w] = (short)(p1 - p0);
+        P.seg0[w] = (short)seg;
+        int ss = s, o = off, q = p0;
+        while (q < p1) {  // one segment per slice the run touches
+            const int len = all ? meta[ss].y : meta[ss].z;
+            if (P.sg[ss] < 0) P.sg[ss] = (short)seg;
+            ++seg;
+            q = min(p1, o + len);
+            if (q < p1) { o += len; ++ss; }
+        }
+    }
+    P.sg[ns] = (short)seg;
+    for (int sl = ns - 1; sl >= 0; --sl)
+        if (P.sg[sl] < 0) P.sg[sl] = P.sg[sl + 1];
+}
+
+// phase 1 of a balanced pass: warp `warp` walks its run and leaves, per segment g, the 16 rows'
+// sums of the slots `pick` admits times x (x_of(lane, window position) gives the 3 entries)
+template <class MT, class Pick, class XOf>
+__device__ __forceinline__ void run_segments(const Part<MT>& s, const WarpPlan& P, bool all, bool gv, double* scratch,
+                                             Pick pick, XOf x_of) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, h = lane & 1;
+    int sl = P.fs[warp], c = P.fc[warp], left = P.nc[warp], g = P.seg0[warp];
+    while (left > 0) {
+        const int4 m = s.meta[sl];
+        const int len = all ? m.y : m.z;
+        const int cend = min(len, c + left);
+        const int lr = kSliceRows * sl + (lane >> 1);
+        const bool ok = lr < s.R;
+        const int nl = ok ? (int)s.nloc[lr] : 0;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+#pragma unroll 2
+        for (int cc = c; cc < cend; ++cc) {
+            const int j = 2 * cc + h;
+            const bool use = pick(j, nl);
+            const int ch = m.x + cc;
+            const int w = s.lc[ch * 32 + lane];
+            MT b[9];
+            ld_blk<MT>(s.val + (size_t)ch * kChunkVals, lane, gv, b);
+            double x0, x1, x2;
+            x_of(use, w, x0, x1, x2);
+            a0 += (double)b[0] * x0 + (double)b[1] * x1 + (double)b[2] * x2;
+            a1 += (double)b[3] * x0 + (double)b[4] * x1 + (double)b[5] * x2;
+            a2 += (double)b[6] * x0 + (double)b[7] * x1 + (double)b[8] * x2;
+        }
+        a0 += __shfl_xor_sync(0xffffffffu, a0, 1);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, 1);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, 1);
+        if (h == 0) {
+            double* o = scratch + ((size_t)g * kSliceRows + (lane >> 1)) * 3;
+            o[0] = a0; o[1] = a1; o[2] = a2;
+        }
+        left -= cend - c;
+        c = 0;
+        ++sl;
+        ++g;
+    }
+}
+
+// the sum of row lr's segments
+__device__ __forceinline__ void seg_sum(const WarpPlan& P, const double* scratch, int lr, double& y0, double& y1,
+                                        double& y2) {
+    const int sl = lr / kSliceRows, r = lr - sl * kSliceRows;
+    y0 = y1 = y2 = 0.0;
+    for (int g = P.sg[sl]; g < P.sg[sl + 1]; ++g) {
+        const double* o = scratch + ((size_t)g * kSliceRows + r) * 3;
+        y0 += o[0]; y1 += o[1]; y2 += o[2];
+    }
+}
+
+// z = L v over the CTA's rows, warp-balanced (the polynomial of part_poly for one vector; v, z,
+// t, u: 3 per row).  Ends synchronised.
+template <class MT>
+__device__ void part_poly_bal(const BlockPlan& p, const Part<MT>& s, const WarpPlan& P, double* scratch,
+                              const double* v, double* z, double* t, double* u) {
+    using DT = typename BlkDinv<MT>::T;
+    const bool gv = !p.stage_vals;
+    const double om = p.omega, om1 = 1.0 - p.omega;
+    const double w0 = poly_weight(p, 0);
+    for (int lr = threadIdx.x; lr < s.R; lr += blockDim.x) {
+        double o0, o1, o2;
+        blk_dinv<DT>(s.dinv, s.R, lr, om, v[3 * lr], v[3 * lr + 1], v[3 * lr + 2], o0, o1, o2);
+        t[3 * lr] = o0; t[3 * lr + 1] = o1; t[3 * lr + 2] = o2;
+        z[3 * lr] = w0 * o0; z[3 * lr + 1] = w0 * o1; z[3 * lr + 2] = w0 * o2;
+    }
+    __syncthreads();
+    double* tc = t;
+    double* tn = u;
+    for (int k = 1; k < p.nterms; ++k) {
+        const double wk = poly_weight(p, k);
+        const double* xs = tc;
+        run_segments<MT>(
+            s, P, false, gv, scratch, [](int j, int nl) { return j >= 1 && j < nl; },  // slot 0: the diagonal
+            [&](bool use, int w, double& x0, double& x1, double& x2) {
+                const int ol = use ? w - s.wown : 0;
+                x0 = use ? xs[3 * ol] : 0.0; x1 = use ? xs[3 * ol + 1] : 0.0; x2 = use ? xs[3 * ol + 2] : 0.0;
+            });
+        __syncthreads();
+        for (int lr = threadIdx.x; lr < s.R; lr += blockDim.x) {
+            double y0, y1, y2, e0, e1, e2;
+            seg_sum(P, scratch, lr, y0, y1, y2);
+            const double c0 = tc[3 * lr], c1 = tc[3 * lr + 1], c2 = tc[3 * lr + 2];
+            double f = om1;
+            const int an = s.dact ? s.aflag[lr] : -1;
+            if (an >= 0) {
+                const double* d = s.dact + 9 * an;
+                y0 += d[0] * c0 + d[1] * c1 + d[2] * c2;
+                y1 += d[3] * c0 + d[4] * c1 + d[5] * c2;
+                y2 += d[6] * c0 + d[7] * c1 + d[8] * c2;
+                f = 1.0;
+            }
+            blk_dinv<DT>(s.dinv, s.R, lr, om, y0, y1, y2, e0, e1, e2);
+            const double n0 = f * c0 - e0, n1 = f * c1 - e1, n2 = f * c2 - e2;
+            tn[3 * lr] = n0; tn[3 * lr + 1] = n1; tn[3 * lr + 2] = n2;
+            z[3 * lr] += wk * n0; z[3 * lr + 1] += wk * n1; z[3 * lr + 2] += wk * n2;
+        }
+        __syncthreads();
+        double* tmp = tc; tc = tn; tn = tmp;
+    }
+}
+
+// out = D m over the CTA's rows, warp-balanced (part_op's product); m from the staged window.
+// Ends synchronised.
+template <class MT>
+__device__ void part_op_bal(const Part<MT>& s, const WarpPlan& P, double* scratch, bool gv, const double* win,
+                            const double* own, double* out) {
+    run_segments<MT>(
+        s, P, true, gv, scratch, [](int, int) { return true; },
+        [&](bool, int w, double& x0, double& x1, double& x2) { x0 = win[3 * w]; x1 = win[3 * w + 1]; x2 = win[3 * w + 2]; });
+    __syncthreads();
+    for (int lr = threadIdx.x; lr < s.R; lr += blockDim.x) {
+        double a0, a1, a2;
+        seg_sum(P, scratch, lr, a0, a1, a2);
+        if (s.dact) {
+            const int an = s.aflag[lr];
+            if (an >= 0) {
+                const double* d = s.dact + 9 * an;
+                const double x0 = own[3 * lr], x1 = own[3 * lr + 1], x2 = own[3 * lr + 2];
+                a0 += d[0] * x0 + d[1] * x1 + d[2] * x2;
+                a1 += d[3] * x0 + d[4] * x1 + d[5] * x2;
+                a2 += d[6] * x0 + d[7] * x1 + d[8] * x2;
+            }
+        }
+        out[3 * lr] = a0; out[3 * lr + 1] = a1; out[3 * lr + 2] = a2;
+    }
+    __syncthreads();
+}
+
 constexpr int kYBatch = 4;  // columns per pass of the Y kernel
 
 // the V^T Y partial kernel's shared memory: the column list and slots, then V's and Y's rows
@@ -592,6 +771,10 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
     double* s_red = reinterpret_cast<double*>(sm + p.off_red);// kWarps x 4 scratch
     __shared__ double s_dot[4];
     __shared__ int s_ok;
+    __shared__ WarpPlan s_plan_loc, s_plan_all;                 // warp runs of the polynomial and the operator
+    double* scr = reinterpret_cast<double*>(sm + p.off_scr);   // segment partial sums
+    if (threadIdx.x == 0) make_warp_plan(sl.meta, sl.ns, false, s_plan_loc);
+    if (threadIdx.x == 32) make_warp_plan(sl.meta, sl.ns, true, s_plan_all);
     for (int e = threadIdx.x; e < sl.na; e += blockDim.x) s_act[e] = p.actp[sl.ab + e] - 3 * sl.rb;
     const int ncols = build_cols(p, cta, s_cols, s_slot);  // synchronises: s_act is complete
     const int k = *p.rank;
@@ -606,10 +789,10 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
         s_srng[2 * j + 1] = g >= 0 ? p.col_off[j + 1] : p.col_off[j];
     }
     int epoch = 0;
-    const bool yc_on = p.stage_yc && ncols <= p.NCOL;
-    if (yc_on) {
+    const int nyc = min(ncols, p.NYC);  // the CTA's first nyc Y columns are staged, the rest read from L2
+    if (nyc > 0) {
         float* yc = reinterpret_cast<float*>(sm + p.off_yc);
-        for (int e = threadIdx.x; e < ncols * R; e += blockDim.x) {
+        for (int e = threadIdx.x; e < nyc * R; e += blockDim.x) {
             const int q = e / R, lr = e - q * R;
             const float4 y = reinterpret_cast<const float4*>(p.Y + (size_t)s_cols[q] * 4 * p.n)[sl.rb + lr];
             float* o = yc + (size_t)q * ld + 3 * lr;
@@ -741,9 +924,9 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
         }
     };
     // the CTA's Y columns at its own dofs: shared memory (FP32) when staged
-    const float* Yc = yc_on ? reinterpret_cast<const float*>(sm + p.off_yc) : nullptr;
+    const float* Yc = reinterpret_cast<const float*>(sm + p.off_yc);
     auto yval = [&](int q, int e) -> double {
-        if (Yc) return (double)Yc[(size_t)q * ld + e];
+        if (q < nyc) return (double)Yc[(size_t)q * ld + e];
         return (double)__ldg(p.Y + (size_t)s_cols[q] * 4 * p.n + 4 * (size_t)(sl.rb + e / 3) + e % 3);
     };
     // partials of Y^T v over the own dofs -> part[slot][j] for the CTA's columns
@@ -762,26 +945,31 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
         if (sl.na == 0) return;
         for (int q = warp; q < ncols; q += kWarps) {
             const double* vq = Vc + (size_t)q * sl.na;
-            double a = 0.0;
-            for (int il = lane; il < sl.na; il += 32) a += __ldg(vq + il) * v[s_act[il]];
-            a = bwarp_sum(a);
+            double a = 0.0, b = 0.0;
+            int il = lane;
+            for (; il + 32 < sl.na; il += 64) {
+                a += __ldg(vq + il) * v[s_act[il]];
+                b += __ldg(vq + il + 32) * v[s_act[il + 32]];
+            }
+            if (il < sl.na) a += __ldg(vq + il) * v[s_act[il]];
+            a = bwarp_sum(a + b);
             if (lane == 0) part[s_slot[q]] = a;
         }
     };
     // out[own coupled dof] -= (V s_t) (s_t = C vt on the CTA's columns)
     auto lowrank_sub = [&](double* out) {
         for (int il = threadIdx.x; il < sl.na; il += blockDim.x) {
-            double a = 0.0;
+            double a = 0.0, b = 0.0;
             int q = 0;
             for (; q + 8 <= ncols; q += 8) {
                 double vv[8];
 #pragma unroll
                 for (int u = 0; u < 8; ++u) vv[u] = __ldg(Vc + (size_t)(q + u) * sl.na + il);
 #pragma unroll
-                for (int u = 0; u < 8; ++u) a += vv[u] * s_t[q + u];
+                for (int u = 0; u < 8; u += 2) { a += vv[u] * s_t[q + u]; b += vv[u + 1] * s_t[q + u + 1]; }
             }
             for (; q < ncols; ++q) a += __ldg(Vc + (size_t)q * sl.na + il) * s_t[q];
-            out[s_act[il]] -= a;
+            out[s_act[il]] -= a + b;
         }
     };
     // stage the window of a published vector (own rows from shared memory)
@@ -828,7 +1016,7 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
     auto schur_apply = [&](const double* pub, const double* vown, const double* part) {
         stage_and_sum(pub, vown, part);
         __syncthreads();
-        part_op<MT>(sl, gv, win, vown, Nn);
+        part_op_bal<MT>(sl, s_plan_all, scr, gv, win, vown, Nn);
         rows_times(cr, p.C, s_vt, s_t);
         __syncthreads();
         lowrank_sub(Nn);
@@ -875,7 +1063,7 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
             cta_partials(g, d, rr, 0.0, 0, 3);
         }
         mark(1);
-        part_poly<MT, 1>(p, sl, Wb, Pz, Pt, Pu, ld);
+        part_poly_bal<MT>(p, sl, s_plan_loc, scr, Wb, Pz, Pt, Pu);
         mark(2);
         if (!barrier()) return;
         mark(3);
@@ -891,8 +1079,16 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
             const int e = threadIdx.x + kThreads * i;
             if (e < R3) {
                 const int lr = e / 3, d = e - 3 * lr;
-                double m = Pz[e];
-                for (int q = 0; q < ncols; ++q) m += yval(q, e) * s_c[q];
+                double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;  // four chains over the columns
+                int q = 0;
+                for (; q + 4 <= ncols; q += 4) {
+                    m0 += yval(q, e) * s_c[q];
+                    m1 += yval(q + 1, e) * s_c[q + 1];
+                    m2 += yval(q + 2, e) * s_c[q + 2];
+                    m3 += yval(q + 3, e) * s_c[q + 3];
+                }
+                for (; q < ncols; ++q) m0 += yval(q, e) * s_c[q];
+                const double m = Pz[e] + ((m0 + m1) + (m2 + m3));
                 Mm[e] = m;
                 p.mpub[4 * (size_t)(sl.rb + lr) + d] = m;
             }
@@ -939,7 +1135,7 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
             stage_and_sum(p.mpub, Mm, p.pV);
             __syncthreads();
             mark(9);
-            part_op<MT>(sl, gv, win, Mm, Nn);
+            part_op_bal<MT>(sl, s_plan_all, scr, gv, win, Mm, Nn);
             rows_times(cr, p.C, s_vt, s_t);
             __syncthreads();
             mark(10);
@@ -1131,7 +1327,7 @@ int block_max_smem() { return 227 * 1024 - 8 * 1024; }
 // blocks, column lists and slot ranges, k-vectors, reduction scratch, the value chunks), then the
 // vectors: the Y kernel's batch region, or the PCG's six FP64 vectors (3 per row) followed by
 // the CTA's Y columns (FP32)
-size_t block_smem_bytes(int precision, BlockPlan& p, bool stage_vals, bool stage_yc) {
+size_t block_smem_bytes(int precision, BlockPlan& p, bool stage_vals, int nyc) {
     const size_t mt = precision == 0 ? 8 : 4, dt = mt;
     auto al = [](size_t b) { return (b + 15) / 16 * 16; };
     size_t off = 0;
@@ -1154,9 +1350,11 @@ size_t block_smem_bytes(int precision, BlockPlan& p, bool stage_vals, bool stage
     p.off_vec = (int)off;
     p.smem_y = off + al(sizeof(double) * y_region_doubles(p.R));
     off += al(sizeof(double) * 6 * 3 * (size_t)p.R);
+    p.off_scr = (int)off;
+    off += al(sizeof(double) * 3 * kSliceRows * (size_t)(kWarps + p.NS));
     p.off_yc = (int)off;
-    p.stage_yc = stage_yc ? 1 : 0;
-    if (stage_yc) off += al(sizeof(float) * 3 * (size_t)p.R * p.NCOL);
+    p.NYC = nyc;
+    off += al(sizeof(float) * 3 * (size_t)p.R * nyc);
     p.smem = off;
     p.gpart_staged = gpart_smem_bytes(p.kmax, p.NA, p.NCOL) <= (size_t)block_max_smem() ? 1 : 0;
     return std::max(p.smem, p.smem_y);

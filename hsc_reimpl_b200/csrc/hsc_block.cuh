@@ -118,9 +118,9 @@ struct BlockPlan {
     int trace_iters;
     // shared-memory layout (bytes from the dynamic base, the same in every CTA)
     int R, NS, NCH, W, NA, NCOL; // maxima over CTAs: rows, slices, chunks, window nodes, coupled dofs, Y columns
-    int stage_vals, stage_yc, gpart_staged;
+    int stage_vals, NYC, gpart_staged;  // value chunks staged; Y columns staged per CTA (its first NYC)
     int off_meta, off_nloc, off_lc, off_val, off_dinv, off_wn, off_win, off_act, off_aflag, off_dact;
-    int off_cols, off_srng, off_kv, off_red, off_vec, off_yc;
+    int off_cols, off_srng, off_kv, off_red, off_vec, off_scr, off_yc;
     size_t smem;                 // the PCG kernel
     size_t smem_y;               // the Y kernel
 };
@@ -140,7 +140,7 @@ void launch_block_k(const BlockPlan& p, int nact_cta, cudaStream_t st);
 // the persistent pipelined PCG (cooperative launch, one CTA per part)
 cudaError_t launch_block_pcg(int precision, const BlockPlan& p, cudaStream_t st);
 // shared-memory layouts of the two block kernels for the maxima in p; returns the larger
-size_t block_smem_bytes(int precision, BlockPlan& p, bool stage_vals, bool stage_yc);
+size_t block_smem_bytes(int precision, BlockPlan& p, bool stage_vals, int nyc);
 int block_max_smem();
 
 }  // namespace hsc

@@ -312,44 +312,57 @@ __global__ void __launch_bounds__(256) aca_kernel(AcaParams p) {
 // ---------------------------------------------------------------------------
 // small dense FP64 algebra
 // ---------------------------------------------------------------------------
-// C = alpha * op(A) * op(B) + beta * C, row-major; op = transpose when t* != 0.
-// M, N, K may be device scalars (dims given as pointers override when non-null).
-__global__ void __launch_bounds__(256) gemm_kernel(GemmArgs g) {
-    __shared__ double As[32][33];
-    __shared__ double Bs[32][33];
+// C = alpha op(A) op(B) + beta C (row-major; op = transpose when t* != 0) in FP64 on the tensor cores (mma.sync m8n8k4, .f64: d = a b + c
+// per 8 x 8 x 4 step).  A CTA of four warps takes a 32 x 32 tile of C, the K loop in steps of 32
+// through shared memory; warp w owns rows 8 w .. 8 w + 7 of the tile as four 8 x 8 accumulator
+// tiles that share its A fragment.  Fragments (PTX m8n8k4 .f64): lane l holds A(l / 4, l % 4),
+// B(l % 4, l / 4) and C(l / 4, 2 (l % 4) + i), i < 2.  The sizes may come from the device (rank).
+__global__ void __launch_bounds__(128) gemm_kernel(GemmArgs g) {
+    __shared__ double As[32][33];   // [row][k]
+    __shared__ double Bs[32][33];   // [k][col]
     const int M = g.dM ? *g.dM : g.M, N = g.dN ? *g.dN : g.N, K = g.dK ? *g.dK : g.K;
     const int bm = blockIdx.y * 32, bn = blockIdx.x * 32;
     if (bm >= M || bn >= N) return;
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 8 rows of 32
-    double acc[4] = {0, 0, 0, 0};
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int gr = lane >> 2, gc = lane & 3;
+    double acc[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
     for (int k0 = 0; k0 < K; k0 += 32) {
-        for (int rr = ty; rr < 32; rr += 8) {
-            const int row = bm + rr, kk = k0 + tx;
+        for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
+            const int rr = e >> 5, cc = e & 31;
+            const int row = bm + rr, kk = k0 + cc;
             double va = 0.0;
             if (row < M && kk < K) va = g.tA ? g.A[(size_t)kk * g.lda + row] : g.A[(size_t)row * g.lda + kk];
-            As[rr][tx] = va;
-            const int kr = k0 + rr, col = bn + tx;
+            As[rr][cc] = va;
+            const int kr = k0 + rr, col = bn + cc;
             double vb = 0.0;
             if (kr < K && col < N) vb = g.tB ? g.B[(size_t)col * g.ldb + kr] : g.B[(size_t)kr * g.ldb + col];
-            Bs[rr][tx] = vb;
+            Bs[rr][cc] = vb;
         }
         __syncthreads();
-#pragma unroll 8
-        for (int kk = 0; kk < 32; ++kk) {
-            const double b = Bs[kk][tx];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) acc[q] += As[ty + 8 * q][kk] * b;
+        for (int k4 = 0; k4 < 8; ++k4) {
+            const double av = As[8 * warp + gr][4 * k4 + gc];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const double bv = Bs[4 * k4 + gc][8 * t + gr];
+                asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                             : "+d"(acc[t][0]), "+d"(acc[t][1])
+                             : "d"(av), "d"(bv));
+            }
         }
         __syncthreads();
     }
-    for (int q = 0; q < 4; ++q) {
-        const int row = bm + ty + 8 * q, col = bn + tx;
-        if (row < M && col < N) {
-            double* c = g.C + (size_t)row * g.ldc + col;
-            const double prev = g.beta == 0.0 ? 0.0 : g.beta * *c;
-            *c = g.alpha * acc[q] + prev;
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int row = bm + 8 * warp + gr, col = bn + 8 * t + 2 * gc + i;
+            if (row < M && col < N) {
+                double* c = g.C + (size_t)row * g.ldc + col;
+                const double prev = g.beta == 0.0 ? 0.0 : g.beta * *c;
+                *c = g.alpha * acc[t][i] + prev;
+            }
         }
-    }
 }
 
 // Cholesky A = L L^T (lower, row-major) in one CTA; L overwrites Lout.
@@ -931,7 +944,8 @@ __global__ void rhs_lowrank_kernel(const double* V, int a, const int* dk, const 
     if (i >= a) return;
     const int k = *dk;
     double s = 0.0;
-    for (int j = 0; j < k; ++j) s += V[(size_t)j * a + i] * c[j];
+#pragma unroll 8
+    for (int j = 0; j < k; ++j) s += V[(size_t)j * a + i] * c[j];  // loads of eight columns in flight
     const int dof = act[i];
     rhs[4 * (size_t)(dof / 3) + dof % 3] -= s;
 }
@@ -942,6 +956,7 @@ __global__ void vt_x_kernel(const double* V, int a, const int* dk, const int* ac
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (gw >= k) return;
     double s = 0.0;
+#pragma unroll 4
     for (int i = lane; i < a; i += 32) {
         const int dof = act[i];
         s += V[(size_t)gw * a + i] * x[4 * (size_t)(dof / 3) + dof % 3];
@@ -1063,7 +1078,7 @@ __global__ void et_xq_kernel(const double* E, int qm, int a, const int* act, con
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= a) return;
     double s = 0.0;
-#pragma unroll 8
+#pragma unroll 16
     for (int r = 0; r < qm; ++r) s += E[(size_t)r * a + c] * xq[r];
     const int dof = act[c];
     ypad[4 * (size_t)(dof / 3) + dof % 3] += s;
@@ -1137,11 +1152,13 @@ __global__ void residual_partial_kernel(const double* bf, const double* yf, cons
     }
 }
 
+// one warp: lane l sums partials l, l + 32, ... in order, then a fixed butterfly (deterministic)
 __global__ void residual_final_kernel(const double* part, int np, double* out) {
-    if (threadIdx.x != 0) return;
+    const int lane = threadIdx.x;
     double s0 = 0, s1 = 0, s2 = 0;
-    for (int i = 0; i < np; ++i) { s0 += part[3 * i]; s1 += part[3 * i + 1]; s2 += part[3 * i + 2]; }
-    out[0] = s0; out[1] = s1; out[2] = s2;
+    for (int i = lane; i < np; i += 32) { s0 += part[3 * i]; s1 += part[3 * i + 1]; s2 += part[3 * i + 2]; }
+    s0 = wsum(s0); s1 = wsum(s1); s2 = wsum(s2);
+    if (lane == 0) { out[0] = s0; out[1] = s1; out[2] = s2; }
 }
 
 // y (contiguous N) from node-padded y_f and yq
@@ -1289,7 +1306,7 @@ int aca_blocks_per_sm() {
 void launch_gemm(const GemmArgs& g, int M, int N, cudaStream_t st) {
     if (M <= 0 || N <= 0) return;
     dim3 grid((N + 31) / 32, (M + 31) / 32);
-    HSC_COUNTED(gemm_kernel<<<grid, 256, 0, st>>>(g));
+    HSC_COUNTED(gemm_kernel<<<grid, 128, 0, st>>>(g));
 }
 
 void launch_cholesky(const double* A, int m, double* L, int* bad, cudaStream_t st) {
@@ -1364,7 +1381,7 @@ void launch_wt_vec(const double* W, int qm, int kmax, const int* dk, const doubl
 
 void launch_rhs_lowrank(const double* V, int a, const int* dk, const double* c, const int* act, double* rhs,
                         cudaStream_t st) {
-    if (a) HSC_COUNTED(rhs_lowrank_kernel<<<blocks(a), 256, 0, st>>>(V, a, dk, c, act, rhs));
+    if (a) HSC_COUNTED(rhs_lowrank_kernel<<<blocks(a, 64), 64, 0, st>>>(V, a, dk, c, act, rhs));
 }
 
 void launch_vt_x(const double* V, int a, int kmax, const int* dk, const int* act, const double* x, double* t,
@@ -1392,7 +1409,7 @@ void launch_full_spmv(const FullSpmv& f, cudaStream_t st) {
     else
         HSC_COUNTED(bsr_spmv64_kernel<<<blocks((long long)f.n * 4), 256, 0, st>>>(f.rowptr, f.colidx, f.v64, f.nnz, f.n,
                                                                                f.xpad, f.ypad));
-    if (f.qm && f.a) HSC_COUNTED(et_xq_kernel<<<blocks(f.a), 256, 0, st>>>(f.E, f.qm, f.a, f.act, f.xq, f.ypad));
+    if (f.qm && f.a) HSC_COUNTED(et_xq_kernel<<<blocks(f.a, 64), 64, 0, st>>>(f.E, f.qm, f.a, f.act, f.xq, f.ypad));
     if (f.qm && f.rowpart) {
         const int nchunk = abd_row_chunks(f.a);
         HSC_COUNTED(abd_rows_part_kernel<<<dim3(nchunk, (f.qm + 7) / 8), 256, 0, st>>>(f.A, f.E, f.qm, f.a, f.act, f.xq,

@@ -67,6 +67,7 @@ class HSCOptions:
     aca_cluster: bool = True               # cluster ACA when the coupling fits; False: the grid kernel
     reorder: bool = True                   # internal FEM node renumbering into compact CTA parts
     aca_components: bool = True            # ACA per coupling component, merged (same factors as global)
+    lanczos_stats: bool = False            # Ritz extremes of every solve (always on for the learned forms)
 
     @classmethod
     def reference(cls):
@@ -125,6 +126,7 @@ class HSCOptions:
         o.aca_cluster = int(bool(self.aca_cluster))
         o.reorder = int(bool(self.reorder))
         o.aca_components = int(bool(self.aca_components))
+        o.lanczos_stats = int(bool(self.lanczos_stats))
         return o
 
 
@@ -261,6 +263,14 @@ class HSCContext:
         ptr = np.zeros(P.value + 1, dtype=np.int32)
         self._check(self.lib.hsc_get_partition(self._ptr, sys_index, None, None, perm.ctypes.data, ptr.ctypes.data))
         return perm[:n.value], ptr
+
+    def block_plan(self):
+        """The block preconditioner's plan of the last block solve (hsc_debug_block_plan)."""
+        keys = ("ctas", "R", "NS", "NCH", "W", "NA", "NCOL", "stage_vals", "NYC", "smem", "smem_y", "ncomp",
+                "nslot", "kmax")
+        out = np.zeros(len(keys), dtype=np.int64)
+        self._check(self.lib.hsc_debug_block_plan(self._ptr, out.ctypes.data, len(keys)))
+        return dict(zip(keys, (int(v) for v in out)))
 
     def factors_full(self, qm, sys_index=0):
         k, a, act = self.factors(sys_index)

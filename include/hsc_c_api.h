@@ -139,6 +139,10 @@ typedef struct hsc_options {
                                     shared FEM nodes, on which E is block diagonal), one CTA each, and merge
                                     the pivot sequences by magnitude: the same pivots, columns and column
                                     order as the global full-pivot ACA; 0: the global cluster / grid ACA */
+    int32_t lanczos_stats;       /* 1: after each solve, the extreme Ritz values of the preconditioned Schur
+                                    operator from the CG coefficients (host bisection) into the stats and the
+                                    next solve's feature record; 0 (default): only for the learned
+                                    preconditioners, which read that record */
 } hsc_options;
 
 typedef struct hsc_stats {        /* superset of the hsc_stats.jsonl record (linear_hsc.cu:420-431) */
@@ -357,6 +361,12 @@ HSC_EXPORT int hsc_debug_barrier_selftest(int32_t ctas, int32_t absent, int64_t 
  * kernel's own block-Jacobi product.  Test hook. */
 HSC_EXPORT int hsc_debug_dmv_accumulate(int32_t bs, int32_t nblocks, const double* d_planes, const double* d_x,
                                         double* d_z, double omega, void* stream);
+
+/* The block preconditioner's plan after a solve with it (first n of: CTAs, and the per-CTA maxima
+ * R (rows), NS (16-row slices), NCH (chunks), W (window nodes), NA (coupled dofs), NCOL (Y columns);
+ * value chunks staged (0/1), Y columns staged per CTA, the two kernels' shared-memory bytes,
+ * coupling components, contributor slots, rank cap).  Test and profiling hook. */
+HSC_EXPORT int hsc_debug_block_plan(hsc_ctx* ctx, int64_t* out, int32_t n);
 
 #ifdef __cplusplus
 }

@@ -137,3 +137,17 @@ def test_block_rejects_batches(api, torch, cube_system):
     ds = api.DeviceSystem.from_system(cube_system)
     with pytest.raises(api.HSCError):
         ctx.solve_batch([ds, ds])
+
+
+def test_block_plan_on_tire_mesh(api, torch, tire):
+    """The FP32 plan keeps every CTA's value chunks and Y columns in shared memory on the vehicle:
+    one CTA per SM-sized part (at most 341 rows), within the 227 KB a CTA may hold."""
+    ctx = api.HSCContext(_block_opts(api, precision="fp32"))
+    _, st = ctx.solve(api.DeviceSystem.from_system(tire))
+    assert st["status"] == 0
+    plan = ctx.block_plan()
+    assert plan["ctas"] == len(ctx.partition()[1]) - 1
+    assert plan["R"] <= 341 and plan["NS"] == (plan["R"] + 15) // 16
+    assert plan["stage_vals"] == 1
+    assert 1 <= plan["NYC"] <= plan["NCOL"]
+    assert max(plan["smem"], plan["smem_y"]) <= 227 * 1024

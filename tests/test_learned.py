@@ -273,7 +273,7 @@ def test_schur_polynomial_vehicle_fewer_iterations(api, torch, vehicle_system):
 def test_device_features_match_oracle(api, torch):
     s, ds = _cube(api)
     opts = dict(omega=2 / 3, aca_rtol=1e-4, abd_inverse="exact")
-    ctx = api.HSCContext(api.HSCOptions(**opts))
+    ctx = api.HSCContext(api.HSCOptions(lanczos_stats=True, **opts))
     _, st = ctx.solve(ds)
     f1 = ctx.features()
     orc = O.HSCOracle(s.H, s.layout, order=2, **opts)
