@@ -1331,7 +1331,7 @@ int build_block_plan(hsc_ctx* ctx, System& S, cudaStream_t st) {
             int ch_rel = 0;
             for (int r0 = rb; r0 < re; r0 += kSliceRows) {
                 const int r1 = std::min(re, r0 + kSliceRows);
-                int width = 0, lwidth = 0;
+                int width = 0, lwidth = 0, lmin = 1 << 30;
                 for (int r = r0; r < r1; ++r) {
                     std::vector<int>& sl = rowslots[r - r0];
                     sl.clear();
@@ -1352,9 +1352,11 @@ int build_block_plan(hsc_ctx* ctx, System& S, cudaStream_t st) {
                     }
                     width = std::max(width, (int)sl.size());
                     lwidth = std::max(lwidth, (int)nloc[r]);
+                    lmin = std::min(lmin, (int)nloc[r]);
                 }
                 const int nch = (width + 1) / 2;
-                sslice.push_back(make_int4(ch_rel, nch, (lwidth + 1) / 2, 0));
+                // chunks holding a local slot of some row: [0, (lwidth + 1) / 2); a remote one: [lmin / 2, nch)
+                sslice.push_back(make_int4(ch_rel, nch, (lwidth + 1) / 2, lmin / 2));
                 const size_t base = ssrc.size();
                 ssrc.resize(base + (size_t)32 * nch, -1);
                 slc.resize(base + (size_t)32 * nch, (unsigned short)win_own[c]);

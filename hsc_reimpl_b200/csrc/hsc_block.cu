@@ -402,22 +402,27 @@ struct WarpPlan {
     short sg[kMaxSlices + 1];    // segments of slice s: sg[s] .. sg[s + 1]
 };
 
-// thread 0: the plan for the slice lengths meta[s].z (local) or meta[s].y (all)
-__device__ void make_warp_plan(const int4* meta, int ns, bool all, WarpPlan& P) {
+// a slice's chunk range in a pass: local slots [0, z), remote slots [w, y)
+enum { kRunLocal = 0, kRunRemote = 1 };
+__device__ __forceinline__ int run_base(const int4& m, int mode) { return mode == kRunRemote ? m.w : 0; }
+__device__ __forceinline__ int run_len(const int4& m, int mode) { return mode == kRunRemote ? m.y - m.w : m.z; }
+
+// thread 0: the plan of a pass over the slices' ranges (mode kRunLocal or kRunRemote)
+__device__ void make_warp_plan(const int4* meta, int ns, int mode, WarpPlan& P) {
     int tot = 0;
-    for (int s = 0; s < ns; ++s) tot += all ? meta[s].y : meta[s].z;
+    for (int s = 0; s < ns; ++s) tot += run_len(meta[s], mode);
     int s = 0, off = 0, seg = 0;
     for (int sl = 0; sl <= ns; ++sl) P.sg[sl] = -1;
     for (int w = 0; w < kWarps; ++w) {
         const int p0 = (int)((long long)tot * w / kWarps), p1 = (int)((long long)tot * (w + 1) / kWarps);
-        while (s < ns && off + (all ? meta[s].y : meta[s].z) <= p0) { off += all ? meta[s].y : meta[s].z; ++s; }
+        while (s < ns && off + run_len(meta[s], mode) <= p0) { off += run_len(meta[s], mode); ++s; }
         P.fs[w] = (short)s;
         P.fc[w] = (short)(p0 - off);
         P.nc[w] = (short)(p1 - p0);
         P.seg0[w] = (short)seg;
         int ss = s, o = off, q = p0;
         while (q < p1) {  // one segment per slice the run touches
-            const int len = all ? meta[ss].y : meta[ss].z;
+            const int len = run_len(meta[ss], mode);
             if (P.sg[ss] < 0) P.sg[ss] = (short)seg;
             ++seg;
             q = min(p1, o + len);
@@ -432,13 +437,15 @@ __device__ void make_warp_plan(const int4* meta, int ns, bool all, WarpPlan& P) 
 // phase 1 of a balanced pass: warp `warp` walks its run and leaves, per segment g, the 16 rows'
 // sums of the slots `pick` admits times x (x_of(lane, window position) gives the 3 entries)
 template <class MT, class Pick, class XOf>
-__device__ __forceinline__ void run_segments(const Part<MT>& s, const WarpPlan& P, bool all, bool gv, double* scratch,
+__device__ __forceinline__ void run_segments(const Part<MT>& s, const WarpPlan& P, int mode, bool gv, double* scratch,
                                              Pick pick, XOf x_of) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, h = lane & 1;
     int sl = P.fs[warp], c = P.fc[warp], left = P.nc[warp], g = P.seg0[warp];
     while (left > 0) {
-        const int4 m = s.meta[sl];
-        const int len = all ? m.y : m.z;
+        const int4 m0 = s.meta[sl];
+        const int base = run_base(m0, mode);
+        const int4 m = make_int4(m0.x + base, 0, 0, 0);   // chunk cc of the run is chunk base + cc of the slice
+        const int len = run_len(m0, mode);
         const int cend = min(len, c + left);
         const int lr = kSliceRows * sl + (lane >> 1);
         const bool ok = lr < s.R;
@@ -446,7 +453,7 @@ __device__ __forceinline__ void run_segments(const Part<MT>& s, const WarpPlan& 
         double a0 = 0.0, a1 = 0.0, a2 = 0.0;
 #pragma unroll 2
         for (int cc = c; cc < cend; ++cc) {
-            const int j = 2 * cc + h;
+            const int j = 2 * (base + cc) + h;
             const bool use = pick(j, nl);
             const int ch = m.x + cc;
             const int w = s.lc[ch * 32 + lane];
@@ -505,7 +512,7 @@ __device__ void part_poly_bal(const BlockPlan& p, const Part<MT>& s, const WarpP
         const double wk = poly_weight(p, k);
         const double* xs = tc;
         run_segments<MT>(
-            s, P, false, gv, scratch, [](int j, int nl) { return j >= 1 && j < nl; },  // slot 0: the diagonal
+            s, P, kRunLocal, gv, scratch, [](int j, int nl) { return j >= 1 && j < nl; },  // slot 0: the diagonal
             [&](bool use, int w, double& x0, double& x1, double& x2) {
                 const int ol = use ? w - s.wown : 0;
                 x0 = use ? xs[3 * ol] : 0.0; x1 = use ? xs[3 * ol + 1] : 0.0; x2 = use ? xs[3 * ol + 2] : 0.0;
@@ -534,14 +541,18 @@ __device__ void part_poly_bal(const BlockPlan& p, const Part<MT>& s, const WarpP
     }
 }
 
-// out = D m over the CTA's rows, warp-balanced (part_op's product); m from the staged window.
-// Ends synchronised.
+// out = (D m) restricted to the blocks whose column is a row of the part (the diagonal included),
+// warp-balanced, m from the part's own rows; the coupled rows' FP64 diagonal blocks in the mixed
+// modes.  Needs no other CTA's data.  Ends synchronised.
 template <class MT>
-__device__ void part_op_bal(const Part<MT>& s, const WarpPlan& P, double* scratch, bool gv, const double* win,
-                            const double* own, double* out) {
+__device__ void part_op_local(const Part<MT>& s, const WarpPlan& P, double* scratch, bool gv, const double* own,
+                              double* out) {
     run_segments<MT>(
-        s, P, true, gv, scratch, [](int, int) { return true; },
-        [&](bool, int w, double& x0, double& x1, double& x2) { x0 = win[3 * w]; x1 = win[3 * w + 1]; x2 = win[3 * w + 2]; });
+        s, P, kRunLocal, gv, scratch, [](int j, int nl) { return j < nl; },
+        [&](bool use, int w, double& x0, double& x1, double& x2) {
+            const int ol = use ? w - s.wown : 0;
+            x0 = use ? own[3 * ol] : 0.0; x1 = use ? own[3 * ol + 1] : 0.0; x2 = use ? own[3 * ol + 2] : 0.0;
+        });
     __syncthreads();
     for (int lr = threadIdx.x; lr < s.R; lr += blockDim.x) {
         double a0, a1, a2;
@@ -557,6 +568,25 @@ __device__ void part_op_bal(const Part<MT>& s, const WarpPlan& P, double* scratc
             }
         }
         out[3 * lr] = a0; out[3 * lr + 1] = a1; out[3 * lr + 2] = a2;
+    }
+    __syncthreads();
+}
+
+// out += the remaining blocks of D m (columns outside the part), warp-balanced, m from the staged
+// window (3 doubles per window node).  Ends synchronised.
+template <class MT>
+__device__ void part_op_remote(const Part<MT>& s, const WarpPlan& P, double* scratch, bool gv, const double* win,
+                               double* out) {
+    run_segments<MT>(
+        s, P, kRunRemote, gv, scratch, [](int j, int nl) { return j >= nl; },
+        [&](bool use, int w, double& x0, double& x1, double& x2) {
+            x0 = use ? win[3 * w] : 0.0; x1 = use ? win[3 * w + 1] : 0.0; x2 = use ? win[3 * w + 2] : 0.0;
+        });
+    __syncthreads();
+    for (int lr = threadIdx.x; lr < s.R; lr += blockDim.x) {
+        double a0, a1, a2;
+        seg_sum(P, scratch, lr, a0, a1, a2);
+        out[3 * lr] += a0; out[3 * lr + 1] += a1; out[3 * lr + 2] += a2;
     }
     __syncthreads();
 }
@@ -752,14 +782,19 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
     const Part<MT> sl = stage_part<MT>(p, cta, sm, true);
     const bool gv = !p.stage_vals;
     const int R = sl.R, R3 = 3 * R, ld = 3 * p.R;
-    AT* Pz = reinterpret_cast<AT*>(sm + p.off_vec);  // L v, then the polynomial's scratch
-    AT* Pt = Pz + ld;
-    AT* Pu = Pt + ld;
-    double* vec = Pu + ld;
-    double* Wb = vec;            // w (r on a (re)start): the preconditioner's input
-    double* Mm = vec + ld;       // m (x during a true-residual check)
-    double* Nn = vec + 2 * ld;   // n = S m
+    double* vec = reinterpret_cast<double*>(sm + p.off_vec);
+    AT* Pz = vec;                // L v
+    double* Wb = vec + ld;       // w (r on a (re)start): the preconditioner's input
+    double* Mm = vec + 2 * ld;   // m (x during a true-residual check)
+    double* Nn = vec + 3 * ld;   // n = S m
+    double* Zv = vec + 4 * ld;   // the recurrences' z, q, s, p
+    double* Qv = vec + 5 * ld;
+    double* Sv = vec + 6 * ld;
+    double* Pv = vec + 7 * ld;
     double* win = reinterpret_cast<double*>(sm + p.off_win);   // 3 per window node
+    // the polynomial's two scratch vectors: the window and n, neither live while it runs
+    AT* Pt = win;
+    AT* Pu = Nn;
     int* s_act = reinterpret_cast<int*>(sm + p.off_act);       // own coupled dofs, local (3 lr + d)
     int* s_cols = reinterpret_cast<int*>(sm + p.off_cols);
     int* s_slot = s_cols + p.kmax;
@@ -771,10 +806,10 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
     double* s_red = reinterpret_cast<double*>(sm + p.off_red);// kWarps x 4 scratch
     __shared__ double s_dot[4];
     __shared__ int s_ok;
-    __shared__ WarpPlan s_plan_loc, s_plan_all;                 // warp runs of the polynomial and the operator
+    __shared__ WarpPlan s_plan_loc, s_plan_rem;  // warp runs over the local slots (polynomial, operator) and the rest
     double* scr = reinterpret_cast<double*>(sm + p.off_scr);   // segment partial sums
-    if (threadIdx.x == 0) make_warp_plan(sl.meta, sl.ns, false, s_plan_loc);
-    if (threadIdx.x == 32) make_warp_plan(sl.meta, sl.ns, true, s_plan_all);
+    if (threadIdx.x == 0) make_warp_plan(sl.meta, sl.ns, kRunLocal, s_plan_loc);
+    if (threadIdx.x == 32) make_warp_plan(sl.meta, sl.ns, kRunRemote, s_plan_rem);
     for (int e = threadIdx.x; e < sl.na; e += blockDim.x) s_act[e] = p.actp[sl.ab + e] - 3 * sl.rb;
     const int ncols = build_cols(p, cta, s_cols, s_slot);  // synchronises: s_act is complete
     const int k = *p.rank;
@@ -813,6 +848,18 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
         }
     __syncthreads();
 
+    // split-phase grid barrier: arrive once the CTA's partials are in global memory, do local work,
+    // then wait (every CTA arrives at every barrier before it waits at it)
+    auto arrive = [&]() {
+        __syncthreads();
+        if (threadIdx.x == 0) red_release_add_u32(&p.bar->count, 1u);
+    };
+    auto wait = [&]() -> bool {
+        if (threadIdx.x == 0) s_ok = grid_wait(p.bar, G, p.spin_limit, epoch);
+        ++epoch;
+        __syncthreads();
+        return s_ok != 0;
+    };
     // grid barrier: the CTA's partials are already in global memory
     auto barrier = [&]() -> bool {
         __syncthreads();
@@ -945,14 +992,22 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
         if (sl.na == 0) return;
         for (int q = warp; q < ncols; q += kWarps) {
             const double* vq = Vc + (size_t)q * sl.na;
-            double a = 0.0, b = 0.0;
-            int il = lane;
-            for (; il + 32 < sl.na; il += 64) {
-                a += __ldg(vq + il) * v[s_act[il]];
-                b += __ldg(vq + il + 32) * v[s_act[il + 32]];
+            // the column's first 256 coupled dofs: every load in flight before the first add
+            constexpr int kPre = 8;
+            double vv[kPre];
+#pragma unroll
+            for (int u = 0; u < kPre; ++u) {
+                const int il = lane + 32 * u;
+                vv[u] = il < sl.na ? __ldg(vq + il) : 0.0;
             }
-            if (il < sl.na) a += __ldg(vq + il) * v[s_act[il]];
-            a = bwarp_sum(a + b);
+            double a = 0.0;
+#pragma unroll
+            for (int u = 0; u < kPre; ++u) {
+                const int il = lane + 32 * u;
+                if (il < sl.na) a += vv[u] * v[s_act[il]];
+            }
+            for (int il = lane + 32 * kPre; il < sl.na; il += 32) a += __ldg(vq + il) * v[s_act[il]];
+            a = bwarp_sum(a);
             if (lane == 0) part[s_slot[q]] = a;
         }
     };
@@ -972,25 +1027,19 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
             out[s_act[il]] -= a + b;
         }
     };
-    // stage the window of a published vector (own rows from shared memory)
-    // stage the window of a published vector (own rows from shared memory) and sum the V^T v
-    // partials into s_vt: the window loads (two per thread in registers) are issued first, so
-    // they are in flight while the column sums wait on theirs
-    auto stage_and_sum = [&](const double* pub, const double* own, const double* part) {
+    // stage the halo of a published vector (the window's nodes outside the part; the remote pass
+    // reads no others) and sum the V^T v partials into s_vt: the window loads (two per thread in
+    // registers) are issued first, so they are in flight while the column sums wait on theirs
+    auto stage_and_sum = [&](const double* pub, const double* part) {
         double wv[2][3];
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
             const int e = threadIdx.x + kThreads * i;
             wv[i][0] = wv[i][1] = wv[i][2] = 0.0;
-            if (e < sl.nwin) {
-                const int node = sl.wn[e];
-                if (node >= sl.rb && node < sl.re) {
-                    const double* o = own + 3 * (node - sl.rb);
-                    wv[i][0] = o[0]; wv[i][1] = o[1]; wv[i][2] = o[2];
-                } else {
-                    const double2 lo = __ldcg(reinterpret_cast<const double2*>(pub) + 2 * (size_t)node);
-                    wv[i][0] = lo.x; wv[i][1] = lo.y; wv[i][2] = __ldcg(pub + 4 * (size_t)node + 2);
-                }
+            const int node = e < sl.nwin ? sl.wn[e] : sl.rb;
+            if (node < sl.rb || node >= sl.re) {
+                const double2 lo = __ldcg(reinterpret_cast<const double2*>(pub) + 2 * (size_t)node);
+                wv[i][0] = lo.x; wv[i][1] = lo.y; wv[i][2] = __ldcg(pub + 4 * (size_t)node + 2);
             }
         }
         sum_cols(part, s_vt, false);
@@ -1001,22 +1050,18 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
         }
         for (int e = threadIdx.x + 2 * kThreads; e < sl.nwin; e += blockDim.x) {
             const int node = sl.wn[e];
-            double a0, a1, a2;
-            if (node >= sl.rb && node < sl.re) {
-                const double* o = own + 3 * (node - sl.rb);
-                a0 = o[0]; a1 = o[1]; a2 = o[2];
-            } else {
-                const double2 lo = __ldcg(reinterpret_cast<const double2*>(pub) + 2 * (size_t)node);
-                a0 = lo.x; a1 = lo.y; a2 = __ldcg(pub + 4 * (size_t)node + 2);
-            }
-            win[3 * e] = a0; win[3 * e + 1] = a1; win[3 * e + 2] = a2;
+            if (node >= sl.rb && node < sl.re) continue;
+            const double2 lo = __ldcg(reinterpret_cast<const double2*>(pub) + 2 * (size_t)node);
+            win[3 * e] = lo.x; win[3 * e + 1] = lo.y; win[3 * e + 2] = __ldcg(pub + 4 * (size_t)node + 2);
         }
     };
-    // n = S v over the own rows: D v (window staged) - V (C vt), vt = V^T v summed from `part`
+    // n = S v over the own rows: D v (the local blocks, then the halo's) - V (C vt), vt = V^T v
+    // summed from `part`
     auto schur_apply = [&](const double* pub, const double* vown, const double* part) {
-        stage_and_sum(pub, vown, part);
+        part_op_local<MT>(sl, s_plan_loc, scr, gv, vown, Nn);
+        stage_and_sum(pub, part);
         __syncthreads();
-        part_op_bal<MT>(sl, s_plan_all, scr, gv, win, vown, Nn);
+        part_op_remote<MT>(sl, s_plan_rem, scr, gv, win, Nn);
         rows_times(cr, p.C, s_vt, s_t);
         __syncthreads();
         lowrank_sub(Nn);
@@ -1024,22 +1069,24 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
     };
 
     // ---- prologue: x = 0, r = rhs, the first pass preconditions r ----
-    double xr[kDofs], rr_[kDofs], ur[kDofs], pr[kDofs], sr[kDofs], qr[kDofs], zr[kDofs];
+    double xr[kDofs], rr_[kDofs], ur[kDofs];
 #pragma unroll
     for (int i = 0; i < kDofs; ++i) {
         const int e = threadIdx.x + kThreads * i;
-        xr[i] = pr[i] = sr[i] = qr[i] = zr[i] = ur[i] = rr_[i] = 0.0;
+        xr[i] = ur[i] = rr_[i] = 0.0;
         if (e < R3) {
             rr_[i] = p.rhs[4 * (size_t)(sl.rb + e / 3) + e % 3];
             Wb[e] = rr_[i];
+            Zv[e] = Qv[e] = Sv[e] = Pv[e] = 0.0;
         }
     }
     __syncthreads();
 
     int pass = kPassStart, it = 0, status = -1, restarts = 0, npass = 0;
-    // phase clocks (trace mode): 0 pass top, 1 Y^T v and dot partials written, 2 polynomial done,
-    // 3 after barrier A, 4 sums read, 5 K s done, 6 m formed, 7 V^T m partials / decisions, 8 after
-    // barrier B, 9 window staged and V^T m summed, 10 D m and C vt done, 11 low-rank done, 12 updates done
+    // phase clocks (trace mode): 0 pass top, 1 Y^T v and dot partials written (arrive A), 2 polynomial
+    // done, 3 after wait A, 4 sums read, 5 K s done, 6 m formed, 7 V^T m partials / decisions (arrive
+    // B), 8 local operator blocks and early recurrences done, 9 after wait B, 10 halo staged and V^T m
+    // summed, 11 halo blocks and C vt done, 12 low-rank done, 13 updates done
     auto mark = [&](int ev) {
         if (p.trace && threadIdx.x == 0 && npass < p.trace_iters)
             p.trace[((size_t)cta * p.trace_iters + npass) * 16 + ev] = (unsigned long long)clock64();
@@ -1047,7 +1094,7 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
     double normb = -1.0, rel = 1.0, alpha = 0.0, beta = 0.0, alpha_prev = 0.0, gamma_prev = 0.0;
     bool fresh = true;  // next normal pass is the first after a (re)start: beta = 0
     for (;;) {
-        // ---------------- phase 1 ----------------
+        // ---------------- phase 1: partials, arrive A, the polynomial, wait A ----------------
         mark(0);
         y_partials(Wb, p.pY);
         {
@@ -1063,9 +1110,10 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
             cta_partials(g, d, rr, 0.0, 0, 3);
         }
         mark(1);
+        arrive();
         part_poly_bal<MT>(p, sl, s_plan_loc, scr, Wb, Pz, Pt, Pu);
         mark(2);
-        if (!barrier()) return;
+        if (!wait()) return;
         mark(3);
         // ---------------- phase 2 ----------------
         sum_cols(p.pY, s_sv, true);
@@ -1081,13 +1129,24 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
                 const int lr = e / 3, d = e - 3 * lr;
                 double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;  // four chains over the columns
                 int q = 0;
-                for (; q + 4 <= ncols; q += 4) {
-                    m0 += yval(q, e) * s_c[q];
-                    m1 += yval(q + 1, e) * s_c[q + 1];
-                    m2 += yval(q + 2, e) * s_c[q + 2];
-                    m3 += yval(q + 3, e) * s_c[q + 3];
+                if (ncols <= nyc) {  // every column staged: plain shared-memory loads
+                    const float* yc = Yc + e;
+                    for (; q + 4 <= ncols; q += 4) {
+                        m0 += (double)yc[(size_t)q * ld] * s_c[q];
+                        m1 += (double)yc[(size_t)(q + 1) * ld] * s_c[q + 1];
+                        m2 += (double)yc[(size_t)(q + 2) * ld] * s_c[q + 2];
+                        m3 += (double)yc[(size_t)(q + 3) * ld] * s_c[q + 3];
+                    }
+                    for (; q < ncols; ++q) m0 += (double)yc[(size_t)q * ld] * s_c[q];
+                } else {
+                    for (; q + 4 <= ncols; q += 4) {
+                        m0 += yval(q, e) * s_c[q];
+                        m1 += yval(q + 1, e) * s_c[q + 1];
+                        m2 += yval(q + 2, e) * s_c[q + 2];
+                        m3 += yval(q + 3, e) * s_c[q + 3];
+                    }
+                    for (; q < ncols; ++q) m0 += yval(q, e) * s_c[q];
                 }
-                for (; q < ncols; ++q) m0 += yval(q, e) * s_c[q];
                 const double m = Pz[e] + ((m0 + m1) + (m2 + m3));
                 Mm[e] = m;
                 p.mpub[4 * (size_t)(sl.rb + lr) + d] = m;
@@ -1128,49 +1187,65 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
         }
         if (status >= 0) break;
         mark(7);
-        if (!barrier()) return;
-        mark(8);
-        // ---------------- phase 3 ----------------
+        // ---------------- arrive B, local work, wait B, phase 3 ----------------
+        arrive();
         if (!check) {
-            stage_and_sum(p.mpub, Mm, p.pV);
-            __syncthreads();
-            mark(9);
-            part_op_bal<MT>(sl, s_plan_all, scr, gv, win, Mm, Nn);
-            rows_times(cr, p.C, s_vt, s_t);
+            // n's blocks inside the part, and the recurrences that do not need n:
+            // q = m + b q, s = w + b s, p = u + b p, x += a p, r -= a s, u -= a q (a start takes u = m)
+            part_op_local<MT>(sl, s_plan_loc, scr, gv, Mm, Nn);
+#pragma unroll
+            for (int i = 0; i < kDofs; ++i) {
+                const int e = threadIdx.x + kThreads * i;
+                if (e < R3) {
+                    if (pass == kPassStart) {
+                        ur[i] = Mm[e];
+                    } else {
+                        const double q = Mm[e] + beta * Qv[e], sv = Wb[e] + beta * Sv[e], pv = ur[i] + beta * Pv[e];
+                        Qv[e] = q; Sv[e] = sv; Pv[e] = pv;
+                        xr[i] += alpha * pv;
+                        rr_[i] -= alpha * sv;
+                        ur[i] -= alpha * q;
+                    }
+                }
+            }
+        }
+        mark(8);
+        if (!wait()) return;
+        mark(9);
+        if (!check) {
+            stage_and_sum(p.mpub, p.pV);
             __syncthreads();
             mark(10);
-            lowrank_sub(Nn);
+            part_op_remote<MT>(sl, s_plan_rem, scr, gv, win, Nn);
+            rows_times(cr, p.C, s_vt, s_t);
             __syncthreads();
             mark(11);
-            if (pass == kPassStart) {
+            lowrank_sub(Nn);
+            __syncthreads();
+            mark(12);
+            // the rest: z = n + b z, w -= a z (a start takes w = n)
 #pragma unroll
-                for (int i = 0; i < kDofs; ++i) {
-                    const int e = threadIdx.x + kThreads * i;
-                    if (e < R3) { ur[i] = Mm[e]; Wb[e] = Nn[e]; }
+            for (int i = 0; i < kDofs; ++i) {
+                const int e = threadIdx.x + kThreads * i;
+                if (e < R3) {
+                    if (pass == kPassStart) {
+                        Wb[e] = Nn[e];
+                    } else {
+                        const double z = Nn[e] + beta * Zv[e];
+                        Zv[e] = z;
+                        Wb[e] -= alpha * z;
+                    }
                 }
+            }
+            if (pass == kPassStart) {
                 pass = kPassNormal;
                 fresh = true;
             } else {
-#pragma unroll
-                for (int i = 0; i < kDofs; ++i) {
-                    const int e = threadIdx.x + kThreads * i;
-                    if (e < R3) {
-                        const double w = Wb[e];
-                        zr[i] = Nn[e] + beta * zr[i];
-                        qr[i] = Mm[e] + beta * qr[i];
-                        sr[i] = w + beta * sr[i];
-                        pr[i] = ur[i] + beta * pr[i];
-                        xr[i] += alpha * pr[i];
-                        rr_[i] -= alpha * sr[i];
-                        ur[i] -= alpha * qr[i];
-                        Wb[e] = w - alpha * zr[i];
-                    }
-                }
                 ++it;
                 fresh = false;
             }
             __syncthreads();
-            mark(12);
+            mark(13);
             ++npass;
             continue;
         }
@@ -1325,7 +1400,7 @@ int block_max_smem() { return 227 * 1024 - 8 * 1024; }
 // shared-memory layouts for the maxima in p (R, NS, NCH, W, NA, NCOL, kmax): a common prefix
 // (slices, local slot counts, window positions, Dd^-1, window, coupled dofs and their diagonal
 // blocks, column lists and slot ranges, k-vectors, reduction scratch, the value chunks), then the
-// vectors: the Y kernel's batch region, or the PCG's six FP64 vectors (3 per row) followed by
+// vectors: the Y kernel's batch region, or the PCG's eight FP64 vectors (3 per row) followed by
 // the CTA's Y columns (FP32)
 size_t block_smem_bytes(int precision, BlockPlan& p, bool stage_vals, int nyc) {
     const size_t mt = precision == 0 ? 8 : 4, dt = mt;
@@ -1349,7 +1424,7 @@ size_t block_smem_bytes(int precision, BlockPlan& p, bool stage_vals, int nyc) {
     if (stage_vals) off += al(mt * kChunkVals * (size_t)p.NCH);
     p.off_vec = (int)off;
     p.smem_y = off + al(sizeof(double) * y_region_doubles(p.R));
-    off += al(sizeof(double) * 6 * 3 * (size_t)p.R);
+    off += al(sizeof(double) * 8 * 3 * (size_t)p.R);
     p.off_scr = (int)off;
     off += al(sizeof(double) * 3 * kSliceRows * (size_t)(kWarps + p.NS));
     p.off_yc = (int)off;

@@ -70,7 +70,7 @@ struct BlockPlan {
     // sliced ELL of the CTAs' rows: slices of 16 rows, two slots of each row per 32-lane chunk
     // (lane 2 r + h holds slot 2 c + h of row r in chunk c); a row's slots are its diagonal block,
     // then the blocks whose column is a row of the same part, then the rest, then zero padding
-    const int4* sell_slice;      // per slice: first chunk, chunks, chunks holding local blocks, 0
+    const int4* sell_slice;      // per slice: first chunk, chunks, chunks holding local slots, first chunk holding a remote one
     const int* cta_slice;        // G + 1: each CTA's slices
     const int* cta_chunk;        // G + 1: each CTA's chunks
     const unsigned short* sell_nloc;  // per row: its diagonal block + local blocks (leading slots)

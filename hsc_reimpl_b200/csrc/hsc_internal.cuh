@@ -57,6 +57,26 @@ __device__ __forceinline__ void red_release_add_u32(unsigned int* p, unsigned in
 // costs no extra round trip for the abort check.  (The counter is reset before
 // each launch and stays below 2^31: epochs x CTAs per launch.)
 constexpr unsigned int kBarAbortBit = 0x80000000u;
+// The wait half alone serves a split-phase barrier: the CTA arrived earlier
+// (red_release_add_u32 on gb->count after a CTA-wide barrier) and did local
+// work in between.
+__device__ __forceinline__ bool grid_wait(GridBar* gb, unsigned int nblocks, long long limit, int epoch) {
+    const unsigned int target = (unsigned int)(epoch + 1) * nblocks;
+    long long n = 0;
+    unsigned int c;
+    while ((c = ld_acquire_u32(&gb->count)) < target) {
+        ++n;
+        if (n > 256) __nanosleep(20);
+        if (n > limit) {
+            atomicExch(&gb->abort, 1);
+            atomicExch(&gb->where, epoch);
+            atomicOr(&gb->count, kBarAbortBit);
+            return false;
+        }
+    }
+    return (c & kBarAbortBit) == 0;
+}
+
 __device__ __forceinline__ bool grid_arrive_wait(GridBar* gb, unsigned int nblocks, long long limit, int epoch) {
     const unsigned int target = (unsigned int)(epoch + 1) * nblocks;
     red_release_add_u32(&gb->count, 1u);
