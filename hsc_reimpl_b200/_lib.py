@@ -84,6 +84,7 @@ class Stats(C.Structure):
         ("lanczos_min", C.c_double), ("lanczos_max", C.c_double),
         ("stage_ms", C.c_double * 8),
         ("nnzb", C.c_int64),
+        ("analysis_ms", C.c_double),
     ]
 
     def as_dict(self):

@@ -19,6 +19,7 @@
 #include <cstring>
 #include <string>
 #include <functional>
+#include <chrono>
 #include <thread>
 #include <unordered_set>
 #include <vector>
@@ -162,6 +163,14 @@ struct hsc_ctx {
     cudaEvent_t ev_blk = nullptr;  // end of the block preconditioner's setup (Y, K) inside the PCG stage
     cudaStream_t side = nullptr;   // the ABD inverses run here, beside the ACA
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    double analysis_ms = 0.0;      // host time of the current call's pattern analysis
+    // after a pattern change behind the same pointers, the next solves hash the pattern before they
+    // start (one small kernel and a sync) instead of finding out after a full solve
+    int pattern_volatile = 0;
+    // node partition cache: the last partition and the hash of the adjacency, weights and part count
+    // it was made for (a contact change leaves the FEM mesh's pattern, hence its partition, as it was)
+    unsigned long long part_hash = 0;
+    std::vector<int> part_cache;
     bool stage_events = false;  // record the per-stage events (single system, no graph)
     // graph cache (batch)
     cudaGraphExec_t gexec = nullptr;
@@ -290,7 +299,20 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
         if (nparts > 1) {
             std::vector<double> wgt(S.n);
             for (int i = 0; i < S.n; ++i) wgt[i] = 1.0 + cnt[i];
-            part = partition_nodes(S.n, aptr, adj, wgt, nparts);
+            // FNV-1a over (n, parts, adjacency, weights): a repeated mesh pattern reuses its partition
+            unsigned long long h = 1469598103934665603ull;
+            auto mix = [&](unsigned long long v) { h = (h ^ v) * 1099511628211ull; };
+            mix((unsigned long long)S.n); mix((unsigned long long)nparts);
+            for (int i = 0; i <= S.n; ++i) mix((unsigned long long)aptr[i]);
+            for (int v : adj) mix((unsigned long long)v);
+            for (int i = 0; i < S.n; ++i) mix((unsigned long long)cnt[i]);
+            if (ctx->part_hash == h && (int)ctx->part_cache.size() == S.n) {
+                part = ctx->part_cache;
+            } else {
+                part = partition_nodes(S.n, aptr, adj, wgt, nparts);
+                ctx->part_hash = h;
+                ctx->part_cache = part;
+            }
         } else {
             part.assign(S.n, 0);
         }
@@ -1886,6 +1908,24 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
     bool any_new = false;
     if ((int)ctx->sys.size() < count) ctx->sys.resize(count);  // moves only; before any analysis of this call
     std::vector<int> idx(count);
+    if (depth == 0) ctx->analysis_ms = 0.0;
+    const auto t_an = std::chrono::steady_clock::now();
+    if (depth == 0 && ctx->pattern_volatile > 0) {
+        bool changed = false;
+        for (int s = 0; s < count && s < (int)ctx->sys.size(); ++s) {
+            System& S = ctx->sys[s];
+            if (!same_key(S, A[s], lay[s], o)) continue;  // analysed again below anyway
+            unsigned long long h = 0;
+            launch_pattern_hash(A[s].d_rows, A[s].d_cols, A[s].nnzb, &S.scal.as<DevScal>()->hash, st);
+            CK(cudaMemcpyAsync(&h, &S.scal.as<DevScal>()->hash, sizeof(h), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (h != S.hash) { S.analyzed = false; changed = true; }
+        }
+        ctx->pattern_volatile = changed ? 16 : ctx->pattern_volatile - 1;
+    }
+    auto add_analysis_time = [&](std::chrono::steady_clock::time_point t0) {
+        ctx->analysis_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    };
     for (int s = 0; s < count; ++s) {
         bool re = false;
         rc = prepare_system(ctx, s, A[s], lay[s], st, re);
@@ -1905,6 +1945,9 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
             rc = build_block_plan(ctx, ctx->sys[0], st);
             if (rc) return rc;
         }
+        add_analysis_time(t_an);
+    } else if (any_new) {
+        add_analysis_time(t_an);
     }
     const bool refine = o.refine_target > 0 && count == 1;
     const bool residual = o.check_residual || refine;
@@ -1993,6 +2036,7 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
     if (stale) {
         if (depth > 0) return fail(ctx, HSC_ERR_INVALID, "sparsity pattern changed during the solve");
         for (int s = 0; s < count; ++s) ctx->sys[s].analyzed = false;
+        ctx->pattern_volatile = 16;
         return solve_impl(ctx, count, A, lay, d_b, d_x, use_graph, st, out, depth + 1);
     }
     float ms_setup = 0, ms_pcg = 0, ms_total = 0;
@@ -2117,6 +2161,7 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
             out[s].setup_ms = ms_setup;
             out[s].pcg_ms = ms_pcg;
             out[s].total_ms = ms_total;
+            out[s].analysis_ms = ctx->analysis_ms;
             for (int i = 0; i < 8; ++i) out[s].stage_ms[i] = ms_stage[i];
             out[s].accepted = st_s == HSC_OK;
             out[s].fallback = 0;

@@ -163,6 +163,8 @@ typedef struct hsc_stats {        /* superset of the hsc_stats.jsonl record (lin
                                          concurrently), reduced core, rhs, PCG, back-sub+residual, block
                                          preconditioner setup (Y = L V, K; the PCG stage excludes it) */
     int64_t nnzb;
+    double analysis_ms;               /* host time of this call's pattern analysis (CSR plans, node partition,
+                                         CTA windows, block plan), 0 when the pattern was already analysed */
 } hsc_stats;
 
 typedef struct hsc_bcoo3 {        /* CBCOOMatrixView<double,3> */
