@@ -18,10 +18,11 @@ timed solve must pass at |b - H x| / |b| <= 1e-6.
 Modes: ``fp64`` (plain FP64 Neumann order 2, the bar) and ``fp32`` (FP32
 bulk SpMV/Neumann with FP64 coupled-node blocks, FP64 residual replacement
 every 50 iterations, FP64-verified result); ``block64`` / ``block32`` (the
-block-local Woodbury preconditioner: a 4-term polynomial in w Dd^-1 D over each
-CTA's part of the mesh plus the exact low-rank correction Y K Y^T, pipelined
-PCG with two grid barriers per iteration; FP64 or FP32 matrix values, FP64
-vectors and arithmetic).  ``value`` is the flagship mode
+block-local Woodbury preconditioner: a polynomial in w Dd^-1 D over each CTA's
+part of the mesh plus the exact low-rank correction Y K Y^T, pipelined PCG with
+two split-phase grid barriers per iteration; FP64 or FP32 matrix values, FP64
+vectors and arithmetic; the polynomial is chosen per system by
+``autotune.tune_block`` before any timing, ``block_tuning`` lists the candidates).  ``value`` is the flagship mode
 (the fastest one that met the FP64-verified residual); every mode's numbers
 are in ``modes``.  ``other_workloads`` repeats fp64/fp32 on the structured
 annulus tires (``make_vehicle_system``).  ``e2e_repattern`` is ``e2e`` with a
@@ -56,7 +57,7 @@ TARGET = 1e-6
 NCU_TRAFFIC_PER_ITER = {"fp64": (24.84e6 + 1.11e6) / 204, "fp32": (32.19e6 + 0.50e6) / 245,
                         # block_pcg_kernel<float>, one solve: 20.21 MB read + 0.22 MB written over 91 iterations
                         "block32": (20.21e6 + 0.22e6) / 91}
-BLOCK_TERMS = 4  # polynomial terms of the block modes: one operator SpMV and three local ones per iteration
+BLOCK_TERMS = 4  # the block modes' default polynomial (Neumann, 4 terms) before the per-system tuning
 
 
 def parse():
@@ -319,7 +320,7 @@ def time_modes(args, s, ds, ctx_holder, mode_opts, flush, dist, dev, lib, sample
         # the block modes apply the FEM blocks BLOCK_TERMS times per iteration (the operator and the
         # polynomial's local terms), counted as full SpMVs over the stored blocks
         bytes_iter = survey_bytes_per_iteration(s, last["active_fem_dofs"], last["rank"],
-                                                BLOCK_TERMS if mode.startswith("block") else 2, sb)
+                                                len(opt.poly_weights) if mode.startswith("block") else 2, sb)
         pcg_launch_ms = pcg_ms / steps
         modes[mode] = {
             "solves_per_s": replica_throughput(steps, ws, total_ms),
@@ -435,6 +436,19 @@ def run_gpu(args):
         "learned32": HSCOptions(learned=True, omega=OMEGA, tol=1e-6, abd_inverse="exact", precision="fp32",
                                 residual_replacement=50),
     }
+    # the block modes' polynomial: tuned once on this system, outside every timed region (a Newton
+    # loop tunes once per system family and reuses the choice)
+    tuning = None
+    if any(m.startswith("block") for m in args.modes.split(",")):
+        from dataclasses import replace
+        from hsc_reimpl_b200.autotune import tune_block
+        best, table = tune_block(ds, base=mode_opts["block32"], reps=3)
+        if best is not None:
+            mode_opts["block32"] = best
+            mode_opts["block64"] = replace(best, precision="fp64")
+            chosen = min((r for r in table if r["ok"]), key=lambda r: r["ms"])
+            tuning = {"chosen": chosen["name"], "weights": chosen["weights"], "omega": chosen["omega"],
+                      "candidates": [{k: r[k] for k in ("name", "ms", "iterations", "ok")} for r in table]}
     from hsc_reimpl_b200 import learned as L
     model = L.load_model()[0] if L.MODEL_PATH.exists() else None
     want = {m: o for m, o in mode_opts.items() if m in args.modes.split(",") and (model is not None or "learned" not in m)}
@@ -462,7 +476,8 @@ def run_gpu(args):
                 "bytes": "per iteration: r SpMVs over the stored one-triangle FEM blocks "
                          "nnzb (9 s + 4) + 4 (n + 1) + 2 N s, low-rank (2 a k + k^2) s, vector passes "
                          "(4N + r (9n + 2N) + 6 (r - 1) N + 6N) s; times the launch's iterations; r = 2 for the "
-                         "Neumann modes, r = 4 for the block modes (operator + three local terms)",
+                         "Neumann modes, r = the polynomial's terms for the block modes (the operator and terms - 1 "
+                         "local products)",
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s",
                 "l2": {"achieved": achieved, "peak": l2_gbs, "unit": "GB/s", "frac": achieved / l2_gbs,
                        "peak_source": "measured in this run: torch copy between two L2-resident 24 MiB buffers"},
@@ -502,7 +517,7 @@ def run_gpu(args):
                 "config": workload_config(s), "mode": flag, "pcg_iterations": F["pcg_iterations"],
                 "full_relative_residual": F["full_relative_residual"], "error_vs_direct": F["error_vs_direct"],
                 "modes": modes, "clocks": clocks, "e2e": e2e, "e2e_repattern": e2e_rep, "gpu_launches": launches,
-                "roofline": roofline, "cpu_baseline": cpu, "other_workloads": other}
+                "roofline": roofline, "cpu_baseline": cpu, "other_workloads": other, "block_tuning": tuning}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -71,3 +71,84 @@ def autotune(systems, base: HSCOptions | None = None, tiles=TILES, ranks=RANKS, 
             best = (opt, ms)
         ctx.close()
     return (best[0] if best else None), table
+
+
+# ---------------------------------------------------------------------------
+# Per-system polynomial of the block preconditioner (HSC_PRECOND_BLOCK)
+# ---------------------------------------------------------------------------
+def chebyshev_weights(n, a, b, omega):
+    """Weights w_0..w_{n-1} of the block polynomial L = sum_k w_k (I - omega B)^k omega Dd^-1,
+    B = Dd^-1 D_loc, whose residual polynomial 1 - lambda p(lambda) is the degree-n Chebyshev
+    polynomial of [a, b] normalised to 1 at lambda = 0: r(lambda) = T_n((b + a - 2 lambda) / (b - a))
+    / T_n((b + a) / (b - a)).  With mu = 1 - omega lambda, sum_k w_k mu^k = (1 - R(mu)) / (1 - mu) for
+    R(mu) = r((1 - mu) / omega), a polynomial of degree n - 1 since R(1) = r(0) = 1.  All-ones weights
+    are the Neumann series, R(mu) = mu^n."""
+    from numpy.polynomial import chebyshev as Ch, polynomial as Po
+    tn = Ch.cheb2poly([0] * n + [1])
+    beta = 2.0 / (omega * (b - a))
+    alpha = (b + a - 2.0 / omega) / (b - a)
+    R, xp = np.zeros(1), np.array([1.0])
+    for c in tn:                      # T_n(alpha + beta mu) in powers of mu
+        R = Po.polyadd(R, c * xp)
+        xp = Po.polymul(xp, [alpha, beta])
+    R = R / Ch.chebval((b + a) / (b - a), [0] * n + [1])
+    q, rem = Po.polydiv(Po.polysub([1.0], R), [1.0, -1.0])
+    if np.max(np.abs(rem)) > 1e-8 * max(1.0, float(np.max(np.abs(R)))):
+        raise ValueError("residual polynomial is not 1 at the origin")
+    q = np.concatenate([q, np.zeros(max(0, n - len(q)))])[:n]
+    return [float(v) for v in q]
+
+
+def block_candidates(lam_max=3.9):
+    """(name, weights, omega) of the polynomials the block tuner times: Neumann series of degree 3-8
+    (odd degrees also at a larger omega: their residual polynomial (1 - omega lambda)^n stays below 1
+    for any omega lambda > 0, so the preconditioner stays SPD) and Chebyshev weights of degree 5-6
+    on [a, lam_max]."""
+    out = [(f"neumann{n} omega=0.5", [1.0] * n, 0.5) for n in (3, 4, 5, 6, 8)]
+    out += [(f"neumann{n} omega={om}", [1.0] * n, om) for n in (3, 5) for om in (0.6, 0.7)]
+    out += [(f"cheb{n} a={a} b={lam_max}", chebyshev_weights(n, a, lam_max, 0.5), 0.5)
+            for n in (5, 6) for a in (0.4, 0.5)]
+    return out
+
+
+def time_solve(ctx, ds, reps=3, warmup=1):
+    """Median milliseconds of one solve (CUDA events) and the stats of the last one."""
+    import torch
+    x = torch.empty_like(ds.b)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    st = None
+    for _ in range(warmup):
+        _, st = ctx.solve(ds, x=x, raise_on_error=False)
+    times = []
+    for _ in range(reps):
+        ev0.record()
+        _, st = ctx.solve(ds, x=x, raise_on_error=False)
+        ev1.record()
+        ev1.synchronize()
+        times.append(ev0.elapsed_time(ev1))
+    return float(np.median(times)), st
+
+
+def tune_block(system, base: HSCOptions | None = None, candidates=None, target=1e-6, reps=3, log=None):
+    """Times every candidate polynomial of the block preconditioner on this system and returns
+    (options of the fastest one whose solve met ``target`` on the FP64-verified full residual,
+    table of every candidate).  A tuned polynomial is a property of the system family (mesh,
+    materials, coupling), so a Newton loop tunes once and reuses it."""
+    base = base or HSCOptions(block=True, precision="fp32", tol=1e-6, abd_inverse="exact")
+    ds = system if isinstance(system, DeviceSystem) else DeviceSystem.from_system(system)
+    cands = candidates if candidates is not None else block_candidates()
+    table, best = [], None
+    for name, w, om in cands:
+        opt = replace(base, block=True, poly_weights=tuple(w), omega=om, fallback_on_stall=False)
+        ctx = HSCContext(opt)
+        ms, st = time_solve(ctx, ds, reps=reps)
+        ok = st["status"] == 0 and st["full_relative_residual"] <= target
+        rec = dict(name=name, omega=om, weights=[round(v, 6) for v in w], ms=ms, ok=bool(ok),
+                   iterations=st["pcg_iterations"], full_relative_residual=st["full_relative_residual"])
+        table.append(rec)
+        if log:
+            log(json.dumps(rec))
+        if ok and (best is None or ms < best[1]):
+            best = (opt, ms)
+        ctx.close()
+    return (best[0] if best else None), table
