@@ -163,6 +163,7 @@ struct hsc_ctx {
     cudaEvent_t ev_blk = nullptr;  // end of the block preconditioner's setup (Y, K) inside the PCG stage
     cudaStream_t side = nullptr;   // the ABD inverses run here, beside the ACA
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_aca = nullptr, ev_pre = nullptr;  // the block setup's start and end on the side stream
     double analysis_ms = 0.0;      // host time of the current call's pattern analysis
     // after a pattern change behind the same pointers, the next solves hash the pattern before they
     // start (one small kernel and a sync) instead of finding out after a full solve
@@ -1507,7 +1508,10 @@ int build_block_plan(hsc_ctx* ctx, System& S, cudaStream_t st) {
 }
 
 // numeric part of the block form: component columns, Y = L V, the Woodbury core K, the PCG
-int launch_block_solve(hsc_ctx* ctx, System& S, cudaStream_t st) {
+// the block setup that needs only the ACA's factors: the sliced-ELL values, the components'
+// columns, Y = L V with the V^T Y partials, and their sum G; it runs on the side stream beside the
+// reduced core and the Schur rhs.  Also sets the plan's polynomial and PCG controls.
+int launch_block_pre(hsc_ctx* ctx, System& S, cudaStream_t st) {
     const hsc_options& o = ctx->opt;
     BlockPlan& b = S.blk;
     const bool learned = o.preconditioner == HSC_PRECOND_BLOCK_LEARNED;
@@ -1532,10 +1536,18 @@ int launch_block_solve(hsc_ctx* ctx, System& S, cudaStream_t st) {
     if (S.kmax > 0) {
         launch_block_columns(b, st);
         CK(launch_block_y(o.precision, b, st));
-        launch_block_k(b, S.blk_nact_cta, st);
+        launch_block_g(b, S.blk_nact_cta, st);
     } else {
         CK(cudaMemsetAsync(S.blk_colptr.p, 0, sizeof(int) * (b.ncomp + 1), st));
     }
+    return HSC_OK;
+}
+
+// the Woodbury core K (needs the reduced core's LDL^T factors) and the PCG
+int launch_block_solve(hsc_ctx* ctx, System& S, cudaStream_t st) {
+    const hsc_options& o = ctx->opt;
+    BlockPlan& b = S.blk;
+    if (S.kmax > 0) launch_block_k(b, st);
     if (ctx->stage_events) CK(cudaEventRecord(ctx->ev_blk, st));
     b.trace = nullptr;
     b.trace_iters = 0;
@@ -1682,6 +1694,8 @@ int ensure_common(hsc_ctx* ctx, cudaStream_t st) {
         CK(cudaEventCreate(&ctx->ev_blk));
         CK(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ctx->ev_aca, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ctx->ev_pre, cudaEventDisableTiming));
         CK(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
     }
     (void)st;
@@ -1876,6 +1890,8 @@ void hsc_destroy(hsc_ctx* ctx) {
     if (ctx->ev_blk) cudaEventDestroy(ctx->ev_blk);
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+    if (ctx->ev_aca) cudaEventDestroy(ctx->ev_aca);
+    if (ctx->ev_pre) cudaEventDestroy(ctx->ev_pre);
     if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
     if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
@@ -1987,6 +2003,16 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
         int r1 = aca_all(ctx, count, st);
         if (r1) return r1;
         stage_mark(ctx, 2, st);
+        // Y = L V and G need only the ACA (and, for the learned weights, the features): side stream,
+        // beside the reduced core and the rhs
+        const bool pre_side = block && o.preconditioner == HSC_PRECOND_BLOCK;
+        if (pre_side) {
+            CK(cudaEventRecord(ctx->ev_aca, st));
+            CK(cudaStreamWaitEvent(ctx->side, ctx->ev_aca, 0));
+            int rb = launch_block_pre(ctx, ctx->sys[0], ctx->side);
+            if (rb) return rb;
+            CK(cudaEventRecord(ctx->ev_pre, ctx->side));
+        }
         CK(cudaStreamWaitEvent(st, ctx->ev_join, 0));
         stage_mark(ctx, 3, st);
         for (int s = 0; s < count; ++s) {
@@ -1997,6 +2023,12 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
         if (learned)
             for (int s = 0; s < count; ++s) CK(launch_features(feat_args(ctx, ctx->sys[s], true), st));
         CK(cudaEventRecord(ctx->ev[5], st));
+        if (pre_side) {
+            CK(cudaStreamWaitEvent(st, ctx->ev_pre, 0));
+        } else if (block) {
+            int rb = launch_block_pre(ctx, ctx->sys[0], st);
+            if (rb) return rb;
+        }
         int r3 = block ? launch_block_solve(ctx, ctx->sys[0], st) : launch_pcg_all(ctx, count, st);
         if (r3) return r3;
         CK(cudaEventRecord(ctx->ev[6], st));

@@ -1345,11 +1345,15 @@ cudaError_t launch_block_y(int precision, const BlockPlan& p, cudaStream_t st) {
     return precision == 0 ? launch_y_t<double>(p, st) : launch_y_t<float>(p, st);
 }
 
-void launch_block_k(const BlockPlan& p, int nact_cta, cudaStream_t st) {
+void launch_block_g(const BlockPlan& p, int nact_cta, cudaStream_t st) {
     const int kk = p.kmax * p.kmax;
-    const int* dk = p.rank;
     count_launch();
     block_g_reduce_kernel<<<(kk + 255) / 256, 256, 0, st>>>(p.pG, nact_cta, kk, p.G);
+}
+
+void launch_block_k(const BlockPlan& p, cudaStream_t st) {
+    const int kk = p.kmax * p.kmax;
+    const int* dk = p.rank;
     // Ka = G Lc, Kb = Lc^T Ka
     GemmArgs g1{p.G, p.Lc, p.Ka, p.kmax, p.kmax, p.kmax, dk, dk, dk, p.kmax, p.kmax, p.kmax, 0, 0, 1.0, 0.0};
     launch_gemm(g1, p.kmax, p.kmax, st);

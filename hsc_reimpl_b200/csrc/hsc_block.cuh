@@ -135,8 +135,10 @@ void launch_block_fill(int precision, const BlockPlan& p, cudaStream_t st);
 void launch_block_columns(const BlockPlan& p, cudaStream_t st);
 // Y = L V over every part, Y at the coupled dofs, and the per-CTA partials of V^T Y
 cudaError_t launch_block_y(int precision, const BlockPlan& p, cudaStream_t st);
-// G = sum of the partials, K^-1 = diag(1/d) - L_c^T G L_c, K = L_c K~ L_c^T (K = 0 if not SPD)
-void launch_block_k(const BlockPlan& p, int nact_cta, cudaStream_t st);
+// G = the sum of the coupled CTAs' partials of V^T Y (fixed order)
+void launch_block_g(const BlockPlan& p, int nact_cta, cudaStream_t st);
+// K^-1 = diag(1/d) - L_c^T G L_c, K = L_c K~ L_c^T (K = 0 if not SPD)
+void launch_block_k(const BlockPlan& p, cudaStream_t st);
 // the persistent pipelined PCG (cooperative launch, one CTA per part)
 cudaError_t launch_block_pcg(int precision, const BlockPlan& p, cudaStream_t st);
 // shared-memory layouts of the two block kernels for the maxima in p; returns the larger
