@@ -71,6 +71,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-other", action="store_true", help="skip the annulus-tire workload lines")
+    ap.add_argument("--block-poly", default=None,
+                    help="the block modes' polynomial by tuner candidate name (e.g. 'cheb6 a=0.5 b=3.9'), "
+                         "skipping the per-system tuning (profiling runs)")
     return ap.parse_args()
 
 
@@ -439,7 +442,17 @@ def run_gpu(args):
     # the block modes' polynomial: tuned once on this system, outside every timed region (a Newton
     # loop tunes once per system family and reuses the choice)
     tuning = None
-    if any(m.startswith("block") for m in args.modes.split(",")):
+    if args.block_poly is not None:
+        from dataclasses import replace
+        from hsc_reimpl_b200.autotune import block_candidates
+        named = {c[0]: c for c in block_candidates()}
+        if args.block_poly not in named:
+            raise SystemExit(f"--block-poly: unknown candidate {args.block_poly!r}; one of {sorted(named)}")
+        _, w, om = named[args.block_poly]
+        mode_opts["block32"] = replace(mode_opts["block32"], poly_weights=tuple(w), omega=om)
+        mode_opts["block64"] = replace(mode_opts["block64"], poly_weights=tuple(w), omega=om)
+        tuning = {"chosen": args.block_poly, "weights": list(w), "omega": om, "candidates": None}
+    elif any(m.startswith("block") for m in args.modes.split(",")):
         from dataclasses import replace
         from hsc_reimpl_b200.autotune import tune_block
         best, table = tune_block(ds, base=mode_opts["block32"], reps=3)

@@ -407,14 +407,16 @@ enum { kRunLocal = 0, kRunRemote = 1 };
 __device__ __forceinline__ int run_base(const int4& m, int mode) { return mode == kRunRemote ? m.w : 0; }
 __device__ __forceinline__ int run_len(const int4& m, int mode) { return mode == kRunRemote ? m.y - m.w : m.z; }
 
-// thread 0: the plan of a pass over the slices' ranges (mode kRunLocal or kRunRemote)
-__device__ void make_warp_plan(const int4* meta, int ns, int mode, WarpPlan& P) {
+// one thread: the plan of a pass over the slices' ranges (mode kRunLocal or kRunRemote) split over
+// warps [0, nw); the warps from nw on get empty runs
+__device__ void make_warp_plan(const int4* meta, int ns, int mode, WarpPlan& P, int nw = kWarps) {
     int tot = 0;
     for (int s = 0; s < ns; ++s) tot += run_len(meta[s], mode);
     int s = 0, off = 0, seg = 0;
     for (int sl = 0; sl <= ns; ++sl) P.sg[sl] = -1;
     for (int w = 0; w < kWarps; ++w) {
-        const int p0 = (int)((long long)tot * w / kWarps), p1 = (int)((long long)tot * (w + 1) / kWarps);
+        const int ww = min(w, nw);
+        const int p0 = (int)((long long)tot * ww / nw), p1 = w < nw ? (int)((long long)tot * (ww + 1) / nw) : p0;
         while (s < ns && off + run_len(meta[s], mode) <= p0) { off += run_len(meta[s], mode); ++s; }
         P.fs[w] = (short)s;
         P.fc[w] = (short)(p0 - off);
@@ -490,11 +492,27 @@ __device__ __forceinline__ void seg_sum(const WarpPlan& P, const double* scratch
     }
 }
 
+// asynchronous 8-byte copy global -> shared (no register holds the value), and the wait for all of
+// the thread's copies
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// the thread of the last warp, which owns no row (R <= kBlockMaxRows) and so idles through every
+// row loop: it signals grid barriers and looks at their counters while the other warps work
+constexpr int kIdleThread = kThreads - 32;
+static_assert(kBlockMaxRows <= kIdleThread, "the last warp must own no row");
+
 // z = L v over the CTA's rows, warp-balanced (the polynomial of part_poly for one vector; v, z,
-// t, u: 3 per row).  Ends synchronised.
-template <class MT>
+// t, u: 3 per row).  Ends synchronised.  hook(0) runs once every thread's earlier writes are
+// ordered before it (after the first product's partial sums, or after the first term when there
+// is no product), hook(1) while the last product's rows are updated; both on every thread, for
+// kIdleThread to act on.
+template <class MT, class Hook>
 __device__ void part_poly_bal(const BlockPlan& p, const Part<MT>& s, const WarpPlan& P, double* scratch,
-                              const double* v, double* z, double* t, double* u) {
+                              const double* v, double* z, double* t, double* u, Hook hook) {
     using DT = typename BlkDinv<MT>::T;
     const bool gv = !p.stage_vals;
     const double om = p.omega, om1 = 1.0 - p.omega;
@@ -506,6 +524,7 @@ __device__ void part_poly_bal(const BlockPlan& p, const Part<MT>& s, const WarpP
         z[3 * lr] = w0 * o0; z[3 * lr + 1] = w0 * o1; z[3 * lr + 2] = w0 * o2;
     }
     __syncthreads();
+    if (p.nterms <= 1) hook(0);
     double* tc = t;
     double* tn = u;
     for (int k = 1; k < p.nterms; ++k) {
@@ -518,6 +537,8 @@ __device__ void part_poly_bal(const BlockPlan& p, const Part<MT>& s, const WarpP
                 x0 = use ? xs[3 * ol] : 0.0; x1 = use ? xs[3 * ol + 1] : 0.0; x2 = use ? xs[3 * ol + 2] : 0.0;
             });
         __syncthreads();
+        if (k == 1) hook(0);
+        if (k == p.nterms - 1) hook(1);
         for (int lr = threadIdx.x; lr < s.R; lr += blockDim.x) {
             double y0, y1, y2, e0, e1, e2;
             seg_sum(P, scratch, lr, y0, y1, y2);
@@ -806,10 +827,15 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
     double* s_red = reinterpret_cast<double*>(sm + p.off_red);// kWarps x 4 scratch
     __shared__ double s_dot[4];
     __shared__ int s_ok;
-    __shared__ WarpPlan s_plan_loc, s_plan_rem;  // warp runs over the local slots (polynomial, operator) and the rest
+    // warp runs over the local slots (polynomial), the same over all warps but the last (the local
+    // operator blocks, while the last warp signals the barrier) and over the rest
+    __shared__ WarpPlan s_plan_loc, s_plan_op, s_plan_rem;
+    __shared__ unsigned int s_pre;  // the barrier counter as kIdleThread saw it during the polynomial (0: not looked)
     double* scr = reinterpret_cast<double*>(sm + p.off_scr);   // segment partial sums
     if (threadIdx.x == 0) make_warp_plan(sl.meta, sl.ns, kRunLocal, s_plan_loc);
     if (threadIdx.x == 32) make_warp_plan(sl.meta, sl.ns, kRunRemote, s_plan_rem);
+    if (threadIdx.x == 64) make_warp_plan(sl.meta, sl.ns, kRunLocal, s_plan_op, kWarps - 1);
+    if (threadIdx.x == 0) s_pre = 0u;
     for (int e = threadIdx.x; e < sl.na; e += blockDim.x) s_act[e] = p.actp[sl.ab + e] - 3 * sl.rb;
     const int ncols = build_cols(p, cta, s_cols, s_slot);  // synchronises: s_act is complete
     const int k = *p.rank;
@@ -850,15 +876,29 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
 
     // split-phase grid barrier: arrive once the CTA's partials are in global memory, do local work,
     // then wait (every CTA arrives at every barrier before it waits at it)
+    // (the signal comes from kIdleThread, so its wait for the CTA's writes to be visible stalls no
+    // warp that has work)
     auto arrive = [&]() {
         __syncthreads();
-        if (threadIdx.x == 0) red_release_add_u32(&p.bar->count, 1u);
+        if (threadIdx.x == kIdleThread) red_release_add_u32(&p.bar->count, 1u);
     };
+    // a counter kIdleThread already saw complete spares the poll's round trip
     auto wait = [&]() -> bool {
-        if (threadIdx.x == 0) s_ok = grid_wait(p.bar, G, p.spin_limit, epoch);
+        if (threadIdx.x == 0) {
+            const unsigned int c = s_pre;
+            s_ok = c >= (unsigned int)(epoch + 1) * G ? (c & kBarAbortBit) == 0 : grid_wait(p.bar, G, p.spin_limit, epoch);
+            s_pre = 0u;
+        }
         ++epoch;
         __syncthreads();
         return s_ok != 0;
+    };
+    // the polynomial's hooks: signal barrier A once the pass's partials are ordered before it, look
+    // at the counter while the last product's rows are updated
+    auto poly_hook = [&](int ev) {
+        if (threadIdx.x != kIdleThread) return;
+        if (ev == 0) red_release_add_u32(&p.bar->count, 1u);
+        else s_pre = ld_acquire_u32(&p.bar->count);
     };
     // grid barrier: the CTA's partials are already in global memory
     auto barrier = [&]() -> bool {
@@ -987,18 +1027,24 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
     };
     // the CTA's coupled rows of V, compact ([list position][own coupled dof], written by the Y kernel)
     const double* Vc = p.Vc + (size_t)p.kmax * sl.ab;
-    // partials of V^T v over the own coupled dofs
+    // phase 2 copies the first nvs values of these rows into the segment scratch (free from the
+    // polynomial's end to the local operator blocks), so V^T m reads shared memory
+    const int nvs = min(ncols * sl.na, 3 * kSliceRows * (kWarps + p.NS));
+    auto stage_v = [&]() {
+        for (int i = threadIdx.x; i < nvs; i += blockDim.x) cp_async8(scr + i, Vc + i);
+    };
+    // partials of V^T v over the own coupled dofs (staged values first)
     auto v_partials = [&](const double* v, double* part) {
         if (sl.na == 0) return;
         for (int q = warp; q < ncols; q += kWarps) {
-            const double* vq = Vc + (size_t)q * sl.na;
+            const int f0 = q * sl.na;
             // the column's first 256 coupled dofs: every load in flight before the first add
             constexpr int kPre = 8;
             double vv[kPre];
 #pragma unroll
             for (int u = 0; u < kPre; ++u) {
-                const int il = lane + 32 * u;
-                vv[u] = il < sl.na ? __ldg(vq + il) : 0.0;
+                const int il = lane + 32 * u, f = f0 + il;
+                vv[u] = il < sl.na ? (f < nvs ? scr[f] : __ldg(Vc + f)) : 0.0;
             }
             double a = 0.0;
 #pragma unroll
@@ -1006,7 +1052,10 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
                 const int il = lane + 32 * u;
                 if (il < sl.na) a += vv[u] * v[s_act[il]];
             }
-            for (int il = lane + 32 * kPre; il < sl.na; il += 32) a += __ldg(vq + il) * v[s_act[il]];
+            for (int il = lane + 32 * kPre; il < sl.na; il += 32) {
+                const int f = f0 + il;
+                a += (f < nvs ? scr[f] : __ldg(Vc + f)) * v[s_act[il]];
+            }
             a = bwarp_sum(a);
             if (lane == 0) part[s_slot[q]] = a;
         }
@@ -1110,12 +1159,12 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
             cta_partials(g, d, rr, 0.0, 0, 3);
         }
         mark(1);
-        arrive();
-        part_poly_bal<MT>(p, sl, s_plan_loc, scr, Wb, Pz, Pt, Pu);
+        part_poly_bal<MT>(p, sl, s_plan_loc, scr, Wb, Pz, Pt, Pu, poly_hook);
         mark(2);
         if (!wait()) return;
         mark(3);
         // ---------------- phase 2 ----------------
+        stage_v();
         sum_cols(p.pY, s_sv, true);
         __syncthreads();
         mark(4);
@@ -1152,6 +1201,7 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
                 p.mpub[4 * (size_t)(sl.rb + lr) + d] = m;
             }
         }
+        cp_async_wait_all();  // the staged V rows
         __syncthreads();
         mark(6);
         v_partials(Mm, p.pV);
@@ -1192,7 +1242,7 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
         if (!check) {
             // n's blocks inside the part, and the recurrences that do not need n:
             // q = m + b q, s = w + b s, p = u + b p, x += a p, r -= a s, u -= a q (a start takes u = m)
-            part_op_local<MT>(sl, s_plan_loc, scr, gv, Mm, Nn);
+            part_op_local<MT>(sl, s_plan_op, scr, gv, Mm, Nn);
 #pragma unroll
             for (int i = 0; i < kDofs; ++i) {
                 const int e = threadIdx.x + kThreads * i;

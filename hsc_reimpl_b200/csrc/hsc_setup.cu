@@ -937,32 +937,68 @@ __global__ void wt_vec_kernel(const double* W, int qm, int kmax, const int* dk, 
     if (lane == 0) c[gw] = s;
 }
 
-// rhs[act_i] -= (V c)_i ; V column-major a x kmax
-__global__ void rhs_lowrank_kernel(const double* V, int a, const int* dk, const double* c, const int* act,
-                                   double* rhs) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a) return;
-    const int k = *dk;
-    double s = 0.0;
-#pragma unroll 8
-    for (int j = 0; j < k; ++j) s += V[(size_t)j * a + i] * c[j];  // loads of eight columns in flight
-    const int dof = act[i];
-    rhs[4 * (size_t)(dof / 3) + dof % 3] -= s;
+// sum_{j < n} M[j a + i] v[j] for the CTA's 32 consecutive i (lane of warp 0 on return; other
+// threads return 0): the 8 warps take j = g, g + 8, ... (coalesced over i, four loads in flight
+// per thread), then warp 0 adds the 8 group sums in group order (deterministic)
+constexpr int kColGroups = 8;
+__device__ __forceinline__ double col_sums_32x8(const double* M, int a, int n, const double* v, int i) {
+    __shared__ double s_part[kColGroups][32];
+    const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
+    double s0 = 0.0, s1 = 0.0;
+    if (i < a) {
+        int j = g;
+        for (; j + kColGroups < n; j += 2 * kColGroups) {
+            s0 += M[(size_t)j * a + i] * v[j];
+            s1 += M[(size_t)(j + kColGroups) * a + i] * v[j + kColGroups];
+        }
+        if (j < n) s0 += M[(size_t)j * a + i] * v[j];
+    }
+    s_part[g][lane] = s0 + s1;
+    __syncthreads();
+    double t = 0.0;
+    if (g == 0)
+        for (int h = 0; h < kColGroups; ++h) t += s_part[h][lane];
+    return t;
 }
 
-// t = V^T x[act] ; one warp per column
-__global__ void vt_x_kernel(const double* V, int a, const int* dk, const int* act, const double* x, double* t) {
-    const int k = *dk;
-    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (gw >= k) return;
-    double s = 0.0;
-#pragma unroll 4
-    for (int i = lane; i < a; i += 32) {
+// rhs[act_i] -= (V c)_i ; V column-major a x kmax; 32 coupled dofs per 256-thread CTA
+__global__ void __launch_bounds__(32 * kColGroups) rhs_lowrank_kernel(const double* V, int a, const int* dk,
+                                                                      const double* c, const int* act, double* rhs) {
+    const int i = blockIdx.x * 32 + (threadIdx.x & 31);
+    const double s = col_sums_32x8(V, a, *dk, c, i);
+    if (threadIdx.x < 32 && i < a) {
         const int dof = act[i];
-        s += V[(size_t)gw * a + i] * x[4 * (size_t)(dof / 3) + dof % 3];
+        rhs[4 * (size_t)(dof / 3) + dof % 3] -= s;
     }
-    s = wsum(s);
-    if (lane == 0) t[gw] = s;
+}
+
+// t = V^T x[act] ; a 256-thread CTA per column, its threads over the coupled dofs (every load
+// in flight at once), then a fixed-order CTA reduction
+__global__ void __launch_bounds__(256) vt_x_kernel(const double* V, int a, const int* dk, const int* act,
+                                                   const double* x, double* t) {
+    __shared__ double s_w[8];
+    const int j = blockIdx.x;
+    if (j >= *dk) return;  // uniform in the CTA
+    const double* vj = V + (size_t)j * a;
+    double s0 = 0.0, s1 = 0.0;
+    int i = threadIdx.x;
+    for (; i + 256 < a; i += 512) {
+        const int d0 = act[i], d1 = act[i + 256];
+        s0 += vj[i] * x[4 * (size_t)(d0 / 3) + d0 % 3];
+        s1 += vj[i + 256] * x[4 * (size_t)(d1 / 3) + d1 % 3];
+    }
+    if (i < a) {
+        const int d0 = act[i];
+        s0 += vj[i] * x[4 * (size_t)(d0 / 3) + d0 % 3];
+    }
+    const double s = wsum(s0 + s1);
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0.0;
+        for (int w = 0; w < 8; ++w) r += s_w[w];
+        t[j] = r;
+    }
 }
 
 // dq = P bq - W t  (one warp per ABD row), written to x_out[qo + i]
@@ -1073,15 +1109,15 @@ __global__ void bcoo_row_spmv_kernel(const int* rowptr, const int* colidx, const
     }
 }
 
-// y_f[act_c] += sum_r E[r, c] xq[r]   (one thread per active column)
-__global__ void et_xq_kernel(const double* E, int qm, int a, const int* act, const double* xq, double* ypad) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= a) return;
-    double s = 0.0;
-#pragma unroll 16
-    for (int r = 0; r < qm; ++r) s += E[(size_t)r * a + c] * xq[r];
-    const int dof = act[c];
-    ypad[4 * (size_t)(dof / 3) + dof % 3] += s;
+// y_f[act_c] += sum_r E[r, c] xq[r]   (32 active columns per 256-thread CTA)
+__global__ void __launch_bounds__(32 * kColGroups) et_xq_kernel(const double* E, int qm, int a, const int* act,
+                                                                const double* xq, double* ypad) {
+    const int c = blockIdx.x * 32 + (threadIdx.x & 31);
+    const double s = col_sums_32x8(E, a, qm, xq, c);
+    if (threadIdx.x < 32 && c < a) {
+        const int dof = act[c];
+        ypad[4 * (size_t)(dof / 3) + dof % 3] += s;
+    }
 }
 
 // yq = A xq + E x_f[act] in two passes: one warp per (ABD row, chunk of
@@ -1381,12 +1417,12 @@ void launch_wt_vec(const double* W, int qm, int kmax, const int* dk, const doubl
 
 void launch_rhs_lowrank(const double* V, int a, const int* dk, const double* c, const int* act, double* rhs,
                         cudaStream_t st) {
-    if (a) HSC_COUNTED(rhs_lowrank_kernel<<<blocks(a, 64), 64, 0, st>>>(V, a, dk, c, act, rhs));
+    if (a) HSC_COUNTED(rhs_lowrank_kernel<<<blocks(a, 32), 32 * kColGroups, 0, st>>>(V, a, dk, c, act, rhs));
 }
 
 void launch_vt_x(const double* V, int a, int kmax, const int* dk, const int* act, const double* x, double* t,
                  cudaStream_t st) {
-    if (kmax) HSC_COUNTED(vt_x_kernel<<<blocks((long long)kmax * 32), 256, 0, st>>>(V, a, dk, act, x, t));
+    if (kmax) HSC_COUNTED(vt_x_kernel<<<kmax, 256, 0, st>>>(V, a, dk, act, x, t));
 }
 
 void launch_backsub(const double* P, const double* W, int qm, int kmax, const int* dk, const double* bq,
@@ -1409,7 +1445,7 @@ void launch_full_spmv(const FullSpmv& f, cudaStream_t st) {
     else
         HSC_COUNTED(bsr_spmv64_kernel<<<blocks((long long)f.n * 4), 256, 0, st>>>(f.rowptr, f.colidx, f.v64, f.nnz, f.n,
                                                                                f.xpad, f.ypad));
-    if (f.qm && f.a) HSC_COUNTED(et_xq_kernel<<<blocks(f.a, 64), 64, 0, st>>>(f.E, f.qm, f.a, f.act, f.xq, f.ypad));
+    if (f.qm && f.a) HSC_COUNTED(et_xq_kernel<<<blocks(f.a, 32), 32 * kColGroups, 0, st>>>(f.E, f.qm, f.a, f.act, f.xq, f.ypad));
     if (f.qm && f.rowpart) {
         const int nchunk = abd_row_chunks(f.a);
         HSC_COUNTED(abd_rows_part_kernel<<<dim3(nchunk, (f.qm + 7) / 8), 256, 0, st>>>(f.A, f.E, f.qm, f.a, f.act, f.xq,
