@@ -64,6 +64,7 @@ class Options(C.Structure):
         ("reorder", C.c_int32),
         ("aca_components", C.c_int32),
         ("lanczos_stats", C.c_int32),
+        ("coupled_part_weight", C.c_double),
     ]
 
 

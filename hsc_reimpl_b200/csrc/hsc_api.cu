@@ -110,7 +110,7 @@ struct System {
     DevBuf blk_Y, blk_Yact, blk_Vc, blk_pG, blk_G, blk_K, blk_Ka, blk_Kb, blk_pY, blk_pV, blk_pX, blk_pdot, blk_mpub,
         blk_xpub, blk_colof, blk_colptr, blk_cols, blk_bad, blk_C, blk_cta_comp_ptr, blk_cta_comp, blk_cta_comp_slot,
         blk_comp_slot_ptr, blk_comp_of_body, blk_ident, blk_sslice, blk_cslice, blk_cchunk, blk_nloc, blk_slc,
-        blk_ssrc, blk_svals, blk_coloff;
+        blk_ssrc, blk_svals, blk_coloff, blk_ctayc;
     BlockPlan blk{};
     int blk_nact_cta = 0;
     // plan
@@ -234,6 +234,7 @@ int validate_options(const hsc_options* o, std::string& why) {
         return 0;
     }
     if (o->spin_limit < 1000) { why = "spin_limit too small"; return 0; }
+    if (!(o->coupled_part_weight >= 1.0 && o->coupled_part_weight <= 8.0)) { why = "coupled_part_weight must be in [1, 8]"; return 0; }
     return 1;
 }
 
@@ -300,17 +301,33 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
         if (nparts > 1) {
             std::vector<double> wgt(S.n);
             for (int i = 0; i < S.n; ++i) wgt[i] = 1.0 + cnt[i];
-            // FNV-1a over (n, parts, adjacency, weights): a repeated mesh pattern reuses its partition
+            const bool blockp = o.preconditioner == HSC_PRECOND_BLOCK || o.preconditioner == HSC_PRECOND_BLOCK_LEARNED;
+            const double cw = blockp ? o.coupled_part_weight : 1.0;
+            // FNV-1a over (n, parts, adjacency, weights, coupled-part factor): a repeated mesh pattern
+            // reuses its partition (also when only the contacts changed)
             unsigned long long h = 1469598103934665603ull;
             auto mix = [&](unsigned long long v) { h = (h ^ v) * 1099511628211ull; };
             mix((unsigned long long)S.n); mix((unsigned long long)nparts);
             for (int i = 0; i <= S.n; ++i) mix((unsigned long long)aptr[i]);
             for (int v : adj) mix((unsigned long long)v);
             for (int i = 0; i < S.n; ++i) mix((unsigned long long)cnt[i]);
+            unsigned long long cwb;
+            std::memcpy(&cwb, &cw, sizeof cwb);
+            mix(cwb);
             if (ctx->part_hash == h && (int)ctx->part_cache.size() == S.n) {
                 part = ctx->part_cache;
             } else {
                 part = partition_nodes(S.n, aptr, adj, wgt, nparts);
+                if (cw > 1.0) {
+                    // the block preconditioner's parts that hold a coupled node also apply their
+                    // components' Y columns on every row: their nodes weigh more in a second pass
+                    std::vector<char> hot(nparts, 0);
+                    for (int i = 0; i < S.n; ++i)
+                        if (fnode_active[i]) hot[part[i]] = 1;
+                    for (int i = 0; i < S.n; ++i)
+                        if (hot[part[i]]) wgt[i] *= cw;
+                    part = partition_nodes(S.n, aptr, adj, wgt, nparts);
+                }
                 ctx->part_hash = h;
                 ctx->part_cache = part;
             }
@@ -1493,21 +1510,41 @@ int build_block_plan(hsc_ctx* ctx, System& S, cudaStream_t st) {
     b.out = S.scal.as<DevScal>()->pcg;
     b.cg_coef = S.cg.as<double>(); b.max_coef = kMaxCoef;
     b.R = R; b.NS = NS; b.NCH = NCH; b.W = W; b.NA = NA; b.NCOL = NCOL;
-    // stage the value planes when they fit, then as many of a CTA's Y columns as the rest holds
+    // stage the value planes when they fit; then each CTA stages as many of its Y columns (3 R
+    // floats each) as fit after its own value chunks
     const size_t cap = (size_t)block_max_smem();
-    bool vals_in = true;
-    if (block_smem_bytes(o.precision, b, true, 0) > cap) vals_in = false;
-    int nyc = 0;
-    for (int t = NCOL; t > 0; --t)
-        if (block_smem_bytes(o.precision, b, vals_in, t) <= cap) { nyc = t; break; }
-    block_smem_bytes(o.precision, b, vals_in, nyc);
+    bool vals_in = block_smem_bytes(o.precision, b, true) <= cap && b.smem_y <= cap;
+    block_smem_bytes(o.precision, b, vals_in);
     if (std::max(b.smem, b.smem_y) > cap)
         return fail(ctx, HSC_ERR_INVALID, "a part of the block preconditioner does not fit one CTA's shared memory");
+    {
+        const size_t mt = o.precision ? sizeof(float) : sizeof(double);
+        std::vector<int> yc(2 * G);
+        size_t need = b.smem;
+        int nyc_max = 0;
+        for (int c = 0; c < G; ++c) {
+            const size_t off = b.off_val + (vals_in ? (mt * kChunkVals * (size_t)(cchunk[c + 1] - cchunk[c]) + 15) / 16 * 16 : 0);
+            const size_t col = sizeof(float) * 3 * (size_t)std::max(1, cta_row[2 * c + 1] - cta_row[2 * c]);
+            int ncap = 0;
+            for (int g : comps[c]) ncap += comp_cap[g];
+            ncap = std::min(ncap, km);
+            const int nyc = off < cap ? (int)std::min<size_t>((size_t)ncap, (cap - off) / col) : 0;
+            yc[2 * c] = (int)off;
+            yc[2 * c + 1] = nyc;
+            need = std::max(need, off + col * nyc);
+            nyc_max = std::max(nyc_max, nyc);
+        }
+        GROW(S.blk_ctayc, sizeof(int) * 2 * G);
+        CK(cudaMemcpyAsync(S.blk_ctayc.p, yc.data(), sizeof(int) * 2 * G, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+        b.cta_yc = S.blk_ctayc.as<int>();
+        b.NYC = nyc_max;
+        b.smem = need;
+    }
     S.blk_nact_cta = nact_cta;
     return HSC_OK;
 }
 
-// numeric part of the block form: component columns, Y = L V, the Woodbury core K, the PCG
 // the block setup that needs only the ACA's factors: the sliced-ELL values, the components'
 // columns, Y = L V with the V^T Y partials, and their sum G; it runs on the side stream beside the
 // reduced core and the Schur rhs.  Also sets the plan's polynomial and PCG controls.
@@ -1845,6 +1882,7 @@ int hsc_options_default(hsc_options* o) {
     o->reorder = 1;
     o->aca_components = 1;
     o->lanczos_stats = 0;
+    o->coupled_part_weight = 1.2;
     return HSC_OK;
 }
 

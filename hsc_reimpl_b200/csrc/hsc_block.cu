@@ -850,13 +850,15 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
         s_srng[2 * j + 1] = g >= 0 ? p.col_off[j + 1] : p.col_off[j];
     }
     int epoch = 0;
-    const int nyc = min(ncols, p.NYC);  // the CTA's first nyc Y columns are staged, the rest read from L2
+    // the CTA's first nyc Y columns are staged (3R floats each, after its value chunks), the rest
+    // read from L2
+    const int nyc = min(ncols, p.cta_yc[2 * cta + 1]);
     if (nyc > 0) {
-        float* yc = reinterpret_cast<float*>(sm + p.off_yc);
+        float* yc = reinterpret_cast<float*>(sm + p.cta_yc[2 * cta]);
         for (int e = threadIdx.x; e < nyc * R; e += blockDim.x) {
             const int q = e / R, lr = e - q * R;
             const float4 y = reinterpret_cast<const float4*>(p.Y + (size_t)s_cols[q] * 4 * p.n)[sl.rb + lr];
-            float* o = yc + (size_t)q * ld + 3 * lr;
+            float* o = yc + (size_t)q * R3 + 3 * lr;
             o[0] = y.x; o[1] = y.y; o[2] = y.z;
         }
     }
@@ -1011,9 +1013,9 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
         }
     };
     // the CTA's Y columns at its own dofs: shared memory (FP32) when staged
-    const float* Yc = reinterpret_cast<const float*>(sm + p.off_yc);
+    const float* Yc = reinterpret_cast<const float*>(sm + p.cta_yc[2 * cta]);
     auto yval = [&](int q, int e) -> double {
-        if (q < nyc) return (double)Yc[(size_t)q * ld + e];
+        if (q < nyc) return (double)Yc[(size_t)q * R3 + e];
         return (double)__ldg(p.Y + (size_t)s_cols[q] * 4 * p.n + 4 * (size_t)(sl.rb + e / 3) + e % 3);
     };
     // partials of Y^T v over the own dofs -> part[slot][j] for the CTA's columns
@@ -1181,12 +1183,12 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
                 if (ncols <= nyc) {  // every column staged: plain shared-memory loads
                     const float* yc = Yc + e;
                     for (; q + 4 <= ncols; q += 4) {
-                        m0 += (double)yc[(size_t)q * ld] * s_c[q];
-                        m1 += (double)yc[(size_t)(q + 1) * ld] * s_c[q + 1];
-                        m2 += (double)yc[(size_t)(q + 2) * ld] * s_c[q + 2];
-                        m3 += (double)yc[(size_t)(q + 3) * ld] * s_c[q + 3];
+                        m0 += (double)yc[(size_t)q * R3] * s_c[q];
+                        m1 += (double)yc[(size_t)(q + 1) * R3] * s_c[q + 1];
+                        m2 += (double)yc[(size_t)(q + 2) * R3] * s_c[q + 2];
+                        m3 += (double)yc[(size_t)(q + 3) * R3] * s_c[q + 3];
                     }
-                    for (; q < ncols; ++q) m0 += (double)yc[(size_t)q * ld] * s_c[q];
+                    for (; q < ncols; ++q) m0 += (double)yc[(size_t)q * R3] * s_c[q];
                 } else {
                     for (; q + 4 <= ncols; q += 4) {
                         m0 += yval(q, e) * s_c[q];
@@ -1384,8 +1386,10 @@ static cudaError_t launch_y_t(const BlockPlan& p, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     cudaMemsetAsync(p.Yact, 0, sizeof(double) * (size_t)p.a * p.kmax, st);
     const int batches = std::max(1, (p.NCOL + kYBatch - 1) / kYBatch);
+    BlockPlan py = p;  // the Y kernel's value chunks follow its own vector region
+    py.off_val = p.off_val_y;
     count_launch();
-    fn<<<dim3(p.G_ctas, batches), kThreads, p.smem_y, st>>>(p);
+    fn<<<dim3(p.G_ctas, batches), kThreads, p.smem_y, st>>>(py);
     count_launch();
     block_gpart_kernel<<<p.G_ctas, kThreads, gsm, st>>>(p);
     return cudaPeekAtLastError();
@@ -1453,10 +1457,12 @@ int block_max_smem() { return 227 * 1024 - 8 * 1024; }
 
 // shared-memory layouts for the maxima in p (R, NS, NCH, W, NA, NCOL, kmax): a common prefix
 // (slices, local slot counts, window positions, Dd^-1, window, coupled dofs and their diagonal
-// blocks, column lists and slot ranges, k-vectors, reduction scratch, the value chunks), then the
-// vectors: the Y kernel's batch region, or the PCG's eight FP64 vectors (3 per row) followed by
-// the CTA's Y columns (FP32)
-size_t block_smem_bytes(int precision, BlockPlan& p, bool stage_vals, int nyc) {
+// blocks, column lists and slot ranges, k-vectors, reduction scratch), then for the PCG its eight
+// FP64 vectors (3 per row), the segment scratch and the CTA's value chunks, after which each CTA
+// stages its Y columns (FP32) at its own offset (cta_yc, set by the host: a small part leaves room
+// for more columns); for the Y kernel its batch region, then the value chunks.  Returns the PCG's
+// bytes without Y columns and sets smem_y.
+size_t block_smem_bytes(int precision, BlockPlan& p, bool stage_vals) {
     const size_t mt = precision == 0 ? 8 : 4, dt = mt;
     auto al = [](size_t b) { return (b + 15) / 16 * 16; };
     size_t off = 0;
@@ -1473,20 +1479,19 @@ size_t block_smem_bytes(int precision, BlockPlan& p, bool stage_vals, int nyc) {
     p.off_srng = (int)off; off += al(sizeof(int) * 2 * p.kmax);
     p.off_kv = (int)off; off += al(sizeof(double) * 4 * p.kmax);
     p.off_red = (int)off; off += al(sizeof(double) * 4 * kWarps);
-    p.off_val = (int)off;
-    p.stage_vals = stage_vals ? 1 : 0;
-    if (stage_vals) off += al(mt * kChunkVals * (size_t)p.NCH);
     p.off_vec = (int)off;
-    p.smem_y = off + al(sizeof(double) * y_region_doubles(p.R));
+    p.stage_vals = stage_vals ? 1 : 0;
+    const size_t vals = stage_vals ? al(mt * kChunkVals * (size_t)p.NCH) : 0;
+    p.off_val_y = (int)(off + al(sizeof(double) * y_region_doubles(p.R)));
+    p.smem_y = p.off_val_y + vals;
     off += al(sizeof(double) * 8 * 3 * (size_t)p.R);
     p.off_scr = (int)off;
     off += al(sizeof(double) * 3 * kSliceRows * (size_t)(kWarps + p.NS));
-    p.off_yc = (int)off;
-    p.NYC = nyc;
-    off += al(sizeof(float) * 3 * (size_t)p.R * nyc);
+    p.off_val = (int)off;
+    off += vals;
     p.smem = off;
     p.gpart_staged = gpart_smem_bytes(p.kmax, p.NA, p.NCOL) <= (size_t)block_max_smem() ? 1 : 0;
-    return std::max(p.smem, p.smem_y);
+    return off;
 }
 
 }  // namespace hsc

@@ -116,11 +116,14 @@ struct BlockPlan {
     int max_coef;
     unsigned long long* trace;   // optional: per CTA x trace_iters x 16 SM clocks at the phase boundaries
     int trace_iters;
-    // shared-memory layout (bytes from the dynamic base, the same in every CTA)
+    // shared-memory layout (bytes from the dynamic base, the same in every CTA but for the Y
+    // columns, which follow the CTA's own value chunks)
     int R, NS, NCH, W, NA, NCOL; // maxima over CTAs: rows, slices, chunks, window nodes, coupled dofs, Y columns
-    int stage_vals, NYC, gpart_staged;  // value chunks staged; Y columns staged per CTA (its first NYC)
+    int stage_vals, NYC, gpart_staged;  // value chunks staged; the most Y columns a CTA stages
     int off_meta, off_nloc, off_lc, off_val, off_dinv, off_wn, off_win, off_act, off_aflag, off_dact;
-    int off_cols, off_srng, off_kv, off_red, off_vec, off_scr, off_yc;
+    int off_cols, off_srng, off_kv, off_red, off_vec, off_scr;
+    int off_val_y;               // the Y kernel's value chunks (after its larger vector region)
+    const int* cta_yc;           // per CTA: byte offset of its staged Y columns, how many it stages
     size_t smem;                 // the PCG kernel
     size_t smem_y;               // the Y kernel
 };
@@ -142,7 +145,7 @@ void launch_block_k(const BlockPlan& p, cudaStream_t st);
 // the persistent pipelined PCG (cooperative launch, one CTA per part)
 cudaError_t launch_block_pcg(int precision, const BlockPlan& p, cudaStream_t st);
 // shared-memory layouts of the two block kernels for the maxima in p; returns the larger
-size_t block_smem_bytes(int precision, BlockPlan& p, bool stage_vals, int nyc);
+size_t block_smem_bytes(int precision, BlockPlan& p, bool stage_vals);
 int block_max_smem();
 
 }  // namespace hsc

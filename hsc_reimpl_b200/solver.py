@@ -68,6 +68,7 @@ class HSCOptions:
     reorder: bool = True                   # internal FEM node renumbering into compact CTA parts
     aca_components: bool = True            # ACA per coupling component, merged (same factors as global)
     lanczos_stats: bool = False            # Ritz extremes of every solve (always on for the learned forms)
+    coupled_part_weight: float = 1.2       # block forms: weight of the coupled parts' nodes in a second partition pass
 
     @classmethod
     def reference(cls):
@@ -127,6 +128,7 @@ class HSCOptions:
         o.reorder = int(bool(self.reorder))
         o.aca_components = int(bool(self.aca_components))
         o.lanczos_stats = int(bool(self.lanczos_stats))
+        o.coupled_part_weight = float(self.coupled_part_weight)
         return o
 
 

@@ -143,6 +143,12 @@ typedef struct hsc_options {
                                     operator from the CG coefficients (host bisection) into the stats and the
                                     next solve's feature record; 0 (default): only for the learned
                                     preconditioners, which read that record */
+    double coupled_part_weight;  /* block preconditioners: the node partition runs twice, the second time
+                                    with the nodes of the first pass's parts that hold a coupled node
+                                    weighted by this factor (those parts also do their components' low-rank
+                                    work on every row), so they come out smaller; 1: one pass.  The
+                                    partition is cached per FEM pattern: a contact change reuses it.
+                                    Default 1.2 */
 } hsc_options;
 
 typedef struct hsc_stats {        /* superset of the hsc_stats.jsonl record (linear_hsc.cu:420-431) */
