@@ -55,8 +55,9 @@ TARGET = 1e-6
 # 204 iterations, FP32 32.19 MB + 0.50 MB over 245.  The learned modes run
 # the same kernel with eight Schur-basis terms and have no capture of their own.
 NCU_TRAFFIC_PER_ITER = {"fp64": (24.84e6 + 1.11e6) / 204, "fp32": (32.19e6 + 0.50e6) / 245,
-                        # block_pcg_kernel<float>, one solve: 20.21 MB read + 0.22 MB written over 91 iterations
-                        "block32": (20.21e6 + 0.22e6) / 91}
+                        # block_pcg_kernel<float>, one solve (Chebyshev degree 6): 20.09 MB read + 0.17 MB
+                        # written over 68 iterations
+                        "block32": (20.09e6 + 0.167e6) / 68}
 BLOCK_TERMS = 4  # the block modes' default polynomial (Neumann, 4 terms) before the per-system tuning
 
 
