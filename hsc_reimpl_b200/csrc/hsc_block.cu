@@ -954,7 +954,7 @@ __global__ void __launch_bounds__(kThreads, 1) block_pcg_kernel(const BlockPlan 
     auto sum_cols = [&](const double* part, double* out, bool dots) {
         const int nw = dots ? kWarps - 2 : kWarps;
         if (dots) sum_dots();
-        if (warp >= nw) return;
+        if (warp >= nw || ncols == 0) return;  // a CTA without columns reads no sum (K s, C vt are per column)
         constexpr int kC = 7;
         for (int j0 = 0; j0 < k; j0 += kC * nw) {
             double a[kC], b2[kC];
