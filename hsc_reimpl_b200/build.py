@@ -4,7 +4,8 @@
 
 Each .cu under csrc/ is compiled to an object with
 ``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` and linked into one
-shared library (static CUDA runtime).  Objects go to csrc/_build/.
+shared library (static CUDA runtime; the host pattern analysis uses OpenMP).  Objects go to
+csrc/_build/.
 """
 import os
 import subprocess
@@ -20,7 +21,7 @@ SOURCES = ["hsc_api.cu", "hsc_setup.cu", "hsc_pcg.cu", "hsc_aca.cu", "hsc_learne
            "hsc_aca_comp.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-         "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",
+         "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "-Xcompiler", "-fopenmp", "--expt-relaxed-constexpr",
          f"-I{HERE.parent / 'include'}"]
 
 
@@ -57,7 +58,7 @@ def build(force=False, verbose=False, checked=False):
             f.result()
     if force or not lib.exists() or lib.stat().st_mtime < max(Path(o).stat().st_mtime for o in objs):
         _run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-cudart", "static",
-              "-o", str(lib), *objs, "-lpthread"])
+              "-o", str(lib), *objs, "-lpthread", "-lgomp"])
     return lib
 
 

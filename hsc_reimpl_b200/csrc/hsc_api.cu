@@ -368,18 +368,21 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
         }
     }
     std::vector<int> colidx(S.nnz), src(S.nnz), diag(S.n, -1);
+    int dup_rows = 0;  // rows are independent: sorted in parallel, errors reported after
+#pragma omp parallel for schedule(static) reduction(+ : dup_rows) if (S.n >= 4096)
     for (int i = 0; i < S.n; ++i) {
         auto b = ent.begin() + S.h_rowptr[i], e = ent.begin() + S.h_rowptr[i + 1];
         std::sort(b, e);
         for (int k = S.h_rowptr[i]; k < S.h_rowptr[i + 1]; ++k) {
             colidx[k] = (int)(ent[k] >> 32);
             src[k] = (int)(ent[k] & 0xffffffffll);
-            if (k > S.h_rowptr[i] && colidx[k] == colidx[k - 1])
-                return fail(ctx, HSC_ERR_INVALID, "duplicate FEM block (both triangles stored?)");
+            if (k > S.h_rowptr[i] && colidx[k] == colidx[k - 1]) ++dup_rows;
             if (colidx[k] == i) diag[i] = k;
         }
-        if (diag[i] < 0) return fail(ctx, HSC_ERR_NONSPD, "HSC: FEM node without a diagonal block");
     }
+    if (dup_rows) return fail(ctx, HSC_ERR_INVALID, "duplicate FEM block (both triangles stored?)");
+    for (int i = 0; i < S.n; ++i)
+        if (diag[i] < 0) return fail(ctx, HSC_ERR_NONSPD, "HSC: FEM node without a diagonal block");
     // ABD duplicates (both triangles of one pair)
     {
         const int nb = L.qm / 3;
@@ -1029,24 +1032,40 @@ int build_partition(hsc_ctx* ctx, const std::vector<int>& idx, cudaStream_t st) 
     std::vector<int> win_off(G + 1, 0), win_nodes, win_own(G, 0), win_flag, win_act_off(G + 1, 0), win_act;
     int Wmax = 0, WAmax = 0;
     bool win_ok = o.resident != 0;
-    {
-        std::vector<int> stamp, pos;
+    if (win_ok) {
+        // each CTA's window on its own (in parallel; per-thread node stamps), then concatenated
+        int maxn = 1;
+        for (int k = 0; k < G; ++k) {
+            System& S = ctx->sys[idx[cta_sys[k]]];
+            maxn = std::max(maxn, S.n);
+            if (S.h_lcol.size() != (size_t)S.nnz) S.h_lcol.assign(S.nnz, 0);
+        }
+        std::vector<std::vector<int>> wl(G);
+        int too_big = 0;
+#pragma omp parallel reduction(+ : too_big) if (G >= 16)
+        {
+            std::vector<int> stamp(maxn, -1), pos(maxn, 0);
+#pragma omp for schedule(dynamic, 4)
+            for (int k = 0; k < G; ++k) {
+                System& S = ctx->sys[idx[cta_sys[k]]];
+                const int rb = cta_row[2 * k], re = cta_row[2 * k + 1];
+                const int kb0 = S.h_rowptr[rb], kb1 = S.h_rowptr[re];
+                std::vector<int>& w = wl[k];
+                for (int e = kb0; e < kb1; ++e) {
+                    const int c = S.h_colidx[e];
+                    if (stamp[c] != k) { stamp[c] = k; w.push_back(c); }
+                }
+                std::sort(w.begin(), w.end());
+                for (int i = 0; i < (int)w.size(); ++i) pos[w[i]] = i;
+                if (w.size() > 65535 || re - rb > 65535) { ++too_big; continue; }
+                for (int e = kb0; e < kb1; ++e) S.h_lcol[e] = (unsigned short)pos[S.h_colidx[e]];
+                win_own[k] = rb < re ? pos[rb] : 0;
+            }
+        }
+        if (too_big) win_ok = false;
         for (int k = 0; k < G && win_ok; ++k) {
             System& S = ctx->sys[idx[cta_sys[k]]];
-            if ((int)stamp.size() < S.n) { stamp.assign(S.n, -1); pos.assign(S.n, 0); }
-            const int rb = cta_row[2 * k], re = cta_row[2 * k + 1];
-            const int kb0 = S.h_rowptr[rb], kb1 = S.h_rowptr[re];
-            std::vector<int> w;
-            for (int e = kb0; e < kb1; ++e) {
-                const int c = S.h_colidx[e];
-                if (stamp[c] != k) { stamp[c] = k; w.push_back(c); }
-            }
-            std::sort(w.begin(), w.end());
-            for (int i = 0; i < (int)w.size(); ++i) pos[w[i]] = i;
-            if (w.size() > 65535 || re - rb > 65535) { win_ok = false; break; }
-            if (S.h_lcol.size() != (size_t)S.nnz) S.h_lcol.assign(S.nnz, 0);
-            for (int e = kb0; e < kb1; ++e) S.h_lcol[e] = (unsigned short)pos[S.h_colidx[e]];
-            win_own[k] = rb < re ? pos[rb] : 0;
+            const std::vector<int>& w = wl[k];
             win_off[k + 1] = win_off[k] + (int)w.size();
             win_nodes.insert(win_nodes.end(), w.begin(), w.end());
             int nwa = 0;
@@ -1364,52 +1383,66 @@ int build_block_plan(hsc_ctx* ctx, System& S, cudaStream_t st) {
     std::vector<unsigned short> nloc(std::max(1, S.n), 0), slc;
     int NS = 1, NCH = 1;
     {
-        std::vector<int> order;
-        std::vector<std::vector<int>> rowslots(kSliceRows);
-        for (int c = 0; c < G; ++c) {
-            const int rb = cta_row[2 * c], re = cta_row[2 * c + 1];
-            int ch_rel = 0;
-            for (int r0 = rb; r0 < re; r0 += kSliceRows) {
-                const int r1 = std::min(re, r0 + kSliceRows);
-                int width = 0, lwidth = 0, lmin = 1 << 30;
-                for (int r = r0; r < r1; ++r) {
-                    std::vector<int>& sl = rowslots[r - r0];
-                    sl.clear();
-                    int diag = -1;
-                    for (int e = S.h_rowptr[r]; e < S.h_rowptr[r + 1]; ++e)
-                        if (S.h_colidx[e] == r) diag = e;
-                    sl.push_back(diag);
-                    for (int e = S.h_rowptr[r]; e < S.h_rowptr[r + 1]; ++e) {
-                        const int col = S.h_colidx[e];
-                        if (col >= rb && col < re && S.h_lcol[e] != win_own[c] + (col - rb))
-                            return fail(ctx, HSC_ERR_INVALID, "a part's rows are not contiguous in its window");
-                        if (col != r && col >= rb && col < re) sl.push_back(e);
+        // each CTA's slices on their own (in parallel), then concatenated in CTA order
+        std::vector<std::vector<int4>> c_slice(G);
+        std::vector<std::vector<int>> c_src(G);
+        std::vector<std::vector<unsigned short>> c_lc(G);
+        int not_contig = 0;
+#pragma omp parallel reduction(+ : not_contig) if (G >= 16)
+        {
+            std::vector<std::vector<int>> rowslots(kSliceRows);
+#pragma omp for schedule(dynamic, 4)
+            for (int c = 0; c < G; ++c) {
+                const int rb = cta_row[2 * c], re = cta_row[2 * c + 1];
+                int ch_rel = 0;
+                for (int r0 = rb; r0 < re; r0 += kSliceRows) {
+                    const int r1 = std::min(re, r0 + kSliceRows);
+                    int width = 0, lwidth = 0, lmin = 1 << 30;
+                    for (int r = r0; r < r1; ++r) {
+                        std::vector<int>& sl = rowslots[r - r0];
+                        sl.clear();
+                        int diag = -1;
+                        for (int e = S.h_rowptr[r]; e < S.h_rowptr[r + 1]; ++e)
+                            if (S.h_colidx[e] == r) diag = e;
+                        sl.push_back(diag);
+                        for (int e = S.h_rowptr[r]; e < S.h_rowptr[r + 1]; ++e) {
+                            const int col = S.h_colidx[e];
+                            if (col >= rb && col < re && S.h_lcol[e] != win_own[c] + (col - rb)) ++not_contig;
+                            if (col != r && col >= rb && col < re) sl.push_back(e);
+                        }
+                        nloc[r] = (unsigned short)sl.size();
+                        for (int e = S.h_rowptr[r]; e < S.h_rowptr[r + 1]; ++e) {
+                            const int col = S.h_colidx[e];
+                            if (col < rb || col >= re) sl.push_back(e);
+                        }
+                        width = std::max(width, (int)sl.size());
+                        lwidth = std::max(lwidth, (int)nloc[r]);
+                        lmin = std::min(lmin, (int)nloc[r]);
                     }
-                    nloc[r] = (unsigned short)sl.size();
-                    for (int e = S.h_rowptr[r]; e < S.h_rowptr[r + 1]; ++e) {
-                        const int col = S.h_colidx[e];
-                        if (col < rb || col >= re) sl.push_back(e);
+                    const int nch = (width + 1) / 2;
+                    // chunks holding a local slot of some row: [0, (lwidth + 1) / 2); a remote one: [lmin / 2, nch)
+                    c_slice[c].push_back(make_int4(ch_rel, nch, (lwidth + 1) / 2, lmin / 2));
+                    const size_t base = c_src[c].size();
+                    c_src[c].resize(base + (size_t)32 * nch, -1);
+                    c_lc[c].resize(base + (size_t)32 * nch, (unsigned short)win_own[c]);
+                    for (int r = r0; r < r1; ++r) {
+                        const std::vector<int>& sl = rowslots[r - r0];
+                        for (int j = 0; j < (int)sl.size(); ++j) {
+                            const size_t at = base + (size_t)32 * (j / 2) + 2 * (r - r0) + (j & 1);
+                            c_src[c][at] = sl[j];
+                            c_lc[c][at] = sl[j] >= 0 ? S.h_lcol[sl[j]] : (unsigned short)win_own[c];
+                        }
                     }
-                    width = std::max(width, (int)sl.size());
-                    lwidth = std::max(lwidth, (int)nloc[r]);
-                    lmin = std::min(lmin, (int)nloc[r]);
+                    ch_rel += nch;
                 }
-                const int nch = (width + 1) / 2;
-                // chunks holding a local slot of some row: [0, (lwidth + 1) / 2); a remote one: [lmin / 2, nch)
-                sslice.push_back(make_int4(ch_rel, nch, (lwidth + 1) / 2, lmin / 2));
-                const size_t base = ssrc.size();
-                ssrc.resize(base + (size_t)32 * nch, -1);
-                slc.resize(base + (size_t)32 * nch, (unsigned short)win_own[c]);
-                for (int r = r0; r < r1; ++r) {
-                    const std::vector<int>& sl = rowslots[r - r0];
-                    for (int j = 0; j < (int)sl.size(); ++j) {
-                        const size_t at = base + (size_t)32 * (j / 2) + 2 * (r - r0) + (j & 1);
-                        ssrc[at] = sl[j];
-                        slc[at] = sl[j] >= 0 ? S.h_lcol[sl[j]] : (unsigned short)win_own[c];
-                    }
-                }
-                ch_rel += nch;
             }
+        }
+        if (not_contig) return fail(ctx, HSC_ERR_INVALID, "a part's rows are not contiguous in its window");
+        for (int c = 0; c < G; ++c) {
+            sslice.insert(sslice.end(), c_slice[c].begin(), c_slice[c].end());
+            ssrc.insert(ssrc.end(), c_src[c].begin(), c_src[c].end());
+            slc.insert(slc.end(), c_lc[c].begin(), c_lc[c].end());
+            const int ch_rel = (int)(c_src[c].size() / 32);
             cslice[c + 1] = (int)sslice.size();
             cchunk[c + 1] = cchunk[c] + ch_rel;
             NS = std::max(NS, cslice[c + 1] - cslice[c]);
