@@ -309,7 +309,19 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
             auto mix = [&](unsigned long long v) { h = (h ^ v) * 1099511628211ull; };
             mix((unsigned long long)S.n); mix((unsigned long long)nparts);
             for (int i = 0; i <= S.n; ++i) mix((unsigned long long)aptr[i]);
-            for (int v : adj) mix((unsigned long long)v);
+            {  // the adjacency in 16 chunks hashed apart (in parallel), then their hashes in order
+                constexpr int kChunks = 16;
+                const size_t na = adj.size();
+                unsigned long long hc[kChunks];
+#pragma omp parallel for schedule(static) if (na >= (1u << 16))
+                for (int q = 0; q < kChunks; ++q) {
+                    unsigned long long g = 1469598103934665603ull;
+                    for (size_t e = na * q / kChunks; e < na * (q + 1) / kChunks; ++e)
+                        g = (g ^ (unsigned long long)adj[e]) * 1099511628211ull;
+                    hc[q] = g;
+                }
+                for (int q = 0; q < kChunks; ++q) mix(hc[q]);
+            }
             for (int i = 0; i < S.n; ++i) mix((unsigned long long)cnt[i]);
             unsigned long long cwb;
             std::memcpy(&cwb, &cw, sizeof cwb);
@@ -341,11 +353,21 @@ int analyze(hsc_ctx* ctx, System& S, const hsc_bcoo3& M, const hsc_dof_layout& L
         S.h_iperm.assign(S.n, 0);
         // inside a part, nodes by decreasing block count (ties by index): rows of similar length sit
         // together, so the 32-row slices of the block preconditioner's layout carry little padding
+        // (a counting sort by part keeps the index order inside a part; each part is then sorted
+        // stably by block count, in parallel)
         std::vector<int> order(S.n);
-        for (int i = 0; i < S.n; ++i) order[i] = i;
-        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-            return part[x] != part[y] ? part[x] < part[y] : cnt[x] > cnt[y];
-        });
+        {
+            const int np = 1 + *std::max_element(part.begin(), part.end());
+            std::vector<int> pstart(np + 1, 0);
+            for (int i = 0; i < S.n; ++i) pstart[part[i] + 1]++;
+            for (int q = 0; q < np; ++q) pstart[q + 1] += pstart[q];
+            std::vector<int> fillq(pstart.begin(), pstart.end() - 1);
+            for (int i = 0; i < S.n; ++i) order[fillq[part[i]]++] = i;
+#pragma omp parallel for schedule(dynamic, 4) if (np >= 16)
+            for (int q = 0; q < np; ++q)
+                std::stable_sort(order.begin() + pstart[q], order.begin() + pstart[q + 1],
+                                 [&](int x, int y) { return cnt[x] > cnt[y]; });
+        }
         for (int ni = 0; ni < S.n; ++ni) {
             S.h_perm[ni] = order[ni];
             S.h_iperm[order[ni]] = ni;
