@@ -9,11 +9,15 @@ its rim body and 5-15 % tread contacts to the ground body, made by
 ``hsc_reimpl_b200.systems.make_reference_vehicle_system`` from a seed.  On this
 mesh lambda_max(Dd^-1 D) = 3.89, so the Neumann step is omega = 0.5 (the
 reference's 0.7 makes the order-2 polynomial indefinite here: PCG breaks down
-at iteration 3).  A step is one full HSC solve through the public API (``HSCContext.solve`` ->
-``hsc_solve``): BCOO->BSR fill, Dd^-1, coupling extraction, ACA, ABD inverse,
-reduced core, the persistent Schur PCG to a relative Schur residual of 1e-6,
-back-substitution and the FP64 full-system residual check, which every
-timed solve must pass at |b - H x| / |b| <= 1e-6.
+at iteration 3).  A step is one full HSC solve through the public API: BCOO->BSR fill, Dd^-1,
+coupling extraction, ACA, ABD inverse, reduced core, the persistent Schur PCG to a relative Schur
+residual of 1e-6, back-substitution and the FP64 full-system residual check, which every timed
+solve must pass at |b - H x| / |b| <= 1e-6.  The timed solves replay the solve's captured CUDA
+graph (``HSCContext.solve_batch(use_graph=True)`` -> ``hsc_solve_batch``: one capture per pattern,
+as a Newton loop with a fixed pattern would use it; ``--no-graph`` times ``hsc_solve``'s direct
+launches); per-stage device times and the kernel count come from one direct solve after the timed
+loop (a replay runs the kernels of its capture).  ``e2e`` goes through ``hsc_solve`` with host
+buffers.
 
 Modes: ``fp64`` (plain FP64 Neumann order 2, the bar) and ``fp32`` (FP32
 bulk SpMV/Neumann with FP64 coupled-node blocks, FP64 residual replacement
@@ -72,6 +76,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-other", action="store_true", help="skip the annulus-tire workload lines")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="time each solve as direct launches (hsc_solve) instead of the replay of its captured "
+                         "CUDA graph (hsc_solve_batch with use_graph)")
     ap.add_argument("--block-poly", default=None,
                     help="the block modes' polynomial by tuner candidate name (e.g. 'cheb6 a=0.5 b=3.9'), "
                          "skipping the per-system tuning (profiling runs)")
@@ -286,35 +293,49 @@ def time_modes(args, s, ds, ctx_holder, mode_opts, flush, dist, dev, lib, sample
             ctx.set_learned_model(ctx_holder[1])
         ctx.set_options(opt)
         x = torch.empty_like(ds.b)
+        graph = not args.no_graph
+        stream = torch.cuda.Stream()
+
+        def one_solve():
+            if graph:  # the captured graph of this pattern, replayed (captured in the first warm-up)
+                xs_, sts = ctx.solve_batch([ds], xs=[x], use_graph=True, stream=stream, raise_on_error=False)
+                return sts[0]
+            return ctx.solve(ds, x=x, stream=stream, raise_on_error=False)[1]
+
         for _ in range(args.warmup):
-            ctx.solve(ds, x=x, raise_on_error=False)
+            one_solve()
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
         sampler = ClockSampler(dev.index) if (mi == 0 and sample_clocks) else None
         if sampler:
             sampler.start()
-        l0 = lib.hsc_kernel_launches()
-        total_ms, pcg_ms, stats_all = 0.0, 0.0, []
+        total_ms, stats_all = 0.0, []
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         for _ in range(steps):
             flush.zero_()
             torch.cuda.synchronize()
-            ev0.record()
-            _, st = ctx.solve(ds, x=x, raise_on_error=False)
-            ev1.record()
+            ev0.record(stream)
+            st = one_solve()
+            ev1.record(stream)
             torch.cuda.synchronize()
             total_ms += ev0.elapsed_time(ev1)
-            pcg_ms += st["pcg_ms"]
             stats_all.append(st)
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
         if sampler:
             clocks = sampler.stop()
+        # the per-stage device times and the kernel count of one solve come from a direct (uncaptured)
+        # solve after the timed loop: a replay runs the same kernels as its capture
+        l0 = lib.hsc_kernel_launches()
+        st_plain = ctx.solve(ds, x=x, stream=stream, raise_on_error=False)[1]
+        torch.cuda.synchronize()
+        per_solve = lib.hsc_kernel_launches() - l0
+        pcg_ms = st_plain["pcg_ms"] * steps
         if mi == 0:
-            launches = lib.hsc_kernel_launches() - l0
+            launches = per_solve * steps
         total_ms = max_over_ranks(total_ms, dist, dev)
         last = stats_all[-1]
         xs = x.cpu().numpy()
@@ -337,8 +358,9 @@ def time_modes(args, s, ds, ctx_holder, mode_opts, flush, dist, dev, lib, sample
             "fallback": last.get("fallback", 0),
             "rank": last["rank"], "active_fem_dofs": last["active_fem_dofs"],
             "residual_replacements": last["residual_replacements"],
-            "stage_ms": [round(v, 4) for v in last["stage_ms"]],
-            "setup_ms": last["setup_ms"], "pcg_ms": pcg_launch_ms,
+            "stage_ms": [round(v, 4) for v in st_plain["stage_ms"]],
+            "setup_ms": st_plain["setup_ms"], "pcg_ms": pcg_launch_ms, "graph_replay": graph,
+            "kernel_launches_per_solve": per_solve,
             "pcg_us_per_iteration": 1000.0 * pcg_launch_ms / max(1, iters),
             "pcg_bytes_per_iteration": bytes_iter,
         }
