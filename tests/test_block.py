@@ -151,3 +151,52 @@ def test_block_plan_on_tire_mesh(api, torch, tire):
     assert plan["stage_vals"] == 1
     assert 1 <= plan["NYC"] <= plan["NCOL"]
     assert max(plan["smem"], plan["smem_y"]) <= 227 * 1024
+
+
+def test_block_graph_replay_matches_direct_solve(api, torch, tire):
+    """The block solve captured into a CUDA graph (hsc_solve_batch with use_graph) and replayed gives
+    the direct solve's x bit for bit: the same kernels in the same order, side stream included."""
+    ctx = api.HSCContext(_block_opts(api, precision="fp32"))
+    ds = api.DeviceSystem.from_system(tire)
+    x1, st1 = ctx.solve(ds)
+    x1 = x1.clone()
+    stream = torch.cuda.Stream()
+    x = torch.empty_like(ds.b)
+    for _ in range(3):  # capture, then two replays
+        with torch.cuda.stream(stream):
+            xs, sts = ctx.solve_batch([ds], xs=[x], use_graph=True, stream=stream)
+        torch.cuda.synchronize()
+        assert sts[0]["status"] == 0 and sts[0]["pcg_iterations"] == st1["pcg_iterations"]
+        assert torch.equal(x, x1)
+
+
+def _coupled_nodes(system):
+    import scipy.sparse as sp
+    qo, qm, fo, fn = system.layout
+    E = sp.csr_matrix(system.H)[qo:qo + qm, fo:fo + fn].tocoo()
+    mask = np.zeros(fn // 3, bool)
+    mask[E.col[E.data != 0] // 3] = True
+    return mask
+
+
+def test_coupled_part_weight_shrinks_the_coupled_parts(api, torch, tire):
+    """A second partition pass with the coupled parts' nodes weighted makes those parts smaller
+    (their mean row count drops) and the others larger; both partitions solve to the target."""
+    coupled = _coupled_nodes(tire)
+    means = {}
+    for cw in (1.0, 1.2):
+        ctx = api.HSCContext(_block_opts(api, precision="fp32", coupled_part_weight=cw))
+        _, st = ctx.solve(api.DeviceSystem.from_system(tire))
+        assert st["status"] == 0 and st["full_relative_residual"] <= 1e-6
+        perm, ptr = ctx.partition()
+        rows = np.diff(ptr)
+        hot = np.array([coupled[perm[ptr[p]:ptr[p + 1]]].any() for p in range(len(ptr) - 1)])
+        assert hot.any() and (~hot).any()
+        means[cw] = (rows[hot].mean(), rows[~hot].mean())
+    assert means[1.2][0] < means[1.0][0]
+    assert means[1.2][1] > means[1.0][1]
+
+
+def test_coupled_part_weight_is_validated(api, torch):
+    with pytest.raises(api.HSCError):
+        api.HSCContext(_block_opts(api, coupled_part_weight=0.5))
