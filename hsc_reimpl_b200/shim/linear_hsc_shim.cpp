@@ -34,6 +34,7 @@ class LinearHSC final : public IterativeSolver {
   private:
     ABDLinearSubsystem* abd = nullptr;
     FEMLinearSubsystem* fem = nullptr;
+    GlobalTrajectoryFilter* contacts = nullptr;  // active contact counts for the record (linear_hsc.cu:179)
     hsc_ctx* ctx = nullptr;
     hsc_options opt{};
     hsc_stats stats{};
@@ -48,6 +49,7 @@ class LinearHSC final : public IterativeSolver {
         if (!attr || attr->view()[0] != "linear_hsc") throw SimSystemException("LinearHSC unused");
         abd = &require<ABDLinearSubsystem>();
         fem = &require<FEMLinearSubsystem>();
+        contacts = &require<GlobalTrajectoryFilter>();
         hsc_options_reference(&opt);  // linear_hsc.cu:162-164, integration.patch:33-54
         opt.max_rank = key<IndexT>("linear_system/hsc/max_rank", opt.max_rank);
         opt.neumann_order = key<IndexT>("linear_system/hsc/neumann_order", opt.neumann_order);
@@ -79,20 +81,26 @@ class LinearHSC final : public IterativeSolver {
     }
 
     void append_record(int rc) {
+        // active contacts as the reference counts them (linear_hsc.cu:410-414): simplex pairs
+        // PT + EE + PE + PP, vertex-half-plane pairs PH
+        size_t mesh_contacts = 0, ground_contacts = 0;
+        if (auto sf = contacts->find<SimplexTrajectoryFilter>())
+            mesh_contacts = sf->PTs().size() + sf->EEs().size() + sf->PEs().size() + sf->PPs().size();
+        if (auto gf = contacts->find<VertexHalfPlaneTrajectoryFilter>()) ground_contacts = gf->PHs().size();
         std::ofstream out(workspace() + "/hsc_stats.jsonl", std::ios::app);
         char buf[2048];
         std::snprintf(buf, sizeof buf,
                       "{\"frame\":%zu,\"newton\":%zu,\"fem_dofs\":%d,\"abd_dofs\":%d,\"active_fem_dofs\":%d,"
                       "\"rank\":%d,\"aca_relative_error\":%.17g,\"pcg_iterations\":%d,"
                       "\"schur_relative_residual\":%.17g,\"full_relative_residual\":%.17g,\"setup_ms\":%.6g,"
-                      "\"total_ms\":%.6g,\"active_mesh_contacts\":0,\"active_ground_contacts\":0,"
+                      "\"total_ms\":%.6g,\"active_mesh_contacts\":%zu,\"active_ground_contacts\":%zu,"
                       "\"adaptive_abd_inverse\":%s,\"neumann_doublings\":%d,\"abd_inverse_residual\":%.17g,"
                       "\"full_residual_limit\":%.17g,\"accepted\":%s,\"solver\":\"linear_hsc\",\"fallback\":%s,"
                       "\"precision_mode\":\"%s\",\"preconditioner\":\"%s\",\"refinement_steps\":%d,"
                       "\"pcg_ms\":%.6g,\"lanczos_min\":%.17g,\"lanczos_max\":%.17g}\n",
                       engine().frame, engine().newton, stats.fem_dofs, stats.abd_dofs, stats.active_fem_dofs,
                       stats.rank, stats.aca_relative_error, stats.pcg_iterations, stats.schur_relative_residual,
-                      stats.full_relative_residual, stats.setup_ms, stats.total_ms,
+                      stats.full_relative_residual, stats.setup_ms, stats.total_ms, mesh_contacts, ground_contacts,
                       opt.abd_inverse == HSC_ABD_ADAPTIVE ? "true" : "false", stats.neumann_doublings,
                       stats.abd_inverse_residual, opt.full_residual_limit, rc == HSC_OK ? "true" : "false",
                       stats.fallback ? "true" : "false",

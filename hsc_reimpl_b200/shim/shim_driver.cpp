@@ -1,6 +1,6 @@
 // Test driver of the LinearHSC shim: builds the plugin from key=value config
 // arguments and, given a system file, runs one do_solve on the GPU.
-//   shim_driver <workspace> <system.bin|-> [key=value ...]
+//   shim_driver <workspace> <system.bin|-> [key=value ...]   (contacts/PT|EE|PE|PP|PH=n: filter sizes)
 // system.bin: int64 nnzb, int32 nblock, qo, qm, fo, fn, then rows (int32),
 // cols (int32), values (9 doubles per triplet, column-major), b (doubles).
 // Writes x to <workspace>/x.bin.  Exit codes: 0 ok, 2 SimSystemException,
@@ -22,12 +22,23 @@ int main(int argc, char** argv) {
     if (argc < 3) return 4;
     Engine eng;
     eng.workspace = argv[1];
+    // contacts/PT, /EE, /PE, /PP give the scene a simplex filter, contacts/PH a half-plane filter
+    SimplexTrajectoryFilter simplex;
+    VertexHalfPlaneTrajectoryFilter half_plane;
     for (int i = 3; i < argc; ++i) {
         std::string kv = argv[i];
         auto eq = kv.find('=');
         std::string k = kv.substr(0, eq), v = kv.substr(eq + 1);
         if (k == "linear_system/solver") eng.w.sc.cfg.strs[k] = v;
-        else eng.w.sc.cfg.nums[k] = std::stod(v);
+        else if (k.rfind("contacts/", 0) == 0) {
+            const SizeT n = (SizeT)std::stoll(v);
+            if (k == "contacts/PH") { half_plane.ph = n; eng.contacts.half_plane = &half_plane; continue; }
+            if (k == "contacts/PT") simplex.pt = n;
+            else if (k == "contacts/EE") simplex.ee = n;
+            else if (k == "contacts/PE") simplex.pe = n;
+            else if (k == "contacts/PP") simplex.pp = n;
+            eng.contacts.simplex = &simplex;
+        } else eng.w.sc.cfg.nums[k] = std::stod(v);
     }
     auto plugin = make_LinearHSC(eng);
     try {

@@ -124,11 +124,40 @@ struct GlobalLinearSystem {
     };
 };
 
+// the contact filters the plugin counts for its record (sizes only): simplex pairs PT, EE, PE, PP
+// and vertex-half-plane pairs PH; GlobalTrajectoryFilter::find<T>() is null for a filter the scene
+// does not have
+struct Count {
+    SizeT n = 0;
+    SizeT size() const { return n; }
+};
+struct SimplexTrajectoryFilter {
+    SizeT pt = 0, ee = 0, pe = 0, pp = 0;
+    Count PTs() const { return {pt}; }
+    Count EEs() const { return {ee}; }
+    Count PEs() const { return {pe}; }
+    Count PPs() const { return {pp}; }
+};
+struct VertexHalfPlaneTrajectoryFilter {
+    SizeT ph = 0;
+    Count PHs() const { return {ph}; }
+};
+struct GlobalTrajectoryFilter {
+    SimplexTrajectoryFilter* simplex = nullptr;
+    VertexHalfPlaneTrajectoryFilter* half_plane = nullptr;
+    template <class T> T* find();
+};
+template <> inline SimplexTrajectoryFilter* GlobalTrajectoryFilter::find<SimplexTrajectoryFilter>() { return simplex; }
+template <> inline VertexHalfPlaneTrajectoryFilter* GlobalTrajectoryFilter::find<VertexHalfPlaneTrajectoryFilter>() {
+    return half_plane;
+}
+
 // the engine side the plugin reaches through SimSystem
 struct Engine {
     World w;
     ABDLinearSubsystem abd;
     FEMLinearSubsystem fem;
+    GlobalTrajectoryFilter contacts;
     std::string workspace = ".";
     SizeT frame = 0, newton = 0;
 };
@@ -147,6 +176,7 @@ class SimSystem {
 };
 template <> inline ABDLinearSubsystem& SimSystem::require<ABDLinearSubsystem>() { return m_engine.abd; }
 template <> inline FEMLinearSubsystem& SimSystem::require<FEMLinearSubsystem>() { return m_engine.fem; }
+template <> inline GlobalTrajectoryFilter& SimSystem::require<GlobalTrajectoryFilter>() { return m_engine.contacts; }
 
 class IterativeSolver : public SimSystem {
   public:

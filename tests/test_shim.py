@@ -89,3 +89,24 @@ def test_shim_solve_matches_python_plugin(driver, tmp_path, cube_system):
         assert rec[k] == ref[k], k
     assert rec["full_relative_residual"] == pytest.approx(ref["full_relative_residual"], rel=1e-12)
     assert np.linalg.norm(cube_system.H @ x_shim - cube_system.b) <= 1e-5 * np.linalg.norm(cube_system.b)
+
+
+@pytest.mark.gpu
+def test_shim_record_counts_active_contacts(driver, tmp_path, cube_system):
+    """The record's active contact counts come from the scene's trajectory filters as in the
+    reference (linear_hsc.cu:410-414): PT + EE + PE + PP simplex pairs, PH vertex-half-plane pairs;
+    a scene without a filter reports 0 for it."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    sysfile = tmp_path / "cube.bin"
+    write_system(sysfile, cube_system)
+    cases = [({"contacts/PT": 3, "contacts/EE": 2, "contacts/PE": 1, "contacts/PP": 4, "contacts/PH": 5}, 10, 5),
+             ({"contacts/PH": 7}, 0, 7), ({}, 0, 0)]
+    for i, (contacts, mesh, ground) in enumerate(cases):
+        ws = tmp_path / f"ws{i}"
+        ws.mkdir()
+        r = run(driver, ws, sysfile, config={**CONFIG, **contacts})
+        assert r.returncode == 0, r.stdout + r.stderr
+        rec = json.loads((ws / "hsc_stats.jsonl").read_text().splitlines()[-1])
+        assert rec["active_mesh_contacts"] == mesh and rec["active_ground_contacts"] == ground, rec
