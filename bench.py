@@ -372,9 +372,14 @@ def timed_e2e(args, ctx, opt, systems_dev, flush, dist, dev, repattern):
     (and of rows/cols when ``repattern``: two systems of different sparsity alternate, so every
     step pays the pattern analysis), the solve, D2H of x."""
     import torch
+    from dataclasses import replace
     from hsc_reimpl_b200.solver import DeviceSystem
     ws = dist.get_world_size() if dist is not None else 1
-    ctx.set_options(opt)
+    # a fixed pattern replays hsc_solve's captured graph (graph_replay, on a non-default stream); an
+    # alternating pattern is analysed again every step, so it launches directly
+    graph = not repattern and not args.no_graph
+    ctx.set_options(replace(opt, graph_replay=graph))
+    stream = torch.cuda.Stream()
     host = []
     for ds in systems_dev:
         host.append(dict(rows=ds.rows.cpu().pin_memory(), cols=ds.cols.cpu().pin_memory(),
@@ -393,6 +398,10 @@ def timed_e2e(args, ctx, opt, systems_dev, flush, dist, dev, repattern):
     fails = 0
 
     def step(i):
+        with torch.cuda.stream(stream):  # the copies, the solve and the read-back in one stream's order
+            step_on_stream(i)
+
+    def step_on_stream(i):
         nonlocal h2d, d2h, fails
         h = host[i % len(host)]
         src = systems_dev[i % len(host)]
@@ -405,7 +414,7 @@ def timed_e2e(args, ctx, opt, systems_dev, flush, dist, dev, repattern):
         b_d[:N].copy_(h["b"], non_blocking=True)
         ds2 = DeviceSystem(rows_d[:nz] if repattern else src.rows, cols_d[:nz] if repattern else src.cols,
                            vals_d[:nz], src.nblock, src.layout, b_d[:N])
-        _, st = ctx.solve(ds2, x=x_d[:N], raise_on_error=False)
+        _, st = ctx.solve(ds2, x=x_d[:N], stream=stream, raise_on_error=False)
         fails += st["status"] != 0
         x_h[:N].copy_(x_d[:N], non_blocking=True)
         h2d = (2 * nz * 4 if repattern else 0) + nz * 72 + N * 8
@@ -423,13 +432,14 @@ def timed_e2e(args, ctx, opt, systems_dev, flush, dist, dev, repattern):
     for i in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
-        ev0.record()
+        ev0.record(stream)
         step(i)
-        ev1.record()
+        ev1.record(stream)
         torch.cuda.synchronize()
         tot += ev0.elapsed_time(ev1)
     tot = max_over_ranks(tot, dist, dev)
     return {"value": replica_throughput(args.steps, ws, tot), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "graph_replay": graph,
             "d2h_bytes_per_step": int(d2h), "failed_solves": int(fails)}
 
 

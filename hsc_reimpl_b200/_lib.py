@@ -65,6 +65,7 @@ class Options(C.Structure):
         ("aca_components", C.c_int32),
         ("lanczos_stats", C.c_int32),
         ("coupled_part_weight", C.c_double),
+        ("graph_replay", C.c_int32),
     ]
 
 

@@ -235,6 +235,7 @@ int validate_options(const hsc_options* o, std::string& why) {
     }
     if (o->spin_limit < 1000) { why = "spin_limit too small"; return 0; }
     if (!(o->coupled_part_weight >= 1.0 && o->coupled_part_weight <= 8.0)) { why = "coupled_part_weight must be in [1, 8]"; return 0; }
+    if (o->graph_replay != 0 && o->graph_replay != 1) { why = "graph_replay must be 0 or 1"; return 0; }
     return 1;
 }
 
@@ -1938,6 +1939,7 @@ int hsc_options_default(hsc_options* o) {
     o->aca_components = 1;
     o->lanczos_stats = 0;
     o->coupled_part_weight = 1.2;
+    o->graph_replay = 0;
     return HSC_OK;
 }
 
@@ -2321,7 +2323,8 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
 int hsc_solve(hsc_ctx* ctx, const hsc_bcoo3* A, const hsc_dof_layout* layout, const double* d_b, double* d_x,
               void* stream, hsc_stats* out) {
     if (!ctx || !A || !layout || !d_b || !d_x) return HSC_ERR_INVALID;
-    int rc = solve_impl(ctx, 1, A, layout, &d_b, &d_x, 0, (cudaStream_t)stream, out, 0);
+    const int graph = ctx->opt.graph_replay && stream != nullptr ? 1 : 0;
+    int rc = solve_impl(ctx, 1, A, layout, &d_b, &d_x, graph, (cudaStream_t)stream, out, 0);
     if (rc && out && out->status == 0) out->status = rc;
     return rc;
 }

@@ -69,6 +69,7 @@ class HSCOptions:
     aca_components: bool = True            # ACA per coupling component, merged (same factors as global)
     lanczos_stats: bool = False            # Ritz extremes of every solve (always on for the learned forms)
     coupled_part_weight: float = 1.2       # block forms: weight of the coupled parts' nodes in a second partition pass
+    graph_replay: bool = False             # solve(): replay the captured CUDA graph (needs a non-default stream)
 
     @classmethod
     def reference(cls):
@@ -129,6 +130,7 @@ class HSCOptions:
         o.aca_components = int(bool(self.aca_components))
         o.lanczos_stats = int(bool(self.lanczos_stats))
         o.coupled_part_weight = float(self.coupled_part_weight)
+        o.graph_replay = int(bool(self.graph_replay))
         return o
 
 

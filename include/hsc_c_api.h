@@ -149,6 +149,11 @@ typedef struct hsc_options {
                                     work on every row), so they come out smaller; 1: one pass.  The
                                     partition is cached per FEM pattern: a contact change reuses it.
                                     Default 1.2 */
+    int32_t graph_replay;        /* 1: hsc_solve on a non-default stream captures its numeric phase into a CUDA
+                                    graph once per pattern (and pointers, options) and replays it (one launch
+                                    instead of ~44; the per-stage times in hsc_stats are then 0, total_ms
+                                    stays); 0 (default): direct launches.  Not with refinement or the
+                                    adaptive ABD inverse (their host decisions run between launches) */
 } hsc_options;
 
 typedef struct hsc_stats {        /* superset of the hsc_stats.jsonl record (linear_hsc.cu:420-431) */
@@ -202,7 +207,9 @@ HSC_EXPORT const char* hsc_last_error(const hsc_ctx* ctx);
 /* do_solve: x = HSC(A, b).  The sparsity analysis is cached while the A
  * pointers, nnzb, nblock and layout stay the same; a changed pattern behind
  * the same pointers is detected on the device and triggers a fresh analysis.
- * `stream` is a cudaStream_t (NULL = legacy default stream). */
+ * `stream` is a cudaStream_t (NULL = legacy default stream).  With the
+ * graph_replay option and a non-default stream the solve replays its
+ * captured CUDA graph. */
 HSC_EXPORT int hsc_solve(hsc_ctx* ctx, const hsc_bcoo3* A, const hsc_dof_layout* layout,
               const double* d_b, double* d_x, void* stream, hsc_stats* out);
 
