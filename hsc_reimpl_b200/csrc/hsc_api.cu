@@ -2317,6 +2317,40 @@ static int solve_impl(hsc_ctx* ctx, int count, const hsc_bcoo3* A, const hsc_dof
         if (out) { out[0].fallback = 1; out[0].pcg_iterations += iters_first; }
         return r;
     }
+    // in a batch, the stalled systems alone are solved again with the plain Neumann series (one
+    // sub-batch, direct launches; their stats replace theirs, the iterations add up)
+    if (count > 1 && out && !refine && depth == 0 && o.fallback_on_stall && o.preconditioner != HSC_PRECOND_NEUMANN &&
+        o.preconditioner != HSC_PRECOND_BLOCK && o.preconditioner != HSC_PRECOND_BLOCK_LEARNED) {
+        std::vector<int> bad;
+        for (int s = 0; s < count; ++s)
+            if (out[s].status == HSC_ERR_BREAKDOWN || out[s].status == HSC_ERR_NOCONV) bad.push_back(s);
+        if (!bad.empty()) {
+            const int nb = (int)bad.size();
+            std::vector<hsc_bcoo3> Ab(nb);
+            std::vector<hsc_dof_layout> Lb(nb);
+            std::vector<const double*> bb(nb);
+            std::vector<double*> xb(nb);
+            std::vector<hsc_stats> ob(nb);
+            for (int i = 0; i < nb; ++i) { Ab[i] = A[bad[i]]; Lb[i] = lay[bad[i]]; bb[i] = d_b[bad[i]]; xb[i] = d_x[bad[i]]; }
+            const hsc_options saved = ctx->opt;
+            ctx->opt.preconditioner = HSC_PRECOND_NEUMANN;
+            ctx->part_key_gen = -1;
+            if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+            solve_impl(ctx, nb, Ab.data(), Lb.data(), bb.data(), xb.data(), 0, st, ob.data(), depth + 1);
+            ctx->opt = saved;
+            ctx->part_key_gen = -1;
+            if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+            for (int i = 0; i < nb; ++i) {
+                const int iters_first = out[bad[i]].pcg_iterations;
+                out[bad[i]] = ob[i];
+                out[bad[i]].fallback = 1;
+                out[bad[i]].pcg_iterations += iters_first;
+            }
+            worst = HSC_OK;
+            for (int s = 0; s < count; ++s)
+                if (out[s].status && !worst) worst = out[s].status;
+        }
+    }
     return worst;
 }
 

@@ -353,3 +353,29 @@ def test_trained_model_beats_neumann_on_held_out_vehicle_steps(api, torch):
     assert np.all(res["learned"]["full"] <= 1e-6 * 1.01)
     assert le < 0.7 * n2
     assert le < n8
+
+
+@pytest.mark.gpu
+def test_learned_batch_falls_back_per_system(api, torch):
+    """In a batch, the systems whose learned polynomial stalls are solved again with the plain
+    Neumann series (a sub-batch); their stats say so and carry the iterations of both attempts."""
+    s, ds = _cube(api)
+    opts = dict(omega=2 / 3, aca_rtol=1e-4, abd_inverse="exact")
+    bits, _ = random_params(41, scale=0.1)
+    ctx = api.HSCContext(api.HSCOptions(learned=True, max_iter=3, **opts))
+    ctx.set_learned_model(bits)
+    _, sts = ctx.solve_batch([ds, ds], raise_on_error=False)
+    from hsc_reimpl_b200 import _lib
+    for st in sts:
+        assert st["fallback"] == 1 and st["status"] == _lib.HSC_ERR_NOCONV  # the redo also stops at max_iter
+    # an indefinite polynomial (negative above mu = 1): every system ends converged
+    p = np.zeros(LO.NPARAM, np.float32)
+    w_bad = np.array([1e-3, 0, 0, 0, 0, 0, 0, 1e5])
+    wb = np.maximum(w_bad, 1e-12)
+    p[LO.OFF_B3:] = np.where(wb > 20, wb, np.log(np.expm1(np.minimum(wb, 20))))
+    ctx2 = api.HSCContext(api.HSCOptions(learned=True, **opts))
+    ctx2.set_learned_model(LO.bf16_round(p))
+    xs, sts = ctx2.solve_batch([ds, ds], raise_on_error=False)
+    for x, st in zip(xs, sts):
+        assert st["status"] == 0
+        assert np.linalg.norm(s.H @ x.cpu().numpy() - s.b) <= 1e-5 * np.linalg.norm(s.b)
