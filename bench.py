@@ -29,7 +29,7 @@ vectors and arithmetic; the polynomial is chosen per system by
 ``autotune.tune_block`` before any timing, ``block_tuning`` lists the candidates).  ``value`` is the flagship mode
 (the fastest one that met the FP64-verified residual); every mode's numbers
 are in ``modes``.  ``other_workloads`` repeats fp64/fp32 on the structured
-annulus tires (``make_vehicle_system``).  ``e2e_repattern`` is ``e2e`` with a
+annulus tires (``make_vehicle_system``) and the reference's C1 cube case.  ``e2e_repattern`` is ``e2e`` with a
 different sparsity pattern every step (two seeds alternate), so the pattern
 analysis is inside the timed region.
 
@@ -549,6 +549,10 @@ def run_gpu(args):
                               steps=min(args.steps, 10))
         other = {"vehicle_annulus_78k_tets": {"nodes": sa.meta["nodes"], "fem_dofs": sa.layout[3], "omega": 0.7,
                                               "modes": om}}
+        # C1, the reference's cube case (1,331 nodes, FP64 Neumann order 2): 20 timed solves, the error
+        # against the FP64 direct solve
+        from hsc_reimpl_b200 import bench_configs
+        other["cube_c1"] = bench_configs.c1(flush)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(s)
