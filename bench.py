@@ -492,7 +492,8 @@ def run_gpu(args):
         if best is not None:
             mode_opts["block32"] = best
             mode_opts["block64"] = replace(best, precision="fp64")
-            chosen = min((r for r in table if r["ok"]), key=lambda r: r["ms"])
+            wb = [round(v, 6) for v in best.poly_weights]
+            chosen = next(r for r in table if r["ok"] and r["omega"] == best.omega and r["weights"] == wb)
             tuning = {"chosen": chosen["name"], "weights": chosen["weights"], "omega": chosen["omega"],
                       "candidates": [{k: r[k] for k in ("name", "ms", "iterations", "ok")} for r in table]}
     from hsc_reimpl_b200 import learned as L

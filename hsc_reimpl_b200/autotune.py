@@ -67,10 +67,14 @@ def autotune(systems, base: HSCOptions | None = None, tiles=TILES, ranks=RANKS, 
         table.append(rec)
         if log:
             log(json.dumps(rec))
-        if ok and (best is None or ms < best[1]):
-            best = (opt, ms)
+        if ok:
+            passed.append((ms, st["pcg_iterations"], len(passed), opt))
         ctx.close()
-    return (best[0] if best else None), table
+    if not passed:
+        return None, table
+    fastest = min(p[0] for p in passed)
+    tied = [p for p in passed if p[0] <= fastest * (1.0 + tie)]
+    return min(tied, key=lambda p: (p[1], p[0], p[2]))[3], table
 
 
 # ---------------------------------------------------------------------------
@@ -129,15 +133,17 @@ def time_solve(ctx, ds, reps=3, warmup=1):
     return float(np.median(times)), st
 
 
-def tune_block(system, base: HSCOptions | None = None, candidates=None, target=1e-6, reps=3, log=None):
+def tune_block(system, base: HSCOptions | None = None, candidates=None, target=1e-6, reps=3, log=None, tie=0.01):
     """Times every candidate polynomial of the block preconditioner on this system and returns
     (options of the fastest one whose solve met ``target`` on the FP64-verified full residual,
-    table of every candidate).  A tuned polynomial is a property of the system family (mesh,
+    table of every candidate).  Candidates within ``tie`` (relative) of the fastest time count as
+    tied and the one with the fewest PCG iterations wins, so timing noise does not flip the choice
+    between near-equal polynomials.  A tuned polynomial is a property of the system family (mesh,
     materials, coupling), so a Newton loop tunes once and reuses it."""
     base = base or HSCOptions(block=True, precision="fp32", tol=1e-6, abd_inverse="exact")
     ds = system if isinstance(system, DeviceSystem) else DeviceSystem.from_system(system)
     cands = candidates if candidates is not None else block_candidates()
-    table, best = [], None
+    table, passed = [], []
     for name, w, om in cands:
         opt = replace(base, block=True, poly_weights=tuple(w), omega=om, fallback_on_stall=False)
         ctx = HSCContext(opt)
@@ -148,7 +154,11 @@ def tune_block(system, base: HSCOptions | None = None, candidates=None, target=1
         table.append(rec)
         if log:
             log(json.dumps(rec))
-        if ok and (best is None or ms < best[1]):
-            best = (opt, ms)
+        if ok:
+            passed.append((ms, st["pcg_iterations"], len(passed), opt))
         ctx.close()
-    return (best[0] if best else None), table
+    if not passed:
+        return None, table
+    fastest = min(p[0] for p in passed)
+    tied = [p for p in passed if p[0] <= fastest * (1.0 + tie)]
+    return min(tied, key=lambda p: (p[1], p[0], p[2]))[3], table

@@ -40,7 +40,8 @@ def test_tune_block_picks_a_converged_candidate_no_slower_than_neumann4():
     assert best is not None and len(table) == 3
     ok = [r for r in table if r["ok"]]
     assert ok, table
-    chosen = min(ok, key=lambda r: r["ms"])
-    assert tuple(best.poly_weights) == tuple(round(v, 6) for v in chosen["weights"]) or \
-        np.allclose(best.poly_weights, chosen["weights"], rtol=1e-5)
-    assert chosen["ms"] <= next(r["ms"] for r in table if r["name"] == "neumann4 omega=0.5")
+    # the fastest, or among those within 1 % of it the one with the fewest iterations
+    fastest = min(r["ms"] for r in ok)
+    chosen = min((r for r in ok if r["ms"] <= 1.01 * fastest), key=lambda r: (r["iterations"], r["ms"]))
+    assert np.allclose(best.poly_weights, chosen["weights"], rtol=1e-5) and best.omega == chosen["omega"]
+    assert chosen["ms"] <= 1.01 * next(r["ms"] for r in table if r["name"] == "neumann4 omega=0.5")
