@@ -609,42 +609,43 @@ __global__ void __launch_bounds__(1024) gj_inverse_blocks_kernel(const double* A
             w[r][c] = (i < mb && j < mb) ? A[(size_t)gi[r] * m + gj[c]] : 0.0;
         }
     if (threadIdx.x == 0) s_bad = 0;
-    for (int k = 0; k < mb; ++k) {
-        const int b = k & 1, kk = k >> 5, ko = k & 31;
-        double ci[kGbR];
+    // the 32-step blocks unrolled: the pivot's register (entry kk of a thread's rows and columns)
+    // is a compile-time index, so no run-time select sits on a step's path
 #pragma unroll
-        for (int r = 0; r < kGbR; ++r) ci[r] = __shfl_sync(0xffffffffu, sel3(w[r], kk), ko);  // column k
-        if (ty == ko) {  // the pivot row's warp publishes it, its pivot lane the reciprocal
+    for (int kk = 0; kk < kGbR; ++kk) {
+        for (int ko = 0; ko < 32; ++ko) {
+            const int k = 32 * kk + ko;
+            if (k >= mb) break;  // uniform
+            const int b = k & 1;
+            double ci[kGbR];
 #pragma unroll
-            for (int c = 0; c < kGbR; ++c) s_row[b][tx + 32 * c] = kk == 0 ? w[0][c] : (kk == 1 ? w[1][c] : w[2][c]);
+            for (int r = 0; r < kGbR; ++r) ci[r] = __shfl_sync(0xffffffffu, w[r][kk], ko);  // column k
+            if (ty == ko) {  // the pivot row's warp publishes it, its pivot lane the reciprocal
+#pragma unroll
+                for (int c = 0; c < kGbR; ++c) s_row[b][tx + 32 * c] = w[kk][c];
+                if (tx == ko) {
+                    double pv = ci[kk];
+                    if (!(pv > 0.0) || !isfinite(pv)) { s_bad = 1; pv = 1.0; }
+                    s_rp[b] = 1.0 / pv;
+                }
+            }
+            __syncthreads();
+            const double rp = s_rp[b];
+            double rs[kGbR];
+#pragma unroll
+            for (int c = 0; c < kGbR; ++c) rs[c] = s_row[b][tx + 32 * c] * rp;  // pivot row / pivot
+#pragma unroll
+            for (int r = 0; r < kGbR; ++r)
+#pragma unroll
+                for (int c = 0; c < kGbR; ++c) w[r][c] = fma(-ci[r], rs[c], w[r][c]);
+            // the owners of column k and row k overwrite theirs: -c_i / p, row_j / p, 1 / p
             if (tx == ko) {
-                double pv = sel3(ci, kk);
-                if (!(pv > 0.0) || !isfinite(pv)) { s_bad = 1; pv = 1.0; }
-                s_rp[b] = 1.0 / pv;
+#pragma unroll
+                for (int r = 0; r < kGbR; ++r) w[r][kk] = -ci[r] * rp;
             }
-        }
-        __syncthreads();
-        const double rp = s_rp[b];
-        double rs[kGbR];
+            if (ty == ko) {
 #pragma unroll
-        for (int c = 0; c < kGbR; ++c) rs[c] = s_row[b][tx + 32 * c] * rp;  // pivot row / pivot
-#pragma unroll
-        for (int r = 0; r < kGbR; ++r)
-#pragma unroll
-            for (int c = 0; c < kGbR; ++c) w[r][c] = fma(-ci[r], rs[c], w[r][c]);
-        // the owners of column k and row k overwrite theirs: -c_i / p, row_j / p, 1 / p
-        if (tx == ko) {
-#pragma unroll
-            for (int r = 0; r < kGbR; ++r) {
-                const double v = -ci[r] * rp;
-                if (kk == 0) w[r][0] = v; else if (kk == 1) w[r][1] = v; else w[r][2] = v;
-            }
-        }
-        if (ty == ko) {
-#pragma unroll
-            for (int c = 0; c < kGbR; ++c) {
-                const double v = (tx + 32 * c == k) ? rp : rs[c];
-                if (kk == 0) w[0][c] = v; else if (kk == 1) w[1][c] = v; else w[2][c] = v;
+                for (int c = 0; c < kGbR; ++c) w[kk][c] = (tx + 32 * c == k) ? rp : rs[c];
             }
         }
     }
@@ -680,36 +681,39 @@ __global__ void __launch_bounds__(1024) ldlt_reg_kernel(const double* C, int kma
             w[r][c] = (i < k && l < k && l <= i) ? 0.5 * (C[(size_t)i * kmax + l] + C[(size_t)l * kmax + i]) : 0.0;
         }
     if (threadIdx.x == 0) s_bad = 0;
-    for (int j = 0; j < k; ++j) {
-        const int b = j & 1, jj = j >> 5, jo = j & 31;
-        double ci[kGbR];
+    // the 32-step blocks unrolled: the pivot column's register is a compile-time index
 #pragma unroll
-        for (int r = 0; r < kGbR; ++r) ci[r] = __shfl_sync(0xffffffffu, sel3(w[r], jj), jo);  // W[i][j]
-        if (tx < kGbR) s_col[b][ty + 32 * tx] = sel3(ci, tx);
-        if (ty == jo && tx == jo) {
-            const double dj = sel3(ci, jj);
-            const bool okj = isfinite(dj) && dj != 0.0;
-            if (!okj) s_bad = 1;
-            s_rd[b] = 1.0 / (okj ? dj : 1.0);
-        }
-        __syncthreads();
-        const double rd = s_rd[b];
-        double cl[kGbR];
+    for (int jj = 0; jj < kGbR; ++jj) {
+        for (int jo = 0; jo < 32; ++jo) {
+            const int j = 32 * jj + jo;
+            if (j >= k) break;  // uniform
+            const int b = j & 1;
+            double ci[kGbR];
 #pragma unroll
-        for (int c = 0; c < kGbR; ++c) cl[c] = (tx + 32 * c > j) ? s_col[b][tx + 32 * c] : 0.0;
+            for (int r = 0; r < kGbR; ++r) ci[r] = __shfl_sync(0xffffffffu, w[r][jj], jo);  // W[i][j]
+            if (tx < kGbR) s_col[b][ty + 32 * tx] = sel3(ci, tx);
+            if (ty == jo && tx == jo) {
+                const double dj = ci[jj];
+                const bool okj = isfinite(dj) && dj != 0.0;
+                if (!okj) s_bad = 1;
+                s_rd[b] = 1.0 / (okj ? dj : 1.0);
+            }
+            __syncthreads();
+            const double rd = s_rd[b];
+            double cl[kGbR];
 #pragma unroll
-        for (int r = 0; r < kGbR; ++r) {
-            const double wij = (ty + 32 * r > j) ? ci[r] * rd : 0.0;
+            for (int c = 0; c < kGbR; ++c) cl[c] = (tx + 32 * c > j) ? s_col[b][tx + 32 * c] : 0.0;
 #pragma unroll
-            for (int c = 0; c < kGbR; ++c) w[r][c] = fma(-wij, cl[c], w[r][c]);
-        }
-        if (tx == jo) {  // column j becomes L[:, j] below the diagonal
+            for (int r = 0; r < kGbR; ++r) {
+                const double wij = (ty + 32 * r > j) ? ci[r] * rd : 0.0;
 #pragma unroll
-            for (int r = 0; r < kGbR; ++r)
-                if (ty + 32 * r > j) {
-                    const double v = ci[r] * rd;
-                    if (jj == 0) w[r][0] = v; else if (jj == 1) w[r][1] = v; else w[r][2] = v;
-                }
+                for (int c = 0; c < kGbR; ++c) w[r][c] = fma(-wij, cl[c], w[r][c]);
+            }
+            if (tx == jo) {  // column j becomes L[:, j] below the diagonal
+#pragma unroll
+                for (int r = 0; r < kGbR; ++r)
+                    if (ty + 32 * r > j) w[r][jj] = ci[r] * rd;
+            }
         }
     }
     __syncthreads();
