@@ -67,14 +67,10 @@ def autotune(systems, base: HSCOptions | None = None, tiles=TILES, ranks=RANKS, 
         table.append(rec)
         if log:
             log(json.dumps(rec))
-        if ok:
-            passed.append((ms, st["pcg_iterations"], len(passed), opt))
+        if ok and (best is None or ms < best[1]):
+            best = (opt, ms)
         ctx.close()
-    if not passed:
-        return None, table
-    fastest = min(p[0] for p in passed)
-    tied = [p for p in passed if p[0] <= fastest * (1.0 + tie)]
-    return min(tied, key=lambda p: (p[1], p[0], p[2]))[3], table
+    return (best[0] if best else None), table
 
 
 # ---------------------------------------------------------------------------
